@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark: RK45 accepted steps/s of the earthquake-cycle hot path.
+
+Workload: seeded random fault network of 800 faults (centres uniform in a
+7 km x 7 km square, lengths log-uniform 50-500 m, strikes N(30, 10) deg,
+10 m elements, ~16k elements with the fake ones), mode II dense shear+normal
+kernel, aging-law rate-and-state friction, 10 MPa pore-pressure step on one
+fault, RK45 with tol 1e-8. One "step" is one accepted Cash-Karp step of the
+reference's solve() loop (6+ right-hand-side evaluations, each one K.V over
+2 x N^2 stored kernel entries, a pressure solve and the friction update).
+
+`value` is whole-job throughput (sum of accepted steps/s over ranks, each rank
+integrating its own network realisation: weak scaling); `e2e` times the
+same steps through the C ABI with host buffers on both sides (state in,
+save_data snapshot out). The K.V matrix (4.3 GB in FP64) is larger than L2,
+so every launch streams it from HBM.
+
+`--impl reference` times the CPU restatement of the reference's own
+algorithm (matrix-free directII, CG pressure, rkqs) with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n_faults=800, box=7000.0, seed=0, tol=1e-8)
+
+
+def make_problem(rank=0, n_faults=None):
+    from demystification_dfn_b200 import networks
+
+    kw = dict(WORKLOAD)
+    if n_faults:
+        kw["n_faults"] = n_faults
+    kw["seed"] = kw["seed"] + rank
+    return networks.fault_network(**kw)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(storage):
+    p = os.path.join(ROOT, "profiles", "kv_traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get(storage)
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(problem, threads, budget_s=20.0):
+    """Time the CPU restatement of the reference path on host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle(problem, threads=threads)
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        st = o.lib.orc_solve_step(o.o)
+        steps += 1
+        if st != 0 or time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return steps, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    problem = make_problem(0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle(problem, threads=threads)
+    for _ in range(args.warmup):
+        o.lib.orc_solve_step(o.o)
+    # bounded sample: at most --steps steps and about --ref-budget seconds
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < args.steps:
+        st = o.lib.orc_solve_step(o.o)
+        steps += 1
+        if st != 0 or time.perf_counter() - t0 > args.ref_budget:
+            break
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    line = {
+        "impl": "reference", "metric": "RK45 accepted steps/s", "value": v, "unit": "steps/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "fault network 800 faults 7x7 km, mode II dense kernel, N=%d" % o.N,
+                   "n_elements": o.N, "tol_solver": WORKLOAD["tol"]},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} accepted steps of the workload after {args.warmup} warm-up steps"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--storage", default="fp64", choices=["fp64", "fp32", "bf16x2"])
+    ap.add_argument("--pressure", default="cg", choices=["cg", "tridiag"])
+    ap.add_argument("--gemv", default="tma", choices=["tma", "ldg"])
+    ap.add_argument("--n-faults", type=int, default=None, help="smaller network (profiling only)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+
+    from demystification_dfn_b200.simulation import Simulation
+
+    problem = make_problem(rank, args.n_faults)
+    sim = Simulation(problem, storage=args.storage, pressure=args.pressure, device=local, gemv=args.gemv)
+    stream = torch.cuda.current_stream()
+    sim.set_stream(stream.cuda_stream)
+    N = sim.N
+    kv_bytes = sim.kernel_bytes
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    sim.solve_steps(args.warmup)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    sim.profile_kv(True)
+    l0 = sim.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    rep = sim.solve_steps(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launches - l0
+    kv_ms, kv_n = sim.profile_kv_read()
+    sim.profile_kv(False)
+    clk = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # end-to-end through the C ABI with pinned host buffers every step
+    st = sim.state()
+    Yh = torch.from_numpy(st["Y"]).pin_memory().numpy()
+    Ph = torch.from_numpy(st["P"]).pin_memory().numpy()
+    outs = [torch.empty(N, dtype=torch.float64).pin_memory().numpy() for _ in range(5)]
+    e2e_steps = max(10, args.steps // 2)
+    tcur, ttry = st["time"], st["t_try"]
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        r = sim.step_host(Yh, Ph, tcur, ttry, outs)
+        # next step's input is this step's result, read back on the host
+        Yh[:N] = outs[0]
+        Yh[N:2 * N] = np.log(outs[1] * sim.arrays.V0 / sim.arrays.Dc)
+        Yh[2 * N:] = outs[4]
+        Ph[:] = outs[2]
+        tcur, ttry = r.time, r.t_try
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(te.item())
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        # mixed-precision storage of the same network (same steps, same start)
+        for store in ("fp32", "bf16x2"):
+            if store == args.storage:
+                continue
+            s2 = Simulation(problem, storage=store, pressure=args.pressure, device=local, gemv=args.gemv)
+            s2.set_stream(stream.cuda_stream)
+            s2.solve_steps(args.warmup)
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            s2.solve_steps(args.steps)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            st2 = s2.state()
+            ref = sim.state()
+            extras[store] = {"steps_per_s": args.steps / (a0.elapsed_time(a1) / 1e3),
+                             "kv_bytes": s2.kernel_bytes,
+                             "kv_ms": s2.time_kernel(10),
+                             "time_after_steps": st2["time"], "time_after_steps_fp64": ref["time"]}
+            s2.close()
+
+    if rank == 0:
+        hbm, src = peaks()
+        kv_avg = kv_ms / max(kv_n, 1)
+        achieved = kv_bytes / (kv_avg / 1e3) / 1e9
+        cpu = None
+        if not args.no_extras:
+            threads = os.cpu_count() or 1
+            steps_c, dt_c = cpu_baseline(make_problem(0, args.n_faults), threads, args.cpu_budget)
+            cpu = {"value": steps_c / dt_c, "unit": "steps/s", "cores": threads, "kind": "port",
+                   "sample": f"{steps_c} accepted steps of the same network from its initial state "
+                             f"({dt_c:.1f} s), matrix-free directII as in the reference"}
+        line = {
+            "metric": "RK45 accepted steps/s", "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"fault network {len(problem.faults)} faults 7x7 km, mode II dense kernel",
+                       "n_elements": N, "kernel_storage": args.storage, "pressure_solver": args.pressure,
+                       "kv_impl": args.gemv, "tol_solver": WORKLOAD["tol"],
+                       "l2": "K.V matrix %.2f GB > 126 MB L2, streamed from HBM each launch" % (kv_bytes / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic_per_launch(args.storage),
+                         "peak_source": src, "kernel": "K.V stream (%s)" % args.gemv,
+                         "algorithmic_bytes_per_launch": kv_bytes, "avg_launch_ms": kv_avg,
+                         "launches_timed": kv_n},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * 4 * N + 16,
+                    "d2h_bytes_per_step": 8 * 5 * N},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "report": {k: rep[k] for k in ("attempts", "rejected", "rhs_evals", "cg_iterations", "time")},
+        }
+        if extras:
+            line["mixed_precision"] = extras
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

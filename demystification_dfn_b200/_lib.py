@@ -1,0 +1,94 @@
+"""ctypes binding of ``libdfn_b200.so`` (the C ABI of include/dfn_b200.h).
+
+The library is loaded from the package's ``_build`` folder. There is no
+fallback: if the library is missing or cannot be loaded this module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB
+from .layout import DfnOptions, DfnProblem, DfnReport
+
+_lib = None
+
+STATUS = {
+    0: "ok", 1: "pressure CG did not converge", 2: "stepsize underflow in rkqs",
+    3: "normal traction became extensional", 4: "non-finite value", 5: "invalid argument",
+    6: "CUDA error", 7: "unsupported", 8: "too many rejected attempts", 9: "device allocation failed",
+}
+
+EXPORTS = [
+    "dfn_abi_version", "dfn_problem_struct_size", "dfn_options_struct_size", "dfn_report_struct_size",
+    "dfn_status_string", "dfn_last_error", "dfn_default_options", "dfn_create", "dfn_destroy",
+    "dfn_set_stream", "dfn_nb_element", "dfn_kernel_bytes", "dfn_kernel", "dfn_compute_P",
+    "dfn_friction_law", "dfn_rkqs", "dfn_solve_steps", "dfn_step_host", "dfn_get_state", "dfn_set_state",
+    "dfn_get_snapshot", "dfn_kernel_device", "dfn_time_kernel", "dfn_launch_count", "dfn_profile_kv",
+    "dfn_profile_kv_read",
+]
+
+
+class DfnError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, 'status ' + str(status))}" + (f": {msg}" if msg else ""))
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise ImportError(f"{LIB} is missing; build it with `python -m demystification_dfn_b200.build`")
+    lib = ctypes.CDLL(LIB)
+    P = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    sig = {
+        "dfn_abi_version": (i32, []),
+        "dfn_problem_struct_size": (i64, []),
+        "dfn_options_struct_size": (i64, []),
+        "dfn_report_struct_size": (i64, []),
+        "dfn_status_string": (ctypes.c_char_p, [i32]),
+        "dfn_last_error": (ctypes.c_char_p, []),
+        "dfn_default_options": (None, [ctypes.POINTER(DfnOptions)]),
+        "dfn_create": (i32, [ctypes.POINTER(DfnProblem), ctypes.POINTER(DfnOptions), ctypes.POINTER(P)]),
+        "dfn_destroy": (i32, [P]),
+        "dfn_set_stream": (i32, [P, P]),
+        "dfn_nb_element": (i64, [P]),
+        "dfn_kernel_bytes": (i64, [P]),
+        "dfn_kernel": (i32, [P, dp, dp, dp]),
+        "dfn_compute_P": (i32, [P, dbl, dp, dp, ctypes.POINTER(i32)]),
+        "dfn_friction_law": (i32, [P, dbl, i64, dp, dp]),
+        "dfn_rkqs": (i32, [P, dp, dp, i64, dp, dbl, dbl, dp, dp, dp]),
+        "dfn_solve_steps": (i32, [P, i64, ctypes.POINTER(DfnReport)]),
+        "dfn_step_host": (i32, [P, dp, dp, dbl, dbl, dp, dp, dp, dp, dp, ctypes.POINTER(DfnReport)]),
+        "dfn_get_state": (i32, [P, dp, dp, dp, dp, ctypes.POINTER(i64)]),
+        "dfn_set_state": (i32, [P, dp, dp, dbl, dbl, i64]),
+        "dfn_get_snapshot": (i32, [P, dp, dp, dp, dp, dp, dp, dp]),
+        "dfn_kernel_device": (i32, [P, P, P, P]),
+        "dfn_time_kernel": (i32, [P, i32, dp]),
+        "dfn_launch_count": (i64, [P]),
+        "dfn_profile_kv": (i32, [P, i32]),
+        "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.dfn_problem_struct_size() != ctypes.sizeof(DfnProblem):
+        raise ImportError("dfn_problem layout mismatch between the library and layout.py")
+    if lib.dfn_options_struct_size() != ctypes.sizeof(DfnOptions):
+        raise ImportError("dfn_options layout mismatch between the library and layout.py")
+    if lib.dfn_report_struct_size() != ctypes.sizeof(DfnReport):
+        raise ImportError("dfn_report layout mismatch between the library and layout.py")
+    _lib = lib
+    return lib
+
+
+def check(status, lib=None):
+    if status != 0:
+        lib = lib or load()
+        raise DfnError(status, (lib.dfn_last_error() or b"").decode())
+    return status

@@ -1,0 +1,967 @@
+// dfn_device.cuh — device code of the B200 earthquake-cycle hot path.
+//
+// Kernels (all FP64 arithmetic unless the stored kernel matrix is FP32/BF16):
+//   geometry_kernel       element midpoints, ds, tangent, normal, loading
+//                         projection, permeability_x
+//                         (src/initialisation.f90:145-205,252-269)
+//   assemble_kernel       dense kernel entries K_T/K_N (unscaled), formulas of
+//                         src/hmatrix/eval_kernel_hmatrix.f90:7-199 (same pair
+//                         terms as src/kernel_calculation/directModeII.f90:41-78)
+//   gemv_kernel           K.V streamed from HBM, per-column-chunk partial sums
+//   pressure_cg_kernel    the reference's Jacobi-scaled CG for compute_P
+//                         (src/fluid_diffusion.f90:24-152), one CTA per system
+//   pressure_tridiag_kernel  exact per-segment Thomas solve of the same system
+//   friction_kernel       closed-form dV/dt, dpsi/dt, dsigma/dt
+//                         (src/friction/RateStateAgingModeII.f90:46-89) fused
+//                         with the Cash-Karp stage combination, the 5th-order
+//                         solution, the embedded error and its max-norm
+//   step kernels          rkqs step control and solve() bookkeeping in FP64
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#define DFN_PI 3.141592653589793238
+
+// ---------------------------------------------------------------------------
+// Device-resident step controller (one per handle).
+struct StepCtl {
+    double time;      // committed simulated time
+    double t_try;     // trial step of the solve loop
+    double x;         // rkqs x (offset of the step start; 0 in solve())
+    double h;         // step of the current attempt
+    double hnext, hdid;
+    double eps;       // tol_solver
+    unsigned long long errmax_bits;  // max |yerr/yscal| as ordered bits
+    long long it_count, attempts, rejected, rhs_evals, cg_iters, halvings;
+    int accepted;
+    int status;       // dfn_status
+    int probe_ier;
+    int pad;
+};
+
+// Cash-Karp tableau, src/ode_solver/ode_bs.f90:200-210.
+#define CK_A2 0.2
+#define CK_A3 0.3
+#define CK_A4 0.6
+#define CK_A5 1.0
+#define CK_A6 0.875
+#define CK_B21 0.2
+#define CK_B31 (3.0 / 40.0)
+#define CK_B32 (9.0 / 40.0)
+#define CK_B41 0.3
+#define CK_B42 (-0.9)
+#define CK_B43 1.2
+#define CK_B51 (-11.0 / 54.0)
+#define CK_B52 2.5
+#define CK_B53 (-70.0 / 27.0)
+#define CK_B54 (35.0 / 27.0)
+#define CK_B61 (1631.0 / 55296.0)
+#define CK_B62 (175.0 / 512.0)
+#define CK_B63 (575.0 / 13824.0)
+#define CK_B64 (44275.0 / 110592.0)
+#define CK_B65 (253.0 / 4096.0)
+#define CK_C1 (37.0 / 378.0)
+#define CK_C3 (250.0 / 621.0)
+#define CK_C4 (125.0 / 594.0)
+#define CK_C6 (512.0 / 1771.0)
+#define CK_DC1 (CK_C1 - 2825.0 / 27648.0)
+#define CK_DC3 (CK_C3 - 18575.0 / 48384.0)
+#define CK_DC4 (CK_C4 - 13525.0 / 55296.0)
+#define CK_DC5 (-277.0 / 14336.0)
+#define CK_DC6 (CK_C6 - 0.25)
+
+// Non-contracted FP64 helpers: the stage combinations are written with
+// explicit round-to-nearest mul/add so that they match the reference's
+// expression order exactly (no FMA formation).
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+
+// Stage abscissae: offset of stage s (1-based, s=2..6) from the step start.
+__device__ __forceinline__ double ck_a(int s)
+{
+    switch (s) {
+    case 2: return CK_A2;
+    case 3: return CK_A3;
+    case 4: return CK_A4;
+    case 5: return CK_A5;
+    default: return CK_A6;
+    }
+}
+
+// ytemp of stage s (2..6) for one component, src/ode_solver/ode_bs.f90:213-221.
+__device__ __forceinline__ double ck_combine(int s, double h, double y, const double *k, int64_t stride, int64_t i)
+{
+    const double k1 = k[i];
+    switch (s) {
+    case 2: return add_(y, mul_(mul_(CK_B21, h), k1));
+    case 3: {
+        const double k2 = k[stride + i];
+        return add_(y, mul_(h, add_(mul_(CK_B31, k1), mul_(CK_B32, k2))));
+    }
+    case 4: {
+        const double k2 = k[stride + i], k3 = k[2 * stride + i];
+        return add_(y, mul_(h, add_(add_(mul_(CK_B41, k1), mul_(CK_B42, k2)), mul_(CK_B43, k3))));
+    }
+    case 5: {
+        const double k2 = k[stride + i], k3 = k[2 * stride + i], k4 = k[3 * stride + i];
+        return add_(y, mul_(h, add_(add_(add_(mul_(CK_B51, k1), mul_(CK_B52, k2)), mul_(CK_B53, k3)),
+                                    mul_(CK_B54, k4))));
+    }
+    default: {
+        const double k2 = k[stride + i], k3 = k[2 * stride + i], k4 = k[3 * stride + i], k5 = k[4 * stride + i];
+        return add_(y, mul_(h, add_(add_(add_(add_(mul_(CK_B61, k1), mul_(CK_B62, k2)), mul_(CK_B63, k3)),
+                                         mul_(CK_B64, k4)),
+                                    mul_(CK_B65, k5))));
+    }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Geometry: src/initialisation.f90:145-153 (element, ds, tangent, normal),
+// :159-205 (loading projection), :252-269 (harmonic face permeability).
+__global__ void geometry_kernel(int64_t N, int mode, const double *__restrict__ node, double *elem, double *ds,
+                                double *tan, double *nrm, double *nload, double *sload, double *sig, const double *perm,
+                                double *permx, double S11d, double S12d, double S22d, double S31d, double S32d)
+{
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < N) {
+        double x0 = node[2 * k], y0 = node[2 * k + 1], x1 = node[2 * k + 2], y1 = node[2 * k + 3];
+        double dx = __dadd_rn(x1, -x0), dy = __dadd_rn(y1, -y0);
+        elem[2 * k] = __dmul_rn(__dadd_rn(x1, x0), 0.5);
+        elem[2 * k + 1] = __dmul_rn(__dadd_rn(y1, y0), 0.5);
+        double d = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        ds[k] = d;
+        double t1 = __ddiv_rn(dx, d), t2 = __ddiv_rn(dy, d);
+        tan[2 * k] = t1; tan[2 * k + 1] = t2;
+        double n1 = -t2, n2 = t1;
+        nrm[2 * k] = n1; nrm[2 * k + 1] = n2;
+        if (mode == 3) {
+            sload[k] = add_(add_(sload[k], -mul_(t2, S31d)), mul_(t1, S32d));
+            sig[k] = add_(add_(sig[k], mul_(n1, add_(mul_(n1, S11d), mul_(n2, S12d)))),
+                          mul_(n2, add_(mul_(n1, S12d), mul_(n2, S22d))));
+        } else {
+            nload[k] = add_(add_(nload[k], mul_(n1, add_(mul_(n1, S11d), mul_(n2, S12d)))),
+                            mul_(n2, add_(mul_(n1, S12d), mul_(n2, S22d))));
+            sload[k] = add_(add_(sload[k], mul_(t1, add_(mul_(n1, S11d), mul_(n2, S12d)))),
+                            mul_(t2, add_(mul_(n1, S12d), mul_(n2, S22d))));
+        }
+    }
+    if (k <= N) {
+        double px = 0.0;
+        if (k >= 1 && k < N) px = __ddiv_rn(mul_(mul_(2.0, perm[k - 1]), perm[k]), add_(perm[k - 1], perm[k]));
+        permx[k] = px;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel-matrix storage formats. Row k (receiver) is contiguous over source
+// columns l; in mode II the shear and normal entries of one column are
+// adjacent, so one pass streams both matrices and reads V once.
+//   FP64   : mode II {T,N} double2 per column; mode III double per column
+//   FP32   : mode II {T,N} float2;            mode III float
+//   BF16X2 : entry = hi + lo, both bf16;      mode II {Th,Tl,Nh,Nl}; mode III {h,l}
+template <int MODE, int STORE> struct KFmt;
+template <> struct KFmt<2, 0> { static constexpr int BPC = 16; };
+template <> struct KFmt<2, 1> { static constexpr int BPC = 8; };
+template <> struct KFmt<2, 2> { static constexpr int BPC = 8; };
+template <> struct KFmt<3, 0> { static constexpr int BPC = 8; };
+template <> struct KFmt<3, 1> { static constexpr int BPC = 4; };
+template <> struct KFmt<3, 2> { static constexpr int BPC = 4; };
+
+// Entry formulas: src/hmatrix/eval_kernel_hmatrix.f90:36-47 (mode III),
+// :91-115 (mode II shear), :160-195 (mode II normal).
+__device__ __forceinline__ double entry_mode3(double e1, double e2, double t1, double t2, double xl, double yl,
+                                              double xr, double yr)
+{
+    double ax = xl - e1, ay = yl - e2, bx = xr - e1, by = yr - e2;
+    double r1 = sqrt(ax * ax + ay * ay);
+    double r2 = sqrt(bx * bx + by * by);
+    double I1 = t1 / (r1 * r1) * (e1 - xl) + t2 / (r1 * r1) * (e2 - yl);
+    double I2 = t1 / (r2 * r2) * (e1 - xr) + t2 / (r2 * r2) * (e2 - yr);
+    return -I1 + I2;
+}
+
+__device__ __forceinline__ void entry_mode2(double e1, double e2, double n1, double n2, double xl, double yl,
+                                            double xr, double yr, double nl1, double nl2, double &T, double &Nn)
+{
+    double dxl = e1 - xl, dyl = e2 - yl, dxr = e1 - xr, dyr = e2 - yr;
+    double rl = sqrt(dxl * dxl + dyl * dyl);
+    double rr = sqrt(dxr * dxr + dyr * dyr);
+    double g1l = dxl / rl, g2l = dyl / rl, g1r = dxr / rr, g2r = dyr / rr;
+    double c4 = 4.0 * n1 * n2, c2 = n2 * n2 - n1 * n1, s2 = 2.0 * n1 * n2;
+    double ql = (c4 * g1l * g2l + c2 * (g2l * g2l - g1l * g1l));
+    double qr = (c4 * g1r * g2r + c2 * (g2r * g2r - g1r * g1r));
+    double I1tl = ql * g1l / rl, I2tl = ql * g2l / rl, I1tr = qr * g1r / rr, I2tr = qr * g2r / rr;
+    double wl = (s2 * (g2l * g2l - g1l * g1l) - c2 * 2.0 * g1l * g2l);
+    double wr = (s2 * (g2r * g2r - g1r * g1r) - c2 * 2.0 * g1r * g2r);
+    double I1nl = g1l / rl - g2l / rl * wl, I2nl = g2l / rl + g1l / rl * wl;
+    double I1nr = g1r / rr - g2r / rr * wr, I2nr = g2r / rr + g1r / rr * wr;
+    T = nl2 * I1tl - nl2 * I1tr - nl1 * I2tl + nl1 * I2tr;
+    Nn = nl1 * I1nl - nl1 * I1nr + nl2 * I2nl - nl2 * I2nr;
+}
+
+__device__ __forceinline__ void split_bf16(double v, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __double2bfloat16(v);
+    lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+}
+
+// One thread per (row k, column l); Np padded columns (zeros beyond N).
+template <int MODE, int STORE>
+__global__ void assemble_kernel(int64_t N, int64_t Np, const double *__restrict__ node,
+                                const double *__restrict__ elem, const double *__restrict__ tan,
+                                const double *__restrict__ nrm, void *Kout)
+{
+    int64_t k = blockIdx.x;
+    int64_t l = blockIdx.y * (int64_t)blockDim.x + threadIdx.x;
+    if (l >= Np || k >= N) return;
+    double T = 0.0, Nn = 0.0;
+    if (l < N) {
+        double e1 = elem[2 * k], e2 = elem[2 * k + 1];
+        double xl = node[2 * l], yl = node[2 * l + 1], xr = node[2 * l + 2], yr = node[2 * l + 3];
+        if (MODE == 3) T = entry_mode3(e1, e2, tan[2 * k], tan[2 * k + 1], xl, yl, xr, yr);
+        else entry_mode2(e1, e2, nrm[2 * k], nrm[2 * k + 1], xl, yl, xr, yr, nrm[2 * l], nrm[2 * l + 1], T, Nn);
+    }
+    int64_t idx = k * Np + l;
+    if (STORE == 0) {
+        if (MODE == 2) reinterpret_cast<double2 *>(Kout)[idx] = make_double2(T, Nn);
+        else reinterpret_cast<double *>(Kout)[idx] = T;
+    } else if (STORE == 1) {
+        if (MODE == 2) reinterpret_cast<float2 *>(Kout)[idx] = make_float2((float)T, (float)Nn);
+        else reinterpret_cast<float *>(Kout)[idx] = (float)T;
+    } else {
+        __nv_bfloat16 th, tl, nh, nl;
+        split_bf16(T, th, tl);
+        if (MODE == 2) {
+            split_bf16(Nn, nh, nl);
+            __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(Kout) + 4 * idx;
+            o[0] = th; o[1] = tl; o[2] = nh; o[3] = nl;
+        } else {
+            __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(Kout) + 2 * idx;
+            o[0] = th; o[1] = tl;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K.V streaming kernel.
+//
+// Work unit: a column chunk of CW columns (4 KiB of one row) for a block of
+// rows. Every lane keeps the V values of its columns in registers and reuses
+// them for all rows of the block; each warp owns rows r0+w, r0+w+8, ... and
+// issues 8 coalesced 128-bit loads per lane per row (two rows in flight).
+// The per-(chunk,row) warp sum goes to part[c*N + row]; the friction kernel
+// adds the chunks in a fixed order, so the result is deterministic.
+constexpr int GEMV_WARPS = 8;
+constexpr int GEMV_LPL = 8;                       // 16-byte loads per lane per row-chunk
+constexpr int GEMV_CHUNK_BYTES = 32 * GEMV_LPL * 16;  // 4096
+constexpr int GEMV_ROWS = 64;                     // rows per CTA
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int MODE, int STORE>
+__device__ __forceinline__ void fma_vec(const uint4 &q, const double *v, double &aT, double &aN)
+{
+    if (STORE == 0) {
+        const double *d = reinterpret_cast<const double *>(&q);
+        if (MODE == 2) { aT = fma(d[0], v[0], aT); aN = fma(d[1], v[0], aN); }
+        else { aT = fma(d[0], v[0], aT); aT = fma(d[1], v[1], aT); }
+    } else if (STORE == 1) {
+        const float *f = reinterpret_cast<const float *>(&q);
+        if (MODE == 2) {
+            aT = fma((double)f[0], v[0], aT); aN = fma((double)f[1], v[0], aN);
+            aT = fma((double)f[2], v[1], aT); aN = fma((double)f[3], v[1], aN);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) aT = fma((double)f[j], v[j], aT);
+        }
+    } else {
+        const __nv_bfloat162 *b = reinterpret_cast<const __nv_bfloat162 *>(&q);
+        if (MODE == 2) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                float2 t = __bfloat1622float2(b[2 * j]);
+                float2 n = __bfloat1622float2(b[2 * j + 1]);
+                aT = fma((double)(t.x + t.y), v[j], aT);
+                aN = fma((double)(n.x + n.y), v[j], aN);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float2 t = __bfloat1622float2(b[j]);
+                aT = fma((double)(t.x + t.y), v[j], aT);
+            }
+        }
+    }
+}
+
+template <int MODE, int STORE>
+__global__ void __launch_bounds__(GEMV_WARPS * 32) gemv_kernel(int64_t N, int64_t Np, const uint4 *__restrict__ K,
+                                                               const double *__restrict__ Vin, double *__restrict__ partT,
+                                                               double *__restrict__ partN)
+{
+    constexpr int BPC = KFmt<MODE, STORE>::BPC;
+    constexpr int CPV = 16 / BPC;                 // columns per 16-byte vector
+    constexpr int CW = GEMV_CHUNK_BYTES / BPC;    // columns per chunk
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t c = blockIdx.x;                 // column chunk
+    const int64_t r0 = (int64_t)blockIdx.y * GEMV_ROWS;
+    const int64_t row_vecs = Np * BPC / 16;       // 16-byte vectors per row
+
+    double v[GEMV_LPL * CPV];
+#pragma unroll
+    for (int i = 0; i < GEMV_LPL; i++)
+#pragma unroll
+        for (int j = 0; j < CPV; j++) {
+            int64_t col = c * CW + (int64_t)(i * 32 + lane) * CPV + j;
+            v[i * CPV + j] = (col < N) ? Vin[col] : 0.0;
+        }
+
+    const int64_t vec0 = c * (CW * BPC / 16) + lane;
+    for (int64_t r = r0 + warp; r < r0 + GEMV_ROWS && r < N; r += 2 * GEMV_WARPS) {
+        const int64_t rb = r + GEMV_WARPS;
+        const bool two = (rb < r0 + GEMV_ROWS) && (rb < N);
+        const uint4 *pa = K + r * row_vecs + vec0;
+        const uint4 *pb = K + (two ? rb : r) * row_vecs + vec0;
+        uint4 qa[GEMV_LPL], qb[GEMV_LPL];
+#pragma unroll
+        for (int i = 0; i < GEMV_LPL; i++) qa[i] = __ldcs(pa + i * 32);
+#pragma unroll
+        for (int i = 0; i < GEMV_LPL; i++) qb[i] = two ? __ldcs(pb + i * 32) : make_uint4(0, 0, 0, 0);
+        double aT = 0.0, aN = 0.0, bT = 0.0, bN = 0.0;
+#pragma unroll
+        for (int i = 0; i < GEMV_LPL; i++) fma_vec<MODE, STORE>(qa[i], v + i * CPV, aT, aN);
+#pragma unroll
+        for (int i = 0; i < GEMV_LPL; i++) fma_vec<MODE, STORE>(qb[i], v + i * CPV, bT, bN);
+        aT = warp_sum(aT); bT = warp_sum(bT);
+        if (MODE == 2) { aN = warp_sum(aN); bN = warp_sum(bN); }
+        if (lane == 0) {
+            partT[c * N + r] = aT;
+            if (MODE == 2) partN[c * N + r] = aN;
+            if (two) {
+                partT[c * N + rb] = bT;
+                if (MODE == 2) partN[c * N + rb] = bN;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// TMA bulk-copy variant: one producer warp streams 4 KiB row-chunks with
+// cp.async.bulk into a ring of shared-memory stages completed on mbarriers;
+// eight consumer warps read the stages with 128-bit shared loads. Rows of the
+// CTA's block are assigned to consumer warps round-robin, one stage per row.
+constexpr int TMA_STAGES = 16;
+constexpr int TMA_CONSUMERS = 8;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Bounded wait: returns false if the phase did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok = 0;
+    for (int it = 0; it < (1 << 22); it++) {
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(smem_u32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <int MODE, int STORE>
+__global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
+    gemv_tma_kernel(int64_t N, int64_t Np, const uint4 *__restrict__ K, const double *__restrict__ Vin,
+                    double *__restrict__ partT, double *__restrict__ partN, int *err_flag)
+{
+    constexpr int BPC = KFmt<MODE, STORE>::BPC;
+    constexpr int CPV = 16 / BPC;
+    constexpr int CW = GEMV_CHUNK_BYTES / BPC;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint4 *stage = reinterpret_cast<uint4 *>(smem_raw);                       // TMA_STAGES x 4 KiB
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + TMA_STAGES * GEMV_CHUNK_BYTES);
+    uint64_t *empty = full + TMA_STAGES;
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.y * GEMV_ROWS;
+    const int64_t rend = (r0 + GEMV_ROWS < N) ? r0 + GEMV_ROWS : N;
+    const int nrows = (int)(rend - r0);
+    const int64_t row_bytes = Np * BPC;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TMA_STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    __shared__ int issued_s, bad_s;
+    if (threadIdx.x == 0) { issued_s = 0; bad_s = 0; }
+    __syncthreads();
+    if (warp == TMA_CONSUMERS) {
+        // producer: one elected lane issues the bulk copies
+        if (lane == 0) {
+            int i = 0;
+            for (; i < nrows; i++) {
+                int s = i % TMA_STAGES;
+                if (i >= TMA_STAGES && !mbar_wait(&empty[s], ((i / TMA_STAGES) - 1) & 1)) { bad_s = 1; break; }
+                mbar_expect_tx(&full[s], GEMV_CHUNK_BYTES);
+                const unsigned char *src =
+                    reinterpret_cast<const unsigned char *>(K) + (r0 + i) * row_bytes + c * GEMV_CHUNK_BYTES;
+                tma_bulk_g2s(stage + s * (GEMV_CHUNK_BYTES / 16), src, GEMV_CHUNK_BYTES, &full[s]);
+            }
+            issued_s = i;
+        }
+    } else {
+        double v[GEMV_LPL * CPV];
+#pragma unroll
+        for (int i = 0; i < GEMV_LPL; i++)
+#pragma unroll
+            for (int j = 0; j < CPV; j++) {
+                int64_t col = c * CW + (int64_t)(i * 32 + lane) * CPV + j;
+                v[i * CPV + j] = (col < N) ? Vin[col] : 0.0;
+            }
+        for (int i = warp; i < nrows; i += TMA_CONSUMERS) {
+            int s = i % TMA_STAGES;
+            if (!mbar_wait(&full[s], (i / TMA_STAGES) & 1)) { bad_s = 1; break; }
+            const uint4 *sp = stage + s * (GEMV_CHUNK_BYTES / 16) + lane;
+            uint4 q[GEMV_LPL];
+#pragma unroll
+            for (int j = 0; j < GEMV_LPL; j++) q[j] = sp[j * 32];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+            double aT = 0.0, aN = 0.0;
+#pragma unroll
+            for (int j = 0; j < GEMV_LPL; j++) fma_vec<MODE, STORE>(q[j], v + j * CPV, aT, aN);
+            aT = warp_sum(aT);
+            if (MODE == 2) aN = warp_sum(aN);
+            if (lane == 0) {
+                partT[c * N + r0 + i] = aT;
+                if (MODE == 2) partN[c * N + r0 + i] = aN;
+            }
+        }
+    }
+    __syncthreads();
+    if (bad_s && threadIdx.x == 0) {
+        // error path: wait (bounded) for the copies still in flight before
+        // the CTA's shared memory is released, then report
+        int issued = issued_s;
+        for (int i = (issued > TMA_STAGES ? issued - TMA_STAGES : 0); i < issued; i++)
+            mbar_wait(&full[i % TMA_STAGES], (i / TMA_STAGES) & 1);
+        atomicExch(err_flag, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pore pressure (src/fluid_diffusion.f90). The parameters of the implicit
+// step are shared by both solvers.
+struct PressParams {
+    int64_t N;
+    const double *P;       // committed pressure
+    const double *permx;   // [N+1] face permeability (0-based: face j between elements j-1 and j)
+    const double *ds;
+    double porosity, dyn_visc, comp;  // comp = fluid_comp + rock_comp
+    double tol;
+    int64_t nsrc;
+    const int64_t *src_fault;   // 1-based fault id
+    const int64_t *src_elem;    // 0-based global element index
+    const double *src_Q, *src_tb, *src_te;
+    const double *ctl_time;     // &ctl->time
+};
+
+// kx*dt/(porosity*dyn_viscosity*(fluid_comp+rock_comp)*ds**2)
+__device__ __forceinline__ double pcoef(const PressParams &p, double kx, double dt, double dsv)
+{
+    return __ddiv_rn(mul_(kx, dt), mul_(mul_(mul_(p.porosity, p.dyn_visc), p.comp), mul_(dsv, dsv)));
+}
+
+// Row coefficients of the unscaled matrix (compute_MatrixVector,
+// src/fluid_diffusion.f90:175-204); A2 equals compute_diag's diagonal.
+__device__ __forceinline__ void prow(const PressParams &p, int64_t k, double dt, double &A1, double &A2, double &A3)
+{
+    const int64_t N = p.N;
+    if (k == 0) {
+        A1 = 0.0;
+        A2 = add_(1.0, pcoef(p, p.permx[1], dt, p.ds[0]));
+        A3 = -pcoef(p, p.permx[1], dt, p.ds[0]);
+    } else if (k == N - 1) {
+        A1 = -pcoef(p, p.permx[N - 1], dt, p.ds[N - 1]);
+        A2 = add_(1.0, pcoef(p, p.permx[N - 1], dt, p.ds[N - 1]));
+        A3 = 0.0;
+    } else {
+        A1 = -pcoef(p, p.permx[k], dt, p.ds[k - 1]);
+        A2 = add_(1.0, pcoef(p, add_(p.permx[k], p.permx[k + 1]), dt, p.ds[k]));
+        A3 = -pcoef(p, p.permx[k + 1], dt, p.ds[k + 1]);
+    }
+}
+
+// Source contribution (before division by diag) at element k for step dt:
+// src/fluid_diffusion.f90:52-64 with the reference's vector subscripts
+// (every source of a fault is added once per active source of that fault).
+__device__ __forceinline__ double psource(const PressParams &p, int64_t k, double dt)
+{
+    double add = 0.0;
+    const double t = add_(*p.ctl_time, dt);
+    for (int64_t s = 0; s < p.nsrc; s++) {
+        if (!(t >= p.src_tb[s] && t < p.src_te[s])) continue;
+        for (int64_t j = 0; j < p.nsrc; j++) {
+            if (p.src_fault[j] != p.src_fault[s] || p.src_elem[j] != k) continue;
+            add = add_(add, __ddiv_rn(__ddiv_rn(mul_(dt, p.src_Q[j]), mul_(p.porosity, p.comp)), p.ds[k]));
+        }
+    }
+    return add;
+}
+
+// Block-wide reductions for the one-CTA CG (blockDim = 1024).
+__device__ __forceinline__ double block_sum(double v, double *red)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = (lane < (blockDim.x >> 5)) ? red[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) red[32] = t;
+    }
+    __syncthreads();
+    return red[32];
+}
+__device__ __forceinline__ double block_max(double v, double *red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = (lane < (blockDim.x >> 5)) ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+        if (lane == 0) red[32] = t;
+    }
+    __syncthreads();
+    return red[32];
+}
+
+// System s of a pressure launch gets its dt from the controller:
+//   kind 0: dt = ctl->t_try (probe / first RHS), halving on non-convergence
+//   kind 1: dt = ctl->x + A_{s+1} * ctl->h   (stage s+1, s = 1..5)
+//   kind 2: dt = explicit value
+struct PressSys {
+    int kind;
+    double dt_explicit;
+};
+
+__device__ __forceinline__ double sys_dt(const StepCtl *ctl, int kind, int sys, double dt_explicit)
+{
+    if (kind == 0) return ctl->t_try;
+    if (kind == 1) return add_(ctl->x, mul_(ck_a(sys + 1), ctl->h));
+    return dt_explicit;
+}
+
+// One Jacobi-scaled CG solve (reference algorithm) by the whole CTA.
+// Work vectors live in global memory (w: 4*N doubles). Returns ier.
+__device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, double *pv, double *Mp, double *red,
+                        long long *iters)
+{
+    const int64_t N = p.N;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    // x = P, r = b1 - M x, p = r
+    double lmax = 0.0;
+    for (int64_t k = tid; k < N; k += nt) {
+        double A1, A2, A3;
+        prow(p, k, dt, A1, A2, A3);
+        double b1 = __ddiv_rn(p.P[k], A2);
+        double src = psource(p, k, dt);
+        if (src != 0.0) b1 = add_(b1, __ddiv_rn(src, A2));
+        double m = A2 * p.P[k];
+        if (k > 0) m = A1 * p.P[k - 1] + m;
+        if (k < N - 1) m = m + A3 * p.P[k + 1];
+        double rk = b1 - m / A2;
+        x[k] = p.P[k];
+        r[k] = rk;
+        pv[k] = rk;
+        lmax = fmax(lmax, fabs(rk));
+    }
+    double errmax = block_max(lmax, red) / p.tol;
+    long long it = 0;
+    // rr carried between iterations: sum(rk**2) of iteration i+1 equals
+    // sum(rk1**2) of iteration i (rk = rk1), so it is computed once.
+    double lrr = 0.0;
+    for (int64_t k = tid; k < N; k += nt) lrr += r[k] * r[k];
+    double rr = block_sum(lrr, red);
+    while (errmax >= 1.0) {
+        it++;
+        double lpap = 0.0;
+        for (int64_t k = tid; k < N; k += nt) {
+            double A1, A2, A3;
+            prow(p, k, dt, A1, A2, A3);
+            double m = A2 * pv[k];
+            if (k > 0) m = A1 * pv[k - 1] + m;
+            if (k < N - 1) m = m + A3 * pv[k + 1];
+            m = m / A2;
+            Mp[k] = m;
+            lpap += pv[k] * m;
+        }
+        double pap = block_sum(lpap, red);
+        double alpha = rr / pap;
+        double lr1 = 0.0, lm = 0.0;
+        for (int64_t k = tid; k < N; k += nt) {
+            x[k] = x[k] + alpha * pv[k];
+            double r1 = r[k] - alpha * Mp[k];
+            r[k] = r1;
+            lr1 += r1 * r1;
+            lm = fmax(lm, fabs(r1));
+        }
+        double r1r1 = block_sum(lr1, red);
+        double beta = r1r1 / rr;
+        for (int64_t k = tid; k < N; k += nt) pv[k] = r[k] + beta * pv[k];
+        rr = r1r1;
+        if (it > 200) { *iters += it; return 1; }
+        errmax = block_max(lm, red) / p.tol;
+    }
+    *iters += it;
+    return 0;
+}
+
+__global__ void __launch_bounds__(1024) pressure_cg_kernel(PressParams p, StepCtl *ctl, int kind, int sys0,
+                                                           double dt_explicit, double *Ptemp, double *Pdot,
+                                                           double *work)
+{
+    __shared__ double red[33];
+    const int sys = sys0 + blockIdx.x;
+    const int64_t N = p.N;
+    double *x = work + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
+    double *Pt = Ptemp + (int64_t)sys * N, *Pd = Pdot + (int64_t)sys * N;
+    __shared__ long long iters;
+    if (threadIdx.x == 0) iters = 0;
+    __syncthreads();
+    double dt = sys_dt(ctl, kind, sys, dt_explicit);
+    int ier = cg_solve(p, dt, x, r, pv, Mp, red, &iters);
+    if (kind == 0) {
+        // probe: src/solver.f90:81-92, halve t_try until the solve converges
+        int guard = 0;
+        while (ier == 1 && guard < 1100) {
+            dt = dt / 2.0;
+            guard++;
+            ier = cg_solve(p, dt, x, r, pv, Mp, red, &iters);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ctl->t_try = dt;
+            ctl->halvings += guard;
+        }
+    }
+    __syncthreads();
+    if (ier == 0) {
+        double lmx = 0.0;
+        for (int64_t k = threadIdx.x; k < N; k += blockDim.x) {
+            Pd[k] = (dt < 1e-9) ? 0.0 : (x[k] - p.P[k]) / dt;
+            Pt[k] = x[k];
+            lmx = fmax(lmx, fabs(x[k]));
+        }
+        double mx = block_max(lmx, red);
+        if (!(mx <= 1.7976931348623157e308)) ier = 1;
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd((unsigned long long *)&ctl->cg_iters, (unsigned long long)iters);
+        if (ier) {
+            if (kind == 0) ctl->probe_ier = 1;
+            atomicCAS(&ctl->status, 0, 1);
+        }
+    }
+}
+
+// Exact solve of the unscaled tridiagonal system A x = P + source, one
+// thread per decoupled segment (a maximal run of elements joined by nonzero
+// face permeability; the fake elements between faults are segments of one).
+__global__ void pressure_tridiag_kernel(PressParams p, StepCtl *ctl, int kind, int sys0, double dt_explicit,
+                                        const int64_t *seg_start, int64_t nseg, double *Ptemp, double *Pdot,
+                                        double *work)
+{
+    const int sys = sys0 + blockIdx.y;
+    const int64_t sg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (sg >= nseg) return;
+    const int64_t N = p.N;
+    const double dt = sys_dt(ctl, kind, sys, dt_explicit);
+    const int64_t k0 = seg_start[sg], k1 = seg_start[sg + 1];
+    double *cp = work + (int64_t)sys * 4 * N;   // modified super-diagonal
+    double *dp = cp + N;                        // modified right-hand side
+    double *Pt = Ptemp + (int64_t)sys * N, *Pd = Pdot + (int64_t)sys * N;
+    // forward sweep
+    double cprev = 0.0, dprev = 0.0;
+    for (int64_t k = k0; k < k1; k++) {
+        double A1, A2, A3;
+        prow(p, k, dt, A1, A2, A3);
+        if (k == k0) A1 = 0.0;
+        if (k == k1 - 1) A3 = 0.0;
+        double rhs = add_(p.P[k], psource(p, k, dt));
+        double den = A2 - A1 * cprev;
+        double c = A3 / den;
+        double d = (rhs - A1 * dprev) / den;
+        cp[k] = c; dp[k] = d;
+        cprev = c; dprev = d;
+    }
+    // back substitution
+    double xn = 0.0;
+    bool bad = false;
+    for (int64_t k = k1 - 1; k >= k0; k--) {
+        double xk = dp[k] - cp[k] * xn;
+        xn = xk;
+        Pt[k] = xk;
+        Pd[k] = (dt < 1e-9) ? 0.0 : (xk - p.P[k]) / dt;
+        if (!isfinite(xk)) bad = true;
+    }
+    if (bad) atomicCAS(&ctl->status, 0, 4);
+}
+
+// ---------------------------------------------------------------------------
+// Friction right-hand side fused with the Cash-Karp stage arithmetic.
+struct FricParams {
+    int64_t N;
+    int mode;
+    int nchunk;
+    double prefT;                 // mu/pi*(1-cs^2/cp^2) (mode II) or mu/(2 pi) (mode III)
+    double mu_2cs;                // mu/(2 cs)
+    const double *a, *b, *Dc, *f0, *V0, *nload, *sload;
+    const unsigned char *fake;
+    const double *partT, *partN;  // [nchunk][N]
+    double *SigT, *SigN;          // stress rates of this evaluation
+    const double *Ptemp, *Pdot;   // pressure of this evaluation
+    const double *y;              // state at the step start
+    double *ytmp;                 // ytemp of this stage (in) / next stage (out)
+    double *kbuf;                 // [6][3N] stage derivatives
+    double *yscal;
+    double *yout;
+    StepCtl *ctl;
+};
+
+__device__ __forceinline__ void rsf_rhs(const FricParams &f, int64_t k, double V, double psi, double sig, double T,
+                                        double Nn, double Pt, double Pd, double &dV, double &dpsi, double &dsig)
+{
+    // src/friction/RateStateAgingModeII.f90:46-76 (mode III: dsig = loading only)
+    dsig = (f.mode == 2) ? (Nn + f.nload[k]) : f.nload[k];
+    const double a = f.a[k], b = f.b[k], V0 = f.V0[k], Dc = f.Dc[k];
+    double B = V / (2.0 * V0);
+    double C = exp((f.f0[k] + b * psi) / a);
+    double D = 1.0 / (C * C) + B * B;
+    D = 1.0 / sqrt(D);
+    double heal = V0 / Dc * exp(-psi) - fabs(V) / Dc;
+    double num = f.sload[k] + T + (dsig + Pd) * a * asinh(B * C) + B * D * (sig + Pt) * b * heal;
+    double den = f.mu_2cs - D * (sig + Pt) * a / (2.0 * V0);
+    dV = num / den;
+    dpsi = heal;
+    if (f.fake[k]) { dV = 0.0; dpsi = 0.0; dsig = 0.0; }
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v)
+{
+    // non-negative doubles order like their bit patterns
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// stage: 0 = standalone evaluation (ytmp in, kbuf[0] out)
+//        1 = k1 at the step start (y in), also yscal
+//        2..5 = k_s, then ytemp of stage s+1 in place
+//        6 = k6, then yout, yerr and the max-norm contribution
+__global__ void friction_kernel(FricParams f, int stage)
+{
+    __shared__ double red[32];
+    const int64_t N = f.N;
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double emax = 0.0;
+    if (k < N) {
+        double T = 0.0, Nn = 0.0;
+        for (int c = 0; c < f.nchunk; c++) T += f.partT[(int64_t)c * N + k];
+        T = f.prefT * T;
+        if (f.mode == 2) {
+            for (int c = 0; c < f.nchunk; c++) Nn += f.partN[(int64_t)c * N + k];
+            Nn = f.prefT * Nn;
+        }
+        f.SigT[k] = T;
+        f.SigN[k] = Nn;
+        const double *yin = (stage == 1) ? f.y : f.ytmp;
+        double V = yin[k], psi = yin[N + k], sig = yin[2 * N + k];
+        double dV, dpsi, dsig;
+        rsf_rhs(f, k, V, psi, sig, T, Nn, f.Ptemp[k], f.Pdot[k], dV, dpsi, dsig);
+        const int slot = (stage == 0) ? 0 : stage - 1;
+        double *ks = f.kbuf + (int64_t)slot * 3 * N;
+        ks[k] = dV; ks[N + k] = dpsi; ks[2 * N + k] = dsig;
+        const int64_t S = 3 * N;
+        if (stage == 1) {
+            const double tt = f.ctl->t_try, tol = f.ctl->eps;
+            // yscal = abs(Y)+abs(Y_dot*t_try)+tol_solver (src/solver.f90:102)
+            f.yscal[k] = add_(add_(fabs(f.y[k]), fabs(mul_(dV, tt))), tol);
+            f.yscal[N + k] = add_(add_(fabs(f.y[N + k]), fabs(mul_(dpsi, tt))), tol);
+            f.yscal[2 * N + k] = add_(add_(fabs(f.y[2 * N + k]), fabs(mul_(dsig, tt))), tol);
+        } else if (stage >= 2 && stage <= 5) {
+            const double h = f.ctl->h;
+#pragma unroll
+            for (int j = 0; j < 3; j++) f.ytmp[j * N + k] = ck_combine(stage + 1, h, f.y[j * N + k], f.kbuf, S, j * N + k);
+        } else if (stage == 6) {
+            const double h = f.ctl->h;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int64_t i = j * N + k;
+                const double k1 = f.kbuf[i], k3 = f.kbuf[2 * S + i], k4 = f.kbuf[3 * S + i],
+                             k5 = f.kbuf[4 * S + i], k6 = f.kbuf[5 * S + i];
+                // src/ode_solver/ode_bs.f90:223-224
+                f.yout[i] = add_(f.y[i], mul_(h, add_(add_(add_(mul_(CK_C1, k1), mul_(CK_C3, k3)), mul_(CK_C4, k4)),
+                                                      mul_(CK_C6, k6))));
+                double yerr = mul_(h, add_(add_(add_(add_(mul_(CK_DC1, k1), mul_(CK_DC3, k3)), mul_(CK_DC4, k4)),
+                                                mul_(CK_DC5, k5)),
+                                           mul_(CK_DC6, k6)));
+                double e = fabs(__ddiv_rn(yerr, f.yscal[i]));
+                if (!(e == e) || isinf(e)) e = 1.0e300;   // non-finite error rejects the attempt
+                emax = fmax(emax, e);
+            }
+        }
+    }
+    if (stage == 6) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) red[w] = emax;
+        __syncthreads();
+        if (w == 0) {
+            double t = (lane < (blockDim.x >> 5)) ? red[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+            if (lane == 0) atomic_max_pos(&f.ctl->errmax_bits, t);
+        }
+    }
+    if (k == 0 && stage >= 1) atomicAdd((unsigned long long *)&f.ctl->rhs_evals, 1ull);
+}
+
+// ytemp of stage 2 at the start of every attempt (h may have changed).
+__global__ void attempt_begin_kernel(int64_t N, const double *y, const double *kbuf, double *ytmp, StepCtl *ctl)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double h = ctl->h;
+    if (i < 3 * N) ytmp[i] = ck_combine(2, h, y[i], kbuf, 3 * N, i);
+    if (i == 0) {
+        ctl->errmax_bits = 0ull;
+        ctl->attempts += 1;
+    }
+}
+
+// Step control after an attempt: src/ode_solver/ode_bs.f90:158-172.
+__global__ void decide_kernel(StepCtl *ctl)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25;
+    const double ERRCON = (double)1.89e-4f;  // default-real literal in the reference
+    double errmax = __longlong_as_double((long long)ctl->errmax_bits) / ctl->eps;
+    double h = ctl->h;
+    if (errmax <= 1.0) {
+        ctl->accepted = 1;
+        ctl->hnext = (errmax > ERRCON) ? SAFETY * h * pow(errmax, PGROW) : 5.0 * h;
+        ctl->hdid = h;
+    } else {
+        ctl->accepted = 0;
+        ctl->rejected += 1;
+        double htemp = SAFETY * h * pow(errmax, PSHRNK);
+        h = copysign(fmax(fabs(htemp), 0.1 * fabs(h)), h);
+        ctl->h = h;
+        if (ctl->x + h == ctl->x) ctl->status = 2;
+    }
+}
+
+// Start of one pass of solve(): src/solver.f90:60-77.
+__global__ void step_begin_kernel(StepCtl *ctl, int64_t nsrc, const double *src_tb)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ctl->it_count += 1;
+    ctl->accepted = 0;
+    ctl->probe_ier = 0;
+    ctl->x = 0.0;
+    if (ctl->t_try > 10.0) {
+        for (int64_t s = 0; s < nsrc; s++)
+            if (ctl->time < src_tb[s] && ctl->time + ctl->t_try > src_tb[s]) ctl->t_try = 10.0;
+    }
+}
+
+__global__ void set_h_kernel(StepCtl *ctl)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) ctl->h = ctl->t_try;
+}
+
+// End of one pass of solve(): src/solver.f90:117-196. The pressure commit
+// compute_P(t_did) equals the stage-5 solve of the accepted attempt
+// (dt = 0 + 1.0*h = t_did), so its result is copied instead of recomputed.
+__global__ void commit_kernel(int64_t N, double *y, const double *yout, double *P, double *Pdot,
+                              const double *Pt5, const double *Pd5, StepCtl *ctl, double t_cap)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < 3 * N) {
+        double v = yout[i];
+        y[i] = v;
+        if (i >= 2 * N && v > 0.0) atomicCAS(&ctl->status, 0, 3);
+        if (!isfinite(v)) atomicCAS(&ctl->status, 0, 4);
+    }
+    if (i < N) {
+        P[i] = Pt5[i];
+        Pdot[i] = Pd5[i];
+    }
+    if (i == 0) {
+        ctl->time = ctl->time + ctl->hdid;
+        double tn = ctl->hnext;
+        if (tn > t_cap) tn = t_cap;
+        ctl->t_try = tn;
+    }
+}
+
+// K.V output for the operator entry point: sum the chunks and scale.
+__global__ void kv_finish_kernel(int64_t N, int mode, int nchunk, double pref, const double *partT,
+                                 const double *partN, double *sT, double *sN)
+{
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double T = 0.0, Nn = 0.0;
+    for (int c = 0; c < nchunk; c++) T += partT[(int64_t)c * N + k];
+    sT[k] = pref * T;
+    if (sN) {
+        if (mode == 2) {
+            for (int c = 0; c < nchunk; c++) Nn += partN[(int64_t)c * N + k];
+            sN[k] = pref * Nn;
+        } else {
+            sN[k] = 0.0;
+        }
+    }
+}

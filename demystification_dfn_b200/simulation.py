@@ -1,0 +1,215 @@
+"""Host-side driver over the C ABI, mirroring the reference's operator API.
+
+``Simulation`` owns one device handle and exposes the reference's internal
+operators with their names, argument meaning and error behaviour:
+
+* ``kernel(slip)``             kernel_ptr (src/variables.f90:17-26)
+* ``compute_P(dt)``            compute_P (src/fluid_diffusion.f90:24), returns ier
+* ``friction_law(x, Y)``       fric_law_ptr (src/variables.f90:9-14)
+* ``rkqs(...)``                rkqs (src/ode_solver/ode_bs.f90:125)
+* ``solve(...)``               solve (src/solver.f90:42-206) with save_data /
+                               write_data into ``output%07d`` files
+
+All arithmetic runs in libdfn_b200 on the GPU; this module only moves
+arrays across the ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from .layout import DfnOptions, DfnReport, ProblemArrays, build_arrays, ptr, to_c
+
+STORAGE = {"fp64": 0, "fp32": 1, "bf16x2": 2}
+PRESSURE = {"cg": 0, "tridiag": 1}
+GEMV = {"tma": 0, "ldg": 1}
+
+
+class Simulation:
+    def __init__(self, problem, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64):
+        self.lib = _lib.load()
+        self.arrays = problem if isinstance(problem, ProblemArrays) else build_arrays(problem)
+        self.N = self.arrays.N
+        opt = DfnOptions()
+        self.lib.dfn_default_options(ctypes.byref(opt))
+        opt.kernel_storage = STORAGE[storage]
+        opt.pressure_solver = PRESSURE[pressure]
+        opt.device = int(device)
+        opt.gemv_impl = GEMV[gemv]
+        opt.max_attempts = int(max_attempts)
+        self.options = {"storage": storage, "pressure": pressure, "gemv": gemv}
+        self._c = to_c(self.arrays)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.dfn_create(ctypes.byref(self._c), ctypes.byref(opt), ctypes.byref(h)), self.lib)
+        self.h = h
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.dfn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: int):
+        _lib.check(self.lib.dfn_set_stream(self.h, ctypes.c_void_p(stream_handle)), self.lib)
+
+    @property
+    def kernel_bytes(self):
+        return int(self.lib.dfn_kernel_bytes(self.h))
+
+    @property
+    def launches(self):
+        return int(self.lib.dfn_launch_count(self.h))
+
+    # -- operators ---------------------------------------------------------
+    def kernel(self, slip):
+        slip = np.ascontiguousarray(slip, dtype=np.float64)
+        if slip.shape != (self.N,):
+            raise ValueError("slip must have nb_element entries")
+        sT = np.empty(self.N)
+        sN = np.empty(self.N)
+        _lib.check(self.lib.dfn_kernel(self.h, ptr(slip), ptr(sT), ptr(sN)), self.lib)
+        return sT, sN
+
+    def compute_P(self, dt):
+        Pt = np.zeros(self.N)
+        Pd = np.zeros(self.N)
+        ier = ctypes.c_int32(0)
+        _lib.check(self.lib.dfn_compute_P(self.h, float(dt), ptr(Pt), ptr(Pd), ctypes.byref(ier)), self.lib)
+        return Pt, Pd, int(ier.value)
+
+    def friction_law(self, x, Y):
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        if Y.shape != (3 * self.N,):
+            raise ValueError("Y must have 3*nb_element entries")
+        Yd = np.empty_like(Y)
+        _lib.check(self.lib.dfn_friction_law(self.h, float(x), Y.size, ptr(Y), ptr(Yd)), self.lib)
+        return Yd
+
+    def rkqs(self, y, dydx, x, htry, eps, yscal):
+        y = np.array(y, dtype=np.float64, copy=True)
+        dydx = np.ascontiguousarray(dydx, dtype=np.float64)
+        yscal = np.ascontiguousarray(yscal, dtype=np.float64)
+        xx = ctypes.c_double(x)
+        hdid = ctypes.c_double(0)
+        hnext = ctypes.c_double(0)
+        _lib.check(self.lib.dfn_rkqs(self.h, ptr(y), ptr(dydx), y.size, ctypes.byref(xx), float(htry), float(eps),
+                                     ptr(yscal), ctypes.byref(hdid), ctypes.byref(hnext)), self.lib)
+        return y, xx.value, hdid.value, hnext.value
+
+    # -- driver ------------------------------------------------------------
+    def solve_steps(self, n):
+        rep = DfnReport()
+        st = self.lib.dfn_solve_steps(self.h, int(n), ctypes.byref(rep))
+        _lib.check(st, self.lib)
+        return rep.as_dict()
+
+    def state(self):
+        Y = np.empty(3 * self.N)
+        P = np.empty(self.N)
+        t = ctypes.c_double()
+        tt = ctypes.c_double()
+        it = ctypes.c_int64()
+        _lib.check(self.lib.dfn_get_state(self.h, ptr(Y), ptr(P), ctypes.byref(t), ctypes.byref(tt),
+                                          ctypes.byref(it)), self.lib)
+        return {"Y": Y, "P": P, "time": t.value, "t_try": tt.value, "it_count": it.value}
+
+    def set_state(self, Y, P, time, t_try, it_count=0):
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        _lib.check(self.lib.dfn_set_state(self.h, ptr(Y), ptr(P), float(time), float(t_try), int(it_count)),
+                   self.lib)
+
+    def snapshot(self):
+        out = {k: np.empty(self.N) for k in ("V", "theta", "P", "tractionTel", "tractionNel", "permeability")}
+        t = ctypes.c_double()
+        _lib.check(self.lib.dfn_get_snapshot(self.h, ptr(out["V"]), ptr(out["theta"]), ptr(out["P"]),
+                                             ptr(out["tractionTel"]), ptr(out["tractionNel"]),
+                                             ptr(out["permeability"]), ctypes.byref(t)), self.lib)
+        out["time"] = t.value
+        return out
+
+    def time_kernel(self, reps=20):
+        ms = ctypes.c_double()
+        _lib.check(self.lib.dfn_time_kernel(self.h, int(reps), ctypes.byref(ms)), self.lib)
+        return ms.value
+
+    def profile_kv(self, enable=True):
+        _lib.check(self.lib.dfn_profile_kv(self.h, 1 if enable else 0), self.lib)
+
+    def profile_kv_read(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        _lib.check(self.lib.dfn_profile_kv_read(self.h, ctypes.byref(ms), ctypes.byref(n)), self.lib)
+        return ms.value, n.value
+
+    def step_host(self, Y, P, time, t_try, out):
+        """One accepted step with host buffers on both sides (dfn_step_host)."""
+        rep = DfnReport()
+        st = self.lib.dfn_step_host(self.h, ptr(Y), ptr(P), float(time), float(t_try), ptr(out[0]), ptr(out[1]),
+                                    ptr(out[2]), ptr(out[3]), ptr(out[4]), ctypes.byref(rep))
+        _lib.check(st, self.lib)
+        return rep
+
+    def solve(self, max_it=None, output_dir=None, stride_time=None, freq_writing_file=None, callback=None):
+        """The solve() loop (src/solver.f90:59-201) with its output schedule.
+
+        A snapshot is saved when ``(it_count-1) % stride_time == 0``
+        (save_data, :211-222); every ``freq_writing_file`` saved snapshots an
+        ``output%07d`` file named after it_count is written (write_data,
+        :190-193, :227-317), and a last file at the end (:201). Returns the list
+        of saved snapshots when ``output_dir`` is None.
+        """
+        a = self.arrays
+        max_it = a.max_it if max_it is None else int(max_it)
+        stride = a.stride_time if stride_time is None else int(stride_time)
+        freq = a.freq_writing_file if freq_writing_file is None else int(freq_writing_file)
+        saved, buf = [], []
+        it = self.state()["it_count"]
+        while True:
+            st = self.lib.dfn_solve_steps(self.h, 1, ctypes.byref(rep := DfnReport()))
+            it = rep.it_count
+            if st not in (0, 3):
+                _lib.check(st, self.lib)
+            if (it - 1) % stride == 0:
+                snap = self.snapshot()
+                buf.append(snap)
+                if callback:
+                    callback(it, snap)
+            if st == 3:
+                # sigmaN > 0: the reference prints and stops (src/solver.f90:412-418)
+                # after the stop/write checks of this step
+                self._flush(buf, it, freq, output_dir, saved, force=True)
+                raise _lib.DfnError(3, f"it_count={it}")
+            if it >= max_it:
+                break
+            if len(buf) == freq:
+                self._flush(buf, it, freq, output_dir, saved)
+        self._flush(buf, it, freq, output_dir, saved, force=True)
+        return saved
+
+    def _flush(self, buf, it, freq, output_dir, saved, force=False):
+        if not buf:
+            return
+        if output_dir is None:
+            saved.extend(buf)
+        else:
+            from .hdf5 import write_output
+
+            os.makedirs(output_dir, exist_ok=True)
+            write_output(os.path.join(output_dir, "output%07d" % it), buf, freq, self.N)
+        buf.clear()

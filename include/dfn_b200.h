@@ -1,0 +1,195 @@
+/*
+ * dfn_b200.h — C ABI of the B200 earthquake-cycle hot path.
+ *
+ * The hot path is one right-hand-side evaluation of the rate-and-state
+ * earthquake-cycle ODE and the adaptive Cash-Karp RK45 driver around it:
+ *   - elastostatic stress-rate transfer K.V (shear and, in mode II, normal),
+ *   - rate-and-state friction with radiation damping (closed-form dV/dt),
+ *   - implicit pore-pressure diffusion along the concatenated fault chain.
+ *
+ * Every entry point takes plain pointers and sizes. Host buffers belong to
+ * the caller; device memory is owned by the handle. A handle is bound to one
+ * CUDA device and one stream and must not be shared between host threads.
+ * All functions return a dfn_status code; nothing here falls back to the CPU.
+ *
+ * State layout (identical to the reference's Y vector,
+ * src/configuration.f90:185-187,235-237):
+ *   Y[0:N)    slip rate V            (m/s)
+ *   Y[N:2N)   log-state psi = ln(theta*V0/Dc)
+ *   Y[2N:3N)  normal traction sigmaN (Pa, compression negative)
+ * N counts one "fake" element between consecutive faults
+ * (src/configuration.f90:126,136); its derivatives are held at zero.
+ */
+#ifndef DFN_B200_H
+#define DFN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFN_ABI_VERSION 1
+
+/* Status codes. DFN_ERR_NOCONV plays the role of the reference's ier=1. */
+typedef enum dfn_status {
+    DFN_OK = 0,
+    DFN_ERR_NOCONV = 1,      /* pressure CG hit its 200-iteration cap (src/fluid_diffusion.f90:120-125) */
+    DFN_ERR_UNDERFLOW = 2,   /* "stepsize underflow in rkqs" (src/ode_solver/ode_bs.f90:164) */
+    DFN_ERR_EXTENSIONAL = 3, /* sigmaN > 0 after a step (src/solver.f90:412-418) */
+    DFN_ERR_NONFINITE = 4,   /* NaN/Inf in the state or in a pressure solve */
+    DFN_ERR_ARG = 5,         /* invalid argument or size */
+    DFN_ERR_CUDA = 6,        /* a CUDA runtime call failed */
+    DFN_ERR_UNSUPPORTED = 7, /* feature not available in this build */
+    DFN_ERR_ATTEMPTS = 8,    /* more rejected RK attempts in one step than the device budget */
+    DFN_ERR_NOMEM = 9        /* device allocation failed */
+} dfn_status;
+
+enum { DFN_MODE_II = 2, DFN_MODE_III = 3 };                    /* hyperparameter/fracture_mode */
+enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter/static_kernel */
+enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2 }; /* stored K entries */
+enum { DFN_PRESSURE_CG = 0, DFN_PRESSURE_TRIDIAG = 1 };         /* pressure solver */
+
+/*
+ * Problem description: the reference's in-memory state after read_config
+ * (src/configuration.f90:70-379), fake elements included. Per-element arrays
+ * have N entries; the node array has N+1 nodes stored x,y,x,y,... (the
+ * Fortran node(2,nb_node) array). Fake elements carry the reader's presets
+ * (a=b=Dc=f0=V0=1) and zeros elsewhere.
+ */
+typedef struct dfn_problem {
+    int64_t nb_element;              /* N (fake elements included) */
+    int64_t nb_fault;                /* F */
+    const int64_t *fault_nb_element; /* [F] elements of each fault */
+    int32_t fracture_mode;           /* DFN_MODE_II or DFN_MODE_III */
+    int32_t static_kernel;           /* DFN_KERNEL_* */
+    const double *node;              /* [2*(N+1)] */
+    const double *a, *b, *Dc, *f0, *V0;        /* [N] friction parameters */
+    const double *V, *theta, *sigmaN, *P;      /* [N] initial state, theta is psi */
+    const double *normal_loading_dot;          /* [N] */
+    const double *shear_loading_dot;           /* [N] */
+    const double *permeability;                /* [N] */
+    double mu, cp, cs;
+    double Sigma11_dot, Sigma12_dot, Sigma22_dot, Sigma31_dot, Sigma32_dot;
+    double rock_comp, fluid_comp, fluid_density, porosity, dyn_viscosity;
+    int64_t nb_source;               /* total sources over all faults */
+    const int64_t *src_fault;        /* [nb_source] 1-based fault id, grouped by fault */
+    const int64_t *src_index;        /* [nb_source] 1-based element index within the fault */
+    const double *src_Q;             /* [nb_source] m/s */
+    const double *src_t_beg, *src_t_end;       /* [nb_source] s */
+    double tol_solver;
+    double time0;
+    int64_t max_it, stride_time, freq_writing_file;
+} dfn_problem;
+
+/* Options of this implementation (no counterpart in the reference). */
+typedef struct dfn_options {
+    int32_t kernel_storage;   /* DFN_STORE_*; FP64 is the plain path */
+    int32_t pressure_solver;  /* DFN_PRESSURE_CG restates the reference; TRIDIAG solves exactly */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t max_attempts;     /* RK attempts per step scheduled on the device before the host looks (>=1) */
+    int32_t gemv_impl;        /* 0 = TMA bulk-copy pipeline, 1 = direct 128-bit loads */
+    int32_t reserved[3];
+} dfn_options;
+
+/* Per-call report of the solve driver. */
+typedef struct dfn_report {
+    int64_t it_count;         /* accepted steps since the start (reference it_count) */
+    int64_t attempts;         /* RK attempts, accepted and rejected */
+    int64_t rejected;
+    int64_t rhs_evals;
+    int64_t cg_iterations;    /* pressure CG iterations summed over all solves */
+    int64_t probe_halvings;   /* t_try halvings forced by CG non-convergence */
+    double time;              /* simulated time after the last step */
+    double t_try;             /* next trial step */
+    double last_hdid;
+    int32_t status;
+    int32_t pad;
+} dfn_report;
+
+typedef struct dfn_handle dfn_handle;
+
+/* ---- lifecycle ------------------------------------------------------- */
+int32_t dfn_abi_version(void);
+int64_t dfn_problem_struct_size(void);
+int64_t dfn_options_struct_size(void);
+int64_t dfn_report_struct_size(void);
+const char *dfn_status_string(int32_t status);
+const char *dfn_last_error(void);
+void dfn_default_options(dfn_options *opt);
+
+/* Reads the problem, builds geometry (src/initialisation.f90:139-272),
+ * assembles the kernel matrices on the device and sets time/t_try/it_count
+ * as solve() does at entry (src/solver.f90:47-56). */
+int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle **out);
+int32_t dfn_destroy(dfn_handle *h);
+int32_t dfn_set_stream(dfn_handle *h, void *cuda_stream);
+int64_t dfn_nb_element(const dfn_handle *h);
+/* Bytes of stored kernel matrices (K.V algorithmic bytes per evaluation). */
+int64_t dfn_kernel_bytes(const dfn_handle *h);
+
+/* ---- operators (host buffers) ---------------------------------------- */
+/* Replaces kernel_ptr => directII/directIII/hmatII/hmatIII,
+ * interface src/variables.f90:17-26: stressT/stressN = K.slip (stress rates
+ * when slip holds V). stressN may be NULL in mode III. */
+int32_t dfn_kernel(dfn_handle *h, const double *slip, double *stressT, double *stressN);
+
+/* Replaces compute_P(dt,P_temp,P_dot_temp,ier), src/fluid_diffusion.f90:24-152:
+ * implicit step of length dt from the committed pressure. On *ier==1 the
+ * outputs are left untouched, as in the reference. */
+int32_t dfn_compute_P(dfn_handle *h, double dt, double *P_temp, double *P_dot, int32_t *ier);
+
+/* Replaces fric_law_ptr => ode_RateStateAgingModeII/III, interface
+ * src/variables.f90:9-14: Y_dot = f(x, Y) with x the offset from the step start. */
+int32_t dfn_friction_law(dfn_handle *h, double x, int64_t nv, const double *Y, double *Y_dot);
+
+/* Replaces rkqs (src/ode_solver/ode_bs.f90:125-174): one adaptive Cash-Karp
+ * step of the handle's ODE from y, with dydx = f(x, y) supplied. */
+int32_t dfn_rkqs(dfn_handle *h, double *y, const double *dydx, int64_t nv, double *x,
+                 double htry, double eps, const double *yscal, double *hdid, double *hnext);
+
+/* ---- solve driver ----------------------------------------------------- */
+/* Advances the solve() loop (src/solver.f90:59-198) by n_steps accepted steps
+ * on the device: injection clamp, CG probe, scaling RHS, rkqs, 1-day cap,
+ * pressure commit, time update, save_data and the sigmaN>0 check. */
+int32_t dfn_solve_steps(dfn_handle *h, int64_t n_steps, dfn_report *rep);
+
+/* One step with host buffers on both sides: uploads Y/P/time/t_try from
+ * pinned or pageable host memory, advances one accepted step and downloads
+ * the save_data snapshot (V, theta, P, tractionT, tractionN). */
+int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, double time_in,
+                      double t_try_in, double *V_out, double *theta_out, double *P_out,
+                      double *tractionT_out, double *tractionN_out, dfn_report *rep);
+
+/* State access. Y has 3N entries. */
+int32_t dfn_get_state(dfn_handle *h, double *Y, double *P, double *time, double *t_try,
+                      int64_t *it_count);
+int32_t dfn_set_state(dfn_handle *h, const double *Y, const double *P, double time, double t_try,
+                      int64_t it_count);
+
+/* The save_data snapshot of the last accepted step (src/solver.f90:211-222):
+ * V, theta=Dc/V0*exp(psi), P, tractionTel=SigmaT_dot of the last RHS
+ * evaluation, tractionNel=sigmaN, permeability, time. Any pointer may be NULL. */
+int32_t dfn_get_snapshot(dfn_handle *h, double *V, double *theta, double *P, double *tractionT,
+                         double *tractionN, double *permeability, double *time);
+
+/* ---- device-pointer entry points (same stream as the handle) ---------- */
+int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_stressT,
+                          double *d_stressN);
+
+/* ---- timing helpers (CUDA events on the handle's stream) --------------- */
+/* Times `reps` K.V launches of the handle's storage on its stream and
+ * returns the mean duration of one launch in milliseconds. */
+int32_t dfn_time_kernel(dfn_handle *h, int32_t reps, double *ms_per_launch);
+/* Number of kernels this library launched since the handle was created. */
+int64_t dfn_launch_count(const dfn_handle *h);
+/* Per-launch CUDA-event timing of the K.V kernel inside the solve driver.
+ * enable!=0 clears the record and starts recording (up to 16384 launches);
+ * read returns the summed duration (ms) and the number of recorded launches. */
+int32_t dfn_profile_kv(dfn_handle *h, int32_t enable);
+int32_t dfn_profile_kv_read(dfn_handle *h, double *total_ms, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DFN_B200_H */

@@ -1,0 +1,702 @@
+/*
+ * dfn_oracle.c — CPU FP64 restatement of DemystiFicatioN's earthquake-cycle
+ * hot path. TEST INFRASTRUCTURE ONLY: it is the checker for the CUDA library
+ * (tests, smoke, and the cpu_baseline / reference arm of bench.py). The
+ * product path never calls it.
+ *
+ * PARITY UNPINNED: the reference is Fortran with no compiler in this image
+ * and ships no golden outputs, so this restatement is checked against
+ * known answers (telescoping sums, steady state, exact ODE solutions, direct
+ * tridiagonal solves) instead of reference outputs.
+ *
+ * Each routine cites the reference file:line it restates. Arithmetic follows
+ * the Fortran expression order; this file is compiled with
+ * -ffp-contract=off so no FMA is formed (the reference's x86-64 -O1 build
+ * has none either).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/dfn_b200.h"
+
+#define PI_F90 3.141592653589793238 /* src/variables.f90:44 */
+
+typedef struct orc {
+    int64_t N, F;
+    int mode, static_kernel;
+    int64_t *fault_n, *fault_first; /* fault_first: 0-based first element */
+    double *node;                   /* 2*(N+1) */
+    double *elem, *ds, *tan, *nrm;  /* ini_value geometry */
+    double *a, *b, *Dc, *f0, *V0, *nload, *sload, *perm, *permx;
+    unsigned char *fake;
+    double mu, cp, cs;
+    double S11d, S12d, S22d, S31d, S32d;
+    double rock_comp, fluid_comp, porosity, dyn_visc;
+    int64_t nsrc;
+    int64_t *src_fault, *src_index;
+    double *src_Q, *src_tb, *src_te;
+    double tol;
+    /* mutable state */
+    double time, t_try;
+    int64_t it_count;
+    double *Y, *P, *Pdot, *SigmaT_dot, *SigmaN_dot;
+    /* dense kernel (optional) */
+    double *KT, *KN;
+    int kernel_impl; /* 0 matrix-free reference routine, 1 dense stored K */
+    int nthreads;
+    /* counters */
+    int64_t cg_iters, rhs_evals, attempts, rejected, halvings;
+    int last_status;
+} orc;
+
+static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
+
+/* ---------------------------------------------------------------------- */
+/* Geometry and loading projection: src/initialisation.f90:145-153,159-205,
+ * permeability_x: src/initialisation.f90:252-269.                         */
+static void orc_ini_value(orc *o)
+{
+    int64_t N = o->N;
+    for (int64_t k = 0; k < N; k++) {
+        double x0 = o->node[2 * k], y0 = o->node[2 * k + 1];
+        double x1 = o->node[2 * k + 2], y1 = o->node[2 * k + 3];
+        o->elem[2 * k] = (x1 + x0) * 0.5;
+        o->elem[2 * k + 1] = (y1 + y0) * 0.5;
+        o->ds[k] = sqrt((x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0));
+        o->tan[2 * k] = (x1 - x0) / o->ds[k];
+        o->tan[2 * k + 1] = (y1 - y0) / o->ds[k];
+        o->nrm[2 * k] = -o->tan[2 * k + 1];
+        o->nrm[2 * k + 1] = o->tan[2 * k];
+    }
+    double *sig = o->Y + 2 * N;
+    for (int64_t k = 0; k < N; k++) {
+        double n1 = o->nrm[2 * k], n2 = o->nrm[2 * k + 1];
+        double t1 = o->tan[2 * k], t2 = o->tan[2 * k + 1];
+        if (o->mode == DFN_MODE_III) {
+            o->sload[k] = o->sload[k] - t2 * o->S31d + t1 * o->S32d;
+            sig[k] = sig[k] + n1 * (n1 * o->S11d + n2 * o->S12d) + n2 * (n1 * o->S12d + n2 * o->S22d);
+        } else {
+            /* Sigma11/12/22 (not _dot) are never read and stay zero. */
+            sig[k] = sig[k] + n1 * (n1 * 0.0 + n2 * 0.0) + n2 * (n1 * 0.0 + n2 * 0.0);
+            o->nload[k] = o->nload[k] + n1 * (n1 * o->S11d + n2 * o->S12d) + n2 * (n1 * o->S12d + n2 * o->S22d);
+            o->sload[k] = o->sload[k] + t1 * (n1 * o->S11d + n2 * o->S12d) + t2 * (n1 * o->S12d + n2 * o->S22d);
+        }
+    }
+    for (int64_t j = 0; j <= N; j++) o->permx[j] = 0.0;
+    for (int64_t k = 1; k < N; k++)
+        o->permx[k] = 2.0 * o->perm[k - 1] * o->perm[k] / (o->perm[k - 1] + o->perm[k]);
+}
+
+orc *orc_create(const dfn_problem *p)
+{
+    if (!p || p->nb_element < 2 || p->nb_fault < 1) return NULL;
+    orc *o = (orc *)xcalloc(1, sizeof(orc));
+    int64_t N = p->nb_element, F = p->nb_fault;
+    o->N = N; o->F = F;
+    o->mode = p->fracture_mode; o->static_kernel = p->static_kernel;
+    o->fault_n = (int64_t *)xcalloc(F, 8); o->fault_first = (int64_t *)xcalloc(F, 8);
+    int64_t cnt = 0;
+    for (int64_t f = 0; f < F; f++) {
+        o->fault_n[f] = p->fault_nb_element[f];
+        o->fault_first[f] = cnt;
+        cnt += p->fault_nb_element[f] + 1;
+    }
+    if (cnt - 1 != N) { free(o->fault_n); free(o->fault_first); free(o); return NULL; }
+    o->node = (double *)xcalloc(2 * (N + 1), 8);
+    memcpy(o->node, p->node, sizeof(double) * 2 * (N + 1));
+    o->elem = (double *)xcalloc(2 * N, 8); o->ds = (double *)xcalloc(N, 8);
+    o->tan = (double *)xcalloc(2 * N, 8); o->nrm = (double *)xcalloc(2 * N, 8);
+#define CP(dst, src) do { dst = (double *)xcalloc(N, 8); memcpy(dst, src, 8 * N); } while (0)
+    CP(o->a, p->a); CP(o->b, p->b); CP(o->Dc, p->Dc); CP(o->f0, p->f0); CP(o->V0, p->V0);
+    CP(o->nload, p->normal_loading_dot); CP(o->sload, p->shear_loading_dot);
+    CP(o->perm, p->permeability);
+    o->permx = (double *)xcalloc(N + 1, 8);
+    o->fake = (unsigned char *)xcalloc(N, 1);
+    /* src/friction/RateStateAgingModeII.f90:81-89: element idx after each fault */
+    int64_t idx = 0;
+    for (int64_t f = 0; f < F; f++) {
+        idx += o->fault_n[f] + 1;
+        if (idx <= N) o->fake[idx - 1] = 1;
+    }
+    o->mu = p->mu; o->cp = p->cp; o->cs = p->cs;
+    o->S11d = p->Sigma11_dot; o->S12d = p->Sigma12_dot; o->S22d = p->Sigma22_dot;
+    o->S31d = p->Sigma31_dot; o->S32d = p->Sigma32_dot;
+    o->rock_comp = p->rock_comp; o->fluid_comp = p->fluid_comp;
+    o->porosity = p->porosity; o->dyn_visc = p->dyn_viscosity;
+    o->nsrc = p->nb_source;
+    o->src_fault = (int64_t *)xcalloc(o->nsrc, 8); o->src_index = (int64_t *)xcalloc(o->nsrc, 8);
+    o->src_Q = (double *)xcalloc(o->nsrc, 8); o->src_tb = (double *)xcalloc(o->nsrc, 8);
+    o->src_te = (double *)xcalloc(o->nsrc, 8);
+    for (int64_t s = 0; s < o->nsrc; s++) {
+        o->src_fault[s] = p->src_fault[s]; o->src_index[s] = p->src_index[s];
+        o->src_Q[s] = p->src_Q[s]; o->src_tb[s] = p->src_t_beg[s]; o->src_te[s] = p->src_t_end[s];
+    }
+    o->tol = p->tol_solver;
+    o->Y = (double *)xcalloc(3 * N, 8);
+    memcpy(o->Y, p->V, 8 * N); memcpy(o->Y + N, p->theta, 8 * N); memcpy(o->Y + 2 * N, p->sigmaN, 8 * N);
+    CP(o->P, p->P);
+#undef CP
+    o->Pdot = (double *)xcalloc(N, 8);
+    o->SigmaT_dot = (double *)xcalloc(N, 8); o->SigmaN_dot = (double *)xcalloc(N, 8);
+    orc_ini_value(o);
+    /* solve() entry: src/solver.f90:50-56 */
+    o->time = p->time0; o->t_try = 100.0; o->it_count = 0;
+    o->kernel_impl = 0;
+    o->nthreads = 1;
+    return o;
+}
+
+void orc_destroy(orc *o)
+{
+    if (!o) return;
+    void *ptrs[] = {o->fault_n, o->fault_first, o->node, o->elem, o->ds, o->tan, o->nrm, o->a, o->b,
+                    o->Dc, o->f0, o->V0, o->nload, o->sload, o->perm, o->permx, o->fake, o->src_fault,
+                    o->src_index, o->src_Q, o->src_tb, o->src_te, o->Y, o->P, o->Pdot, o->SigmaT_dot,
+                    o->SigmaN_dot, o->KT, o->KN};
+    for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
+    free(o);
+}
+
+void orc_set_threads(orc *o, int n) { o->nthreads = n < 1 ? 1 : n; }
+void orc_set_kernel_impl(orc *o, int impl) { o->kernel_impl = impl; }
+int64_t orc_n(const orc *o) { return o->N; }
+
+/* ---------------------------------------------------------------------- */
+/* Matrix-free kernels, the reference's "direct" routines.                 */
+
+/* directII: src/kernel_calculation/directModeII.f90:33-103 */
+static void orc_directII(const orc *o, const double *slip, double *sT, double *sN)
+{
+    int64_t N = o->N;
+    const double *el = o->elem, *nd = o->node, *nr = o->nrm;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(o->nthreads)
+#endif
+    for (int64_t k = 0; k < N; k++) {
+        double T = 0.0, Nn = 0.0;
+        double e1 = el[2 * k], e2 = el[2 * k + 1];
+        double n1 = nr[2 * k], n2 = nr[2 * k + 1];
+        for (int64_t l = 0; l < N; l++) {
+            double dxl = e1 - nd[2 * l], dyl = e2 - nd[2 * l + 1];
+            double dxr = e1 - nd[2 * l + 2], dyr = e2 - nd[2 * l + 3];
+            double rl = sqrt(dxl * dxl + dyl * dyl);
+            double rr = sqrt(dxr * dxr + dyr * dyr);
+            double g1l = dxl / rl, g2l = dyl / rl, g1r = dxr / rr, g2r = dyr / rr;
+            double I1tl = (4.0 * n1 * n2 * g1l * g2l + (n2 * n2 - n1 * n1) * (g2l * g2l - g1l * g1l)) * g1l / rl;
+            double I2tl = (4.0 * n1 * n2 * g1l * g2l + (n2 * n2 - n1 * n1) * (g2l * g2l - g1l * g1l)) * g2l / rl;
+            double I1tr = (4.0 * n1 * n2 * g1r * g2r + (n2 * n2 - n1 * n1) * (g2r * g2r - g1r * g1r)) * g1r / rr;
+            double I2tr = (4.0 * n1 * n2 * g1r * g2r + (n2 * n2 - n1 * n1) * (g2r * g2r - g1r * g1r)) * g2r / rr;
+            double I1nl = g1l / rl - g2l / rl * (2.0 * n1 * n2 * (g2l * g2l - g1l * g1l) - (n2 * n2 - n1 * n1) * 2.0 * g1l * g2l);
+            double I2nl = g2l / rl + g1l / rl * (2.0 * n1 * n2 * (g2l * g2l - g1l * g1l) - (n2 * n2 - n1 * n1) * 2.0 * g1l * g2l);
+            double I1nr = g1r / rr - g2r / rr * (2.0 * n1 * n2 * (g2r * g2r - g1r * g1r) - (n2 * n2 - n1 * n1) * 2.0 * g1r * g2r);
+            double I2nr = g2r / rr + g1r / rr * (2.0 * n1 * n2 * (g2r * g2r - g1r * g1r) - (n2 * n2 - n1 * n1) * 2.0 * g1r * g2r);
+            /* normal_left = normal_right = normal (src/initialisation.f90:203-204) */
+            double nl1 = nr[2 * l], nl2 = nr[2 * l + 1];
+            T = T + slip[l] * (nl2 * I1tl - nl2 * I1tr - nl1 * I2tl + nl1 * I2tr);
+            Nn = Nn + slip[l] * (nl1 * I1nl - nl1 * I1nr + nl2 * I2nl - nl2 * I2nr);
+        }
+        sT[k] = T; sN[k] = Nn;
+    }
+    double pref = o->mu / PI_F90 * (1.0 - o->cs * o->cs / (o->cp * o->cp));
+    for (int64_t k = 0; k < N; k++) { sN[k] = pref * sN[k]; sT[k] = pref * sT[k]; }
+}
+
+/* directIII: src/kernel_calculation/directModeIII.f:35-80, with its own
+ * element/tangent (node + 0.5*(dnode), real 0.5 literal). */
+static void orc_directIII(const orc *o, const double *slip, double *sT)
+{
+    int64_t N = o->N;
+    const double *nd = o->node;
+    double *el = (double *)malloc(16 * N), *t = (double *)malloc(16 * N);
+    for (int64_t k = 0; k < N; k++) {
+        t[2 * k] = nd[2 * k + 2] - nd[2 * k];
+        t[2 * k + 1] = nd[2 * k + 3] - nd[2 * k + 1];
+        double nt = sqrt(t[2 * k] * t[2 * k] + t[2 * k + 1] * t[2 * k + 1]);
+        t[2 * k] = t[2 * k] / nt; t[2 * k + 1] = t[2 * k + 1] / nt;
+        el[2 * k] = nd[2 * k] + 0.5 * (nd[2 * k + 2] - nd[2 * k]);
+        el[2 * k + 1] = nd[2 * k + 1] + 0.5 * (nd[2 * k + 3] - nd[2 * k + 1]);
+    }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(o->nthreads)
+#endif
+    for (int64_t k = 0; k < N; k++) {
+        double acc = 0.0;
+        for (int64_t l = 1; l <= N + 1; l++) { /* 1-based node index */
+            double dx = el[2 * k] - nd[2 * (l - 1)], dy = el[2 * k + 1] - nd[2 * (l - 1) + 1];
+            double r1 = sqrt(dx * dx + dy * dy);
+            double I1 = t[2 * k] / (r1 * r1) * dx + t[2 * k + 1] / (r1 * r1) * dy;
+            if (l - 1 >= 1 && l <= N) acc = acc - (slip[l - 1] - slip[l - 2]) * I1;
+            else if (l == 1) acc = acc - slip[l - 1] * I1;
+            else acc = acc + slip[l - 2] * I1;
+        }
+        sT[k] = acc;
+    }
+    for (int64_t k = 0; k < N; k++) sT[k] = sT[k] * o->mu / (2 * PI_F90);
+    free(el); free(t);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Kernel entries: src/hmatrix/eval_kernel_hmatrix.f90:7-199 with
+ * node_left=node(l), node_right=node(l+1) (src/initialisation.f90:212-213).
+ * which: 0 = mode III, 1 = mode II shear (T), 2 = mode II normal (N).     */
+double orc_kernel_entry(const orc *o, int64_t k, int64_t l, int which)
+{
+    const double *el = o->elem, *nd = o->node;
+    double e1 = el[2 * k], e2 = el[2 * k + 1];
+    if (which == 0) {
+        double t1 = o->tan[2 * k], t2 = o->tan[2 * k + 1];
+        double ax = nd[2 * l] - e1, ay = nd[2 * l + 1] - e2;
+        double bx = nd[2 * l + 2] - e1, by = nd[2 * l + 3] - e2;
+        double r1 = sqrt(ax * ax + ay * ay);
+        double r2 = sqrt(bx * bx + by * by);
+        double I1 = t1 / (r1 * r1) * (e1 - nd[2 * l]) + t2 / (r1 * r1) * (e2 - nd[2 * l + 1]);
+        double I2 = t1 / (r2 * r2) * (e1 - nd[2 * l + 2]) + t2 / (r2 * r2) * (e2 - nd[2 * l + 3]);
+        return -I1 + I2;
+    }
+    double n1 = o->nrm[2 * k], n2 = o->nrm[2 * k + 1];
+    double dxl = e1 - nd[2 * l], dyl = e2 - nd[2 * l + 1];
+    double dxr = e1 - nd[2 * l + 2], dyr = e2 - nd[2 * l + 3];
+    double rl = sqrt(dxl * dxl + dyl * dyl);
+    double rr = sqrt(dxr * dxr + dyr * dyr);
+    double g1l = dxl / rl, g2l = dyl / rl, g1r = dxr / rr, g2r = dyr / rr;
+    double nl1 = o->nrm[2 * l], nl2 = o->nrm[2 * l + 1];
+    if (which == 1) {
+        double I1tl = (4.0 * n1 * n2 * g1l * g2l + (n2 * n2 - n1 * n1) * (g2l * g2l - g1l * g1l)) * g1l / rl;
+        double I2tl = (4.0 * n1 * n2 * g1l * g2l + (n2 * n2 - n1 * n1) * (g2l * g2l - g1l * g1l)) * g2l / rl;
+        double I1tr = (4.0 * n1 * n2 * g1r * g2r + (n2 * n2 - n1 * n1) * (g2r * g2r - g1r * g1r)) * g1r / rr;
+        double I2tr = (4.0 * n1 * n2 * g1r * g2r + (n2 * n2 - n1 * n1) * (g2r * g2r - g1r * g1r)) * g2r / rr;
+        return nl2 * I1tl - nl2 * I1tr - nl1 * I2tl + nl1 * I2tr;
+    }
+    double I1nl = g1l / rl - g2l / rl * (2.0 * n1 * n2 * (g2l * g2l - g1l * g1l) - (n2 * n2 - n1 * n1) * 2.0 * g1l * g2l);
+    double I2nl = g2l / rl + g1l / rl * (2.0 * n1 * n2 * (g2l * g2l - g1l * g1l) - (n2 * n2 - n1 * n1) * 2.0 * g1l * g2l);
+    double I1nr = g1r / rr - g2r / rr * (2.0 * n1 * n2 * (g2r * g2r - g1r * g1r) - (n2 * n2 - n1 * n1) * 2.0 * g1r * g2r);
+    double I2nr = g2r / rr + g1r / rr * (2.0 * n1 * n2 * (g2r * g2r - g1r * g1r) - (n2 * n2 - n1 * n1) * 2.0 * g1r * g2r);
+    return nl1 * I1nl - nl1 * I1nr + nl2 * I2nl - nl2 * I2nr;
+}
+
+/* Dense unscaled K (row-major, K[k*N+l]); KN only in mode II. */
+int orc_assemble_dense(orc *o)
+{
+    int64_t N = o->N;
+    free(o->KT); free(o->KN); o->KT = o->KN = NULL;
+    o->KT = (double *)malloc(sizeof(double) * N * N);
+    if (!o->KT) return -1;
+    if (o->mode == DFN_MODE_II) {
+        o->KN = (double *)malloc(sizeof(double) * N * N);
+        if (!o->KN) return -1;
+    }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(o->nthreads)
+#endif
+    for (int64_t k = 0; k < N; k++)
+        for (int64_t l = 0; l < N; l++) {
+            if (o->mode == DFN_MODE_II) {
+                o->KT[k * N + l] = orc_kernel_entry(o, k, l, 1);
+                o->KN[k * N + l] = orc_kernel_entry(o, k, l, 2);
+            } else {
+                o->KT[k * N + l] = orc_kernel_entry(o, k, l, 0);
+            }
+        }
+    return 0;
+}
+
+void orc_copy_dense(const orc *o, double *KT, double *KN)
+{
+    int64_t NN = o->N * o->N;
+    if (KT && o->KT) memcpy(KT, o->KT, 8 * NN);
+    if (KN && o->KN) memcpy(KN, o->KN, 8 * NN);
+}
+
+/* K.V with the stored dense K, sequential sums per row, then the reference
+ * prefactor (hmatII src/kernel_calculation/hmatrixModeII.f90:65-69,
+ * hmatIII src/kernel_calculation/hmatrixModeIII.f90:53-56). */
+static void orc_dense_kv(const orc *o, const double *slip, double *sT, double *sN)
+{
+    int64_t N = o->N;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(o->nthreads)
+#endif
+    for (int64_t k = 0; k < N; k++) {
+        double t = 0.0, n = 0.0;
+        const double *rt = o->KT + k * N;
+        for (int64_t l = 0; l < N; l++) t = t + rt[l] * slip[l];
+        if (o->KN) {
+            const double *rn = o->KN + k * N;
+            for (int64_t l = 0; l < N; l++) n = n + rn[l] * slip[l];
+        }
+        sT[k] = t; if (sN) sN[k] = n;
+    }
+    if (o->mode == DFN_MODE_II) {
+        double pref = o->mu / PI_F90 * (1.0 - o->cs * o->cs / (o->cp * o->cp));
+        for (int64_t k = 0; k < N; k++) { sT[k] = pref * sT[k]; if (sN) sN[k] = pref * sN[k]; }
+    } else {
+        for (int64_t k = 0; k < N; k++) { sT[k] = o->mu / (2.0 * PI_F90) * sT[k]; if (sN) sN[k] = 0.0; }
+    }
+}
+
+/* kernel_ptr dispatch (src/initialisation.f90:105-128). */
+void orc_kernel(orc *o, const double *slip, double *sT, double *sN)
+{
+    if (o->kernel_impl == 1 && o->KT) { orc_dense_kv(o, slip, sT, sN); return; }
+    if (o->mode == DFN_MODE_II) orc_directII(o, slip, sT, sN);
+    else { orc_directIII(o, slip, sT); if (sN) memset(sN, 0, 8 * o->N); }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Pore pressure: src/fluid_diffusion.f90. No fault crossings (the crossing
+ * terms of :213-295 apply only to coincident nodes).                       */
+static inline double orc_coef(const orc *o, double kx, double dt, double dsv)
+{
+    /* kx*dt/(porosity*dyn_viscosity*(fluid_comp+rock_comp)*ds**2) */
+    return kx * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (dsv * dsv));
+}
+
+/* compute_diag: src/fluid_diffusion.f90:308-334 */
+static void orc_diag(const orc *o, double dt, double *diag)
+{
+    int64_t N = o->N;
+    const double *px = o->permx, *ds = o->ds;
+    diag[0] = 1.0 + orc_coef(o, px[1], dt, ds[0]);
+    diag[N - 1] = 1.0 + orc_coef(o, px[N - 1], dt, ds[N - 1]);
+    for (int64_t k = 1; k < N - 1; k++)
+        diag[k] = 1.0 + (px[k] + px[k + 1]) * dt /
+                            (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k] * ds[k]));
+}
+
+/* compute_MatrixVector: src/fluid_diffusion.f90:163-204 */
+static void orc_matvec(const orc *o, const double *v, double dt, const double *diag, double *out)
+{
+    int64_t N = o->N;
+    const double *px = o->permx, *ds = o->ds;
+    double A1, A2, A3;
+    A2 = 1.0 + orc_coef(o, px[1], dt, ds[0]);
+    A3 = -px[1] * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[0] * ds[0]));
+    out[0] = (A2 * v[0] + A3 * v[1]) / diag[0];
+    A1 = -px[N - 1] * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[N - 1] * ds[N - 1]));
+    A2 = 1.0 + orc_coef(o, px[N - 1], dt, ds[N - 1]);
+    out[N - 1] = (A1 * v[N - 2] + A2 * v[N - 1]) / diag[N - 1];
+    for (int64_t k = 1; k < N - 1; k++) {
+        A1 = -px[k] * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k - 1] * ds[k - 1]));
+        A2 = 1.0 + (px[k] + px[k + 1]) * dt /
+                       (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k] * ds[k]));
+        A3 = -px[k + 1] * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k + 1] * ds[k + 1]));
+        out[k] = (A1 * v[k - 1] + A2 * v[k] + A3 * v[k + 1]) / diag[k];
+    }
+}
+
+/* Right-hand side b1 with the injection sources (src/fluid_diffusion.f90:44-64).
+ * Sources are vector subscripts in the reference: when source s of a fault
+ * is active, every source of that fault is added once more. */
+static void orc_rhs_b1(const orc *o, double dt, const double *diag, double *b1)
+{
+    int64_t N = o->N;
+    for (int64_t k = 0; k < N; k++) b1[k] = o->P[k] / diag[k];
+    for (int64_t s = 0; s < o->nsrc; s++) {
+        double t = o->time + dt;
+        if (!(t >= o->src_tb[s] && t < o->src_te[s])) continue;
+        int64_t f = o->src_fault[s] - 1;
+        for (int64_t j = 0; j < o->nsrc; j++) {
+            if (o->src_fault[j] != o->src_fault[s]) continue;
+            int64_t e = o->fault_first[f] + o->src_index[j] - 1;
+            b1[e] = b1[e] + (dt * o->src_Q[j] / (o->porosity * (o->fluid_comp + o->rock_comp)) / o->ds[e]) / diag[e];
+        }
+    }
+}
+
+/* compute_P: src/fluid_diffusion.f90:24-152. Returns ier. */
+int orc_compute_P(orc *o, double dt, double *P_temp, double *P_dot)
+{
+    int64_t N = o->N;
+    double *w = (double *)malloc(sizeof(double) * 7 * N);
+    double *pk = w, *rk = w + N, *rk1 = w + 2 * N, *xk = w + 3 * N, *b1 = w + 4 * N, *diag = w + 5 * N,
+           *Mp = w + 6 * N;
+    int ier = 0;
+    orc_diag(o, dt, diag);
+    orc_rhs_b1(o, dt, diag, b1);
+    /* permeability_coupling == 0: permeability_x is recomputed from the
+     * unchanged permeability (src/fluid_diffusion.f90:74-75) */
+    for (int64_t k = 0; k < N; k++) xk[k] = o->P[k];
+    orc_matvec(o, xk, dt, diag, Mp);
+    for (int64_t k = 0; k < N; k++) { rk[k] = b1[k] - Mp[k]; pk[k] = rk[k]; }
+    int64_t it = 0;
+    double errmax = 0.0;
+    for (int64_t k = 0; k < N; k++) errmax = fmax(errmax, fabs(rk[k] / 1.0));
+    errmax = errmax / o->tol;
+    while (errmax >= 1.0) {
+        it++;
+        orc_matvec(o, pk, dt, diag, Mp);
+        double s_rr = 0.0, s_pAp = 0.0;
+        for (int64_t k = 0; k < N; k++) s_rr = s_rr + rk[k] * rk[k];
+        for (int64_t k = 0; k < N; k++) s_pAp = s_pAp + pk[k] * Mp[k];
+        double alpha = s_rr / s_pAp;
+        for (int64_t k = 0; k < N; k++) xk[k] = xk[k] + alpha * pk[k];
+        for (int64_t k = 0; k < N; k++) rk1[k] = rk[k] - alpha * Mp[k];
+        double s_r1 = 0.0;
+        for (int64_t k = 0; k < N; k++) s_r1 = s_r1 + rk1[k] * rk1[k];
+        double beta = s_r1 / s_rr;
+        for (int64_t k = 0; k < N; k++) pk[k] = rk1[k] + beta * pk[k];
+        for (int64_t k = 0; k < N; k++) rk[k] = rk1[k];
+        if (it > 200) {
+            ier = 1;
+            o->cg_iters += it;
+            free(w);
+            return ier;
+        }
+        errmax = 0.0;
+        for (int64_t k = 0; k < N; k++) errmax = fmax(errmax, fabs(rk[k] / 1.0));
+        errmax = errmax / o->tol;
+    }
+    o->cg_iters += it;
+    if (dt < 1e-9) for (int64_t k = 0; k < N; k++) P_dot[k] = 0.0;
+    else for (int64_t k = 0; k < N; k++) P_dot[k] = (xk[k] - o->P[k]) / dt;
+    double mx = 0.0;
+    for (int64_t k = 0; k < N; k++) { P_temp[k] = xk[k]; mx = fmax(mx, fabs(P_temp[k])); }
+    if (mx > DBL_MAX) ier = 1;
+    free(w);
+    return ier;
+}
+
+/* Exact solve of the same implicit step with the unscaled tridiagonal
+ * system (Thomas algorithm); used by tests to check both CG and the GPU
+ * tridiagonal solver. Not a reference routine. */
+void orc_pressure_exact(const orc *o, double dt, double *P_temp)
+{
+    int64_t N = o->N;
+    double *diag = (double *)malloc(8 * N), *b1 = (double *)malloc(8 * N);
+    double *lo = (double *)malloc(8 * N), *di = (double *)malloc(8 * N), *up = (double *)malloc(8 * N);
+    orc_diag(o, dt, diag);
+    orc_rhs_b1(o, dt, diag, b1);
+    double c = o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp);
+    const double *px = o->permx, *ds = o->ds;
+    for (int64_t k = 0; k < N; k++) {
+        b1[k] *= diag[k];
+        double dsm = ds[k > 0 ? k - 1 : 0], dsp = ds[k < N - 1 ? k + 1 : N - 1];
+        if (k == 0) { lo[k] = 0; di[k] = 1.0 + px[1] * dt / (c * ds[0] * ds[0]); up[k] = -px[1] * dt / (c * ds[0] * ds[0]); }
+        else if (k == N - 1) { lo[k] = -px[k] * dt / (c * ds[k] * ds[k]); di[k] = 1.0 + px[k] * dt / (c * ds[k] * ds[k]); up[k] = 0; }
+        else { lo[k] = -px[k] * dt / (c * dsm * dsm); di[k] = 1.0 + (px[k] + px[k + 1]) * dt / (c * ds[k] * ds[k]); up[k] = -px[k + 1] * dt / (c * dsp * dsp); }
+    }
+    for (int64_t k = 1; k < N; k++) {
+        double m = lo[k] / di[k - 1];
+        di[k] -= m * up[k - 1];
+        b1[k] -= m * b1[k - 1];
+    }
+    P_temp[N - 1] = b1[N - 1] / di[N - 1];
+    for (int64_t k = N - 2; k >= 0; k--) P_temp[k] = (b1[k] - up[k] * P_temp[k + 1]) / di[k];
+    free(diag); free(b1); free(lo); free(di); free(up);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Friction RHS: src/friction/RateStateAgingModeII.f90:19-92 and
+ * src/friction/RateStateAgingModeIII.f90:112-214. Returns compute_P's ier. */
+int orc_rhs(orc *o, double dt, const double *Y1, double *Y1dot)
+{
+    int64_t N = o->N;
+    double *Pt = (double *)malloc(8 * N);
+    memset(Pt, 0, 8 * N);
+    orc_kernel(o, Y1, o->SigmaT_dot, o->SigmaN_dot);
+    int ier = orc_compute_P(o, dt, Pt, o->Pdot);
+    o->rhs_evals++;
+    const double *V = Y1, *psi = Y1 + N, *sig = Y1 + 2 * N;
+    for (int64_t k = 0; k < N; k++) {
+        double dsig = (o->mode == DFN_MODE_II) ? o->SigmaN_dot[k] + o->nload[k] : o->nload[k];
+        Y1dot[2 * N + k] = dsig;
+        double B = V[k] / (2.0 * o->V0[k]);
+        double C = exp((o->f0[k] + o->b[k] * psi[k]) / o->a[k]);
+        double D = 1.0 / (C * C) + B * B;
+        D = 1.0 / sqrt(D);
+        double num = o->sload[k] + o->SigmaT_dot[k] + (Y1dot[2 * N + k] + o->Pdot[k]) * o->a[k] * asinh(B * C) +
+                     B * D * (sig[k] + Pt[k]) * o->b[k] * (o->V0[k] / o->Dc[k] * exp(-psi[k]) - fabs(V[k]) / o->Dc[k]);
+        double den = o->mu / (2.0 * o->cs) - D * (sig[k] + Pt[k]) * o->a[k] / (2.0 * o->V0[k]);
+        Y1dot[k] = num / den;
+        Y1dot[N + k] = o->V0[k] / o->Dc[k] * exp(-psi[k]) - fabs(V[k]) / o->Dc[k];
+    }
+    for (int64_t k = 0; k < N; k++)
+        if (o->fake[k]) { Y1dot[k] = 0.0; Y1dot[N + k] = 0.0; Y1dot[2 * N + k] = 0.0; }
+    free(Pt);
+    return ier;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Cash-Karp tableau and step control: src/ode_solver/ode_bs.f90:125-226. */
+static const double A2 = 0.2, A3 = 0.3, A4 = 0.6, A5 = 1.0, A6 = 0.875;
+static const double B21 = 0.2, B31 = 3.0 / 40.0, B32 = 9.0 / 40.0, B41 = 0.3, B42 = -0.9, B43 = 1.2;
+static const double B51 = -11.0 / 54.0, B52 = 2.5, B53 = -70.0 / 27.0, B54 = 35.0 / 27.0;
+static const double B61 = 1631.0 / 55296.0, B62 = 175.0 / 512.0, B63 = 575.0 / 13824.0,
+                    B64 = 44275.0 / 110592.0, B65 = 253.0 / 4096.0;
+static const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
+#define DC1 (C1 - 2825.0 / 27648.0)
+#define DC3 (C3 - 18575.0 / 48384.0)
+#define DC4 (C4 - 13525.0 / 55296.0)
+#define DC5 (-277.0 / 14336.0)
+#define DC6 (C6 - 0.25)
+
+/* derivs callback: the friction RHS of the handle, or a user function. */
+typedef void (*orc_derivs_fn)(double x, int64_t n, const double *y, double *dydx, void *ctx);
+
+static void orc_rhs_cb(double x, int64_t n, const double *y, double *dydx, void *ctx)
+{
+    (void)n;
+    orc_rhs((orc *)ctx, x, y, dydx);
+}
+
+/* rkck: src/ode_solver/ode_bs.f90:177-226 */
+static void orc_rkck_cb(orc_derivs_fn derivs, void *ctx, const double *y, const double *dydx, int64_t n, double x,
+                        double h, double *yout, double *yerr)
+{
+    double *w = (double *)malloc(sizeof(double) * 6 * n);
+    double *ak2 = w, *ak3 = w + n, *ak4 = w + 2 * n, *ak5 = w + 3 * n, *ak6 = w + 4 * n, *yt = w + 5 * n;
+    for (int64_t i = 0; i < n; i++) yt[i] = y[i] + B21 * h * dydx[i];
+    derivs(x + A2 * h, n, yt, ak2, ctx);
+    for (int64_t i = 0; i < n; i++) yt[i] = y[i] + h * (B31 * dydx[i] + B32 * ak2[i]);
+    derivs(x + A3 * h, n, yt, ak3, ctx);
+    for (int64_t i = 0; i < n; i++) yt[i] = y[i] + h * (B41 * dydx[i] + B42 * ak2[i] + B43 * ak3[i]);
+    derivs(x + A4 * h, n, yt, ak4, ctx);
+    for (int64_t i = 0; i < n; i++) yt[i] = y[i] + h * (B51 * dydx[i] + B52 * ak2[i] + B53 * ak3[i] + B54 * ak4[i]);
+    derivs(x + A5 * h, n, yt, ak5, ctx);
+    for (int64_t i = 0; i < n; i++)
+        yt[i] = y[i] + h * (B61 * dydx[i] + B62 * ak2[i] + B63 * ak3[i] + B64 * ak4[i] + B65 * ak5[i]);
+    derivs(x + A6 * h, n, yt, ak6, ctx);
+    for (int64_t i = 0; i < n; i++) yout[i] = y[i] + h * (C1 * dydx[i] + C3 * ak3[i] + C4 * ak4[i] + C6 * ak6[i]);
+    for (int64_t i = 0; i < n; i++)
+        yerr[i] = h * (DC1 * dydx[i] + DC3 * ak3[i] + DC4 * ak4[i] + DC5 * ak5[i] + DC6 * ak6[i]);
+    free(w);
+}
+
+/* rkqs: src/ode_solver/ode_bs.f90:125-174. Returns 0 or DFN_ERR_UNDERFLOW.
+ * counters (attempts, rejected) may be NULL. */
+int orc_rkqs_cb(orc_derivs_fn derivs, void *ctx, int64_t *counters, double *y, const double *dydx, int64_t n,
+                double *x, double htry, double eps, const double *yscal, double *hdid, double *hnext)
+{
+    const double SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25;
+    const double ERRCON = (double)1.89e-4f; /* default-real literal in the reference */
+    double *yerr = (double *)malloc(8 * n), *ytemp = (double *)malloc(8 * n);
+    double h = htry, errmax;
+    for (;;) {
+        if (counters) counters[0]++;
+        orc_rkck_cb(derivs, ctx, y, dydx, n, *x, h, ytemp, yerr);
+        errmax = 0.0;
+        for (int64_t i = 0; i < n; i++) errmax = fmax(errmax, fabs(yerr[i] / yscal[i]));
+        errmax = errmax / eps;
+        if (errmax <= 1.0) break;
+        if (counters) counters[1]++;
+        double htemp = SAFETY * h * pow(errmax, PSHRNK);
+        h = copysign(fmax(fabs(htemp), 0.1 * fabs(h)), h);
+        double xnew = *x + h;
+        if (xnew == *x) { free(yerr); free(ytemp); return DFN_ERR_UNDERFLOW; }
+    }
+    if (errmax > ERRCON) *hnext = SAFETY * h * pow(errmax, PGROW);
+    else *hnext = 5.0 * h;
+    *hdid = h;
+    *x = *x + h;
+    for (int64_t i = 0; i < n; i++) y[i] = ytemp[i];
+    free(yerr); free(ytemp);
+    return 0;
+}
+
+int orc_rkqs(orc *o, double *y, const double *dydx, int64_t n, double *x, double htry, double eps,
+             const double *yscal, double *hdid, double *hnext)
+{
+    int64_t c[2] = {0, 0};
+    int st = orc_rkqs_cb(orc_rhs_cb, o, c, y, dydx, n, x, htry, eps, yscal, hdid, hnext);
+    o->attempts += c[0];
+    o->rejected += c[1];
+    return st;
+}
+
+/* ---------------------------------------------------------------------- */
+/* One pass of the solve() loop: src/solver.f90:59-198 (printing and file
+ * output excluded). Returns 0, or a dfn_status code. */
+int orc_solve_step(orc *o)
+{
+    int64_t N = o->N, n = 3 * N;
+    o->it_count++;
+    if (o->t_try > 10.0) {
+        for (int64_t s = 0; s < o->nsrc; s++)
+            if (o->time < o->src_tb[s] && o->time + o->t_try > o->src_tb[s]) o->t_try = 10.0;
+    }
+    double *Pt = (double *)malloc(8 * N);
+    int ier = orc_compute_P(o, o->t_try, Pt, o->Pdot);
+    int guard = 0;
+    while (ier == 1) {
+        o->t_try = o->t_try / 2.0;
+        o->halvings++;
+        ier = orc_compute_P(o, o->t_try, Pt, o->Pdot);
+        if (++guard > 2000) { free(Pt); return DFN_ERR_NOCONV; }
+    }
+    double *Ydot = (double *)malloc(8 * n), *yscal = (double *)malloc(8 * n);
+    double time_temp = 0.0;
+    orc_rhs(o, o->t_try, o->Y, Ydot);
+    for (int64_t i = 0; i < n; i++) yscal[i] = fabs(o->Y[i]) + fabs(Ydot[i] * o->t_try) + o->tol;
+    double t_did = 0, t_next = 0;
+    int st = orc_rkqs(o, o->Y, Ydot, n, &time_temp, o->t_try, o->tol, yscal, &t_did, &t_next);
+    free(Ydot); free(yscal);
+    if (st) { free(Pt); return st; }
+    o->t_try = t_next;
+    if (o->t_try > 24 * 60 * 60) o->t_try = 24 * 60 * 60;
+    ier = orc_compute_P(o, t_did, o->P, o->Pdot);
+    free(Pt);
+    o->time = o->time + t_did;
+    for (int64_t k = 0; k < N; k++)
+        if (o->Y[2 * N + k] > 0) return DFN_ERR_EXTENSIONAL;
+    for (int64_t i = 0; i < n; i++)
+        if (!isfinite(o->Y[i])) return DFN_ERR_NONFINITE;
+    return 0;
+}
+
+int orc_solve_steps(orc *o, int64_t nsteps, double *hdid_log)
+{
+    for (int64_t s = 0; s < nsteps; s++) {
+        double t0 = o->time;
+        int st = orc_solve_step(o);
+        if (hdid_log) hdid_log[s] = o->time - t0;
+        if (st) { o->last_status = st; return st; }
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Accessors */
+void orc_get_state(const orc *o, double *Y, double *P, double *scal)
+{
+    if (Y) memcpy(Y, o->Y, 8 * 3 * o->N);
+    if (P) memcpy(P, o->P, 8 * o->N);
+    if (scal) { scal[0] = o->time; scal[1] = o->t_try; scal[2] = (double)o->it_count; }
+}
+void orc_set_state(orc *o, const double *Y, const double *P, double time, double t_try, int64_t it)
+{
+    if (Y) memcpy(o->Y, Y, 8 * 3 * o->N);
+    if (P) memcpy(o->P, P, 8 * o->N);
+    o->time = time; o->t_try = t_try; o->it_count = it;
+}
+void orc_get_geometry(const orc *o, double *elem, double *ds, double *tan, double *nrm, double *permx)
+{
+    int64_t N = o->N;
+    if (elem) memcpy(elem, o->elem, 16 * N);
+    if (ds) memcpy(ds, o->ds, 8 * N);
+    if (tan) memcpy(tan, o->tan, 16 * N);
+    if (nrm) memcpy(nrm, o->nrm, 16 * N);
+    if (permx) memcpy(permx, o->permx, 8 * (N + 1));
+}
+void orc_get_loads(const orc *o, double *nload, double *sload, unsigned char *fake)
+{
+    if (nload) memcpy(nload, o->nload, 8 * o->N);
+    if (sload) memcpy(sload, o->sload, 8 * o->N);
+    if (fake) memcpy(fake, o->fake, o->N);
+}
+void orc_get_last_stress(const orc *o, double *sT, double *sN, double *Pdot)
+{
+    if (sT) memcpy(sT, o->SigmaT_dot, 8 * o->N);
+    if (sN) memcpy(sN, o->SigmaN_dot, 8 * o->N);
+    if (Pdot) memcpy(Pdot, o->Pdot, 8 * o->N);
+}
+void orc_counters(const orc *o, int64_t *c)
+{
+    c[0] = o->cg_iters; c[1] = o->rhs_evals; c[2] = o->attempts; c[3] = o->rejected; c[4] = o->halvings;
+    c[5] = o->it_count;
+}

@@ -1,0 +1,194 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU FP64 oracle.
+
+Tolerances (relative to the largest magnitude of the compared quantity):
+* K.V with FP64 storage: 1e-12 (entry rounding and summation order only)
+* K.V with FP32 storage: 2e-6; BF16 hi+lo: 5e-5
+* friction RHS: 1e-10; pressure (tridiagonal vs exact): 1e-12
+* pressure CG vs oracle CG: both stop at max|r| < tol_solver, so they agree
+  to well below 1e3 * tol_solver Pa
+* whole RK45 steps: slip rate and log-state within 1e-8 (the parity target)
+"""
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from demystification_dfn_b200 import networks
+from demystification_dfn_b200.simulation import Simulation
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    s = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / s
+
+
+def net(seed=1, n=4, mode="modeII", **kw):
+    return networks.small_network(seed=seed, n_faults=n, mode=mode, **kw)
+
+
+@pytest.mark.parametrize("mode", ["modeII", "modeIII"])
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 2e-6), ("bf16x2", 5e-5)])
+@pytest.mark.parametrize("gemv", ["tma", "ldg"])
+def test_kernel_matches_oracle(mode, storage, tol, gemv):
+    p = net(seed=2, n=5, mode=mode)
+    o = Oracle(p)
+    o.use_dense()
+    with Simulation(p, storage=storage, gemv=gemv) as s:
+        rng = np.random.default_rng(3)
+        v = 1e-9 * np.exp(rng.normal(size=s.N))
+        v[s.arrays.fake_mask] = 0.0
+        gT, gN = s.kernel(v)
+        oT, oN = o.kernel(v)
+        assert rel(gT, oT) < tol
+        if mode == "modeII":
+            assert rel(gN, oN) < tol
+
+
+def test_kernel_large_single_fault_and_linearity():
+    p = networks.single_fault(n_el=3000, length=30e3, mode="modeII")
+    o = Oracle(p, threads=8)
+    with Simulation(p) as s:
+        rng = np.random.default_rng(0)
+        v1, v2 = rng.normal(size=s.N), rng.normal(size=s.N)
+        g1, _ = s.kernel(v1)
+        g2, _ = s.kernel(v2)
+        g12, _ = s.kernel(2.0 * v1 - 3.0 * v2)
+        assert rel(g12, 2.0 * g1 - 3.0 * g2) < 1e-12
+        oT, _ = o.kernel(v1)   # matrix-free reference routine
+        assert rel(g1, oT) < 1e-11
+
+
+def test_tma_and_ldg_agree_bitwise():
+    p = net(seed=4, n=6)
+    with Simulation(p, gemv="tma") as a, Simulation(p, gemv="ldg") as b:
+        v = np.random.default_rng(1).normal(size=a.N)
+        ta, na = a.kernel(v)
+        tb, nb = b.kernel(v)
+        assert np.array_equal(ta, tb) and np.array_equal(na, nb)
+
+
+@pytest.mark.parametrize("dt", [1.0, 100.0, 5000.0])
+def test_pressure_cg_matches_oracle(dt):
+    p = networks.single_fault(n_el=300, length=3000.0, mode="modeIII", tol=1e-6)
+    o = Oracle(p)
+    with Simulation(p, pressure="cg") as s:
+        gP, gd, gi = s.compute_P(dt)
+        oP, od, oi = o.compute_P(dt)
+        assert gi == oi == 0
+        assert np.abs(gP - oP).max() < 1e3 * 1e-6
+        ex = o.pressure_exact(dt)
+        assert np.abs(gP - ex).max() < 1e3 * 1e-6
+
+
+def test_pressure_cg_nonconvergence_sets_ier():
+    p = networks.single_fault(n_el=400, length=4000.0, mode="modeIII", tol=1e-14)
+    with Simulation(p, pressure="cg") as s:
+        _, _, ier = s.compute_P(86400.0)
+        assert ier == 1
+        # the handle stays usable after ier=1
+        _, _, ier2 = s.compute_P(1e-3)
+        assert ier2 in (0, 1)
+
+
+@pytest.mark.parametrize("dt", [0.5, 300.0, 86400.0])
+def test_pressure_tridiag_is_exact(dt):
+    p = net(seed=6, n=5, mode="modeII", q_kgs=20.0)
+    o = Oracle(p)
+    with Simulation(p, pressure="tridiag") as s:
+        gP, gd, gi = s.compute_P(dt)
+        assert gi == 0
+        ex = o.pressure_exact(dt)
+        assert rel(gP, ex) < 1e-12
+
+
+@pytest.mark.parametrize("mode", ["modeII", "modeIII"])
+def test_friction_law_matches_oracle(mode):
+    p = net(seed=7, n=4, mode=mode, tol=1e-6)
+    o = Oracle(p)
+    o.use_dense()
+    with Simulation(p, pressure="cg") as s:
+        Y = s.arrays.Y0().copy()
+        rng = np.random.default_rng(2)
+        N = s.N
+        Y[:N] *= np.exp(rng.normal(0, 0.3, N))
+        Y[:N][s.arrays.fake_mask] = 0
+        for x in (0.0, 10.0, 1000.0):
+            g = s.friction_law(x, Y)
+            r = o.friction_law(x, Y)
+            for j in range(3):
+                assert rel(g[j * N:(j + 1) * N], r[j * N:(j + 1) * N]) < 1e-9, (x, j)
+
+
+def test_rkqs_matches_oracle():
+    p = net(seed=8, n=4, tol=1e-6)
+    o = Oracle(p)
+    o.use_dense()
+    with Simulation(p, pressure="cg") as s:
+        Y = s.arrays.Y0()
+        ht = 50.0
+        dydx = o.friction_law(ht, Y)
+        yscal = np.abs(Y) + np.abs(dydx * ht) + 1e-6
+        gy, gx, ghd, ghn = s.rkqs(Y, dydx, 0.0, ht, 1e-6, yscal)
+        oy, ox, ohd, ohn = o.rkqs(Y, dydx, 0.0, ht, 1e-6, yscal)
+        assert np.isclose(ghd, ohd, rtol=1e-12) and np.isclose(ghn, ohn, rtol=1e-9)
+        assert rel(gy, oy) < 1e-10
+
+
+@pytest.mark.parametrize("pressure", ["cg", "tridiag"])
+def test_solve_steps_match_oracle(pressure):
+    p = net(seed=9, n=4, tol=1e-6)
+    o = Oracle(p)
+    o.use_dense()
+    with Simulation(p, pressure=pressure) as s:
+        nsteps = 25
+        rep = s.solve_steps(nsteps)
+        st, log = o.solve_steps(nsteps)
+        assert st == 0 and rep["status"] == 0
+        g, r = s.state(), o.state()
+        assert g["it_count"] == r["it_count"] == nsteps
+        assert abs(g["time"] - r["time"]) <= 1e-8 * r["time"]
+        N = s.N
+        for j in range(3):
+            assert rel(g["Y"][j * N:(j + 1) * N], r["Y"][j * N:(j + 1) * N]) < 1e-8, j
+        assert rel(g["P"], r["P"]) < 1e-8
+
+
+def test_single_fault_injection_run_matches_oracle():
+    p = networks.single_fault(n_el=500, length=5000.0, mode="modeII", tol=1e-6)
+    o = Oracle(p, threads=8)
+    o.use_dense()
+    with Simulation(p, pressure="cg") as s:
+        rep = s.solve_steps(30)
+        st, _ = o.solve_steps(30)
+        g, r = s.state(), o.state()
+        assert st == 0 and rep["status"] == 0
+        assert abs(g["time"] - r["time"]) <= 1e-8 * r["time"]
+        N = s.N
+        assert rel(g["Y"][:N], r["Y"][:N]) < 1e-8
+        assert rel(g["Y"][N:2 * N], r["Y"][N:2 * N]) < 1e-8
+        assert rel(g["P"], r["P"]) < 1e-8
+
+
+def test_snapshot_and_step_host():
+    p = net(seed=10, n=3, tol=1e-6)
+    with Simulation(p) as s:
+        s.solve_steps(3)
+        snap = s.snapshot()
+        st = s.state()
+        N = s.N
+        assert np.array_equal(snap["V"], st["Y"][:N])
+        a = s.arrays
+        assert np.allclose(snap["theta"], a.Dc / a.V0 * np.exp(st["Y"][N:2 * N]), rtol=1e-14)
+        assert np.array_equal(snap["tractionNel"], st["Y"][2 * N:])
+        assert snap["time"] == st["time"]
+
+
+def test_fp32_storage_run_close_to_fp64():
+    p = net(seed=11, n=5, tol=1e-6)
+    with Simulation(p, storage="fp64", pressure="tridiag") as a, Simulation(p, storage="fp32", pressure="tridiag") as b:
+        a.solve_steps(20)
+        b.solve_steps(20)
+        ga, gb = a.state(), b.state()
+        N = a.N
+        assert rel(gb["Y"][:N], ga["Y"][:N]) < 1e-4

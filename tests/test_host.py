@@ -1,0 +1,103 @@
+"""CPU tests of the host layer and of the C ABI library (no GPU calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from demystification_dfn_b200 import networks, build_arrays, DemystiFicatioN
+from demystification_dfn_b200.layout import DfnOptions, DfnProblem, DfnReport
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_layout_fake_elements_and_nodes():
+    p = networks.small_network(seed=0, n_faults=3)
+    a = build_arrays(p)
+    n = [f.nb_element for f in p.faults]
+    assert a.N == sum(n) + 2
+    first = a.fault_first
+    assert list(first) == [0, n[0] + 1, n[0] + n[1] + 2]
+    fk = a.fake_mask
+    assert list(np.where(fk)[0]) == [n[0], n[0] + n[1] + 1]
+    # fake elements carry the reader's presets and zero state
+    assert np.all(a.a[fk] == 1) and np.all(a.V0[fk] == 1) and np.all(a.V[fk] == 0)
+    assert np.all(a.permeability[fk] == 0)
+    # nodes: fault f occupies node rows first_f .. first_f + n_f
+    for f, s in zip(p.faults, first):
+        assert np.array_equal(a.node[s:s + f.nb_element + 1], f.node.T)
+
+
+def test_sources_are_one_based():
+    p = networks.single_fault(n_el=100, length=1000.0)
+    a = build_arrays(p)
+    assert a.src_fault.tolist() == [1]
+    assert 1 <= a.src_index[0] <= 100
+    assert np.isclose(a.src_Q[0], 1.25e-6 * 50 / 50)
+
+
+def test_network_is_seeded_and_gapped():
+    p1 = networks.fault_network(n_faults=40, box=2000.0, seed=7)
+    p2 = networks.fault_network(n_faults=40, box=2000.0, seed=7)
+    assert all(np.array_equal(f.node, g.node) for f, g in zip(p1.faults, p2.faults))
+    segs = np.array([[f.node[0, 0], f.node[1, 0], f.node[0, -1], f.node[1, -1]] for f in p1.faults])
+    d = networks._seg_dist(segs[0, :2][None], segs[0, 2:][None], segs[1:, :2], segs[1:, 2:])
+    assert d.min() >= 10.0
+
+
+def test_problem_setters_reallocate():
+    p = DemystiFicatioN(2)
+    p.faults[0].nb_element = 7
+    assert p.faults[0].a.shape == (7,) and p.faults[0].node.shape == (2, 8)
+    p.faults[0].nb_source = 2
+    assert p.faults[0].Q.shape == (2,) and p.faults[0].index_injection.dtype == np.int64
+    with pytest.raises(ValueError):
+        p.faults[0].nb_element = 0
+
+
+def _header_functions():
+    txt = open(os.path.join(ROOT, "include", "dfn_b200.h")).read()
+    return sorted(set(re.findall(r"\b(dfn_[a-z_]+)\s*\(", txt)) - {"dfn_status"})
+
+
+def test_library_exports_every_header_symbol(lib):
+    from demystification_dfn_b200.build import LIB
+
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (dfn_\w+)", out))
+    missing = [f for f in _header_functions() if f not in exported]
+    assert not missing, missing
+
+
+def test_struct_layouts_match(lib):
+    assert lib.dfn_problem_struct_size() == ctypes.sizeof(DfnProblem)
+    assert lib.dfn_options_struct_size() == ctypes.sizeof(DfnOptions)
+    assert lib.dfn_report_struct_size() == ctypes.sizeof(DfnReport)
+    assert lib.dfn_abi_version() == 1
+    assert lib.dfn_status_string(1).startswith(b"pressure CG")
+
+
+def test_create_fails_loudly_without_gpu(lib):
+    from conftest import gpu_available
+
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from demystification_dfn_b200.simulation import Simulation
+    from demystification_dfn_b200._lib import DfnError
+
+    with pytest.raises(DfnError) as e:
+        Simulation(networks.small_network(seed=0, n_faults=2))
+    assert e.value.status == 6
+
+
+def test_create_rejects_bad_problem(lib):
+    from demystification_dfn_b200.layout import to_c
+
+    a = build_arrays(networks.small_network(seed=0, n_faults=2))
+    c = to_c(a)
+    c.nb_element = a.N + 1       # inconsistent with the fault sizes
+    h = ctypes.c_void_p()
+    assert lib.dfn_create(ctypes.byref(c), None, ctypes.byref(h)) == 5
+    assert b"nb_element" in lib.dfn_last_error()

@@ -1,0 +1,173 @@
+"""CPU checks of the FP64 oracle against known answers (parity unpinned:
+the reference ships no golden outputs, so the restatement is pinned by the
+mathematics of each routine)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import Oracle, load
+from demystification_dfn_b200 import networks
+from demystification_dfn_b200.layout import ptr
+
+
+def straight(n=64, mode="modeIII", **kw):
+    kw.setdefault("q_kgs", 50.0)
+    return networks.single_fault(n_el=n, length=10.0 * n, mode=mode, **kw)
+
+
+def test_geometry_straight_fault():
+    o = Oracle(straight(32))
+    g = o.geometry()
+    assert np.allclose(g["ds"], 10.0, rtol=0, atol=1e-12)
+    assert np.allclose(g["tangent"], [1.0, 0.0])
+    assert np.allclose(g["normal"], [0.0, 1.0])
+    # harmonic mean of equal permeabilities, zero at the two ends
+    px = g["permeability_x"]
+    assert px[0] == 0 and px[-1] == 0 and np.allclose(px[1:-1], 1e-13, rtol=1e-15)
+
+
+def test_mode3_uniform_slip_telescopes_to_tips():
+    # directModeIII.f:59-65: with uniform slip only the two tip nodes remain
+    n = 50
+    o = Oracle(straight(n))
+    a = o.arrays
+    sT, _ = o.kernel(np.ones(a.N))
+    g = o.geometry()
+    el = g["element"]
+    x0, x1 = a.node[0, 0], a.node[-1, 0]
+    mu = a.mu
+    # I(node) = t.(e-node)/r^2 = 1/(e_x - node_x) on the x axis
+    expect = mu / (2 * np.pi) * (-1.0 / (el[:, 0] - x0) + 1.0 / (el[:, 0] - x1))
+    assert np.allclose(sT, expect, rtol=1e-12, atol=1e-6)
+
+
+@pytest.mark.parametrize("mode", ["modeII", "modeIII"])
+def test_direct_equals_dense(mode):
+    p = networks.small_network(seed=3, n_faults=3, mode=mode)
+    o = Oracle(p)
+    rng = np.random.default_rng(0)
+    v = rng.normal(size=o.N) * 1e-9
+    v[o.arrays.fake_mask] = 0.0
+    d_T, d_N = o.kernel(v)
+    o.use_dense()
+    k_T, k_N = o.kernel(v)
+    scale = np.abs(d_T).max()
+    if mode == "modeII":
+        # identical pair terms in identical order: bitwise equal
+        assert np.array_equal(d_T, k_T) and np.array_equal(d_N, k_N)
+    else:
+        # directIII sums node differences, the entries element differences
+        assert np.allclose(d_T, k_T, rtol=0, atol=1e-11 * scale)
+
+
+def test_entries_match_dense_matrix():
+    p = networks.small_network(seed=5, n_faults=2)
+    o = Oracle(p)
+    KT, KN = o.dense()
+    for (k, l) in [(0, 0), (3, 7), (o.N - 1, 2)]:
+        assert KT[k, l] == o.entry(k, l, 1)
+        assert KN[k, l] == o.entry(k, l, 2)
+
+
+def test_steady_state_has_no_state_rate():
+    o = Oracle(straight(40, q_kgs=0.0))
+    Y = o.arrays.Y0()
+    Yd = o.friction_law(10.0, Y)
+    N = o.N
+    # psi = ln(V0/V): dpsi/dt = V0/Dc e^-psi - V/Dc = 0
+    assert np.abs(Yd[N:2 * N]).max() < 1e-20
+    # uniform V on a straight fault with no pressure: no normal stress rate
+    assert np.abs(Yd[2 * N:]).max() == 0.0
+
+
+def test_fake_elements_have_zero_derivatives():
+    o = Oracle(networks.small_network(seed=2, n_faults=4))
+    Yd = o.friction_law(5.0, o.arrays.Y0())
+    fk = o.arrays.fake_mask
+    N = o.N
+    assert fk.sum() == 3
+    for j in range(3):
+        assert np.all(Yd[j * N:(j + 1) * N][fk] == 0.0)
+
+
+def test_cg_matches_exact_and_conserves_mass():
+    p = straight(200, q_kgs=50.0)
+    p.hyperparameter.tol_solver = 1e-6
+    o = Oracle(p)
+    a = o.arrays
+    for dt in (10.0, 1000.0, 20000.0):
+        Pt, Pd, ier = o.compute_P(dt)
+        assert ier == 0
+        ex = o.pressure_exact(dt)
+        assert np.abs(Pt - ex).max() < 1e-3
+        # implicit Euler with no-flux ends conserves the injected volume
+        injected = dt * a.src_Q[0] / (a.porosity * (a.fluid_comp + a.rock_comp)) / 10.0
+        assert abs(ex.sum() - a.P.sum() - injected) < 1e-9 * injected
+        assert np.allclose(Pd, (Pt - a.P) / dt)
+
+
+def test_cg_iteration_cap_reports_ier():
+    p = straight(400, q_kgs=50.0)
+    p.hyperparameter.tol_solver = 1e-14      # unreachable: max|r| < 1e-14 Pa
+    o = Oracle(p)
+    Pt, Pd, ier = o.compute_P(86400.0)
+    assert ier == 1
+    assert np.all(Pt == 0)                  # outputs untouched, as in the reference
+
+
+CB = ctypes.CFUNCTYPE(None, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+
+
+def _rkqs_generic(f, y0, x_end, eps=1e-8, h0=0.1):
+    lib = load()
+    fn = lib.orc_rkqs_cb
+    fn.restype = ctypes.c_int
+    dp = ctypes.POINTER(ctypes.c_double)
+    fn.argtypes = [CB, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), dp, dp, ctypes.c_int64, dp,
+                   ctypes.c_double, ctypes.c_double, dp, dp, dp]
+
+    def derivs(x, n, y, dy, ctx):
+        yy = np.ctypeslib.as_array(y, shape=(n,))
+        out = f(x, yy)
+        for i in range(n):
+            dy[i] = out[i]
+
+    cb = CB(derivs)
+    y = np.array(y0, dtype=float)
+    x, h, steps = 0.0, h0, 0
+    cnt = (ctypes.c_int64 * 2)()
+    while x < x_end - 1e-12:
+        h = min(h, x_end - x)
+        dydx = np.array(f(x, y))
+        yscal = np.abs(y) + np.abs(dydx * h) + 1e-30
+        xx, hd, hn = ctypes.c_double(x), ctypes.c_double(), ctypes.c_double()
+        assert fn(cb, None, cnt, ptr(y), ptr(dydx), y.size, ctypes.byref(xx), h, eps, ptr(yscal),
+                  ctypes.byref(hd), ctypes.byref(hn)) == 0
+        x, h = xx.value, hn.value
+        steps += 1
+    return y, steps
+
+
+def test_rkqs_exponential_decay():
+    y, steps = _rkqs_generic(lambda x, y: -y, [1.0], 5.0)
+    assert abs(y[0] - np.exp(-5.0)) < 1e-9 and steps < 200
+
+
+def test_rkqs_cosine():
+    y, _ = _rkqs_generic(lambda x, y: [np.cos(x)], [0.0], 3.0)
+    assert abs(y[0] - np.sin(3.0)) < 1e-8
+
+
+def test_solve_loop_policies():
+    p = straight(80, q_kgs=50.0, tol=1e-6)
+    p.faults[0].t_injection_beg[:] = 5000.0   # clamp to 10 s before the injection starts
+    o = Oracle(p)
+    st, log = o.solve_steps(12)
+    assert st == 0
+    s = o.state()
+    assert s["it_count"] == 12
+    assert np.isclose(s["time"], log.sum(), rtol=1e-12)
+    assert log.max() <= 86400.0
+    assert o.counters()["rhs_evals"] >= 6 * 12
