@@ -169,7 +169,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--storage", default="fp64", choices=["fp64", "fp32", "bf16x2"])
@@ -233,6 +233,7 @@ def main():
     kv_ms, kv_n = sim.profile_kv_read()
     sim.profile_kv(False)
     clk = clocks.stop()
+    st_ref = sim.state()        # FP64 state after the timed steps, for the mixed-precision check
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -280,11 +281,15 @@ def main():
             a1.record(stream)
             torch.cuda.synchronize()
             st2 = s2.state()
-            ref = sim.state()
+            Vr, V2 = st_ref["Y"][:N], st2["Y"][:N]
+            pr, p2 = st_ref["Y"][N:2 * N], st2["Y"][N:2 * N]
             extras[store] = {"steps_per_s": args.steps / (a0.elapsed_time(a1) / 1e3),
                              "kv_bytes": s2.kernel_bytes,
                              "kv_ms": s2.time_kernel(10),
-                             "time_after_steps": st2["time"], "time_after_steps_fp64": ref["time"]}
+                             "rel_err_V_vs_fp64": float(np.abs(V2 - Vr).max() / np.abs(Vr).max()),
+                             "rel_err_psi_vs_fp64": float(np.abs(p2 - pr).max() / np.abs(pr).max()),
+                             "rel_err_time_vs_fp64": abs(st2["time"] - st_ref["time"]) / st_ref["time"],
+                             "compared_after": f"{args.warmup}+{args.steps} accepted steps from the same start"}
             s2.close()
 
     if rank == 0:
