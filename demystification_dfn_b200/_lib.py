@@ -72,6 +72,8 @@ def load():
         "dfn_launch_count": (i64, [P]),
         "dfn_profile_kv": (i32, [P, i32]),
         "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
+        "dfn_compute_P_noalloc": (i32, [i64, dbl, dbl, P, P, P, dbl, dbl, dbl, dbl, dbl, i64, P, P, P, P, P, P,
+                                        P, ctypes.POINTER(i32), P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

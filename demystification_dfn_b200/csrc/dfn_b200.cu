@@ -8,6 +8,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -717,6 +718,100 @@ int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, dou
     TRY(dfn_get_snapshot(h, V_out, theta_out, P_out, tT_out, tN_out, nullptr, nullptr));
     fill_report(h, rep);
     return h->h_ctl->status;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free pressure step. The CG work vectors of dfn_compute_P_noalloc
+// live in this fixed device array: the first 32 doubles (256 bytes) hold the
+// step controller the CG kernel reports into, then 4 vectors of
+// DFN_NOALLOC_MAX_ELEMENTS doubles (x, r, p, M.p). In host code the symbol is
+// only a handle for cudaGetSymbolAddress, never a device address.
+static const int64_t kNoAllocCtlDoubles = 32;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocCtlDoubles + 4 * (int64_t)DFN_NOALLOC_MAX_ELEMENTS];
+static_assert(sizeof(StepCtl) <= kNoAllocCtlDoubles * sizeof(double), "controller does not fit the scratch header");
+
+static const int kNoAllocMaxDevices = 128;
+static double *g_noalloc_addr[kNoAllocMaxDevices];  // device address per device ordinal, set once
+static std::mutex g_noalloc_mu;
+
+// Device address of the scratch array on the current device, looked up
+// once per device with that device current.
+static int noalloc_scratch(double **out)
+{
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        g_err = "device ordinal out of range for the allocation-free scratch table";
+        return DFN_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_err("cudaGetSymbolAddress(g_noalloc_scratch)", e, __FILE__, __LINE__);
+            return DFN_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return DFN_OK;
+}
+
+// Clears the shared controller (status, counters) and sets time and tol:
+// the array keeps the previous call's contents.
+static __global__ void noalloc_reset_kernel(StepCtl *ctl, double time, double tol)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    StepCtl c;
+    memset(&c, 0, sizeof(c));
+    c.time = time;
+    c.eps = tol;
+    *ctl = c;
+}
+
+extern "C" {
+
+int32_t dfn_compute_P_noalloc(int64_t N, double dt, double time, const double *d_P, const double *d_permx,
+                              const double *d_ds, double porosity, double dyn_viscosity, double fluid_comp,
+                              double rock_comp, double tol_solver, int64_t nsrc, const int64_t *d_src_fault,
+                              const int64_t *d_src_elem, const double *d_src_Q, const double *d_src_tb,
+                              const double *d_src_te, double *d_P_temp, double *d_P_dot, int32_t *ier,
+                              void *stream)
+{
+    if (N > DFN_NOALLOC_MAX_ELEMENTS) {
+        g_err = "nb_element exceeds DFN_NOALLOC_MAX_ELEMENTS (65536) of the allocation-free pressure step";
+        return DFN_ERR_ARG;
+    }
+    if (N < 2 || !d_P || !d_permx || !d_ds || !d_P_temp || !d_P_dot || !ier || !(tol_solver > 0) ||
+        nsrc < 0 || (nsrc > 0 && (!d_src_fault || !d_src_elem || !d_src_Q || !d_src_tb || !d_src_te))) {
+        g_err = "dfn_compute_P_noalloc: invalid argument";
+        return DFN_ERR_ARG;
+    }
+    double *scratch = nullptr;
+    TRY(noalloc_scratch(&scratch));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    StepCtl *ctl = reinterpret_cast<StepCtl *>(scratch);
+    double *work = scratch + kNoAllocCtlDoubles;
+
+    PressParams pp{};
+    pp.N = N; pp.P = d_P; pp.permx = d_permx; pp.ds = d_ds;
+    pp.porosity = porosity; pp.dyn_visc = dyn_viscosity; pp.comp = fluid_comp + rock_comp;
+    pp.tol = tol_solver; pp.nsrc = nsrc; pp.src_fault = d_src_fault; pp.src_elem = d_src_elem;
+    pp.src_Q = d_src_Q; pp.src_tb = d_src_tb; pp.src_te = d_src_te; pp.ctl_time = &ctl->time;
+
+    noalloc_reset_kernel<<<1, 32, 0, s>>>(ctl, time, tol_solver);
+    CKL();
+    pressure_cg_kernel<<<1, 1024, 0, s>>>(pp, ctl, 2, 0, dt, d_P_temp, d_P_dot, work);
+    CKL();
+    StepCtl c;
+    CK(cudaMemcpyAsync(&c, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *ier = (c.status == 1) ? 1 : 0;
+    if (c.status != 0 && c.status != 1) return c.status;
+    return DFN_OK;
 }
 
 int32_t dfn_profile_kv(dfn_handle *h, int32_t enable)

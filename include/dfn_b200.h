@@ -177,6 +177,41 @@ int32_t dfn_get_snapshot(dfn_handle *h, double *V, double *theta, double *P, dou
 int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_stressT,
                           double *d_stressN);
 
+/* ---- allocation-free pressure step ------------------------------------ */
+/* No counterpart in the reference: an extra entry point of this library.
+ *
+ * The same implicit pressure step as dfn_compute_P (the reference's CG, with
+ * its 200-iteration cap), for callers that must not allocate device memory:
+ * host programs that give all device memory to their own pool allocator at
+ * start-up (so a cudaMalloc would fail or fight the pool), and time-stepping
+ * loops that cannot afford the device-wide synchronisation cudaMalloc and
+ * cudaFree may cause. It needs no handle and allocates nothing; the caller
+ * passes every input and output as device pointers.
+ *
+ * Its CG work vectors live in one fixed device array inside this library,
+ * sized for DFN_NOALLOC_MAX_ELEMENTS elements (about 2 MiB); every GPU that
+ * loads the library holds that array until the process exits. Larger
+ * problems are rejected with DFN_ERR_ARG. Work runs on the calling thread's
+ * current device and on `stream` (NULL = legacy default stream); the call
+ * returns after the step has finished. The first call on a device looks up
+ * the array's device address once for that device; make that first call
+ * before any stream capture. All calls share the one array, so calls that
+ * overlap on the GPU (other threads or streams) race; serialise them.
+ *
+ * Inputs: d_P (committed pressure), d_permeability_x (N+1 face values as
+ * built by the reference, src/initialisation.f90:252-269), d_ds (element
+ * lengths), the fluid constants, tol_solver, and the sources (fault id
+ * 1-based, element index 0-based into the concatenated element arrays).
+ * Outputs: d_P_temp, d_P_dot; *ier = 1 when CG hits its iteration cap, in
+ * which case the outputs are left untouched, as in the reference. */
+#define DFN_NOALLOC_MAX_ELEMENTS 65536
+int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const double *d_P,
+                              const double *d_permeability_x, const double *d_ds, double porosity,
+                              double dyn_viscosity, double fluid_comp, double rock_comp, double tol_solver,
+                              int64_t nb_source, const int64_t *d_src_fault, const int64_t *d_src_element,
+                              const double *d_src_Q, const double *d_src_t_beg, const double *d_src_t_end,
+                              double *d_P_temp, double *d_P_dot, int32_t *ier, void *stream);
+
 /* ---- timing helpers (CUDA events on the handle's stream) --------------- */
 /* Times `reps` K.V launches of the handle's storage on its stream and
  * returns the mean duration of one launch in milliseconds. */

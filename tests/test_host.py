@@ -59,7 +59,7 @@ def test_problem_setters_reallocate():
 
 def _header_functions():
     txt = open(os.path.join(ROOT, "include", "dfn_b200.h")).read()
-    return sorted(set(re.findall(r"\b(dfn_[a-z_]+)\s*\(", txt)) - {"dfn_status"})
+    return sorted(set(re.findall(r"\b(dfn_[A-Za-z0-9_]+)\s*\(", txt)) - {"dfn_status"})
 
 
 def test_library_exports_every_header_symbol(lib):
