@@ -177,6 +177,8 @@ def main():
     ap.add_argument("--gemv", default="tma", choices=["tma", "ldg"])
     ap.add_argument("--n-faults", type=int, default=None, help="smaller network (profiling only)")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
+    ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -292,6 +294,53 @@ def main():
                              "compared_after": f"{args.warmup}+{args.steps} accepted steps from the same start"}
             s2.close()
 
+    if rank == 0 and args.ensemble > 0 and not args.no_extras:
+        # batched ensemble: many networks of uneven size in one handle, one
+        # launch per kernel for the whole batch, per-network step control
+        from demystification_dfn_b200 import networks
+        from demystification_dfn_b200.ensemble import Ensemble
+
+        members = networks.ensemble(args.ensemble)
+        hbm, _ = peaks()
+        ens_out = {"networks": len(members), "steps_per_network": args.ensemble_steps}
+        for store in ("fp64", "fp32", "bf16x2"):
+            ens = Ensemble(members, storage=store, pressure=args.pressure, device=local, gemv=args.gemv)
+            ens.set_stream(stream.cuda_stream)
+            ens.solve(n_steps=3)
+            torch.cuda.synchronize()
+            ens.profile_kv(True)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            reps = ens.solve(n_steps=args.ensemble_steps, check=False)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            kms, kn = ens.profile_kv_read()
+            ms_e = a0.elapsed_time(a1)
+            done = sum(1 for r in reps if r["status"] == 0)
+            kavg = kms / max(kn, 1)
+            gbs = ens.kernel_bytes / (kavg / 1e3) / 1e9
+            ens_out[store] = {"steps_per_s": len(members) * args.ensemble_steps / (ms_e / 1e3),
+                              "ms_per_round_avg": ms_e / max(kn // 6, 1), "networks_ok": done,
+                              "elements_total": int(sum(ens.n_elements)), "kv_bytes": ens.kernel_bytes,
+                              "kv_avg_ms": kavg, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
+                              "rejected": int(sum(r["rejected"] for r in reps)),
+                              "probe_halvings": int(sum(r["probe_halvings"] for r in reps)),
+                              "stage_cg_failures": int(sum(r["stage_cg_failures"] for r in reps)),
+                              "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
+                                                for s in sorted({r["status"] for r in reps})}}
+            if store == "fp64":
+                ref_states = [ens.state(i) for i in range(len(members))]
+            else:
+                err = 0.0
+                for i in range(len(members)):
+                    s_i = ens.state(i)
+                    n_i = len(s_i["P"])
+                    v_ref = ref_states[i]["Y"][:n_i]
+                    err = max(err, float(np.abs(s_i["Y"][:n_i] - v_ref).max() / np.abs(v_ref).max()))
+                ens_out[store]["max_rel_err_V_vs_fp64"] = err
+            ens.close()
+        extras["ensemble"] = ens_out
+
     if rank == 0:
         hbm, src = peaks()
         kv_avg = kv_ms / max(kv_n, 1)
@@ -322,7 +371,8 @@ def main():
                     "d2h_bytes_per_step": 8 * 5 * N},
             "gpu_launches": launches,
             "clocks": clk,
-            "report": {k: rep[k] for k in ("attempts", "rejected", "rhs_evals", "cg_iterations", "time")},
+            "report": {k: rep[k] for k in ("attempts", "rejected", "rhs_evals", "cg_iterations", "probe_halvings",
+                                           "time")},
         }
         if extras:
             line["mixed_precision"] = extras

@@ -72,7 +72,11 @@ def load():
         "dfn_launch_count": (i64, [P]),
         "dfn_profile_kv": (i32, [P, i32]),
         "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
-        "dfn_compute_P_noalloc": (i32, [i64, dbl, dbl, P, P, P, dbl, dbl, dbl, dbl, dbl, i64, P, P, P, P, P, P,
+        "dfn_create_batch": (i32, [ctypes.POINTER(DfnProblem), i32, ctypes.POINTER(DfnOptions), ctypes.POINTER(P)]),
+        "dfn_batch_size": (i32, [P]),
+        "dfn_solve_batch": (i32, [P, i64, dbl, ctypes.POINTER(DfnReport)]),
+        "dfn_get_state_instance": (i32, [P, i32, dp, dp, dp, dp, ctypes.POINTER(i64)]),
+        "dfn_compute_P_noalloc":(i32, [i64, dbl, dbl, P, P, P, dbl, dbl, dbl, dbl, dbl, i64, P, P, P, P, P, P,
                                         P, ctypes.POINTER(i32), P]),
     }
     for name, (res, args) in sig.items():

@@ -3,9 +3,17 @@
 // stream and moves caller buffers; every arithmetic step of the hot path runs
 // on the GPU. There is no CPU fallback: without a usable CUDA device,
 // dfn_create fails with DFN_ERR_CUDA.
+//
+// A handle holds a batch of independent networks (a single network is a
+// batch of one). Each "round" gives every active network one RK attempt:
+// networks starting a step do the probe and the scaling RHS first, networks
+// whose last attempt was rejected retry with their new step. Every kernel is
+// predicated on the network's phase, so the host launches rounds back to back
+// and reads the controllers only between groups of rounds.
 #include "../../include/dfn_b200.h"
 #include "dfn_device.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -41,6 +49,12 @@ void set_err(const char *what, cudaError_t e, const char *file, int line)
         }                                                                                           \
     } while (0)
 
+#define TRY(x)                       \
+    do {                             \
+        int s_ = (x);                \
+        if (s_ != DFN_OK) return s_; \
+    } while (0)
+
 int bytes_per_col(int mode, int store)
 {
     if (mode == DFN_MODE_II) return store == DFN_STORE_FP64 ? 16 : 8;
@@ -53,19 +67,25 @@ struct dfn_handle {
     int dev = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    int64_t N = 0, F = 0, Np = 0;
+    int B = 1;                    // networks in the batch
     int mode = 2, store = 0, pressure = 0, gemv_impl = 0, max_attempts = 64;
-    int nchunk = 0;
-    double tol = 0, prefT = 0, mu_2cs = 0;
-    int64_t nsrc = 0, nseg = 0;
-    // geometry and parameters
+    int64_t Ntot = 0;             // elements of all networks
+    std::vector<Inst> hinst;      // host copy of the instance table
+    Inst *inst = nullptr;
+    int *inst_of = nullptr;
+    int4 *tiles = nullptr;
+    int64_t ntiles = 0, ntiles0 = 0;      // all tiles / tiles of network 0
+    int64_t *seg_start = nullptr;
+    int *seg_inst = nullptr;
+    int64_t nseg = 0, nseg0 = 0;
+    int64_t nsrc_tot = 0, part_tot = 0;
+    // geometry and parameters (concatenated)
     double *node = nullptr, *elem = nullptr, *ds = nullptr, *tan = nullptr, *nrm = nullptr, *permx = nullptr;
     double *a = nullptr, *b = nullptr, *Dc = nullptr, *f0 = nullptr, *V0 = nullptr, *nload = nullptr,
            *sload = nullptr, *perm = nullptr;
     unsigned char *fake = nullptr;
-    int64_t *src_fault = nullptr, *src_elem = nullptr, *seg_start = nullptr;
+    int64_t *src_fault = nullptr, *src_elem = nullptr;
     double *src_Q = nullptr, *src_tb = nullptr, *src_te = nullptr;
-    std::vector<double> h_src_tb;
     // state and work
     double *Y = nullptr, *P = nullptr, *Pdot = nullptr, *yout = nullptr, *yscal = nullptr, *ytmp = nullptr;
     double *kbuf = nullptr, *SigT = nullptr, *SigN = nullptr, *partT = nullptr, *partN = nullptr;
@@ -73,11 +93,12 @@ struct dfn_handle {
     int *err_flag = nullptr;
     void *K = nullptr;
     size_t K_bytes = 0;
+    int64_t kv_bytes = 0;         // algorithmic bytes of one K.V over the batch
     StepCtl *ctl = nullptr;
-    StepCtl *h_ctl = nullptr;  // pinned mirror
+    StepCtl *h_ctl = nullptr;     // pinned mirror, B entries
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
-    PressParams pp{};
+    PressGlobal pg{};
     // K.V launch timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -89,8 +110,10 @@ static const int kProfMax = 16384;
 // ---------------------------------------------------------------------------
 // launch helpers
 
-typedef void (*gemv_fn)(int64_t, int64_t, const uint4 *, const double *, double *, double *);
-typedef void (*gemv_tma_fn)(int64_t, int64_t, const uint4 *, const double *, double *, double *, int *);
+typedef void (*gemv_fn)(const int4 *, const Inst *, const StepCtl *, int, const uint4 *, const double *, int,
+                        double *, double *);
+typedef void (*gemv_tma_fn)(const int4 *, const Inst *, const StepCtl *, int, const uint4 *, const double *, int,
+                            double *, double *, int *);
 
 static gemv_fn pick_gemv(int mode, int store)
 {
@@ -117,18 +140,21 @@ static gemv_tma_fn pick_gemv_tma(int mode, int store)
 
 static const size_t kTmaSmem = TMA_STAGES * GEMV_CHUNK_BYTES + 2 * TMA_STAGES * sizeof(uint64_t);
 
-static int launch_gemv(dfn_handle *h, const double *Vin)
+// K.V over the first `ntiles` tiles (all networks, or network 0 only);
+// V of network i is Vbase[vmul*eoff_i + l].
+static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, int64_t ntiles)
 {
     const bool rec = h->prof && h->pcount < kProfMax;
     if (rec) CK(cudaEventRecord(h->pev[2 * h->pcount], h->stream));
-    dim3 grid((unsigned)h->nchunk, (unsigned)((h->N + GEMV_ROWS - 1) / GEMV_ROWS));
+    const uint4 *K = static_cast<const uint4 *>(h->K);
     if (h->gemv_impl == 0) {
         gemv_tma_fn fn = pick_gemv_tma(h->mode, h->store);
-        fn<<<grid, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(h->N, h->Np, (const uint4 *)h->K, Vin, h->partT,
-                                                                     h->partN, h->err_flag);
+        fn<<<(unsigned)ntiles, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(
+            h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul, h->partT, h->partN, h->err_flag);
     } else {
         gemv_fn fn = pick_gemv(h->mode, h->store);
-        fn<<<grid, GEMV_WARPS * 32, 0, h->stream>>>(h->N, h->Np, (const uint4 *)h->K, Vin, h->partT, h->partN);
+        fn<<<(unsigned)ntiles, GEMV_WARPS * 32, 0, h->stream>>>(h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul,
+                                                                h->partT, h->partN);
     }
     h->launches++;
     CKL();
@@ -139,61 +165,94 @@ static int launch_gemv(dfn_handle *h, const double *Vin)
     return DFN_OK;
 }
 
-static int launch_pressure(dfn_handle *h, int kind, int sys0, int nsys, double dt_explicit)
+// Pressure systems sys0..sys0+nsys-1 of the first `ninst` networks.
+static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys, double dt_explicit, int ninst)
 {
-    if (h->pressure == DFN_PRESSURE_CG) {
-        pressure_cg_kernel<<<nsys, 1024, 0, h->stream>>>(h->pp, h->ctl, kind, sys0, dt_explicit, h->Ptemp, h->Pdot_s,
-                                                         h->pwork);
+    if (h->pressure != DFN_PRESSURE_TRIDIAG) {
+        dim3 grid((unsigned)nsys, (unsigned)ninst);
+        pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
+                                                               h->Ptemp, h->Pdot_s, h->pwork,
+                                                               h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0);
     } else {
-        dim3 grid((unsigned)((h->nseg + 127) / 128), (unsigned)nsys);
-        pressure_tridiag_kernel<<<grid, 128, 0, h->stream>>>(h->pp, h->ctl, kind, sys0, dt_explicit, h->seg_start,
-                                                             h->nseg, h->Ptemp, h->Pdot_s, h->pwork);
+        const int64_t nseg = (ninst == h->B) ? h->nseg : h->nseg0;
+        dim3 grid((unsigned)((nseg + 127) / 128), (unsigned)nsys);
+        pressure_tridiag_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
+                                                             h->seg_start, h->seg_inst, nseg, h->Ptemp, h->Pdot_s,
+                                                             h->pwork);
     }
     h->launches++;
     CKL();
     return DFN_OK;
 }
 
-static FricParams fric_params(dfn_handle *h, int sys, double *yin_tmp)
+static FricParams fric_params(dfn_handle *h, int64_t nelem)
 {
     FricParams f;
-    f.N = h->N; f.mode = h->mode; f.nchunk = h->nchunk; f.prefT = h->prefT; f.mu_2cs = h->mu_2cs;
+    f.Ntot = nelem; f.mode = h->mode; f.inst = h->inst; f.inst_of = h->inst_of;
     f.a = h->a; f.b = h->b; f.Dc = h->Dc; f.f0 = h->f0; f.V0 = h->V0; f.nload = h->nload; f.sload = h->sload;
     f.fake = h->fake; f.partT = h->partT; f.partN = h->partN; f.SigT = h->SigT; f.SigN = h->SigN;
-    f.Ptemp = h->Ptemp + (int64_t)sys * h->N; f.Pdot = h->Pdot_s + (int64_t)sys * h->N;
-    f.y = h->Y; f.ytmp = yin_tmp; f.kbuf = h->kbuf; f.yscal = h->yscal; f.yout = h->yout; f.ctl = h->ctl;
+    f.Ptemp = h->Ptemp; f.Pdot = h->Pdot_s; f.y = h->Y; f.ytmp = h->ytmp; f.kbuf = h->kbuf; f.yscal = h->yscal;
+    f.yout = h->yout; f.ctl = h->ctl;
     return f;
 }
 
-static int launch_friction(dfn_handle *h, int stage, int sys, double *ytmp)
+static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t nelem)
 {
-    FricParams f = fric_params(h, sys, ytmp);
-    unsigned nb = (unsigned)((h->N + 255) / 256);
-    friction_kernel<<<nb, 256, 0, h->stream>>>(f, stage);
+    FricParams f = fric_params(h, nelem);
+    friction_kernel<<<(unsigned)((nelem + 255) / 256), 256, 0, h->stream>>>(f, stage, sys, mask);
     h->launches++;
     CKL();
     return DFN_OK;
 }
 
-#define TRY(x)                       \
-    do {                             \
-        int s_ = (x);                \
-        if (s_ != DFN_OK) return s_; \
-    } while (0)
-
-// One RK attempt (stages 2..6 and the error test) with the current ctl->h.
-static int run_attempt(dfn_handle *h)
+static ElemParams elem_params(dfn_handle *h)
 {
-    const int64_t n3 = 3 * h->N;
-    attempt_begin_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, h->stream>>>(h->N, h->Y, h->kbuf, h->ytmp, h->ctl);
+    ElemParams ep;
+    ep.Ntot = h->Ntot; ep.inst = h->inst; ep.inst_of = h->inst_of; ep.ctl = h->ctl;
+    return ep;
+}
+
+static unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// One RK attempt (stages 2..6 and the error test) of every network in `mask`.
+static int run_attempt(dfn_handle *h, int mask)
+{
+    attempt_begin_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(elem_params(h), h->Y, h->kbuf, h->ytmp,
+                                                                         mask);
     h->launches++;
     CKL();
-    TRY(launch_pressure(h, 1, 1, 5, 0.0));
+    TRY(launch_pressure(h, mask, 1, 1, 5, 0.0, h->B));
     for (int s = 2; s <= 6; s++) {
-        TRY(launch_gemv(h, h->ytmp));
-        TRY(launch_friction(h, s, s - 1, h->ytmp));
+        TRY(launch_gemv(h, mask, h->ytmp, 3, h->ntiles));
+        TRY(launch_friction(h, s, s - 1, mask, h->Ntot));
     }
-    decide_kernel<<<1, 32, 0, h->stream>>>(h->ctl);
+    decide_kernel<<<blocks_of(h->B, 128), 128, 0, h->stream>>>(h->ctl, h->B, mask);
+    h->launches++;
+    CKL();
+    return DFN_OK;
+}
+
+// One round of the solve() loop for every network of the batch.
+static int run_round(dfn_handle *h)
+{
+    const unsigned bb = blocks_of(h->B, 128);
+    step_begin_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->inst, h->B, h->src_tb);
+    h->launches++;
+    CKL();
+    // CG probe at t_try (halving on non-convergence); its solution is the
+    // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
+    TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
+    TRY(launch_gemv(h, M_NEW, h->Y, 3, h->ntiles));
+    TRY(launch_friction(h, 1, 0, M_NEW, h->Ntot));
+    set_h_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B);
+    h->launches++;
+    CKL();
+    TRY(run_attempt(h, M_ACTIVE));
+    commit_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(elem_params(h), h->Y, h->yout, h->P, h->Pdot,
+                                                                  h->Ptemp, h->Pdot_s);
+    h->launches++;
+    CKL();
+    finish_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B, 86400.0);
     h->launches++;
     CKL();
     return DFN_OK;
@@ -201,7 +260,7 @@ static int run_attempt(dfn_handle *h)
 
 static int sync_ctl(dfn_handle *h)
 {
-    CK(cudaMemcpyAsync(h->h_ctl, h->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_ctl, h->ctl, sizeof(StepCtl) * h->B, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     int flag = 0;
     CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
@@ -212,38 +271,39 @@ static int sync_ctl(dfn_handle *h)
     return DFN_OK;
 }
 
-// Attempt loop of rkqs (src/ode_solver/ode_bs.f90:155-165) with k1 and
-// yscal already on the device and ctl->h set.
-static int rkqs_device(dfn_handle *h)
+static int put_ctl(dfn_handle *h)
 {
-    for (int att = 0;; att++) {
-        TRY(run_attempt(h));
-        TRY(sync_ctl(h));
-        if (h->h_ctl->status) return h->h_ctl->status;
-        if (h->h_ctl->accepted) return DFN_OK;
-        if (att + 1 >= h->max_attempts) return DFN_ERR_ATTEMPTS;
-    }
+    CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(StepCtl) * h->B, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DFN_OK;
 }
 
-static int solve_one_step(dfn_handle *h)
+// Advances every network by `nsteps` accepted steps, or until its time
+// reaches t_end (> 0). Rounds are launched in groups; the controllers are
+// read between groups only.
+static int solve_impl(dfn_handle *h, int64_t nsteps, double t_end)
 {
-    step_begin_kernel<<<1, 32, 0, h->stream>>>(h->ctl, h->nsrc, h->src_tb);
+    arm_kernel<<<blocks_of(h->B, 128), 128, 0, h->stream>>>(h->ctl, h->B, (long long)nsteps, t_end,
+                                                            h->max_attempts);
     h->launches++;
     CKL();
-    // CG probe at t_try (halving on non-convergence); its solution is the
-    // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
-    TRY(launch_pressure(h, 0, 0, 1, 0.0));
-    TRY(launch_gemv(h, h->Y));
-    TRY(launch_friction(h, 1, 0, h->ytmp));
-    set_h_kernel<<<1, 32, 0, h->stream>>>(h->ctl);
-    h->launches++;
-    CKL();
-    TRY(rkqs_device(h));
-    commit_kernel<<<(unsigned)((3 * h->N + 255) / 256), 256, 0, h->stream>>>(
-        h->N, h->Y, h->yout, h->P, h->Pdot, h->Ptemp + 4 * h->N, h->Pdot_s + 4 * h->N, h->ctl, 86400.0);
-    h->launches++;
-    CKL();
-    return DFN_OK;
+    int64_t group = (t_end > 0.0) ? 8 : std::max<int64_t>(nsteps, 1);
+    for (int64_t guard = 0; guard < 1000000; guard++) {
+        for (int64_t r = 0; r < group; r++) TRY(run_round(h));
+        TRY(sync_ctl(h));
+        int64_t remaining = 0;
+        bool active = false;
+        for (int i = 0; i < h->B; i++) {
+            const StepCtl &c = h->h_ctl[i];
+            if (c.phase == PH_DONE) continue;
+            active = true;
+            remaining = std::max<int64_t>(remaining, c.target_steps - c.steps_done);
+        }
+        if (!active) return DFN_OK;
+        group = (t_end > 0.0) ? 8 : std::max<int64_t>(remaining, 1);
+    }
+    g_err = "solve did not finish";
+    return DFN_ERR_ATTEMPTS;
 }
 
 static __global__ void snapshot_kernel(int64_t N, const double *Y, const double *Dc, const double *V0,
@@ -258,6 +318,22 @@ static __global__ void snapshot_kernel(int64_t N, const double *Y, const double 
     out[4 * N + k] = Y[2 * N + k];
 }
 
+static void fill_report(const StepCtl &c, dfn_report *r)
+{
+    if (!r) return;
+    r->it_count = c.it_count; r->attempts = c.attempts; r->rejected = c.rejected; r->rhs_evals = c.rhs_evals;
+    r->cg_iterations = c.cg_iters; r->probe_halvings = c.halvings; r->time = c.time; r->t_try = c.t_try;
+    r->last_hdid = c.hdid; r->status = c.status; r->pad = 0; r->stage_cg_failures = c.stage_noconv;
+}
+
+static int single_only(const dfn_handle *h)
+{
+    if (h->B != 1) {
+        g_err = "this entry point works on a handle holding one network";
+        return DFN_ERR_UNSUPPORTED;
+    }
+    return DFN_OK;
+}
 // ---------------------------------------------------------------------------
 extern "C" {
 
@@ -300,11 +376,11 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->node, h->elem, h->ds, h->tan, h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0,
-                    h->nload, h->sload, h->perm, h->fake, h->src_fault, h->src_elem, h->seg_start, h->src_Q,
-                    h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout, h->yscal, h->ytmp, h->kbuf, h->SigT,
-                    h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s, h->pwork, h->vin, h->vout, h->snap,
-                    h->err_flag, h->K, h->ctl};
+    void *ptrs[] = {h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->node, h->elem, h->ds, h->tan,
+                    h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
+                    h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
+                    h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
+                    h->pwork, h->vin, h->vout, h->snap, h->err_flag, h->K, h->ctl};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -316,9 +392,33 @@ int32_t dfn_destroy(dfn_handle *h)
     return DFN_OK;
 }
 
+static int check_problem(const dfn_problem *p)
+{
+    const int64_t N = p->nb_element, F = p->nb_fault;
+    if (N < 2 || F < 1 || !p->fault_nb_element || !p->node) { g_err = "need nb_element >= 2 and nb_fault >= 1"; return DFN_ERR_ARG; }
+    int64_t cnt = 0;
+    for (int64_t f = 0; f < F; f++) {
+        if (p->fault_nb_element[f] < 1) { g_err = "every fault needs at least one element"; return DFN_ERR_ARG; }
+        cnt += p->fault_nb_element[f] + 1;
+    }
+    if (cnt - 1 != N) { g_err = "nb_element must equal sum(fault_nb_element) + nb_fault - 1"; return DFN_ERR_ARG; }
+    if (p->fracture_mode != DFN_MODE_II && p->fracture_mode != DFN_MODE_III) { g_err = "fracture_mode must be 2 or 3"; return DFN_ERR_ARG; }
+    if (!(p->tol_solver > 0)) { g_err = "tol_solver must be positive"; return DFN_ERR_ARG; }
+    if (!p->a || !p->b || !p->Dc || !p->f0 || !p->V0 || !p->V || !p->theta || !p->sigmaN || !p->P ||
+        !p->normal_loading_dot || !p->shear_loading_dot || !p->permeability) { g_err = "null array in dfn_problem"; return DFN_ERR_ARG; }
+    for (int64_t s = 0; s < p->nb_source; s++) {
+        int64_t f = p->src_fault[s];
+        if (f < 1 || f > F || p->src_index[s] < 1 || p->src_index[s] > p->fault_nb_element[f - 1]) {
+            g_err = "source fault/index out of range";
+            return DFN_ERR_ARG;
+        }
+    }
+    return DFN_OK;
+}
+
 #define DALLOC(ptr, count)                                                \
     do {                                                                  \
-        cudaError_t e_ = cudaMalloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count)); \
+        cudaError_t e_ = cudaMalloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)std::max<int64_t>((count), 1)); \
         if (e_ != cudaSuccess) {                                          \
             set_err("cudaMalloc " #ptr, e_, __FILE__, __LINE__);          \
             dfn_destroy(h);                                               \
@@ -328,11 +428,13 @@ int32_t dfn_destroy(dfn_handle *h)
 
 #define HCOPY(dst, src, count)                                                                          \
     do {                                                                                                \
-        cudaError_t e_ = cudaMemcpy((dst), (src), sizeof(*(dst)) * (size_t)(count), cudaMemcpyHostToDevice); \
-        if (e_ != cudaSuccess) {                                                                        \
-            set_err("cudaMemcpy " #dst, e_, __FILE__, __LINE__);                                        \
-            dfn_destroy(h);                                                                             \
-            return DFN_ERR_CUDA;                                                                        \
+        if ((count) > 0) {                                                                              \
+            cudaError_t e_ = cudaMemcpy((dst), (src), sizeof(*(dst)) * (size_t)(count), cudaMemcpyHostToDevice); \
+            if (e_ != cudaSuccess) {                                                                    \
+                set_err("cudaMemcpy " #dst, e_, __FILE__, __LINE__);                                    \
+                dfn_destroy(h);                                                                         \
+                return DFN_ERR_CUDA;                                                                    \
+            }                                                                                           \
         }                                                                                               \
     } while (0)
 
@@ -346,30 +448,17 @@ int32_t dfn_destroy(dfn_handle *h)
         }                                                      \
     } while (0)
 
-int32_t dfn_create(const dfn_problem *p, const dfn_options *opt_in, dfn_handle **out)
+int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_options *opt_in, dfn_handle **out)
 {
-    if (!p || !out) { g_err = "null argument"; return DFN_ERR_ARG; }
+    if (!probs || !out || count < 1) { g_err = "null argument or empty batch"; return DFN_ERR_ARG; }
     *out = nullptr;
     dfn_options opt;
     if (opt_in) opt = *opt_in; else dfn_default_options(&opt);
-    const int64_t N = p->nb_element, F = p->nb_fault;
-    if (N < 2 || F < 1 || !p->fault_nb_element || !p->node) { g_err = "need nb_element >= 2 and nb_fault >= 1"; return DFN_ERR_ARG; }
-    int64_t cnt = 0;
-    for (int64_t f = 0; f < F; f++) {
-        if (p->fault_nb_element[f] < 1) { g_err = "every fault needs at least one element"; return DFN_ERR_ARG; }
-        cnt += p->fault_nb_element[f] + 1;
-    }
-    if (cnt - 1 != N) { g_err = "nb_element must equal sum(fault_nb_element) + nb_fault - 1"; return DFN_ERR_ARG; }
-    if (p->fracture_mode != DFN_MODE_II && p->fracture_mode != DFN_MODE_III) { g_err = "fracture_mode must be 2 or 3"; return DFN_ERR_ARG; }
     if (opt.kernel_storage < 0 || opt.kernel_storage > 2) { g_err = "bad kernel_storage"; return DFN_ERR_ARG; }
-    if (opt.pressure_solver < 0 || opt.pressure_solver > 1) { g_err = "bad pressure_solver"; return DFN_ERR_ARG; }
-    if (p->tol_solver <= 0) { g_err = "tol_solver must be positive"; return DFN_ERR_ARG; }
-    for (int64_t s = 0; s < p->nb_source; s++) {
-        int64_t f = p->src_fault[s];
-        if (f < 1 || f > F || p->src_index[s] < 1 || p->src_index[s] > p->fault_nb_element[f - 1]) {
-            g_err = "source fault/index out of range";
-            return DFN_ERR_ARG;
-        }
+    if (opt.pressure_solver < 0 || opt.pressure_solver > 2) { g_err = "bad pressure_solver"; return DFN_ERR_ARG; }
+    for (int i = 0; i < count; i++) {
+        TRY(check_problem(&probs[i]));
+        if (probs[i].fracture_mode != probs[0].fracture_mode) { g_err = "all networks of a batch need the same fracture_mode"; return DFN_ERR_ARG; }
     }
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
@@ -383,92 +472,131 @@ int32_t dfn_create(const dfn_problem *p, const dfn_options *opt_in, dfn_handle *
     CKC(cudaSetDevice(h->dev));
     CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
-    h->N = N; h->F = F; h->mode = p->fracture_mode; h->store = opt.kernel_storage;
+    h->B = count;
+    h->mode = probs[0].fracture_mode; h->store = opt.kernel_storage;
     h->pressure = opt.pressure_solver; h->gemv_impl = opt.gemv_impl;
     h->max_attempts = opt.max_attempts > 0 ? opt.max_attempts : 64;
-    h->tol = p->tol_solver;
     const int bpc = bytes_per_col(h->mode, h->store);
     const int64_t CW = GEMV_CHUNK_BYTES / bpc;
-    h->Np = ((N + CW - 1) / CW) * CW;
-    h->nchunk = (int)(h->Np / CW);
-    // prefactors: src/kernel_calculation/hmatrixModeII.f90:67-68, hmatrixModeIII.f90:55
-    if (h->mode == DFN_MODE_II) h->prefT = p->mu / DFN_PI * (1.0 - p->cs * p->cs / (p->cp * p->cp));
-    else h->prefT = p->mu / (2.0 * DFN_PI);
-    h->mu_2cs = p->mu / (2.0 * p->cs);
 
-    DALLOC(h->node, 2 * (N + 1)); DALLOC(h->elem, 2 * N); DALLOC(h->ds, N); DALLOC(h->tan, 2 * N);
-    DALLOC(h->nrm, 2 * N); DALLOC(h->permx, N + 1);
-    DALLOC(h->a, N); DALLOC(h->b, N); DALLOC(h->Dc, N); DALLOC(h->f0, N); DALLOC(h->V0, N);
-    DALLOC(h->nload, N); DALLOC(h->sload, N); DALLOC(h->perm, N); DALLOC(h->fake, N);
-    DALLOC(h->Y, 3 * N); DALLOC(h->P, N); DALLOC(h->Pdot, N); DALLOC(h->yout, 3 * N); DALLOC(h->yscal, 3 * N);
-    DALLOC(h->ytmp, 3 * N); DALLOC(h->kbuf, 18 * N); DALLOC(h->SigT, N); DALLOC(h->SigN, N);
-    DALLOC(h->partT, (int64_t)h->nchunk * N); DALLOC(h->partN, (int64_t)h->nchunk * N);
-    DALLOC(h->Ptemp, 6 * N); DALLOC(h->Pdot_s, 6 * N); DALLOC(h->pwork, 24 * N);
-    DALLOC(h->vin, 3 * N); DALLOC(h->vout, 3 * N); DALLOC(h->snap, 5 * N);
-    DALLOC(h->err_flag, 1); DALLOC(h->ctl, 1);
+    // instance table
+    int64_t eoff = 0, kvec = 0, poff = 0, soff = 0;
+    h->hinst.resize(count);
+    for (int i = 0; i < count; i++) {
+        const dfn_problem &p = probs[i];
+        Inst &I = h->hinst[i];
+        I.N = p.nb_element;
+        I.Np = ((I.N + CW - 1) / CW) * CW;
+        I.eoff = eoff;
+        I.nchunk = I.Np / CW;
+        I.kvec = kvec;
+        I.poff = poff;
+        I.soff = soff;
+        I.nsrc = p.nb_source;
+        // prefactors: src/kernel_calculation/hmatrixModeII.f90:67-68, hmatrixModeIII.f90:55
+        I.prefT = (h->mode == DFN_MODE_II) ? p.mu / DFN_PI * (1.0 - p.cs * p.cs / (p.cp * p.cp)) : p.mu / (2.0 * DFN_PI);
+        I.mu_2cs = p.mu / (2.0 * p.cs);
+        I.porosity = p.porosity; I.dyn_visc = p.dyn_viscosity; I.comp = p.fluid_comp + p.rock_comp;
+        I.tol = p.tol_solver;
+        eoff += I.N;
+        kvec += I.N * I.Np * bpc / 16;
+        poff += I.nchunk * I.N;
+        soff += I.nsrc;
+        h->kv_bytes += I.N * I.N * bpc;
+    }
+    const int64_t Nt = eoff;
+    h->Ntot = Nt;
+    h->part_tot = poff;
+    h->nsrc_tot = soff;
+    const int64_t Nnode = Nt + count;   // every network has N_i + 1 nodes and faces
+
+    DALLOC(h->inst, count); DALLOC(h->inst_of, Nt);
+    DALLOC(h->node, 2 * Nnode); DALLOC(h->elem, 2 * Nt); DALLOC(h->ds, Nt); DALLOC(h->tan, 2 * Nt);
+    DALLOC(h->nrm, 2 * Nt); DALLOC(h->permx, Nnode);
+    DALLOC(h->a, Nt); DALLOC(h->b, Nt); DALLOC(h->Dc, Nt); DALLOC(h->f0, Nt); DALLOC(h->V0, Nt);
+    DALLOC(h->nload, Nt); DALLOC(h->sload, Nt); DALLOC(h->perm, Nt); DALLOC(h->fake, Nt);
+    DALLOC(h->Y, 3 * Nt); DALLOC(h->P, Nt); DALLOC(h->Pdot, Nt); DALLOC(h->yout, 3 * Nt); DALLOC(h->yscal, 3 * Nt);
+    DALLOC(h->ytmp, 3 * Nt); DALLOC(h->kbuf, 18 * Nt); DALLOC(h->SigT, Nt); DALLOC(h->SigN, Nt);
+    DALLOC(h->partT, poff); DALLOC(h->partN, poff);
+    DALLOC(h->Ptemp, 6 * Nt); DALLOC(h->Pdot_s, 6 * Nt); DALLOC(h->pwork, 24 * Nt);
+    DALLOC(h->vin, 3 * h->hinst[0].N); DALLOC(h->vout, 3 * h->hinst[0].N); DALLOC(h->snap, 5 * Nt);
+    DALLOC(h->err_flag, 1); DALLOC(h->ctl, count);
+    DALLOC(h->src_fault, soff); DALLOC(h->src_elem, soff); DALLOC(h->src_Q, soff); DALLOC(h->src_tb, soff);
+    DALLOC(h->src_te, soff);
     CKC(cudaMemset(h->err_flag, 0, sizeof(int)));
-    CKC(cudaMemset(h->partN, 0, sizeof(double) * h->nchunk * N));
-    CKC(cudaMemset(h->Pdot, 0, sizeof(double) * N));
-    CKC(cudaMemset(h->SigT, 0, sizeof(double) * N));
-    CKC(cudaMemset(h->SigN, 0, sizeof(double) * N));
-    CKC(cudaMallocHost((void **)&h->h_ctl, sizeof(StepCtl)));
+    CKC(cudaMemset(h->partN, 0, sizeof(double) * std::max<int64_t>(poff, 1)));
+    CKC(cudaMemset(h->Pdot, 0, sizeof(double) * Nt));
+    CKC(cudaMemset(h->SigT, 0, sizeof(double) * Nt));
+    CKC(cudaMemset(h->SigN, 0, sizeof(double) * Nt));
+    CKC(cudaMallocHost((void **)&h->h_ctl, sizeof(StepCtl) * count));
+    HCOPY(h->inst, h->hinst.data(), count);
 
-    HCOPY(h->node, p->node, 2 * (N + 1));
-    HCOPY(h->a, p->a, N); HCOPY(h->b, p->b, N); HCOPY(h->Dc, p->Dc, N); HCOPY(h->f0, p->f0, N);
-    HCOPY(h->V0, p->V0, N); HCOPY(h->nload, p->normal_loading_dot, N); HCOPY(h->sload, p->shear_loading_dot, N);
-    HCOPY(h->perm, p->permeability, N);
-    HCOPY(h->Y, p->V, N); HCOPY(h->Y + N, p->theta, N); HCOPY(h->Y + 2 * N, p->sigmaN, N); HCOPY(h->P, p->P, N);
-
-    // fake elements (src/friction/RateStateAgingModeII.f90:81-89) and
-    // 0-based fault starts (src/configuration.f90:245-246)
-    std::vector<unsigned char> fake(N, 0);
-    std::vector<int64_t> first(F);
-    {
+    std::vector<int> inst_of(Nt);
+    std::vector<unsigned char> fake(Nt, 0);
+    for (int i = 0; i < count; i++) {
+        const dfn_problem &p = probs[i];
+        const Inst &I = h->hinst[i];
+        const int64_t N = I.N, e0 = I.eoff, F = p.nb_fault;
+        for (int64_t k = 0; k < N; k++) inst_of[e0 + k] = i;
+        HCOPY(h->node + 2 * (e0 + i), p.node, 2 * (N + 1));
+        HCOPY(h->a + e0, p.a, N); HCOPY(h->b + e0, p.b, N); HCOPY(h->Dc + e0, p.Dc, N); HCOPY(h->f0 + e0, p.f0, N);
+        HCOPY(h->V0 + e0, p.V0, N); HCOPY(h->nload + e0, p.normal_loading_dot, N);
+        HCOPY(h->sload + e0, p.shear_loading_dot, N); HCOPY(h->perm + e0, p.permeability, N);
+        HCOPY(h->Y + 3 * e0, p.V, N); HCOPY(h->Y + 3 * e0 + N, p.theta, N); HCOPY(h->Y + 3 * e0 + 2 * N, p.sigmaN, N);
+        HCOPY(h->P + e0, p.P, N);
+        // fake elements (src/friction/RateStateAgingModeII.f90:81-89) and
+        // 0-based fault starts (src/configuration.f90:245-246)
+        std::vector<int64_t> first(F);
         int64_t idx = 0, c2 = 0;
         for (int64_t f = 0; f < F; f++) {
             first[f] = c2;
-            c2 += p->fault_nb_element[f] + 1;
-            idx += p->fault_nb_element[f] + 1;
-            if (idx <= N) fake[idx - 1] = 1;
+            c2 += p.fault_nb_element[f] + 1;
+            idx += p.fault_nb_element[f] + 1;
+            if (idx <= N) fake[e0 + idx - 1] = 1;
         }
+        if (p.nb_source > 0) {
+            std::vector<int64_t> se(p.nb_source);
+            for (int64_t s = 0; s < p.nb_source; s++) se[s] = first[p.src_fault[s] - 1] + p.src_index[s] - 1;
+            HCOPY(h->src_fault + I.soff, p.src_fault, p.nb_source); HCOPY(h->src_elem + I.soff, se.data(), p.nb_source);
+            HCOPY(h->src_Q + I.soff, p.src_Q, p.nb_source); HCOPY(h->src_tb + I.soff, p.src_t_beg, p.nb_source);
+            HCOPY(h->src_te + I.soff, p.src_t_end, p.nb_source);
+        }
+        // geometry (device), src/initialisation.f90:145-205
+        geometry_kernel<<<blocks_of(N + 1, 256), 256, 0, h->stream>>>(
+            N, h->mode, h->node + 2 * (e0 + i), h->elem + 2 * e0, h->ds + e0, h->tan + 2 * e0, h->nrm + 2 * e0,
+            h->nload + e0, h->sload + e0, h->Y + 3 * e0 + 2 * N, h->perm + e0, h->permx + e0 + i, p.Sigma11_dot,
+            p.Sigma12_dot, p.Sigma22_dot, p.Sigma31_dot, p.Sigma32_dot);
+        h->launches++;
+        CKC(cudaGetLastError());
     }
-    HCOPY(h->fake, fake.data(), N);
-
-    h->nsrc = p->nb_source;
-    int64_t ns = h->nsrc > 0 ? h->nsrc : 1;
-    DALLOC(h->src_fault, ns); DALLOC(h->src_elem, ns); DALLOC(h->src_Q, ns); DALLOC(h->src_tb, ns); DALLOC(h->src_te, ns);
-    if (h->nsrc > 0) {
-        std::vector<int64_t> se(h->nsrc);
-        for (int64_t s = 0; s < h->nsrc; s++) se[s] = first[p->src_fault[s] - 1] + p->src_index[s] - 1;
-        HCOPY(h->src_fault, p->src_fault, h->nsrc); HCOPY(h->src_elem, se.data(), h->nsrc);
-        HCOPY(h->src_Q, p->src_Q, h->nsrc); HCOPY(h->src_tb, p->src_t_beg, h->nsrc); HCOPY(h->src_te, p->src_t_end, h->nsrc);
-        h->h_src_tb.assign(p->src_t_beg, p->src_t_beg + h->nsrc);
-    }
-
-    // geometry (device)
-    geometry_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, h->stream>>>(
-        N, h->mode, h->node, h->elem, h->ds, h->tan, h->nrm, h->nload, h->sload, h->Y + 2 * N, h->perm, h->permx,
-        p->Sigma11_dot, p->Sigma12_dot, p->Sigma22_dot, p->Sigma31_dot, p->Sigma32_dot);
-    h->launches++;
-    CKC(cudaGetLastError());
+    HCOPY(h->inst_of, inst_of.data(), Nt);
+    HCOPY(h->fake, fake.data(), Nt);
 
     // decoupled pressure segments from the face permeabilities
     {
-        std::vector<double> px(N + 1);
-        CKC(cudaMemcpyAsync(px.data(), h->permx, sizeof(double) * (N + 1), cudaMemcpyDeviceToHost, h->stream));
+        std::vector<double> px(Nnode);
+        CKC(cudaMemcpyAsync(px.data(), h->permx, sizeof(double) * Nnode, cudaMemcpyDeviceToHost, h->stream));
         CKC(cudaStreamSynchronize(h->stream));
         std::vector<int64_t> seg;
-        seg.push_back(0);
-        for (int64_t k = 1; k < N; k++)
-            if (px[k] == 0.0) seg.push_back(k);
-        seg.push_back(N);
+        std::vector<int> sinst;
+        for (int i = 0; i < count; i++) {
+            const Inst &I = h->hinst[i];
+            seg.push_back(I.eoff);
+            sinst.push_back(i);
+            for (int64_t k = 1; k < I.N; k++)
+                if (px[I.eoff + i + k] == 0.0) { seg.push_back(I.eoff + k); sinst.push_back(i); }
+            if (i == 0) h->nseg0 = (int64_t)seg.size();
+        }
+        seg.push_back(Nt);
         h->nseg = (int64_t)seg.size() - 1;
         DALLOC(h->seg_start, seg.size());
+        DALLOC(h->seg_inst, sinst.size());
         HCOPY(h->seg_start, seg.data(), seg.size());
+        HCOPY(h->seg_inst, sinst.data(), sinst.size());
     }
 
-    // dense kernel matrix
-    h->K_bytes = (size_t)N * (size_t)h->Np * (size_t)bpc;
+    // dense kernel matrices, one per network
+    h->K_bytes = (size_t)kvec * 16;
     {
         cudaError_t e = cudaMalloc(&h->K, h->K_bytes);
         if (e != cudaSuccess) {
@@ -477,9 +605,14 @@ int32_t dfn_create(const dfn_problem *p, const dfn_options *opt_in, dfn_handle *
             return DFN_ERR_NOMEM;
         }
     }
-    {
-        dim3 grid((unsigned)N, (unsigned)((h->Np + 255) / 256));
-#define ASM(MODE, STORE) assemble_kernel<MODE, STORE><<<grid, 256, 0, h->stream>>>(N, h->Np, h->node, h->elem, h->tan, h->nrm, h->K)
+    std::vector<int4> tiles;
+    for (int i = 0; i < count; i++) {
+        const Inst &I = h->hinst[i];
+        const int64_t e0 = I.eoff;
+        void *Ki = static_cast<unsigned char *>(h->K) + I.kvec * 16;
+        dim3 grid((unsigned)I.N, (unsigned)((I.Np + 255) / 256));
+#define ASM(MODE, STORE) \
+    assemble_kernel<MODE, STORE><<<grid, 256, 0, h->stream>>>(I.N, I.Np, h->node + 2 * (e0 + i), h->elem + 2 * e0, h->tan + 2 * e0, h->nrm + 2 * e0, Ki)
         if (h->mode == 2) {
             if (h->store == 0) ASM(2, 0); else if (h->store == 1) ASM(2, 1); else ASM(2, 2);
         } else {
@@ -488,7 +621,14 @@ int32_t dfn_create(const dfn_problem *p, const dfn_options *opt_in, dfn_handle *
 #undef ASM
         h->launches++;
         CKC(cudaGetLastError());
+        const int64_t nrb = (I.N + GEMV_ROWS - 1) / GEMV_ROWS;
+        for (int64_t rb = 0; rb < nrb; rb++)
+            for (int64_t c = 0; c < I.nchunk; c++) tiles.push_back(make_int4(i, (int)c, (int)rb, 0));
+        if (i == 0) h->ntiles0 = (int64_t)tiles.size();
     }
+    h->ntiles = (int64_t)tiles.size();
+    DALLOC(h->tiles, tiles.size());
+    HCOPY(h->tiles, tiles.data(), tiles.size());
     // TMA pipeline needs the dynamic shared memory opt-in
     {
         gemv_tma_fn fns[6] = {gemv_tma_kernel<2, 0>, gemv_tma_kernel<2, 1>, gemv_tma_kernel<2, 2>,
@@ -496,23 +636,28 @@ int32_t dfn_create(const dfn_problem *p, const dfn_options *opt_in, dfn_handle *
         for (auto fn : fns) CKC(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem));
     }
 
-    // pressure parameters
-    PressParams &pp = h->pp;
-    pp.N = N; pp.P = h->P; pp.permx = h->permx; pp.ds = h->ds;
-    pp.porosity = p->porosity; pp.dyn_visc = p->dyn_viscosity; pp.comp = p->fluid_comp + p->rock_comp;
-    pp.tol = p->tol_solver; pp.nsrc = h->nsrc; pp.src_fault = h->src_fault; pp.src_elem = h->src_elem;
-    pp.src_Q = h->src_Q; pp.src_tb = h->src_tb; pp.src_te = h->src_te; pp.ctl_time = &h->ctl->time;
+    PressGlobal &pg = h->pg;
+    pg.P = h->P; pg.permx = h->permx; pg.ds = h->ds; pg.src_fault = h->src_fault; pg.src_elem = h->src_elem;
+    pg.src_Q = h->src_Q; pg.src_tb = h->src_tb; pg.src_te = h->src_te;
 
-    // controller: solve() entry, src/solver.f90:50-56
-    StepCtl c;
-    memset(&c, 0, sizeof(c));
-    c.time = p->time0; c.t_try = 100.0; c.eps = p->tol_solver; c.h = 100.0;
-    CKC(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+    // controllers: solve() entry, src/solver.f90:50-56
+    for (int i = 0; i < count; i++) {
+        StepCtl &c = h->h_ctl[i];
+        memset(&c, 0, sizeof(c));
+        c.time = probs[i].time0; c.t_try = 100.0; c.eps = probs[i].tol_solver; c.h = 100.0;
+        c.phase = PH_DONE; c.max_attempts = h->max_attempts;
+    }
+    CKC(cudaMemcpy(h->ctl, h->h_ctl, sizeof(StepCtl) * count, cudaMemcpyHostToDevice));
     CKC(cudaEventCreate(&h->ev0));
     CKC(cudaEventCreate(&h->ev1));
     CKC(cudaStreamSynchronize(h->stream));
     *out = h;
     return DFN_OK;
+}
+
+int32_t dfn_create(const dfn_problem *p, const dfn_options *opt, dfn_handle **out)
+{
+    return dfn_create_batch(p, 1, opt, out);
 }
 
 int32_t dfn_set_stream(dfn_handle *h, void *s)
@@ -526,21 +671,20 @@ int32_t dfn_set_stream(dfn_handle *h, void *s)
     return DFN_OK;
 }
 
-int64_t dfn_nb_element(const dfn_handle *h) { return h ? h->N : -1; }
-int64_t dfn_kernel_bytes(const dfn_handle *h)
-{
-    if (!h) return -1;
-    return (int64_t)h->N * (int64_t)h->N * bytes_per_col(h->mode, h->store);
-}
+int32_t dfn_batch_size(const dfn_handle *h) { return h ? h->B : -1; }
+int64_t dfn_nb_element(const dfn_handle *h) { return h ? h->hinst[0].N : -1; }
+int64_t dfn_kernel_bytes(const dfn_handle *h) { return h ? h->kv_bytes : -1; }
 int64_t dfn_launch_count(const dfn_handle *h) { return h ? h->launches : -1; }
 
 int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_sT, double *d_sN)
 {
     if (!h || !d_slip || !d_sT) return DFN_ERR_ARG;
+    TRY(single_only(h));
     CK(cudaSetDevice(h->dev));
-    TRY(launch_gemv(h, d_slip));
-    kv_finish_kernel<<<(unsigned)((h->N + 255) / 256), 256, 0, h->stream>>>(h->N, h->mode, h->nchunk, h->prefT,
-                                                                             h->partT, h->partN, d_sT, d_sN);
+    const Inst &I = h->hinst[0];
+    TRY(launch_gemv(h, M_ALL, d_slip, 1, h->ntiles0));
+    kv_finish_kernel<<<blocks_of(I.N, 256), 256, 0, h->stream>>>(I.N, h->mode, (int)I.nchunk, I.prefT, h->partT,
+                                                                 h->partN, d_sT, d_sN);
     h->launches++;
     CKL();
     return DFN_OK;
@@ -549,36 +693,35 @@ int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_sT, dou
 int32_t dfn_kernel(dfn_handle *h, const double *slip, double *sT, double *sN)
 {
     if (!h || !slip || !sT) return DFN_ERR_ARG;
-    const int64_t N = h->N;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
     CK(cudaMemcpyAsync(h->vin, slip, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
     TRY(dfn_kernel_device(h, h->vin, h->vout, h->vout + N));
     CK(cudaMemcpyAsync(sT, h->vout, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
     if (sN) CK(cudaMemcpyAsync(sN, h->vout + N, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    int flag = 0;
-    CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) { g_err = "bounded wait expired in the TMA K.V pipeline"; return DFN_ERR_CUDA; }
+    TRY(sync_ctl(h));
     return DFN_OK;
 }
 
-static int reset_status(dfn_handle *h)
+static int reset_status0(dfn_handle *h)
 {
-    CK(cudaMemsetAsync(&h->ctl->status, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(&h->ctl[0].status, 0, sizeof(int), h->stream));
     return DFN_OK;
 }
 
 int32_t dfn_compute_P(dfn_handle *h, double dt, double *P_temp, double *P_dot, int32_t *ier)
 {
     if (!h || !P_temp || !P_dot) return DFN_ERR_ARG;
-    const int64_t N = h->N;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
-    TRY(reset_status(h));
-    TRY(launch_pressure(h, 2, 0, 1, dt));
+    TRY(reset_status0(h));
+    TRY(launch_pressure(h, M_ALL, 2, 0, 1, dt, 1));
     TRY(sync_ctl(h));
-    int st = h->h_ctl->status;
+    int st = h->h_ctl[0].status;
     if (ier) *ier = (st == 1) ? 1 : 0;
-    if (st == 1) { TRY(reset_status(h)); return DFN_OK; }
+    if (st == 1) { TRY(reset_status0(h)); return DFN_OK; }
     if (st) return st;
     CK(cudaMemcpy(P_temp, h->Ptemp, sizeof(double) * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(P_dot, h->Pdot_s, sizeof(double) * N, cudaMemcpyDeviceToHost));
@@ -587,98 +730,118 @@ int32_t dfn_compute_P(dfn_handle *h, double dt, double *P_temp, double *P_dot, i
 
 int32_t dfn_friction_law(dfn_handle *h, double x, int64_t nv, const double *Y, double *Ydot)
 {
-    if (!h || !Y || !Ydot || nv != 3 * h->N) return DFN_ERR_ARG;
-    const int64_t N = h->N;
+    if (!h || !Y || !Ydot) return DFN_ERR_ARG;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
+    if (nv != 3 * N) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
-    TRY(reset_status(h));
+    TRY(reset_status0(h));
     CK(cudaMemcpyAsync(h->ytmp, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
-    TRY(launch_pressure(h, 2, 0, 1, x));
-    TRY(launch_gemv(h, h->ytmp));
-    TRY(launch_friction(h, 0, 0, h->ytmp));
+    TRY(launch_pressure(h, M_ALL, 2, 0, 1, x, 1));
+    TRY(launch_gemv(h, M_ALL, h->ytmp, 3, h->ntiles0));
+    TRY(launch_friction(h, 0, 0, M_ALL, N));
     CK(cudaMemcpyAsync(Ydot, h->kbuf, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync_ctl(h));
-    int st = h->h_ctl->status;
-    TRY(reset_status(h));
+    int st = h->h_ctl[0].status;
+    TRY(reset_status0(h));
     return st;
 }
 
 int32_t dfn_rkqs(dfn_handle *h, double *y, const double *dydx, int64_t nv, double *x, double htry, double eps,
                  const double *yscal, double *hdid, double *hnext)
 {
-    if (!h || !y || !dydx || !x || !yscal || !hdid || !hnext || nv != 3 * h->N) return DFN_ERR_ARG;
-    const int64_t n3 = 3 * h->N;
+    if (!h || !y || !dydx || !x || !yscal || !hdid || !hnext) return DFN_ERR_ARG;
+    TRY(single_only(h));
+    const int64_t n3 = 3 * h->hinst[0].N;
+    if (nv != n3) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
     CK(cudaMemcpyAsync(h->Y, y, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->kbuf, dydx, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->yscal, yscal, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     TRY(sync_ctl(h));
-    StepCtl c = *h->h_ctl;
-    double eps_saved = c.eps;
-    c.x = *x; c.h = htry; c.eps = eps; c.accepted = 0; c.status = 0;
-    CK(cudaMemcpyAsync(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
-    int st = rkqs_device(h);
-    if (st != DFN_OK) return st;
+    StepCtl saved = h->h_ctl[0];
+    StepCtl &c = h->h_ctl[0];
+    c.x = *x; c.h = htry; c.eps = eps; c.accepted = 0; c.status = 0; c.phase = PH_RETRY; c.step_attempts = 0;
+    c.max_attempts = h->max_attempts;
+    TRY(put_ctl(h));
+    for (;;) {
+        TRY(run_attempt(h, M_ACTIVE));
+        TRY(sync_ctl(h));
+        if (h->h_ctl[0].status) return h->h_ctl[0].status;
+        if (h->h_ctl[0].accepted) break;
+    }
     CK(cudaMemcpyAsync(h->Y, h->yout, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(y, h->yout, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync_ctl(h));
-    *hdid = h->h_ctl->hdid;
-    *hnext = h->h_ctl->hnext;
+    *hdid = h->h_ctl[0].hdid;
+    *hnext = h->h_ctl[0].hnext;
     *x = *x + *hdid;
-    c = *h->h_ctl;
-    c.eps = eps_saved; c.x = 0.0;
-    CK(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+    StepCtl &d = h->h_ctl[0];
+    d.eps = saved.eps; d.x = 0.0; d.phase = PH_DONE;
+    TRY(put_ctl(h));
     return DFN_OK;
-}
-
-static void fill_report(dfn_handle *h, dfn_report *r)
-{
-    if (!r) return;
-    const StepCtl &c = *h->h_ctl;
-    r->it_count = c.it_count; r->attempts = c.attempts; r->rejected = c.rejected; r->rhs_evals = c.rhs_evals;
-    r->cg_iterations = c.cg_iters; r->probe_halvings = c.halvings; r->time = c.time; r->t_try = c.t_try;
-    r->last_hdid = c.hdid; r->status = c.status; r->pad = 0;
 }
 
 int32_t dfn_solve_steps(dfn_handle *h, int64_t n_steps, dfn_report *rep)
 {
     if (!h || n_steps < 0) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
-    int st = DFN_OK;
-    for (int64_t s = 0; s < n_steps; s++) {
-        st = solve_one_step(h);
-        if (st != DFN_OK) break;
-    }
+    int st = solve_impl(h, n_steps, 0.0);
     int st2 = sync_ctl(h);
     if (st == DFN_OK) st = st2;
-    if (st == DFN_OK && h->h_ctl->status) st = h->h_ctl->status;
-    fill_report(h, rep);
+    if (st == DFN_OK) {
+        for (int i = 0; i < h->B; i++)
+            if (h->h_ctl[i].status) { st = h->h_ctl[i].status; break; }
+    }
+    fill_report(h->h_ctl[0], rep);
     return st;
+}
+
+int32_t dfn_solve_batch(dfn_handle *h, int64_t n_steps, double t_end, dfn_report *reps)
+{
+    if (!h || n_steps < 0 || !(t_end >= 0.0)) return DFN_ERR_ARG;
+    if (t_end > 0.0 && n_steps == 0) n_steps = (int64_t)1 << 62;
+    CK(cudaSetDevice(h->dev));
+    int st = solve_impl(h, n_steps, t_end);
+    int st2 = sync_ctl(h);
+    if (st == DFN_OK) st = st2;
+    if (reps)
+        for (int i = 0; i < h->B; i++) fill_report(h->h_ctl[i], &reps[i]);
+    return st;
+}
+
+int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, double *time, double *t_try,
+                               int64_t *it_count)
+{
+    if (!h || i < 0 || i >= h->B) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    TRY(sync_ctl(h));
+    const Inst &I = h->hinst[i];
+    if (Y) CK(cudaMemcpy(Y, h->Y + 3 * I.eoff, sizeof(double) * 3 * I.N, cudaMemcpyDeviceToHost));
+    if (P) CK(cudaMemcpy(P, h->P + I.eoff, sizeof(double) * I.N, cudaMemcpyDeviceToHost));
+    if (time) *time = h->h_ctl[i].time;
+    if (t_try) *t_try = h->h_ctl[i].t_try;
+    if (it_count) *it_count = h->h_ctl[i].it_count;
+    return DFN_OK;
 }
 
 int32_t dfn_get_state(dfn_handle *h, double *Y, double *P, double *time, double *t_try, int64_t *it_count)
 {
-    if (!h) return DFN_ERR_ARG;
-    CK(cudaSetDevice(h->dev));
-    TRY(sync_ctl(h));
-    if (Y) CK(cudaMemcpy(Y, h->Y, sizeof(double) * 3 * h->N, cudaMemcpyDeviceToHost));
-    if (P) CK(cudaMemcpy(P, h->P, sizeof(double) * h->N, cudaMemcpyDeviceToHost));
-    if (time) *time = h->h_ctl->time;
-    if (t_try) *t_try = h->h_ctl->t_try;
-    if (it_count) *it_count = h->h_ctl->it_count;
-    return DFN_OK;
+    return dfn_get_state_instance(h, 0, Y, P, time, t_try, it_count);
 }
 
 int32_t dfn_set_state(dfn_handle *h, const double *Y, const double *P, double time, double t_try, int64_t it_count)
 {
     if (!h) return DFN_ERR_ARG;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
-    if (Y) CK(cudaMemcpyAsync(h->Y, Y, sizeof(double) * 3 * h->N, cudaMemcpyHostToDevice, h->stream));
-    if (P) CK(cudaMemcpyAsync(h->P, P, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+    if (Y) CK(cudaMemcpyAsync(h->Y, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
+    if (P) CK(cudaMemcpyAsync(h->P, P, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
     TRY(sync_ctl(h));
-    StepCtl c = *h->h_ctl;
+    StepCtl &c = h->h_ctl[0];
     c.time = time; c.t_try = t_try; c.it_count = it_count; c.status = 0;
-    CK(cudaMemcpyAsync(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    TRY(put_ctl(h));
     return DFN_OK;
 }
 
@@ -686,9 +849,10 @@ int32_t dfn_get_snapshot(dfn_handle *h, double *V, double *theta, double *P, dou
                          double *permeability, double *time)
 {
     if (!h) return DFN_ERR_ARG;
-    const int64_t N = h->N;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
-    snapshot_kernel<<<(unsigned)((N + 255) / 256), 256, 0, h->stream>>>(N, h->Y, h->Dc, h->V0, h->P, h->SigT, h->snap);
+    snapshot_kernel<<<blocks_of(N, 256), 256, 0, h->stream>>>(N, h->Y, h->Dc, h->V0, h->P, h->SigT, h->snap);
     h->launches++;
     CKL();
     double *dst[5] = {V, theta, P, tT, tN};
@@ -696,7 +860,7 @@ int32_t dfn_get_snapshot(dfn_handle *h, double *V, double *theta, double *P, dou
         if (dst[i]) CK(cudaMemcpyAsync(dst[i], h->snap + i * N, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
     if (permeability) CK(cudaMemcpyAsync(permeability, h->perm, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync_ctl(h));
-    if (time) *time = h->h_ctl->time;
+    if (time) *time = h->h_ctl[0].time;
     return DFN_OK;
 }
 
@@ -705,19 +869,20 @@ int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, dou
                       dfn_report *rep)
 {
     if (!h || !Y_in || !P_in) return DFN_ERR_ARG;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
     TRY(sync_ctl(h));
-    StepCtl c = *h->h_ctl;
-    CK(cudaMemcpyAsync(h->Y, Y_in, sizeof(double) * 3 * h->N, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->P, P_in, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->Y, Y_in, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->P, P_in, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
+    StepCtl &c = h->h_ctl[0];
     c.time = time_in; c.t_try = t_try_in; c.status = 0;
-    *h->h_ctl = c;
-    CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(c), cudaMemcpyHostToDevice, h->stream));
-    int st = solve_one_step(h);
-    if (st != DFN_OK) { sync_ctl(h); fill_report(h, rep); return st; }
+    CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, h->stream));
+    int st = solve_impl(h, 1, 0.0);
+    if (st != DFN_OK) { sync_ctl(h); fill_report(h->h_ctl[0], rep); return st; }
     TRY(dfn_get_snapshot(h, V_out, theta_out, P_out, tT_out, tN_out, nullptr, nullptr));
-    fill_report(h, rep);
-    return h->h_ctl->status;
+    fill_report(h->h_ctl[0], rep);
+    return h->h_ctl[0].status;
 }
 
 }  // extern "C"
@@ -847,9 +1012,9 @@ int32_t dfn_time_kernel(dfn_handle *h, int32_t reps, double *ms)
 {
     if (!h || reps < 1 || !ms) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
-    TRY(launch_gemv(h, h->Y));
+    TRY(launch_gemv(h, M_ALL, h->Y, 3, h->ntiles));
     CK(cudaEventRecord(h->ev0, h->stream));
-    for (int i = 0; i < reps; i++) TRY(launch_gemv(h, h->Y));
+    for (int i = 0; i < reps; i++) TRY(launch_gemv(h, M_ALL, h->Y, 3, h->ntiles));
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     float t = 0.f;

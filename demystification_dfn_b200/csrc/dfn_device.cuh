@@ -8,6 +8,7 @@
 //                         src/hmatrix/eval_kernel_hmatrix.f90:7-199 (same pair
 //                         terms as src/kernel_calculation/directModeII.f90:41-78)
 //   gemv_kernel           K.V streamed from HBM, per-column-chunk partial sums
+//                         (one launch covers every network of a batch)
 //   pressure_cg_kernel    the reference's Jacobi-scaled CG for compute_P
 //                         (src/fluid_diffusion.f90:24-152), one CTA per system
 //   pressure_tridiag_kernel  exact per-segment Thomas solve of the same system
@@ -24,7 +25,7 @@
 #define DFN_PI 3.141592653589793238
 
 // ---------------------------------------------------------------------------
-// Device-resident step controller (one per handle).
+// Device-resident step controller (one per network).
 struct StepCtl {
     double time;      // committed simulated time
     double t_try;     // trial step of the solve loop
@@ -37,7 +38,13 @@ struct StepCtl {
     int accepted;
     int status;       // dfn_status
     int probe_ier;
-    int pad;
+    int phase;        // PH_NEW / PH_RETRY / PH_DONE
+    long long steps_done, target_steps;  // accepted steps in this solve call, and the goal
+    double t_end;     // stop when time >= t_end (t_end > 0)
+    int step_attempts, max_attempts;
+    int pfail_mask;   // bit s: pressure system s of this attempt hit the CG cap
+    int pad2;
+    long long stage_noconv;  // stage pressure solves that hit the CG cap
 };
 
 // Cash-Karp tableau, src/ode_solver/ode_bs.f90:200-210.
@@ -301,18 +308,58 @@ __device__ __forceinline__ void fma_vec(const uint4 &q, const double *v, double 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Batch of independent networks ("instances"). A single network is a batch
+// of one. Per-instance data are concatenated; Inst gives the offsets.
+enum { PH_NEW = 0, PH_RETRY = 1, PH_DONE = 2 };
+enum { M_NEW = 1, M_RETRY = 2, M_ACTIVE = 3, M_ALL = 7 };
+
+struct Inst {
+    int64_t N;        // elements of the instance (fake ones included)
+    int64_t Np;       // padded columns of its kernel matrix
+    int64_t eoff;     // first element in the concatenated element arrays
+    int64_t nchunk;   // 4 KiB column chunks per row
+    int64_t kvec;     // offset of its kernel matrix in 16-byte vectors
+    int64_t poff;     // offset of its K.V partial sums (nchunk*N per component)
+    int64_t soff, nsrc;  // its injection sources
+    double prefT, mu_2cs;
+    double porosity, dyn_visc, comp, tol;
+};
+
+__device__ __forceinline__ bool takes_part(const StepCtl *ctl, int i, int mask)
+{
+    return (mask >> ctl[i].phase) & 1;
+}
+
+// K.V streaming kernel (direct 128-bit loads).
+//
+// Work unit (tile): one 4 KiB column chunk of one instance for a block of
+// GEMV_ROWS rows. Every lane keeps the V values of its columns in registers
+// and reuses them for all rows of the block; each warp owns rows r0+w,
+// r0+w+8, ... and issues 8 coalesced 128-bit loads per lane per row (two rows
+// in flight). The per-(chunk,row) warp sum goes to part[c*N + row]; the
+// consumer adds the chunks in a fixed order, so the result is deterministic.
+// V of instance i is Vbase[vmul*eoff_i + l].
 template <int MODE, int STORE>
-__global__ void __launch_bounds__(GEMV_WARPS * 32) gemv_kernel(int64_t N, int64_t Np, const uint4 *__restrict__ K,
-                                                               const double *__restrict__ Vin, double *__restrict__ partT,
-                                                               double *__restrict__ partN)
+__global__ void __launch_bounds__(GEMV_WARPS * 32)
+    gemv_kernel(const int4 *__restrict__ tiles, const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
+                int mask, const uint4 *__restrict__ Kbase, const double *__restrict__ Vbase, int vmul,
+                double *__restrict__ partT, double *__restrict__ partN)
 {
     constexpr int BPC = KFmt<MODE, STORE>::BPC;
     constexpr int CPV = 16 / BPC;                 // columns per 16-byte vector
     constexpr int CW = GEMV_CHUNK_BYTES / BPC;    // columns per chunk
+    const int4 t = tiles[blockIdx.x];
+    if (!takes_part(ctl, t.x, mask)) return;
+    const Inst I = inst[t.x];
+    const int64_t N = I.N;
+    const uint4 *K = Kbase + I.kvec;
+    const double *Vin = Vbase + (int64_t)vmul * I.eoff;
+    double *pT = partT + I.poff, *pN = partN + I.poff;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t c = blockIdx.x;                 // column chunk
-    const int64_t r0 = (int64_t)blockIdx.y * GEMV_ROWS;
-    const int64_t row_vecs = Np * BPC / 16;       // 16-byte vectors per row
+    const int64_t c = t.y;
+    const int64_t r0 = (int64_t)t.z * GEMV_ROWS;
+    const int64_t row_vecs = I.Np * BPC / 16;
 
     double v[GEMV_LPL * CPV];
 #pragma unroll
@@ -342,11 +389,11 @@ __global__ void __launch_bounds__(GEMV_WARPS * 32) gemv_kernel(int64_t N, int64_
         aT = warp_sum(aT); bT = warp_sum(bT);
         if (MODE == 2) { aN = warp_sum(aN); bN = warp_sum(bN); }
         if (lane == 0) {
-            partT[c * N + r] = aT;
-            if (MODE == 2) partN[c * N + r] = aN;
+            pT[c * N + r] = aT;
+            if (MODE == 2) pN[c * N + r] = aN;
             if (two) {
-                partT[c * N + rb] = bT;
-                if (MODE == 2) partN[c * N + rb] = bN;
+                pT[c * N + rb] = bT;
+                if (MODE == 2) pN[c * N + rb] = bN;
             }
         }
     }
@@ -400,9 +447,15 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_
                  : "memory");
 }
 
+// TMA bulk-copy variant of the same tiling: one producer warp streams the
+// 4 KiB row-chunks of the tile with cp.async.bulk into a 16-stage ring of
+// shared memory completed on mbarriers; eight consumer warps read the stages
+// with 128-bit shared loads. Rows of the tile go to consumer warps
+// round-robin, one stage per row (stage s is always read by warp s % 8).
 template <int MODE, int STORE>
 __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
-    gemv_tma_kernel(int64_t N, int64_t Np, const uint4 *__restrict__ K, const double *__restrict__ Vin,
+    gemv_tma_kernel(const int4 *__restrict__ tiles, const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
+                    int mask, const uint4 *__restrict__ Kbase, const double *__restrict__ Vbase, int vmul,
                     double *__restrict__ partT, double *__restrict__ partN, int *err_flag)
 {
     constexpr int BPC = KFmt<MODE, STORE>::BPC;
@@ -412,22 +465,28 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
     uint4 *stage = reinterpret_cast<uint4 *>(smem_raw);                       // TMA_STAGES x 4 KiB
     uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + TMA_STAGES * GEMV_CHUNK_BYTES);
     uint64_t *empty = full + TMA_STAGES;
+    __shared__ int issued_s, bad_s;
 
+    const int4 t = tiles[blockIdx.x];
+    if (!takes_part(ctl, t.x, mask)) return;   // CTA-uniform: before any barrier
+    const Inst I = inst[t.x];
+    const int64_t N = I.N;
+    const unsigned char *K = reinterpret_cast<const unsigned char *>(Kbase + I.kvec);
+    const double *Vin = Vbase + (int64_t)vmul * I.eoff;
+    double *pT = partT + I.poff, *pN = partN + I.poff;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t c = blockIdx.x;
-    const int64_t r0 = (int64_t)blockIdx.y * GEMV_ROWS;
+    const int64_t c = t.y;
+    const int64_t r0 = (int64_t)t.z * GEMV_ROWS;
     const int64_t rend = (r0 + GEMV_ROWS < N) ? r0 + GEMV_ROWS : N;
     const int nrows = (int)(rend - r0);
-    const int64_t row_bytes = Np * BPC;
+    const int64_t row_bytes = I.Np * BPC;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TMA_STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issued_s = 0;
+        bad_s = 0;
     }
-    __syncthreads();
-
-    __shared__ int issued_s, bad_s;
-    if (threadIdx.x == 0) { issued_s = 0; bad_s = 0; }
     __syncthreads();
     if (warp == TMA_CONSUMERS) {
         // producer: one elected lane issues the bulk copies
@@ -437,9 +496,8 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
                 int s = i % TMA_STAGES;
                 if (i >= TMA_STAGES && !mbar_wait(&empty[s], ((i / TMA_STAGES) - 1) & 1)) { bad_s = 1; break; }
                 mbar_expect_tx(&full[s], GEMV_CHUNK_BYTES);
-                const unsigned char *src =
-                    reinterpret_cast<const unsigned char *>(K) + (r0 + i) * row_bytes + c * GEMV_CHUNK_BYTES;
-                tma_bulk_g2s(stage + s * (GEMV_CHUNK_BYTES / 16), src, GEMV_CHUNK_BYTES, &full[s]);
+                tma_bulk_g2s(stage + s * (GEMV_CHUNK_BYTES / 16), K + (r0 + i) * row_bytes + c * GEMV_CHUNK_BYTES,
+                             GEMV_CHUNK_BYTES, &full[s]);
             }
             issued_s = i;
         }
@@ -467,8 +525,8 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
             aT = warp_sum(aT);
             if (MODE == 2) aN = warp_sum(aN);
             if (lane == 0) {
-                partT[c * N + r0 + i] = aT;
-                if (MODE == 2) partN[c * N + r0 + i] = aN;
+                pT[c * N + r0 + i] = aT;
+                if (MODE == 2) pN[c * N + r0 + i] = aN;
             }
         }
     }
@@ -597,61 +655,104 @@ __device__ __forceinline__ double sys_dt(const StepCtl *ctl, int kind, int sys, 
 
 // One Jacobi-scaled CG solve (reference algorithm) by the whole CTA.
 // Work vectors live in global memory (w: 4*N doubles). Returns ier.
+// Row k of compute_MatrixVector (src/fluid_diffusion.f90:175-204): the
+// Jacobi-scaled stencil (A1 v(k-1) + A2 v(k) + A3 v(k+1)) / diag(k), in the
+// reference's operand order without FMA (diag(k) equals A2 of row k).
+__device__ __forceinline__ double pmatvec_row(const PressParams &p, int64_t k, double dt, const double *v)
+{
+    double A1, A2, A3;
+    prow(p, k, dt, A1, A2, A3);
+    double m;
+    if (k == 0) m = add_(mul_(A2, v[0]), mul_(A3, v[1]));
+    else if (k == p.N - 1) m = add_(mul_(A1, v[k - 1]), mul_(A2, v[k]));
+    else m = add_(add_(mul_(A1, v[k - 1]), mul_(A2, v[k])), mul_(A3, v[k + 1]));
+    return __ddiv_rn(m, A2);
+}
+
+// b1(k) = P(k)/diag(k) plus the injection terms, each added separately as
+// in src/fluid_diffusion.f90:45-64.
+__device__ __forceinline__ double pb1(const PressParams &p, int64_t k, double dt, double diag)
+{
+    double b1 = __ddiv_rn(p.P[k], diag);
+    const double t = add_(*p.ctl_time, dt);
+    for (int64_t s = 0; s < p.nsrc; s++) {
+        if (!(t >= p.src_tb[s] && t < p.src_te[s])) continue;
+        for (int64_t j = 0; j < p.nsrc; j++) {
+            if (p.src_fault[j] != p.src_fault[s] || p.src_elem[j] != k) continue;
+            const double c = __ddiv_rn(__ddiv_rn(mul_(dt, p.src_Q[j]), mul_(p.porosity, p.comp)), p.ds[k]);
+            b1 = add_(b1, __ddiv_rn(c, diag));
+        }
+    }
+    return b1;
+}
+
+// sum(a*b) over the vectors in index order by one thread (the reference's
+// sequential summation); every thread gets the result.
+__device__ __forceinline__ double seq_dot(const double *a, const double *b, int64_t N, double *red)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int64_t k = 0; k < N; k++) s = add_(s, mul_(a[k], b[k]));
+        red[32] = s;
+    }
+    __syncthreads();
+    const double v = red[32];
+    __syncthreads();
+    return v;
+}
+
+// One Jacobi-scaled CG solve (src/fluid_diffusion.f90:79-131) by the whole
+// CTA. Work vectors live in global memory. Element-wise arithmetic follows
+// the reference's operand order without FMA. exact = 1 also sums the dot
+// products sequentially, which reproduces the reference's rounding and so
+// its iteration counts bit for bit (needed where a solve sits at the
+// 200-iteration cap or at the tolerance, since that decides t_try halving);
+// exact = 0 sums them with a tree reduction. Returns ier.
 __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, double *pv, double *Mp, double *red,
-                        long long *iters)
+                        long long *iters, int exact)
 {
     const int64_t N = p.N;
     const int tid = threadIdx.x, nt = blockDim.x;
     // x = P, r = b1 - M x, p = r
-    double lmax = 0.0;
+    double lmax = 0.0, lrr = 0.0;
     for (int64_t k = tid; k < N; k += nt) {
         double A1, A2, A3;
         prow(p, k, dt, A1, A2, A3);
-        double b1 = __ddiv_rn(p.P[k], A2);
-        double src = psource(p, k, dt);
-        if (src != 0.0) b1 = add_(b1, __ddiv_rn(src, A2));
-        double m = A2 * p.P[k];
-        if (k > 0) m = A1 * p.P[k - 1] + m;
-        if (k < N - 1) m = m + A3 * p.P[k + 1];
-        double rk = b1 - m / A2;
+        const double rk = add_(pb1(p, k, dt, A2), -pmatvec_row(p, k, dt, p.P));
         x[k] = p.P[k];
         r[k] = rk;
         pv[k] = rk;
         lmax = fmax(lmax, fabs(rk));
+        lrr += rk * rk;
     }
     double errmax = block_max(lmax, red) / p.tol;
     long long it = 0;
     // rr carried between iterations: sum(rk**2) of iteration i+1 equals
-    // sum(rk1**2) of iteration i (rk = rk1), so it is computed once.
-    double lrr = 0.0;
-    for (int64_t k = tid; k < N; k += nt) lrr += r[k] * r[k];
-    double rr = block_sum(lrr, red);
+    // sum(rk1**2) of iteration i (rk = rk1, same summation), so it is
+    // computed once.
+    double rr = exact ? seq_dot(r, r, N, red) : block_sum(lrr, red);
     while (errmax >= 1.0) {
         it++;
         double lpap = 0.0;
         for (int64_t k = tid; k < N; k += nt) {
-            double A1, A2, A3;
-            prow(p, k, dt, A1, A2, A3);
-            double m = A2 * pv[k];
-            if (k > 0) m = A1 * pv[k - 1] + m;
-            if (k < N - 1) m = m + A3 * pv[k + 1];
-            m = m / A2;
+            const double m = pmatvec_row(p, k, dt, pv);
             Mp[k] = m;
             lpap += pv[k] * m;
         }
-        double pap = block_sum(lpap, red);
-        double alpha = rr / pap;
+        const double pap = exact ? seq_dot(pv, Mp, N, red) : block_sum(lpap, red);
+        const double alpha = rr / pap;
         double lr1 = 0.0, lm = 0.0;
         for (int64_t k = tid; k < N; k += nt) {
-            x[k] = x[k] + alpha * pv[k];
-            double r1 = r[k] - alpha * Mp[k];
+            x[k] = add_(x[k], mul_(alpha, pv[k]));
+            const double r1 = add_(r[k], -mul_(alpha, Mp[k]));
             r[k] = r1;
             lr1 += r1 * r1;
             lm = fmax(lm, fabs(r1));
         }
-        double r1r1 = block_sum(lr1, red);
-        double beta = r1r1 / rr;
-        for (int64_t k = tid; k < N; k += nt) pv[k] = r[k] + beta * pv[k];
+        const double r1r1 = exact ? seq_dot(r, r, N, red) : block_sum(lr1, red);
+        const double beta = r1r1 / rr;
+        for (int64_t k = tid; k < N; k += nt) pv[k] = add_(r[k], mul_(beta, pv[k]));
         rr = r1r1;
         if (it > 200) { *iters += it; return 1; }
         errmax = block_max(lm, red) / p.tol;
@@ -660,27 +761,22 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
     return 0;
 }
 
-__global__ void __launch_bounds__(1024) pressure_cg_kernel(PressParams p, StepCtl *ctl, int kind, int sys0,
-                                                           double dt_explicit, double *Ptemp, double *Pdot,
-                                                           double *work)
+// One system of the reference CG for one instance (whole CTA), shared by
+// the batched solver and the allocation-free entry point.
+__device__ void cg_system(const PressParams &p, StepCtl *ctl, int kind, int sys, double dt_explicit, double *Pt,
+                          double *Pd, double *x, double *r, double *pv, double *Mp, double *red, long long *iters,
+                          int exact)
 {
-    __shared__ double red[33];
-    const int sys = sys0 + blockIdx.x;
     const int64_t N = p.N;
-    double *x = work + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
-    double *Pt = Ptemp + (int64_t)sys * N, *Pd = Pdot + (int64_t)sys * N;
-    __shared__ long long iters;
-    if (threadIdx.x == 0) iters = 0;
-    __syncthreads();
     double dt = sys_dt(ctl, kind, sys, dt_explicit);
-    int ier = cg_solve(p, dt, x, r, pv, Mp, red, &iters);
+    int ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact);
     if (kind == 0) {
         // probe: src/solver.f90:81-92, halve t_try until the solve converges
         int guard = 0;
         while (ier == 1 && guard < 1100) {
             dt = dt / 2.0;
             guard++;
-            ier = cg_solve(p, dt, x, r, pv, Mp, red, &iters);
+            ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -689,7 +785,14 @@ __global__ void __launch_bounds__(1024) pressure_cg_kernel(PressParams p, StepCt
         }
     }
     __syncthreads();
-    if (ier == 0) {
+    // A stage solve (kind 1) that hits the cap: the reference goes on with an
+    // uninitialised P_temp and a stale P_dot (RateStateAgingModeII.f90:37-68
+    // after compute_P returned early); here the stage uses the last CG
+    // iterate instead, the attempt goes on, and the failure is counted. If it
+    // is the stage-5 system, the commit keeps P unchanged, as the reference's
+    // commit compute_P(t_did) (the same solve) returns early too.
+    const int write = (ier == 0) || (kind == 1);
+    if (write) {
         double lmx = 0.0;
         for (int64_t k = threadIdx.x; k < N; k += blockDim.x) {
             Pd[k] = (dt < 1e-9) ? 0.0 : (x[k] - p.P[k]) / dt;
@@ -697,34 +800,101 @@ __global__ void __launch_bounds__(1024) pressure_cg_kernel(PressParams p, StepCt
             lmx = fmax(lmx, fabs(x[k]));
         }
         double mx = block_max(lmx, red);
-        if (!(mx <= 1.7976931348623157e308)) ier = 1;
-    }
-    if (threadIdx.x == 0) {
-        atomicAdd((unsigned long long *)&ctl->cg_iters, (unsigned long long)iters);
-        if (ier) {
-            if (kind == 0) ctl->probe_ier = 1;
-            atomicCAS(&ctl->status, 0, 1);
+        if (!(mx <= 1.7976931348623157e308)) {
+            if (threadIdx.x == 0) atomicCAS(&ctl->status, 0, 4);
         }
     }
+    if (threadIdx.x == 0) {
+        atomicAdd((unsigned long long *)&ctl->cg_iters, (unsigned long long)*iters);
+        if (ier) {
+            if (kind == 1) {
+                atomicOr(&ctl->pfail_mask, 1 << sys);
+                atomicAdd((unsigned long long *)&ctl->stage_noconv, 1ull);
+            } else {
+                if (kind == 0) ctl->probe_ier = 1;
+                atomicCAS(&ctl->status, 0, 1);
+            }
+        }
+    }
+}
+
+// Single system with explicit pointers (allocation-free entry point).
+__global__ void __launch_bounds__(1024) pressure_cg_kernel(PressParams p, StepCtl *ctl, int kind, int sys0,
+                                                           double dt_explicit, double *Ptemp, double *Pdot,
+                                                           double *work)
+{
+    __shared__ double red[33];
+    __shared__ long long iters;
+    const int sys = sys0 + blockIdx.x;
+    const int64_t N = p.N;
+    double *x = work + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
+    if (threadIdx.x == 0) iters = 0;
+    __syncthreads();
+    cg_system(p, ctl, kind, sys, dt_explicit, Ptemp + (int64_t)sys * N, Pdot + (int64_t)sys * N, x, r, pv, Mp, red,
+              &iters, 0);
+}
+
+// Global (all-instance) pressure arrays; instance i's slice starts at eoff_i
+// (face permeabilities at eoff_i + i, they have N_i + 1 entries).
+struct PressGlobal {
+    const double *P, *permx, *ds;
+    const int64_t *src_fault, *src_elem;   // src_elem: 0-based within the instance
+    const double *src_Q, *src_tb, *src_te;
+};
+
+__device__ __forceinline__ PressParams press_params(const PressGlobal &g, const Inst &I, int i, const StepCtl *ctl)
+{
+    PressParams p;
+    p.N = I.N; p.P = g.P + I.eoff; p.permx = g.permx + I.eoff + i; p.ds = g.ds + I.eoff;
+    p.porosity = I.porosity; p.dyn_visc = I.dyn_visc; p.comp = I.comp; p.tol = I.tol;
+    p.nsrc = I.nsrc; p.src_fault = g.src_fault + I.soff; p.src_elem = g.src_elem + I.soff;
+    p.src_Q = g.src_Q + I.soff; p.src_tb = g.src_tb + I.soff; p.src_te = g.src_te + I.soff;
+    p.ctl_time = &ctl[i].time;
+    return p;
+}
+
+// Batched CG: CTA (system s, instance i). Work of instance i: 24*eoff, then
+// 4*N_i per system; outputs Ptemp/Pdot at 6*eoff + sys*N_i.
+__global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
+                                                                 int mask, int kind, int sys0, double dt_explicit,
+                                                                 double *Ptemp, double *Pdot, double *work, int exact)
+{
+    __shared__ double red[33];
+    __shared__ long long iters;
+    const int i = blockIdx.y;
+    if (!takes_part(ctl, i, mask)) return;
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.x;
+    const int64_t N = I.N;
+    double *x = work + 24 * I.eoff + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
+    if (threadIdx.x == 0) iters = 0;
+    __syncthreads();
+    cg_system(p, ctl + i, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
+              Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact);
 }
 
 // Exact solve of the unscaled tridiagonal system A x = P + source, one
 // thread per decoupled segment (a maximal run of elements joined by nonzero
 // face permeability; the fake elements between faults are segments of one).
-__global__ void pressure_tridiag_kernel(PressParams p, StepCtl *ctl, int kind, int sys0, double dt_explicit,
-                                        const int64_t *seg_start, int64_t nseg, double *Ptemp, double *Pdot,
-                                        double *work)
+// seg_start holds global element indices; segments never cross instances.
+__global__ void pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl, int mask, int kind, int sys0,
+                                        double dt_explicit, const int64_t *seg_start, const int *seg_inst,
+                                        int64_t nseg, double *Ptemp, double *Pdot, double *work)
 {
-    const int sys = sys0 + blockIdx.y;
     const int64_t sg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (sg >= nseg) return;
-    const int64_t N = p.N;
-    const double dt = sys_dt(ctl, kind, sys, dt_explicit);
-    const int64_t k0 = seg_start[sg], k1 = seg_start[sg + 1];
-    double *cp = work + (int64_t)sys * 4 * N;   // modified super-diagonal
-    double *dp = cp + N;                        // modified right-hand side
-    double *Pt = Ptemp + (int64_t)sys * N, *Pd = Pdot + (int64_t)sys * N;
-    // forward sweep
+    const int i = seg_inst[sg];
+    if (!takes_part(ctl, i, mask)) return;
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.y;
+    const int64_t N = I.N;
+    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
+    const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+    double *cp = work + 24 * I.eoff + (int64_t)sys * 4 * N;   // modified super-diagonal
+    double *dp = cp + N;                                       // modified right-hand side
+    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
     double cprev = 0.0, dprev = 0.0;
     for (int64_t k = k0; k < k1; k++) {
         double A1, A2, A3;
@@ -738,7 +908,6 @@ __global__ void pressure_tridiag_kernel(PressParams p, StepCtl *ctl, int kind, i
         cp[k] = c; dp[k] = d;
         cprev = c; dprev = d;
     }
-    // back substitution
     double xn = 0.0;
     bool bad = false;
     for (int64_t k = k1 - 1; k >= k0; k--) {
@@ -748,46 +917,45 @@ __global__ void pressure_tridiag_kernel(PressParams p, StepCtl *ctl, int kind, i
         Pd[k] = (dt < 1e-9) ? 0.0 : (xk - p.P[k]) / dt;
         if (!isfinite(xk)) bad = true;
     }
-    if (bad) atomicCAS(&ctl->status, 0, 4);
+    if (bad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
 // ---------------------------------------------------------------------------
 // Friction right-hand side fused with the Cash-Karp stage arithmetic.
 struct FricParams {
-    int64_t N;
+    int64_t Ntot;                 // elements of all instances
     int mode;
-    int nchunk;
-    double prefT;                 // mu/pi*(1-cs^2/cp^2) (mode II) or mu/(2 pi) (mode III)
-    double mu_2cs;                // mu/(2 cs)
+    const Inst *inst;
+    const int *inst_of;           // instance of each global element
     const double *a, *b, *Dc, *f0, *V0, *nload, *sload;
     const unsigned char *fake;
-    const double *partT, *partN;  // [nchunk][N]
+    const double *partT, *partN;  // per instance [nchunk][N] at poff
     double *SigT, *SigN;          // stress rates of this evaluation
-    const double *Ptemp, *Pdot;   // pressure of this evaluation
-    const double *y;              // state at the step start
+    const double *Ptemp, *Pdot;   // per instance [6][N] at 6*eoff
+    const double *y;              // state at the step start, [3N] at 3*eoff
     double *ytmp;                 // ytemp of this stage (in) / next stage (out)
-    double *kbuf;                 // [6][3N] stage derivatives
-    double *yscal;
-    double *yout;
+    double *kbuf;                 // per instance [6][3N] at 18*eoff
+    double *yscal, *yout;         // [3N] at 3*eoff
     StepCtl *ctl;
 };
 
-__device__ __forceinline__ void rsf_rhs(const FricParams &f, int64_t k, double V, double psi, double sig, double T,
-                                        double Nn, double Pt, double Pd, double &dV, double &dpsi, double &dsig)
+__device__ __forceinline__ void rsf_rhs(const FricParams &f, int mode, int64_t e, double mu_2cs, double V, double psi,
+                                        double sig, double T, double Nn, double Pt, double Pd, double &dV,
+                                        double &dpsi, double &dsig)
 {
     // src/friction/RateStateAgingModeII.f90:46-76 (mode III: dsig = loading only)
-    dsig = (f.mode == 2) ? (Nn + f.nload[k]) : f.nload[k];
-    const double a = f.a[k], b = f.b[k], V0 = f.V0[k], Dc = f.Dc[k];
+    dsig = (mode == 2) ? (Nn + f.nload[e]) : f.nload[e];
+    const double a = f.a[e], b = f.b[e], V0 = f.V0[e], Dc = f.Dc[e];
     double B = V / (2.0 * V0);
-    double C = exp((f.f0[k] + b * psi) / a);
+    double C = exp((f.f0[e] + b * psi) / a);
     double D = 1.0 / (C * C) + B * B;
     D = 1.0 / sqrt(D);
     double heal = V0 / Dc * exp(-psi) - fabs(V) / Dc;
-    double num = f.sload[k] + T + (dsig + Pd) * a * asinh(B * C) + B * D * (sig + Pt) * b * heal;
-    double den = f.mu_2cs - D * (sig + Pt) * a / (2.0 * V0);
+    double num = f.sload[e] + T + (dsig + Pd) * a * asinh(B * C) + B * D * (sig + Pt) * b * heal;
+    double den = mu_2cs - D * (sig + Pt) * a / (2.0 * V0);
     dV = num / den;
     dpsi = heal;
-    if (f.fake[k]) { dV = 0.0; dpsi = 0.0; dsig = 0.0; }
+    if (f.fake[e]) { dV = 0.0; dpsi = 0.0; dsig = 0.0; }
 }
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v)
@@ -796,155 +964,236 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-// stage: 0 = standalone evaluation (ytmp in, kbuf[0] out)
+// stage: 0 = standalone evaluation (ytmp in, kbuf slot 0 out)
 //        1 = k1 at the step start (y in), also yscal
 //        2..5 = k_s, then ytemp of stage s+1 in place
 //        6 = k6, then yout, yerr and the max-norm contribution
-__global__ void friction_kernel(FricParams f, int stage)
+// sys: pressure system of this evaluation; mask: phases that take part.
+__global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
 {
-    __shared__ double red[32];
-    const int64_t N = f.N;
-    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int myi = -1;
     double emax = 0.0;
-    if (k < N) {
+    if (e < f.Ntot) {
+        const int i = f.inst_of[e];
+        if (takes_part(f.ctl, i, mask)) myi = i;
+    }
+    if (myi >= 0) {
+        const Inst &I = f.inst[myi];
+        const int64_t N = I.N, k = e - I.eoff, S = 3 * N;
+        StepCtl *ctl = f.ctl + myi;
         double T = 0.0, Nn = 0.0;
-        for (int c = 0; c < f.nchunk; c++) T += f.partT[(int64_t)c * N + k];
-        T = f.prefT * T;
+        const double *pT = f.partT + I.poff + k;
+        for (int64_t c = 0; c < I.nchunk; c++) T += pT[c * N];
+        T = I.prefT * T;
         if (f.mode == 2) {
-            for (int c = 0; c < f.nchunk; c++) Nn += f.partN[(int64_t)c * N + k];
-            Nn = f.prefT * Nn;
+            const double *pN = f.partN + I.poff + k;
+            for (int64_t c = 0; c < I.nchunk; c++) Nn += pN[c * N];
+            Nn = I.prefT * Nn;
         }
-        f.SigT[k] = T;
-        f.SigN[k] = Nn;
-        const double *yin = (stage == 1) ? f.y : f.ytmp;
-        double V = yin[k], psi = yin[N + k], sig = yin[2 * N + k];
+        f.SigT[e] = T;
+        f.SigN[e] = Nn;
+        const double *yi = f.y + 3 * I.eoff;
+        double *yt = f.ytmp + 3 * I.eoff;
+        const double *yin = (stage == 1) ? yi : yt;
+        const double V = yin[k], psi = yin[N + k], sig = yin[2 * N + k];
+        const double Pt = f.Ptemp[6 * I.eoff + (int64_t)sys * N + k];
+        const double Pd = f.Pdot[6 * I.eoff + (int64_t)sys * N + k];
         double dV, dpsi, dsig;
-        rsf_rhs(f, k, V, psi, sig, T, Nn, f.Ptemp[k], f.Pdot[k], dV, dpsi, dsig);
+        rsf_rhs(f, f.mode, e, I.mu_2cs, V, psi, sig, T, Nn, Pt, Pd, dV, dpsi, dsig);
+        double *kb = f.kbuf + 18 * I.eoff;
         const int slot = (stage == 0) ? 0 : stage - 1;
-        double *ks = f.kbuf + (int64_t)slot * 3 * N;
+        double *ks = kb + (int64_t)slot * S;
         ks[k] = dV; ks[N + k] = dpsi; ks[2 * N + k] = dsig;
-        const int64_t S = 3 * N;
         if (stage == 1) {
-            const double tt = f.ctl->t_try, tol = f.ctl->eps;
+            const double tt = ctl->t_try, tol = ctl->eps;
+            double *ysc = f.yscal + 3 * I.eoff;
             // yscal = abs(Y)+abs(Y_dot*t_try)+tol_solver (src/solver.f90:102)
-            f.yscal[k] = add_(add_(fabs(f.y[k]), fabs(mul_(dV, tt))), tol);
-            f.yscal[N + k] = add_(add_(fabs(f.y[N + k]), fabs(mul_(dpsi, tt))), tol);
-            f.yscal[2 * N + k] = add_(add_(fabs(f.y[2 * N + k]), fabs(mul_(dsig, tt))), tol);
+            ysc[k] = add_(add_(fabs(yi[k]), fabs(mul_(dV, tt))), tol);
+            ysc[N + k] = add_(add_(fabs(yi[N + k]), fabs(mul_(dpsi, tt))), tol);
+            ysc[2 * N + k] = add_(add_(fabs(yi[2 * N + k]), fabs(mul_(dsig, tt))), tol);
         } else if (stage >= 2 && stage <= 5) {
-            const double h = f.ctl->h;
+            const double h = ctl->h;
 #pragma unroll
-            for (int j = 0; j < 3; j++) f.ytmp[j * N + k] = ck_combine(stage + 1, h, f.y[j * N + k], f.kbuf, S, j * N + k);
+            for (int j = 0; j < 3; j++) yt[j * N + k] = ck_combine(stage + 1, h, yi[j * N + k], kb, S, j * N + k);
         } else if (stage == 6) {
-            const double h = f.ctl->h;
+            const double h = ctl->h;
+            const double *ysc = f.yscal + 3 * I.eoff;
+            double *yo = f.yout + 3 * I.eoff;
 #pragma unroll
             for (int j = 0; j < 3; j++) {
-                const int64_t i = j * N + k;
-                const double k1 = f.kbuf[i], k3 = f.kbuf[2 * S + i], k4 = f.kbuf[3 * S + i],
-                             k5 = f.kbuf[4 * S + i], k6 = f.kbuf[5 * S + i];
+                const int64_t q = j * N + k;
+                const double k1 = kb[q], k3 = kb[2 * S + q], k4 = kb[3 * S + q], k5 = kb[4 * S + q],
+                             k6 = kb[5 * S + q];
                 // src/ode_solver/ode_bs.f90:223-224
-                f.yout[i] = add_(f.y[i], mul_(h, add_(add_(add_(mul_(CK_C1, k1), mul_(CK_C3, k3)), mul_(CK_C4, k4)),
-                                                      mul_(CK_C6, k6))));
+                yo[q] = add_(yi[q], mul_(h, add_(add_(add_(mul_(CK_C1, k1), mul_(CK_C3, k3)), mul_(CK_C4, k4)),
+                                                 mul_(CK_C6, k6))));
                 double yerr = mul_(h, add_(add_(add_(add_(mul_(CK_DC1, k1), mul_(CK_DC3, k3)), mul_(CK_DC4, k4)),
                                                 mul_(CK_DC5, k5)),
                                            mul_(CK_DC6, k6)));
-                double e = fabs(__ddiv_rn(yerr, f.yscal[i]));
-                if (!(e == e) || isinf(e)) e = 1.0e300;   // non-finite error rejects the attempt
-                emax = fmax(emax, e);
+                double er = fabs(__ddiv_rn(yerr, ysc[q]));
+                if (!(er == er) || isinf(er)) er = 1.0e300;   // non-finite error rejects the attempt
+                emax = fmax(emax, er);
             }
         }
+        if (k == 0 && stage >= 1) atomicAdd((unsigned long long *)&ctl->rhs_evals, 1ull);
     }
     if (stage == 6) {
+        // warp-level max when the warp lies in one instance, else per lane
+        const unsigned full = 0xffffffffu;
+        const int i0 = __shfl_sync(full, myi, 0);
+        if (__all_sync(full, myi == i0)) {
+            double w = emax;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        if (lane == 0) red[w] = emax;
-        __syncthreads();
-        if (w == 0) {
-            double t = (lane < (blockDim.x >> 5)) ? red[lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
-            if (lane == 0) atomic_max_pos(&f.ctl->errmax_bits, t);
+            for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(full, w, o));
+            if ((threadIdx.x & 31) == 0 && i0 >= 0) atomic_max_pos(&f.ctl[i0].errmax_bits, w);
+        } else if (myi >= 0) {
+            atomic_max_pos(&f.ctl[myi].errmax_bits, emax);
         }
     }
-    if (k == 0 && stage >= 1) atomicAdd((unsigned long long *)&f.ctl->rhs_evals, 1ull);
 }
+
+// Element-wise kernels over all instances; k == 0 of an instance also
+// updates that instance's scalars.
+struct ElemParams {
+    int64_t Ntot;
+    const Inst *inst;
+    const int *inst_of;
+    StepCtl *ctl;
+};
 
 // ytemp of stage 2 at the start of every attempt (h may have changed).
-__global__ void attempt_begin_kernel(int64_t N, const double *y, const double *kbuf, double *ytmp, StepCtl *ctl)
+__global__ void attempt_begin_kernel(ElemParams ep, const double *y, const double *kbuf, double *ytmp, int mask)
 {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const double h = ctl->h;
-    if (i < 3 * N) ytmp[i] = ck_combine(2, h, y[i], kbuf, 3 * N, i);
-    if (i == 0) {
-        ctl->errmax_bits = 0ull;
-        ctl->attempts += 1;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ep.Ntot) return;
+    const int i = ep.inst_of[e];
+    if (!takes_part(ep.ctl, i, mask)) return;
+    const Inst &I = ep.inst[i];
+    const int64_t N = I.N, k = e - I.eoff;
+    const double h = ep.ctl[i].h;
+    const double *yi = y + 3 * I.eoff, *kb = kbuf + 18 * I.eoff;
+    double *yt = ytmp + 3 * I.eoff;
+#pragma unroll
+    for (int j = 0; j < 3; j++) yt[j * N + k] = ck_combine(2, h, yi[j * N + k], kb, 3 * N, j * N + k);
+    if (k == 0) {
+        ep.ctl[i].errmax_bits = 0ull;
+        ep.ctl[i].pfail_mask = 0;
+        ep.ctl[i].attempts += 1;
     }
 }
 
-// Step control after an attempt: src/ode_solver/ode_bs.f90:158-172.
-__global__ void decide_kernel(StepCtl *ctl)
+// Step control after an attempt, one thread per instance:
+// src/ode_solver/ode_bs.f90:158-172.
+__global__ void decide_kernel(StepCtl *ctl, int B, int mask)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || !takes_part(ctl, i, mask)) return;
+    StepCtl &c = ctl[i];
     const double SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25;
     const double ERRCON = (double)1.89e-4f;  // default-real literal in the reference
-    double errmax = __longlong_as_double((long long)ctl->errmax_bits) / ctl->eps;
-    double h = ctl->h;
+    double errmax = __longlong_as_double((long long)c.errmax_bits) / c.eps;
+    double h = c.h;
+    c.step_attempts += 1;
     if (errmax <= 1.0) {
-        ctl->accepted = 1;
-        ctl->hnext = (errmax > ERRCON) ? SAFETY * h * pow(errmax, PGROW) : 5.0 * h;
-        ctl->hdid = h;
+        c.accepted = 1;
+        c.hnext = (errmax > ERRCON) ? SAFETY * h * pow(errmax, PGROW) : 5.0 * h;
+        c.hdid = h;
     } else {
-        ctl->accepted = 0;
-        ctl->rejected += 1;
+        c.accepted = 0;
+        c.rejected += 1;
         double htemp = SAFETY * h * pow(errmax, PSHRNK);
         h = copysign(fmax(fabs(htemp), 0.1 * fabs(h)), h);
-        ctl->h = h;
-        if (ctl->x + h == ctl->x) ctl->status = 2;
+        c.h = h;
+        if (c.x + h == c.x) atomicCAS(&c.status, 0, 2);
+        else if (c.step_attempts >= c.max_attempts) atomicCAS(&c.status, 0, 8);
     }
 }
 
-// Start of one pass of solve(): src/solver.f90:60-77.
-__global__ void step_begin_kernel(StepCtl *ctl, int64_t nsrc, const double *src_tb)
+// Start of one pass of solve() for instances beginning a step:
+// src/solver.f90:60-77.
+__global__ void step_begin_kernel(StepCtl *ctl, const Inst *inst, int B, const double *src_tb)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    ctl->it_count += 1;
-    ctl->accepted = 0;
-    ctl->probe_ier = 0;
-    ctl->x = 0.0;
-    if (ctl->t_try > 10.0) {
-        for (int64_t s = 0; s < nsrc; s++)
-            if (ctl->time < src_tb[s] && ctl->time + ctl->t_try > src_tb[s]) ctl->t_try = 10.0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || ctl[i].phase != PH_NEW) return;
+    StepCtl &c = ctl[i];
+    c.it_count += 1;
+    c.accepted = 0;
+    c.probe_ier = 0;
+    c.step_attempts = 0;
+    c.x = 0.0;
+    if (c.t_try > 10.0) {
+        const Inst &I = inst[i];
+        for (int64_t s = 0; s < I.nsrc; s++) {
+            const double tb = src_tb[I.soff + s];
+            if (c.time < tb && c.time + c.t_try > tb) c.t_try = 10.0;
+        }
     }
 }
 
-__global__ void set_h_kernel(StepCtl *ctl)
+__global__ void set_h_kernel(StepCtl *ctl, int B)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) ctl->h = ctl->t_try;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || ctl[i].phase != PH_NEW) return;
+    ctl[i].h = ctl[i].t_try;
 }
 
-// End of one pass of solve(): src/solver.f90:117-196. The pressure commit
-// compute_P(t_did) equals the stage-5 solve of the accepted attempt
-// (dt = 0 + 1.0*h = t_did), so its result is copied instead of recomputed.
-__global__ void commit_kernel(int64_t N, double *y, const double *yout, double *P, double *Pdot,
-                              const double *Pt5, const double *Pd5, StepCtl *ctl, double t_cap)
+// Accepted attempts: Y = yout, and the pressure commit compute_P(t_did),
+// which equals the stage-5 solve of the accepted attempt (dt = 0 + 1.0*h).
+__global__ void commit_kernel(ElemParams ep, double *y, const double *yout, double *P, double *Pdot,
+                              const double *Ptemp, const double *Pdot_s)
 {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < 3 * N) {
-        double v = yout[i];
-        y[i] = v;
-        if (i >= 2 * N && v > 0.0) atomicCAS(&ctl->status, 0, 3);
-        if (!isfinite(v)) atomicCAS(&ctl->status, 0, 4);
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ep.Ntot) return;
+    const int i = ep.inst_of[e];
+    const StepCtl &c = ep.ctl[i];
+    if (!takes_part(ep.ctl, i, M_ACTIVE) || !c.accepted || c.status != 0) return;
+    const Inst &I = ep.inst[i];
+    const int64_t N = I.N, k = e - I.eoff;
+    double *yi = y + 3 * I.eoff;
+    const double *yo = yout + 3 * I.eoff;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const double v = yo[j * N + k];
+        yi[j * N + k] = v;
+        if (j == 2 && v > 0.0) atomicCAS(&ep.ctl[i].status, 0, 3);
+        if (!isfinite(v)) atomicCAS(&ep.ctl[i].status, 0, 4);
     }
-    if (i < N) {
-        P[i] = Pt5[i];
-        Pdot[i] = Pd5[i];
+    if (!(c.pfail_mask & (1 << 4))) {
+        P[e] = Ptemp[6 * I.eoff + 4 * N + k];
+        Pdot[e] = Pdot_s[6 * I.eoff + 4 * N + k];
     }
-    if (i == 0) {
-        ctl->time = ctl->time + ctl->hdid;
-        double tn = ctl->hnext;
-        if (tn > t_cap) tn = t_cap;
-        ctl->t_try = tn;
-    }
+}
+
+// End of one pass of solve() per instance (src/solver.f90:117-196): time,
+// t_try with the 1-day cap, and the instance's next phase.
+__global__ void finish_kernel(StepCtl *ctl, int B, double t_cap)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || !takes_part(ctl, i, M_ACTIVE)) return;
+    StepCtl &c = ctl[i];
+    if (c.status != 0) { c.phase = PH_DONE; return; }
+    if (!c.accepted) { c.phase = PH_RETRY; return; }
+    c.time = c.time + c.hdid;
+    double tn = c.hnext;
+    if (tn > t_cap) tn = t_cap;
+    c.t_try = tn;
+    c.steps_done += 1;
+    bool done = (c.steps_done >= c.target_steps) || (c.t_end > 0.0 && c.time >= c.t_end);
+    c.phase = done ? PH_DONE : PH_NEW;
+}
+
+// Arms every instance for `nsteps` more accepted steps (or until t_end).
+__global__ void arm_kernel(StepCtl *ctl, int B, long long nsteps, double t_end, int max_attempts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    StepCtl &c = ctl[i];
+    c.steps_done = 0;
+    c.target_steps = nsteps;
+    c.t_end = t_end;
+    c.max_attempts = max_attempts;
+    c.phase = (c.status == 0 && nsteps > 0 && !(t_end > 0.0 && c.time >= t_end)) ? PH_NEW : PH_DONE;
 }
 
 // K.V output for the operator entry point: sum the chunks and scale.

@@ -1,0 +1,100 @@
+"""Many independent fault networks advanced together on one GPU.
+
+``Ensemble`` wraps ``dfn_create_batch``: every network keeps its own state,
+adaptive step size, controller and done flag (the reference's solve() loop
+per network), while each kernel launch covers the whole batch, so networks
+of uneven size share the GPU without per-network launches.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .layout import DfnOptions, DfnProblem, DfnReport, ProblemArrays, build_arrays, to_c
+from .simulation import GEMV, PRESSURE, STORAGE
+from .layout import ptr
+
+
+class Ensemble:
+    def __init__(self, problems, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64):
+        self.lib = _lib.load()
+        self.arrays = [p if isinstance(p, ProblemArrays) else build_arrays(p) for p in problems]
+        if not self.arrays:
+            raise ValueError("an ensemble needs at least one problem")
+        self.B = len(self.arrays)
+        opt = DfnOptions()
+        self.lib.dfn_default_options(ctypes.byref(opt))
+        opt.kernel_storage = STORAGE[storage]
+        opt.pressure_solver = PRESSURE[pressure]
+        opt.device = int(device)
+        opt.gemv_impl = GEMV[gemv]
+        opt.max_attempts = int(max_attempts)
+        self._cs = [to_c(a) for a in self.arrays]
+        arr = (DfnProblem * self.B)(*self._cs)
+        self._arr = arr
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.dfn_create_batch(arr, self.B, ctypes.byref(opt), ctypes.byref(h)), self.lib)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.dfn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: int):
+        _lib.check(self.lib.dfn_set_stream(self.h, ctypes.c_void_p(stream_handle)), self.lib)
+
+    @property
+    def kernel_bytes(self):
+        return int(self.lib.dfn_kernel_bytes(self.h))
+
+    @property
+    def launches(self):
+        return int(self.lib.dfn_launch_count(self.h))
+
+    @property
+    def n_elements(self):
+        return [a.N for a in self.arrays]
+
+    def solve(self, n_steps=0, t_end=0.0, check=True):
+        """Advance every network by n_steps accepted steps, or to time t_end."""
+        reps = (DfnReport * self.B)()
+        st = self.lib.dfn_solve_batch(self.h, int(n_steps), float(t_end), reps)
+        if check:
+            _lib.check(st, self.lib)
+        return [r.as_dict() for r in reps]
+
+    def state(self, i):
+        N = self.arrays[i].N
+        Y, P = np.empty(3 * N), np.empty(N)
+        t, tt, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _lib.check(self.lib.dfn_get_state_instance(self.h, int(i), ptr(Y), ptr(P), ctypes.byref(t),
+                                                   ctypes.byref(tt), ctypes.byref(it)), self.lib)
+        return {"Y": Y, "P": P, "time": t.value, "t_try": tt.value, "it_count": it.value}
+
+    def time_kernel(self, reps=10):
+        ms = ctypes.c_double()
+        _lib.check(self.lib.dfn_time_kernel(self.h, int(reps), ctypes.byref(ms)), self.lib)
+        return ms.value
+
+    def profile_kv(self, enable=True):
+        _lib.check(self.lib.dfn_profile_kv(self.h, 1 if enable else 0), self.lib)
+
+    def profile_kv_read(self):
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        _lib.check(self.lib.dfn_profile_kv_read(self.h, ctypes.byref(ms), ctypes.byref(n)), self.lib)
+        return ms.value, n.value

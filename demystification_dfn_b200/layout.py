@@ -193,7 +193,8 @@ class DfnReport(ctypes.Structure):
     _fields_ = [("it_count", ctypes.c_int64), ("attempts", ctypes.c_int64), ("rejected", ctypes.c_int64),
                 ("rhs_evals", ctypes.c_int64), ("cg_iterations", ctypes.c_int64),
                 ("probe_halvings", ctypes.c_int64), ("time", ctypes.c_double), ("t_try", ctypes.c_double),
-                ("last_hdid", ctypes.c_double), ("status", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("last_hdid", ctypes.c_double), ("status", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("stage_cg_failures", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}

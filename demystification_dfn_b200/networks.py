@@ -182,6 +182,28 @@ def fault_network(n_faults=800, box=7000.0, seed=0, length_range=(50.0, 500.0), 
     return p
 
 
+def ensemble_member(seed, n_faults=None, q_kgs=None, diffusivity=None, ref_faults=800, ref_box=7000.0, **kw):
+    """One realisation of the network ensemble: 100-400 faults drawn like
+    :func:`fault_network` (the box scaled to keep the fault density of 800
+    faults in 7 km x 7 km), one point injection of 10-100 kg/s at the centre
+    of a random fault, and a log-uniform diffusivity in 0.01-1 m^2/s."""
+    rng = np.random.default_rng(10_000 + seed)
+    n = int(rng.integers(100, 401)) if n_faults is None else int(n_faults)
+    q = float(rng.uniform(10.0, 100.0)) if q_kgs is None else float(q_kgs)
+    D = float(np.exp(rng.uniform(np.log(0.01), np.log(1.0)))) if diffusivity is None else float(diffusivity)
+    box = ref_box * np.sqrt(n / ref_faults)
+    # permeability giving diffusivity D with the module's fluid constants
+    perm = D * 0.1 * 1e-3 * (0.9e-8 + 0.1e-8)
+    p = fault_network(n_faults=n, box=box, seed=seed, dP=0.0, permeability=perm, q_kgs=q,
+                      name=f"ensemble_{seed}", **kw)
+    p.diffusivity = D
+    return p
+
+
+def ensemble(count=64, seed0=0, **kw):
+    return [ensemble_member(seed0 + i, **kw) for i in range(count)]
+
+
 def small_network(seed=0, n_faults=4, mode="modeII", **kw):
     """A few-fault network for exhaustive parity tests (N of a few hundred)."""
     kw.setdefault("box", 600.0)

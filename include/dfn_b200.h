@@ -48,7 +48,11 @@ typedef enum dfn_status {
 enum { DFN_MODE_II = 2, DFN_MODE_III = 3 };                    /* hyperparameter/fracture_mode */
 enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter/static_kernel */
 enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2 }; /* stored K entries */
-enum { DFN_PRESSURE_CG = 0, DFN_PRESSURE_TRIDIAG = 1 };         /* pressure solver */
+/* Pressure solver: DFN_PRESSURE_CG is the reference's CG with tree-reduced
+ * dot products; DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
+ * does, reproducing its rounding and iteration counts bit for bit (slower
+ * for large N); DFN_PRESSURE_TRIDIAG solves the same implicit step exactly. */
+enum { DFN_PRESSURE_CG = 0, DFN_PRESSURE_TRIDIAG = 1, DFN_PRESSURE_CG_EXACT = 2 };
 
 /*
  * Problem description: the reference's in-memory state after read_config
@@ -85,7 +89,7 @@ typedef struct dfn_problem {
 /* Options of this implementation (no counterpart in the reference). */
 typedef struct dfn_options {
     int32_t kernel_storage;   /* DFN_STORE_*; FP64 is the plain path */
-    int32_t pressure_solver;  /* DFN_PRESSURE_CG restates the reference; TRIDIAG solves exactly */
+    int32_t pressure_solver;  /* DFN_PRESSURE_* */
     int32_t device;           /* CUDA device ordinal */
     int32_t max_attempts;     /* RK attempts per step scheduled on the device before the host looks (>=1) */
     int32_t gemv_impl;        /* 0 = TMA bulk-copy pipeline, 1 = direct 128-bit loads */
@@ -105,6 +109,8 @@ typedef struct dfn_report {
     double last_hdid;
     int32_t status;
     int32_t pad;
+    int64_t stage_cg_failures; /* stage pressure solves that hit the CG cap (the stage then uses the last
+                                  CG iterate; the reference would use an uninitialised P_temp) */
 } dfn_report;
 
 typedef struct dfn_handle dfn_handle;
@@ -122,6 +128,15 @@ void dfn_default_options(dfn_options *opt);
  * assembles the kernel matrices on the device and sets time/t_try/it_count
  * as solve() does at entry (src/solver.f90:47-56). */
 int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle **out);
+/* A batch of independent networks in one handle (no counterpart in the
+ * reference, which runs one network per process). All networks share the
+ * fracture mode and the options; each keeps its own state, step size,
+ * controller and done flag, and every kernel launch covers the whole batch.
+ * dfn_create(p, ...) is dfn_create_batch(p, 1, ...). The per-network
+ * operator entry points below (kernel, compute_P, friction_law, rkqs,
+ * set_state, snapshot, step_host) need a batch of one. */
+int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_options *opt, dfn_handle **out);
+int32_t dfn_batch_size(const dfn_handle *h);
 int32_t dfn_destroy(dfn_handle *h);
 int32_t dfn_set_stream(dfn_handle *h, void *cuda_stream);
 int64_t dfn_nb_element(const dfn_handle *h);
@@ -160,6 +175,14 @@ int32_t dfn_solve_steps(dfn_handle *h, int64_t n_steps, dfn_report *rep);
 int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, double time_in,
                       double t_try_in, double *V_out, double *theta_out, double *P_out,
                       double *tractionT_out, double *tractionN_out, dfn_report *rep);
+
+/* Advances every network of the batch by n_steps accepted steps of its own
+ * solve() loop, or, when t_end > 0, until its simulated time reaches t_end
+ * (n_steps = 0 then means no step limit). Networks that finish or fail stop
+ * while the others go on. reps (may be NULL) receives one report per network. */
+int32_t dfn_solve_batch(dfn_handle *h, int64_t n_steps, double t_end, dfn_report *reps);
+int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, double *time, double *t_try,
+                               int64_t *it_count);
 
 /* State access. Y has 3N entries. */
 int32_t dfn_get_state(dfn_handle *h, double *Y, double *P, double *time, double *t_try,

@@ -51,7 +51,7 @@ typedef struct orc {
     int kernel_impl; /* 0 matrix-free reference routine, 1 dense stored K */
     int nthreads;
     /* counters */
-    int64_t cg_iters, rhs_evals, attempts, rejected, halvings;
+    int64_t cg_iters, rhs_evals, attempts, rejected, halvings, stage_noconv;
     int last_status;
 } orc;
 
@@ -409,8 +409,19 @@ static void orc_rhs_b1(const orc *o, double dt, const double *diag, double *b1)
     }
 }
 
-/* compute_P: src/fluid_diffusion.f90:24-152. Returns ier. */
+/* compute_P: src/fluid_diffusion.f90:24-152. Returns ier. With stage != 0
+ * (a pressure solve inside a right-hand-side evaluation) a solve that hits
+ * the cap still writes its last iterate: the reference would go on with an
+ * uninitialised P_temp there (undefined), this restatement and the GPU path
+ * both use the last iterate and count the event. */
+static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, int stage);
+
 int orc_compute_P(orc *o, double dt, double *P_temp, double *P_dot)
+{
+    return orc_compute_P_mode(o, dt, P_temp, P_dot, 0);
+}
+
+static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, int stage)
 {
     int64_t N = o->N;
     double *w = (double *)malloc(sizeof(double) * 7 * N);
@@ -445,6 +456,13 @@ int orc_compute_P(orc *o, double dt, double *P_temp, double *P_dot)
         if (it > 200) {
             ier = 1;
             o->cg_iters += it;
+            if (stage) {
+                o->stage_noconv++;
+                for (int64_t k = 0; k < N; k++) {
+                    P_dot[k] = (dt < 1e-9) ? 0.0 : (xk[k] - o->P[k]) / dt;
+                    P_temp[k] = xk[k];
+                }
+            }
             free(w);
             return ier;
         }
@@ -500,7 +518,7 @@ int orc_rhs(orc *o, double dt, const double *Y1, double *Y1dot)
     double *Pt = (double *)malloc(8 * N);
     memset(Pt, 0, 8 * N);
     orc_kernel(o, Y1, o->SigmaT_dot, o->SigmaN_dot);
-    int ier = orc_compute_P(o, dt, Pt, o->Pdot);
+    int ier = orc_compute_P_mode(o, dt, Pt, o->Pdot, 1);
     o->rhs_evals++;
     const double *V = Y1, *psi = Y1 + N, *sig = Y1 + 2 * N;
     for (int64_t k = 0; k < N; k++) {
@@ -698,5 +716,5 @@ void orc_get_last_stress(const orc *o, double *sT, double *sN, double *Pdot)
 void orc_counters(const orc *o, int64_t *c)
 {
     c[0] = o->cg_iters; c[1] = o->rhs_evals; c[2] = o->attempts; c[3] = o->rejected; c[4] = o->halvings;
-    c[5] = o->it_count;
+    c[5] = o->it_count; c[6] = o->stage_noconv;
 }

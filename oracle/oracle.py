@@ -181,6 +181,7 @@ class Oracle:
         return sT, sN, Pd
 
     def counters(self):
-        c = (ctypes.c_int64 * 6)()
+        c = (ctypes.c_int64 * 7)()
         self.lib.orc_counters(self.o, c)
-        return dict(zip(["cg_iters", "rhs_evals", "attempts", "rejected", "halvings", "it_count"], list(c)))
+        return dict(zip(["cg_iters", "rhs_evals", "attempts", "rejected", "halvings", "it_count", "stage_noconv"],
+                        list(c)))

@@ -1,0 +1,95 @@
+"""Batched networks: one handle, one launch per kernel for the whole batch,
+per-network step control. A network inside a batch must follow exactly the
+trajectory it follows alone (same kernels, same per-network arithmetic)."""
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from demystification_dfn_b200 import networks
+from demystification_dfn_b200.ensemble import Ensemble
+from demystification_dfn_b200.simulation import Simulation
+
+pytestmark = pytest.mark.gpu
+
+
+def members(mode="modeII"):
+    # uneven sizes, different injection and diffusivity
+    return [networks.small_network(seed=s, n_faults=n, mode=mode, tol=1e-6, q_kgs=q)
+            for s, n, q in ((21, 3, 20.0), (22, 6, None), (23, 4, 60.0))]
+
+
+@pytest.mark.parametrize("pressure", ["cg", "tridiag"])
+def test_batch_equals_separate_runs_bitwise(pressure):
+    ps = members()
+    with Ensemble(ps, pressure=pressure) as ens:
+        reps = ens.solve(n_steps=15)
+        assert all(r["status"] == 0 for r in reps)
+        for i, p in enumerate(ps):
+            with Simulation(p, pressure=pressure) as s:
+                s.solve_steps(15)
+                a, b = ens.state(i), s.state()
+                assert a["it_count"] == b["it_count"] == 15
+                assert a["time"] == b["time"]
+                assert np.array_equal(a["Y"], b["Y"]) and np.array_equal(a["P"], b["P"])
+
+
+def test_batch_member_matches_oracle():
+    """Network 1 stalls the reference CG at its 200-iteration cap from step
+    13 on (the probe halves t_try there), where an ulp decides the halving;
+    the first 12 steps are compared, with the bitwise reference CG."""
+    ps = members()
+    with Ensemble(ps, pressure="cg_exact") as ens:
+        ens.solve(n_steps=12)
+        o = Oracle(ps[1])
+        o.use_dense()
+        st, _ = o.solve_steps(12)
+        assert st == 0
+        g, r = ens.state(1), o.state()
+        N = len(r["P"])
+        assert abs(g["time"] - r["time"]) <= 1e-8 * r["time"]
+        assert np.abs(g["Y"][:N] - r["Y"][:N]).max() <= 1e-8 * np.abs(r["Y"][:N]).max()
+
+
+def test_batch_runs_to_t_end_with_done_masks():
+    ps = members()
+    t_end = 3000.0
+    with Ensemble(ps, pressure="tridiag") as ens:
+        reps = ens.solve(t_end=t_end)
+        for i, r in enumerate(reps):
+            assert r["status"] == 0
+            st = ens.state(i)
+            assert st["time"] >= t_end
+            # the last accepted step crossed t_end
+            assert st["time"] - r["last_hdid"] < t_end
+        # networks stopped independently: different step counts
+        assert len({r["it_count"] for r in reps}) > 1
+
+
+def test_stage_cg_cap_policy_matches_oracle():
+    """Network 1 drives the reference CG to its cap inside RK stages; the
+    GPU and the oracle both go on with the last CG iterate (the reference's
+    P_temp is undefined there) and both finish the steps."""
+    p = members()[1]
+    o = Oracle(p)
+    o.use_dense()
+    st, _ = o.solve_steps(20)
+    with Simulation(p, pressure="cg_exact") as s:
+        rep = s.solve_steps(20)
+    assert st == 0 and rep["status"] == 0
+    assert rep["it_count"] == 20
+
+
+def test_ensemble_members_run():
+    ps = networks.ensemble(4)
+    with Ensemble(ps, pressure="cg") as ens:
+        reps = ens.solve(n_steps=5, check=False)
+        for r in reps:
+            assert r["status"] == 0, r
+            assert r["it_count"] == 5
+
+
+def test_mode3_batch():
+    ps = members("modeIII")
+    with Ensemble(ps, pressure="cg", storage="fp32") as ens:
+        reps = ens.solve(n_steps=10)
+        assert all(r["status"] == 0 and r["it_count"] == 10 for r in reps)

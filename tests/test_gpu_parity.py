@@ -81,6 +81,21 @@ def test_pressure_cg_matches_oracle(dt):
         assert np.abs(gP - ex).max() < 1e3 * 1e-6
 
 
+@pytest.mark.parametrize("dt", [1.0, 100.0, 1000.0, 5000.0])
+def test_pressure_cg_exact_is_bitwise_reference_cg(dt):
+    """Sequential dot products and the reference's operand order: the same
+    iterates, the same iteration count, the same ier as the oracle (on this
+    network CG stalls at dt = 1000 and 5000 s, as in the reference)."""
+    p = net(seed=22, n=6, tol=1e-6)
+    o = Oracle(p)
+    with Simulation(p, pressure="cg_exact") as s:
+        gP, gd, gi = s.compute_P(dt)
+        oP, od, oi = o.compute_P(dt)
+        assert gi == oi
+        if oi == 0:
+            assert np.array_equal(gP, oP) and np.array_equal(gd, od)
+
+
 def test_pressure_cg_nonconvergence_sets_ier():
     p = networks.single_fault(n_el=400, length=4000.0, mode="modeIII", tol=1e-14)
     with Simulation(p, pressure="cg") as s:
@@ -138,7 +153,7 @@ def test_rkqs_matches_oracle():
         assert rel(gy, oy) < 1e-10
 
 
-@pytest.mark.parametrize("pressure", ["cg", "tridiag"])
+@pytest.mark.parametrize("pressure", ["cg", "cg_exact", "tridiag"])
 def test_solve_steps_match_oracle(pressure):
     p = net(seed=9, n=4, tol=1e-6)
     o = Oracle(p)
@@ -161,7 +176,7 @@ def test_single_fault_injection_run_matches_oracle():
     p = networks.single_fault(n_el=500, length=5000.0, mode="modeII", tol=1e-6)
     o = Oracle(p, threads=8)
     o.use_dense()
-    with Simulation(p, pressure="cg") as s:
+    with Simulation(p, pressure="cg_exact") as s:
         rep = s.solve_steps(30)
         st, _ = o.solve_steps(30)
         g, r = s.state(), o.state()
@@ -207,7 +222,7 @@ def test_reference_shipped_problems(tag, steps):
     p = refconfigs.problem(tag)
     o = Oracle(p, threads=8)
     o.use_dense()
-    with Simulation(p, pressure="cg") as s:
+    with Simulation(p, pressure="cg_exact") as s:
         rep = s.solve_steps(steps)
         st, _ = o.solve_steps(steps)
         assert st == 0 and rep["status"] == 0
