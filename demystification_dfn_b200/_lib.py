@@ -72,7 +72,9 @@ def load():
         "dfn_launch_count": (i64, [P]),
         "dfn_profile_kv": (i32, [P, i32]),
         "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
-        "dfn_create_batch": (i32, [ctypes.POINTER(DfnProblem), i32, ctypes.POINTER(DfnOptions), ctypes.POINTER(P)]),
+        "dfn_hmat_stats": (i32, [P, ctypes.POINTER(i64)]),
+        "dfn_hmat_perm": (i32, [P, ctypes.POINTER(i32)]),
+        "dfn_create_batch":(i32, [ctypes.POINTER(DfnProblem), i32, ctypes.POINTER(DfnOptions), ctypes.POINTER(P)]),
         "dfn_batch_size": (i32, [P]),
         "dfn_solve_batch": (i32, [P, i64, dbl, ctypes.POINTER(DfnReport)]),
         "dfn_get_state_instance": (i32, [P, i32, dp, dp, dp, dp, ctypes.POINTER(i64)]),

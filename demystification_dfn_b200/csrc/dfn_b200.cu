@@ -12,6 +12,7 @@
 // and reads the controllers only between groups of rounds.
 #include "../../include/dfn_b200.h"
 #include "dfn_device.cuh"
+#include "hmat_device.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -54,6 +55,8 @@ void set_err(const char *what, cudaError_t e, const char *file, int line)
         int s_ = (x);                \
         if (s_ != DFN_OK) return s_; \
     } while (0)
+
+unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 int bytes_per_col(int mode, int store)
 {
@@ -99,6 +102,18 @@ struct dfn_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     PressGlobal pg{};
+    // H-matrix representation (static_kernel = hmatrix)
+    bool hmat = false;
+    int ncomp = 1;                        // 2 in mode II (shear and normal), 1 in mode III
+    HBlk *hblk = nullptr;
+    HTask *ht1 = nullptr, *ht2 = nullptr;
+    int64_t hn1 = 0, hn2 = 0, hn1_0 = 0, hn2_0 = 0;
+    void *hvals = nullptr;
+    int *hperm = nullptr;
+    int64_t *hrowptr = nullptr, *hslots = nullptr;
+    double *hz = nullptr, *hout = nullptr;
+    std::vector<int> hranks;              // rank of every low-rank leaf (report)
+    int64_t hdense_vals = 0, hlr_vals = 0, hblocks = 0;
     // K.V launch timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -140,14 +155,50 @@ static gemv_tma_fn pick_gemv_tma(int mode, int store)
 
 static const size_t kTmaSmem = TMA_STAGES * GEMV_CHUNK_BYTES + 2 * TMA_STAGES * sizeof(uint64_t);
 
-// K.V over the first `ntiles` tiles (all networks, or network 0 only);
+// H-matrix K.V: low-rank products, leaf rows, fixed-order row gather.
+static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, bool only0)
+{
+    const int64_t n1 = only0 ? h->hn1_0 : h->hn1, n2 = only0 ? h->hn2_0 : h->hn2;
+    const int64_t ne = only0 ? h->hinst[0].N : h->Ntot;
+    if (n1 > 0) {
+        if (h->store == 0)
+            hm_lowrank_kernel<double><<<(unsigned)n1, 256, 0, h->stream>>>(
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hperm, Vbase, vmul, h->hz);
+        else
+            hm_lowrank_kernel<float><<<(unsigned)n1, 256, 0, h->stream>>>(
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hperm, Vbase, vmul, h->hz);
+        h->launches++;
+        CKL();
+    }
+    if (h->store == 0)
+        hm_rows_kernel<double><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                    (const double *)h->hvals, h->hperm, Vbase, vmul,
+                                                                    h->hz, h->hout);
+    else
+        hm_rows_kernel<float><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                   (const float *)h->hvals, h->hperm, Vbase, vmul,
+                                                                   h->hz, h->hout);
+    h->launches++;
+    CKL();
+    hm_gather_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->ncomp, h->inst_of, h->inst, h->ctl, mask,
+                                                                h->hperm, h->hrowptr, h->hslots, h->hout, h->partT,
+                                                                h->partN);
+    h->launches++;
+    CKL();
+    return DFN_OK;
+}
+
+// K.V of all networks (only0 = false) or of network 0 (only0 = true);
 // V of network i is Vbase[vmul*eoff_i + l].
-static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, int64_t ntiles)
+static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, bool only0)
 {
     const bool rec = h->prof && h->pcount < kProfMax;
     if (rec) CK(cudaEventRecord(h->pev[2 * h->pcount], h->stream));
     const uint4 *K = static_cast<const uint4 *>(h->K);
-    if (h->gemv_impl == 0) {
+    const int64_t ntiles = only0 ? h->ntiles0 : h->ntiles;
+    if (h->hmat) {
+        TRY(launch_hmat(h, mask, Vbase, vmul, only0));
+    } else if (h->gemv_impl == 0) {
         gemv_tma_fn fn = pick_gemv_tma(h->mode, h->store);
         fn<<<(unsigned)ntiles, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(
             h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul, h->partT, h->partN, h->err_flag);
@@ -212,7 +263,6 @@ static ElemParams elem_params(dfn_handle *h)
     return ep;
 }
 
-static unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // One RK attempt (stages 2..6 and the error test) of every network in `mask`.
 static int run_attempt(dfn_handle *h, int mask)
@@ -223,7 +273,7 @@ static int run_attempt(dfn_handle *h, int mask)
     CKL();
     TRY(launch_pressure(h, mask, 1, 1, 5, 0.0, h->B));
     for (int s = 2; s <= 6; s++) {
-        TRY(launch_gemv(h, mask, h->ytmp, 3, h->ntiles));
+        TRY(launch_gemv(h, mask, h->ytmp, 3, false));
         TRY(launch_friction(h, s, s - 1, mask, h->Ntot));
     }
     decide_kernel<<<blocks_of(h->B, 128), 128, 0, h->stream>>>(h->ctl, h->B, mask);
@@ -242,7 +292,7 @@ static int run_round(dfn_handle *h)
     // CG probe at t_try (halving on non-convergence); its solution is the
     // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
     TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
-    TRY(launch_gemv(h, M_NEW, h->Y, 3, h->ntiles));
+    TRY(launch_gemv(h, M_NEW, h->Y, 3, false));
     TRY(launch_friction(h, 1, 0, M_NEW, h->Ntot));
     set_h_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B);
     h->launches++;
@@ -326,6 +376,158 @@ static void fill_report(const StepCtl &c, dfn_report *r)
     r->last_hdid = c.hdid; r->status = c.status; r->pad = 0; r->stage_cg_failures = c.stage_noconv;
 }
 
+// ---------------------------------------------------------------------------
+// H-matrix construction on the host (setup) and upload: hmat_build.h builds
+// the cluster tree, the block leaves and the factors of each network from
+// the element geometry the device computed; entries are the same formulas
+// as the dense assembly (entry_mode2/entry_mode3).
+struct HostLeaf {
+    int dense, rank;
+    std::vector<double> F, A, B;   // row-major F (nr x nc), A (nr x rank), B (nc x rank)
+};
+
+static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_options &opt)
+{
+    const int leaf = opt.hmat_leaf > 0 ? opt.hmat_leaf : 100;
+    const double eta = opt.hmat_eta > 0 ? opt.hmat_eta : 3.0;
+    const double eps = opt.hmat_eps > 0 ? opt.hmat_eps : 1e-8;
+    const int B = h->B, nc = h->ncomp;
+    const int64_t Nt = h->Ntot;
+    std::vector<double> el(2 * Nt), tn(2 * Nt), nr(2 * Nt), nd(2 * (Nt + B));
+    CK(cudaMemcpy(el.data(), h->elem, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tn.data(), h->tan, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nr.data(), h->nrm, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nd.data(), h->node, sizeof(double) * 2 * (Nt + B), cudaMemcpyDeviceToHost));
+
+    std::vector<int> perm(Nt);
+    std::vector<HBlk> blks;
+    std::vector<HTask> t1, t2;
+    std::vector<double> vals;
+    int64_t zoff = 0, slot = 0;
+    // row contributions: per component, per global position, slot indices
+    std::vector<std::vector<int64_t>> rows((size_t)nc * Nt);
+    for (int i = 0; i < B; i++) {
+        const Inst &I = h->hinst[i];
+        const int64_t e0 = I.eoff, N = I.N;
+        const double *E = el.data() + 2 * e0, *T = tn.data() + 2 * e0, *R = nr.data() + 2 * e0,
+                     *D = nd.data() + 2 * (e0 + i);
+        hmat::Tree tree = hmat::build_tree(E, (int)N, leaf);
+        for (int64_t p = 0; p < N; p++) perm[e0 + p] = tree.perm[p];
+        std::vector<hmat::Block> leaves;
+        hmat::build_blocks(tree, hmat::boxes(tree, E), eta, 0, 0, leaves);
+        for (int c = 0; c < nc; c++) {
+            auto entry = [&](int64_t k, int64_t l) -> double {
+                if (h->mode == DFN_MODE_III)
+                    return entry_mode3(E[2 * k], E[2 * k + 1], T[2 * k], T[2 * k + 1], D[2 * l], D[2 * l + 1],
+                                       D[2 * l + 2], D[2 * l + 3]);
+                double kt, kn;
+                entry_mode2(E[2 * k], E[2 * k + 1], R[2 * k], R[2 * k + 1], D[2 * l], D[2 * l + 1], D[2 * l + 2],
+                            D[2 * l + 3], R[2 * l], R[2 * l + 1], kt, kn);
+                return c == 0 ? kt : kn;
+            };
+            std::vector<HostLeaf> host(leaves.size());
+#pragma omp parallel for schedule(dynamic, 4)
+            for (int64_t b = 0; b < (int64_t)leaves.size(); b++) {
+                const hmat::Block &L = leaves[b];
+                HostLeaf &H = host[b];
+                auto ent = [&](int ii, int jj) { return entry(tree.perm[L.r0 + ii], tree.perm[L.c0 + jj]); };
+                int rank = -1;
+                std::vector<double> A, Bm;
+                if (!L.dense) {
+                    rank = hmat::aca_partial(L.nr, L.nc, ent, eps, hmat::kMaxRank, A, Bm);
+                    if (rank >= 0) rank = hmat::recompress(L.nr, L.nc, rank, eps, A, Bm);
+                    if (rank > hmat::kMaxRank) rank = -1;
+                }
+                if (rank < 0) {   // dense leaf, or low-rank leaf whose ACA did not converge
+                    H.dense = 1;
+                    H.rank = 0;
+                    H.F.resize((size_t)L.nr * L.nc);
+                    for (int ii = 0; ii < L.nr; ii++)
+                        for (int jj = 0; jj < L.nc; jj++) H.F[(size_t)ii * L.nc + jj] = ent(ii, jj);
+                } else {
+                    H.dense = 0;
+                    H.rank = rank;
+                    H.A.resize((size_t)L.nr * rank);
+                    H.B.resize((size_t)L.nc * rank);
+                    for (int q = 0; q < rank; q++) {
+                        for (int ii = 0; ii < L.nr; ii++) H.A[(size_t)ii * rank + q] = A[(size_t)q * L.nr + ii];
+                        for (int jj = 0; jj < L.nc; jj++) H.B[(size_t)jj * rank + q] = Bm[(size_t)q * L.nc + jj];
+                    }
+                }
+            }
+            for (size_t b = 0; b < leaves.size(); b++) {
+                const hmat::Block &L = leaves[b];
+                HostLeaf &H = host[b];
+                if (H.rank == 0 && !H.dense) continue;   // zero block
+                HBlk hb{};
+                hb.inst = i; hb.comp = c; hb.dense = H.dense; hb.rank = H.rank;
+                hb.r0 = L.r0; hb.nr = L.nr; hb.c0 = L.c0; hb.nc = L.nc;
+                hb.outoff = slot;
+                hb.foff = (int64_t)vals.size();
+                if (H.dense) {
+                    vals.insert(vals.end(), H.F.begin(), H.F.end());
+                    h->hdense_vals += (int64_t)H.F.size();
+                } else {
+                    vals.insert(vals.end(), H.A.begin(), H.A.end());
+                    hb.goff = (int64_t)vals.size();
+                    vals.insert(vals.end(), H.B.begin(), H.B.end());
+                    hb.zoff = zoff;
+                    hb.ntask1 = (L.nc + HM_COLS - 1) / HM_COLS;
+                    zoff += (int64_t)hb.ntask1 * H.rank;
+                    h->hlr_vals += (int64_t)(H.A.size() + H.B.size());
+                    h->hranks.push_back(H.rank);
+                }
+                const int bi = (int)blks.size();
+                blks.push_back(hb);
+                if (!H.dense)
+                    for (int j = 0; j < hb.ntask1; j++)
+                        t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
+                for (int r = 0; r < L.nr; r += HM_ROWS) t2.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
+                for (int r = 0; r < L.nr; r++) rows[(size_t)c * Nt + e0 + L.r0 + r].push_back(slot + r);
+                slot += L.nr;
+            }
+        }
+        if (i == 0) {
+            h->hn1_0 = (int64_t)t1.size();
+            h->hn2_0 = (int64_t)t2.size();
+        }
+    }
+    // tasks must list network 0 first for the operator entry points; they
+    // do, since networks are built in order. Row slot lists (CSR).
+    std::vector<int64_t> rowptr((size_t)nc * Nt + 1, 0), slots;
+    for (size_t q = 0; q < rows.size(); q++) {
+        rowptr[q + 1] = rowptr[q] + (int64_t)rows[q].size();
+        slots.insert(slots.end(), rows[q].begin(), rows[q].end());
+    }
+    h->hn1 = (int64_t)t1.size();
+    h->hn2 = (int64_t)t2.size();
+    h->hblocks = (int64_t)blks.size();
+    const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
+    h->kv_bytes = (int64_t)(vals.size() * vsz);
+    CK(cudaMalloc(&h->hvals, std::max<size_t>(vals.size(), 1) * vsz));
+    if (h->store == DFN_STORE_FP64) {
+        CK(cudaMemcpy(h->hvals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(vals.begin(), vals.end());
+        CK(cudaMemcpy(h->hvals, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc((void **)&h->hblk, std::max<size_t>(blks.size(), 1) * sizeof(HBlk)));
+    CK(cudaMemcpy(h->hblk, blks.data(), blks.size() * sizeof(HBlk), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->ht1, std::max<size_t>(t1.size(), 1) * sizeof(HTask)));
+    if (!t1.empty()) CK(cudaMemcpy(h->ht1, t1.data(), t1.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->ht2, std::max<size_t>(t2.size(), 1) * sizeof(HTask)));
+    CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
+    CK(cudaMemcpy(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hrowptr, sizeof(int64_t) * rowptr.size()));
+    CK(cudaMemcpy(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
+    CK(cudaMemcpy(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hz, sizeof(double) * std::max<int64_t>(zoff, 1)));
+    CK(cudaMalloc((void **)&h->hout, sizeof(double) * std::max<int64_t>(slot, 1)));
+    return DFN_OK;
+}
+
 static int single_only(const dfn_handle *h)
 {
     if (h->B != 1) {
@@ -376,7 +578,8 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->node, h->elem, h->ds, h->tan,
+    void *ptrs[] = {h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
+                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
                     h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
@@ -478,6 +681,21 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     h->max_attempts = opt.max_attempts > 0 ? opt.max_attempts : 64;
     const int bpc = bytes_per_col(h->mode, h->store);
     const int64_t CW = GEMV_CHUNK_BYTES / bpc;
+    // static_kernel selects the dense kernel ("direct") or the H-matrix
+    // ("hmatrix"), as kernel_ptr does in src/initialisation.f90:105-128
+    h->hmat = probs[0].static_kernel == DFN_KERNEL_HMATRIX;
+    for (int i = 1; i < count; i++)
+        if ((probs[i].static_kernel == DFN_KERNEL_HMATRIX) != h->hmat) {
+            g_err = "all networks of a batch need the same static_kernel";
+            dfn_destroy(h);
+            return DFN_ERR_ARG;
+        }
+    if (h->hmat && h->store == DFN_STORE_BF16X2) {
+        g_err = "the H-matrix path stores FP64 or FP32 factors";
+        dfn_destroy(h);
+        return DFN_ERR_UNSUPPORTED;
+    }
+    h->ncomp = (h->mode == DFN_MODE_II) ? 2 : 1;
 
     // instance table
     int64_t eoff = 0, kvec = 0, poff = 0, soff = 0;
@@ -486,9 +704,9 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         const dfn_problem &p = probs[i];
         Inst &I = h->hinst[i];
         I.N = p.nb_element;
-        I.Np = ((I.N + CW - 1) / CW) * CW;
+        I.Np = h->hmat ? I.N : ((I.N + CW - 1) / CW) * CW;
         I.eoff = eoff;
-        I.nchunk = I.Np / CW;
+        I.nchunk = h->hmat ? 1 : I.Np / CW;
         I.kvec = kvec;
         I.poff = poff;
         I.soff = soff;
@@ -499,10 +717,10 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         I.porosity = p.porosity; I.dyn_visc = p.dyn_viscosity; I.comp = p.fluid_comp + p.rock_comp;
         I.tol = p.tol_solver;
         eoff += I.N;
-        kvec += I.N * I.Np * bpc / 16;
+        if (!h->hmat) kvec += I.N * I.Np * bpc / 16;
         poff += I.nchunk * I.N;
         soff += I.nsrc;
-        h->kv_bytes += I.N * I.N * bpc;
+        if (!h->hmat) h->kv_bytes += I.N * I.N * bpc;
     }
     const int64_t Nt = eoff;
     h->Ntot = Nt;
@@ -595,9 +813,16 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         HCOPY(h->seg_inst, sinst.data(), sinst.size());
     }
 
+    if (h->hmat) {
+        const int st = build_hmatrix(h, probs, opt);
+        if (st != DFN_OK) {
+            dfn_destroy(h);
+            return st;
+        }
+    }
     // dense kernel matrices, one per network
-    h->K_bytes = (size_t)kvec * 16;
-    {
+    h->K_bytes = (size_t)std::max<int64_t>(kvec, 1) * 16;
+    if (!h->hmat) {
         cudaError_t e = cudaMalloc(&h->K, h->K_bytes);
         if (e != cudaSuccess) {
             set_err("cudaMalloc K", e, __FILE__, __LINE__);
@@ -606,7 +831,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
     }
     std::vector<int4> tiles;
-    for (int i = 0; i < count; i++) {
+    for (int i = 0; i < count && !h->hmat; i++) {
         const Inst &I = h->hinst[i];
         const int64_t e0 = I.eoff;
         void *Ki = static_cast<unsigned char *>(h->K) + I.kvec * 16;
@@ -628,7 +853,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     }
     h->ntiles = (int64_t)tiles.size();
     DALLOC(h->tiles, tiles.size());
-    HCOPY(h->tiles, tiles.data(), tiles.size());
+    if (!tiles.empty()) HCOPY(h->tiles, tiles.data(), tiles.size());
     // TMA pipeline needs the dynamic shared memory opt-in
     {
         gemv_tma_fn fns[6] = {gemv_tma_kernel<2, 0>, gemv_tma_kernel<2, 1>, gemv_tma_kernel<2, 2>,
@@ -682,7 +907,7 @@ int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_sT, dou
     TRY(single_only(h));
     CK(cudaSetDevice(h->dev));
     const Inst &I = h->hinst[0];
-    TRY(launch_gemv(h, M_ALL, d_slip, 1, h->ntiles0));
+    TRY(launch_gemv(h, M_ALL, d_slip, 1, true));
     kv_finish_kernel<<<blocks_of(I.N, 256), 256, 0, h->stream>>>(I.N, h->mode, (int)I.nchunk, I.prefT, h->partT,
                                                                  h->partN, d_sT, d_sN);
     h->launches++;
@@ -738,7 +963,7 @@ int32_t dfn_friction_law(dfn_handle *h, double x, int64_t nv, const double *Y, d
     TRY(reset_status0(h));
     CK(cudaMemcpyAsync(h->ytmp, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
     TRY(launch_pressure(h, M_ALL, 2, 0, 1, x, 1));
-    TRY(launch_gemv(h, M_ALL, h->ytmp, 3, h->ntiles0));
+    TRY(launch_gemv(h, M_ALL, h->ytmp, 3, true));
     TRY(launch_friction(h, 0, 0, M_ALL, N));
     CK(cudaMemcpyAsync(Ydot, h->kbuf, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync_ctl(h));
@@ -979,6 +1204,27 @@ int32_t dfn_compute_P_noalloc(int64_t N, double dt, double time, const double *d
     return DFN_OK;
 }
 
+int32_t dfn_hmat_stats(const dfn_handle *h, int64_t *st)
+{
+    if (!h || !st) return DFN_ERR_ARG;
+    if (!h->hmat) { g_err = "handle uses the dense kernel"; return DFN_ERR_UNSUPPORTED; }
+    const int64_t nlr = (int64_t)h->hranks.size();
+    int64_t mx = 0, sum = 0;
+    for (int r : h->hranks) { mx = std::max<int64_t>(mx, r); sum += r; }
+    st[0] = h->hblocks; st[1] = h->hblocks - nlr; st[2] = nlr; st[3] = mx;
+    st[4] = nlr ? (1000 * sum) / nlr : 0;
+    st[5] = h->hdense_vals + h->hlr_vals; st[6] = h->hdense_vals; st[7] = h->hlr_vals;
+    return DFN_OK;
+}
+
+int32_t dfn_hmat_perm(const dfn_handle *h, int32_t *perm)
+{
+    if (!h || !perm) return DFN_ERR_ARG;
+    if (!h->hmat) { g_err = "handle uses the dense kernel"; return DFN_ERR_UNSUPPORTED; }
+    CK(cudaMemcpy(perm, h->hperm, sizeof(int) * h->hinst[0].N, cudaMemcpyDeviceToHost));
+    return DFN_OK;
+}
+
 int32_t dfn_profile_kv(dfn_handle *h, int32_t enable)
 {
     if (!h) return DFN_ERR_ARG;
@@ -1012,9 +1258,9 @@ int32_t dfn_time_kernel(dfn_handle *h, int32_t reps, double *ms)
 {
     if (!h || reps < 1 || !ms) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
-    TRY(launch_gemv(h, M_ALL, h->Y, 3, h->ntiles));
+    TRY(launch_gemv(h, M_ALL, h->Y, 3, false));
     CK(cudaEventRecord(h->ev0, h->stream));
-    for (int i = 0; i < reps; i++) TRY(launch_gemv(h, M_ALL, h->Y, 3, h->ntiles));
+    for (int i = 0; i < reps; i++) TRY(launch_gemv(h, M_ALL, h->Y, 3, false));
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     float t = 0.f;

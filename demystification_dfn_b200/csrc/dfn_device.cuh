@@ -178,7 +178,7 @@ template <> struct KFmt<3, 2> { static constexpr int BPC = 4; };
 
 // Entry formulas: src/hmatrix/eval_kernel_hmatrix.f90:36-47 (mode III),
 // :91-115 (mode II shear), :160-195 (mode II normal).
-__device__ __forceinline__ double entry_mode3(double e1, double e2, double t1, double t2, double xl, double yl,
+__host__ __device__ inline double entry_mode3(double e1, double e2, double t1, double t2, double xl, double yl,
                                               double xr, double yr)
 {
     double ax = xl - e1, ay = yl - e2, bx = xr - e1, by = yr - e2;
@@ -189,7 +189,7 @@ __device__ __forceinline__ double entry_mode3(double e1, double e2, double t1, d
     return -I1 + I2;
 }
 
-__device__ __forceinline__ void entry_mode2(double e1, double e2, double n1, double n2, double xl, double yl,
+__host__ __device__ inline void entry_mode2(double e1, double e2, double n1, double n2, double xl, double yl,
                                             double xr, double yr, double nl1, double nl2, double &T, double &Nn)
 {
     double dxl = e1 - xl, dyl = e2 - yl, dxr = e1 - xr, dyr = e2 - yr;

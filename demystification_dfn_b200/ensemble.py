@@ -12,25 +12,19 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .layout import DfnOptions, DfnProblem, DfnReport, ProblemArrays, build_arrays, to_c
-from .simulation import GEMV, PRESSURE, STORAGE
-from .layout import ptr
+from .layout import DfnProblem, DfnReport, ProblemArrays, build_arrays, ptr, to_c
+from .simulation import make_options
 
 
 class Ensemble:
-    def __init__(self, problems, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64):
+    def __init__(self, problems, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
+                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0):
         self.lib = _lib.load()
         self.arrays = [p if isinstance(p, ProblemArrays) else build_arrays(p) for p in problems]
         if not self.arrays:
             raise ValueError("an ensemble needs at least one problem")
         self.B = len(self.arrays)
-        opt = DfnOptions()
-        self.lib.dfn_default_options(ctypes.byref(opt))
-        opt.kernel_storage = STORAGE[storage]
-        opt.pressure_solver = PRESSURE[pressure]
-        opt.device = int(device)
-        opt.gemv_impl = GEMV[gemv]
-        opt.max_attempts = int(max_attempts)
+        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps)
         self._cs = [to_c(a) for a in self.arrays]
         arr = (DfnProblem * self.B)(*self._cs)
         self._arr = arr

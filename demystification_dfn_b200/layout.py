@@ -186,7 +186,8 @@ class DfnProblem(ctypes.Structure):
 class DfnOptions(ctypes.Structure):
     _fields_ = [("kernel_storage", ctypes.c_int32), ("pressure_solver", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
-                ("gemv_impl", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("gemv_impl", ctypes.c_int32), ("hmat_leaf", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("hmat_eta", ctypes.c_double), ("hmat_eps", ctypes.c_double)]
 
 
 class DfnReport(ctypes.Structure):

@@ -55,12 +55,12 @@ def diffusivity(problem, permeability):
 
 def single_fault(n_el=4000, length=40e3, mode="modeII", a=0.007, b=0.005, Dc=4e-3, f0=0.6, V0=1e-6,
                  sigmaN=-50e6, V_init=1e-12, q_kgs=50.0, t_inj=(0.0, YEAR), permeability=1e-13,
-                 tol=1e-8, max_it=10, name="single_fault"):
+                 tol=1e-8, max_it=10, name="single_fault", kernel="direct"):
     p = DemystiFicatioN(1)
     hp = p.hyperparameter
     hp.simulation_name = name
     hp.fracture_mode = mode
-    hp.static_kernel = "direct"
+    hp.static_kernel = kernel
     hp.friction_law = "RateStateAging"
     hp.tol_solver = tol
     hp.freq_writing_file = 1000
@@ -116,7 +116,7 @@ def _seg_dist(p1, p2, q1, q2):
 def fault_network(n_faults=800, box=7000.0, seed=0, length_range=(50.0, 500.0), strike_deg=(30.0, 10.0),
                   ds=10.0, a=0.010, b=0.015, noise=0.10, Dc=1e-3, f0=0.6, V0=1e-6, sigmaN=-50e6, V_init=1e-12,
                   dP=10e6, permeability=1e-13, mode="modeII", tol=1e-8, max_it=10, min_gap=None,
-                  q_kgs=None, name=None):
+                  q_kgs=None, name=None, kernel="direct"):
     """Seeded random fault network (see module docstring)."""
     rng = np.random.default_rng(seed)
     gap = ds if min_gap is None else min_gap
@@ -143,7 +143,7 @@ def fault_network(n_faults=800, box=7000.0, seed=0, length_range=(50.0, 500.0), 
     hp = p.hyperparameter
     hp.simulation_name = name or f"network_{n_faults}_seed{seed}"
     hp.fracture_mode = mode
-    hp.static_kernel = "direct"
+    hp.static_kernel = kernel
     hp.friction_law = "RateStateAging"
     hp.tol_solver = tol
     hp.freq_writing_file = 1000

@@ -28,18 +28,30 @@ PRESSURE = {"cg": 0, "tridiag": 1, "cg_exact": 2}
 GEMV = {"tma": 0, "ldg": 1}
 
 
+def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64, hmat_leaf=0,
+                 hmat_eta=0.0, hmat_eps=0.0):
+    """dfn_options; the H-matrix parameters default (0) to the reference's
+    nleaf=100, eta=3, eps_ACA=1e-8 (src/variables.f90:122-124)."""
+    opt = DfnOptions()
+    lib.dfn_default_options(ctypes.byref(opt))
+    opt.kernel_storage = STORAGE[storage]
+    opt.pressure_solver = PRESSURE[pressure]
+    opt.device = int(device)
+    opt.gemv_impl = GEMV[gemv]
+    opt.max_attempts = int(max_attempts)
+    opt.hmat_leaf = int(hmat_leaf)
+    opt.hmat_eta = float(hmat_eta)
+    opt.hmat_eps = float(hmat_eps)
+    return opt
+
+
 class Simulation:
-    def __init__(self, problem, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64):
+    def __init__(self, problem, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
+                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0):
         self.lib = _lib.load()
         self.arrays = problem if isinstance(problem, ProblemArrays) else build_arrays(problem)
         self.N = self.arrays.N
-        opt = DfnOptions()
-        self.lib.dfn_default_options(ctypes.byref(opt))
-        opt.kernel_storage = STORAGE[storage]
-        opt.pressure_solver = PRESSURE[pressure]
-        opt.device = int(device)
-        opt.gemv_impl = GEMV[gemv]
-        opt.max_attempts = int(max_attempts)
+        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps)
         self.options = {"storage": storage, "pressure": pressure, "gemv": gemv}
         self._c = to_c(self.arrays)
         h = ctypes.c_void_p()
@@ -147,6 +159,18 @@ class Simulation:
         ms = ctypes.c_double()
         _lib.check(self.lib.dfn_time_kernel(self.h, int(reps), ctypes.byref(ms)), self.lib)
         return ms.value
+
+    def hmat_stats(self):
+        st = (ctypes.c_int64 * 8)()
+        _lib.check(self.lib.dfn_hmat_stats(self.h, st), self.lib)
+        keys = ["leaves", "dense_leaves", "lowrank_leaves", "max_rank", "mean_rank_x1000", "values",
+                "dense_values", "lowrank_values"]
+        return dict(zip(keys, list(st)))
+
+    def hmat_perm(self):
+        perm = np.empty(self.N, dtype=np.int32)
+        _lib.check(self.lib.dfn_hmat_perm(self.h, perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))), self.lib)
+        return perm
 
     def profile_kv(self, enable=True):
         _lib.check(self.lib.dfn_profile_kv(self.h, 1 if enable else 0), self.lib)

@@ -93,7 +93,12 @@ typedef struct dfn_options {
     int32_t device;           /* CUDA device ordinal */
     int32_t max_attempts;     /* RK attempts per step scheduled on the device before the host looks (>=1) */
     int32_t gemv_impl;        /* 0 = TMA bulk-copy pipeline, 1 = direct 128-bit loads */
-    int32_t reserved[3];
+    /* H-matrix parameters for static_kernel = hmatrix (0 = the reference's
+     * defaults nleaf=100, eta=3, eps_ACA=1e-8, src/variables.f90:122-124) */
+    int32_t hmat_leaf;
+    int32_t reserved;
+    double hmat_eta;
+    double hmat_eps;
 } dfn_options;
 
 /* Per-call report of the solve driver. */
@@ -234,6 +239,14 @@ int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const 
                               int64_t nb_source, const int64_t *d_src_fault, const int64_t *d_src_element,
                               const double *d_src_Q, const double *d_src_t_beg, const double *d_src_t_end,
                               double *d_P_temp, double *d_P_dot, int32_t *ier, void *stream);
+
+/* ---- H-matrix introspection (static_kernel = hmatrix) ------------------ */
+/* stats[0..7]: leaves, dense leaves, low-rank leaves, max rank, mean rank x 1000,
+ * stored values, dense values, low-rank values (all networks, all components).
+ * Returns DFN_ERR_UNSUPPORTED for a dense-kernel handle. */
+int32_t dfn_hmat_stats(const dfn_handle *h, int64_t *stats);
+/* Cluster order of network 0: perm[pos] = element index (the reference's mat_corr). */
+int32_t dfn_hmat_perm(const dfn_handle *h, int32_t *perm);
 
 /* ---- timing helpers (CUDA events on the handle's stream) --------------- */
 /* Times `reps` K.V launches of the handle's storage on its stream and

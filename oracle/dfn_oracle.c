@@ -48,7 +48,8 @@ typedef struct orc {
     double *Y, *P, *Pdot, *SigmaT_dot, *SigmaN_dot;
     /* dense kernel (optional) */
     double *KT, *KN;
-    int kernel_impl; /* 0 matrix-free reference routine, 1 dense stored K */
+    int kernel_impl; /* 0 matrix-free reference routine, 1 dense stored K, 2 H-matrix */
+    void *hmat;      /* orc_hmat */
     int nthreads;
     /* counters */
     int64_t cg_iters, rhs_evals, attempts, rejected, halvings, stage_noconv;
@@ -56,6 +57,9 @@ typedef struct orc {
 } orc;
 
 static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
+
+struct orc_hmat;
+static void orc_hmat_free(struct orc_hmat *H);
 
 /* ---------------------------------------------------------------------- */
 /* Geometry and loading projection: src/initialisation.f90:145-153,159-205,
@@ -160,6 +164,7 @@ void orc_destroy(orc *o)
                     o->src_index, o->src_Q, o->src_tb, o->src_te, o->Y, o->P, o->Pdot, o->SigmaT_dot,
                     o->SigmaN_dot, o->KT, o->KN};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
+    orc_hmat_free((struct orc_hmat *)o->hmat);
     free(o);
 }
 
@@ -340,9 +345,12 @@ static void orc_dense_kv(const orc *o, const double *slip, double *sT, double *s
     }
 }
 
+static void orc_hmat_kv(const orc *o, const double *slip, double *sT, double *sN);
+
 /* kernel_ptr dispatch (src/initialisation.f90:105-128). */
 void orc_kernel(orc *o, const double *slip, double *sT, double *sN)
 {
+    if (o->kernel_impl == 2 && o->hmat) { orc_hmat_kv(o, slip, sT, sN); return; }
     if (o->kernel_impl == 1 && o->KT) { orc_dense_kv(o, slip, sT, sN); return; }
     if (o->mode == DFN_MODE_II) orc_directII(o, slip, sT, sN);
     else { orc_directIII(o, slip, sT); if (sN) memset(sN, 0, 8 * o->N); }
@@ -680,6 +688,253 @@ int orc_solve_steps(orc *o, int64_t nsteps, double *hdid_log)
 
 /* ---------------------------------------------------------------------- */
 /* Accessors */
+/* ---------------------------------------------------------------------- */
+/* H-matrix (static_kernel = hmatrix): the src/hmatrix/ sources.           */
+
+typedef struct { int first, last, son1, son2; } orc_clus;
+typedef struct { int r0, nr, c0, nc, dense, rank; double *A, *B, *F; } orc_leaf;
+
+struct orc_hmat {
+    int N, ncl, nleaf_blocks, cap;
+    int *perm;              /* mat_corr: perm[pos] = element */
+    orc_clus *cl;
+    orc_leaf *lv[2];        /* per component (T, N) */
+    int nlv;
+    int failed;             /* an ACA needed more than 20 terms (the reference STOPs) */
+};
+typedef struct orc_hmat orc_hmat;
+
+/* cluster_tree.f90: bisection of the bounding box along its longer side
+ * (ties: second coordinate), points >= midpoint form one son, order kept,
+ * the son holding the smallest current position placed first. */
+static void orc_split(double *x, double *y, int *perm, int first, int last, int nleaf, orc_hmat *H)
+{
+    int me = H->ncl++;
+    H->cl[me].first = first; H->cl[me].last = last; H->cl[me].son1 = -1; H->cl[me].son2 = -1;
+    if (last - first + 1 <= nleaf) return;
+    double bx0 = x[first], bx1 = x[first], by0 = y[first], by1 = y[first];
+    for (int i = first; i <= last; i++) {
+        bx0 = fmin(bx0, x[i]); bx1 = fmax(bx1, x[i]); by0 = fmin(by0, y[i]); by1 = fmax(by1, y[i]);
+    }
+    double box[2] = {bx1 - bx0, by1 - by0};
+    int dir = 0;
+    for (int d = 0; d < 2; d++) if (box[d] >= box[dir]) dir = d;
+    const double *c = dir == 0 ? x : y;
+    double lo = dir == 0 ? bx0 : by0, hi = dir == 0 ? bx1 : by1;
+    double mid = lo + (hi - lo) / 2;
+    int n = last - first + 1, n1 = 0, n2 = 0;
+    int *s1 = (int *)malloc(sizeof(int) * n), *s2 = (int *)malloc(sizeof(int) * n);
+    for (int i = first; i <= last; i++) { if (c[i] >= mid) s1[n1++] = i; else s2[n2++] = i; }
+    if (n1 == 0 || n2 == 0) { free(s1); free(s2); return; }
+    int *A = s1[0] <= s2[0] ? s1 : s2, *B = s1[0] <= s2[0] ? s2 : s1;
+    int nA = s1[0] <= s2[0] ? n1 : n2, nB = n - nA;
+    double *nx = (double *)malloc(8 * n), *ny = (double *)malloc(8 * n);
+    int *np = (int *)malloc(sizeof(int) * n);
+    for (int i = 0; i < nA; i++) { nx[i] = x[A[i]]; ny[i] = y[A[i]]; np[i] = perm[A[i]]; }
+    for (int i = 0; i < nB; i++) { nx[nA + i] = x[B[i]]; ny[nA + i] = y[B[i]]; np[nA + i] = perm[B[i]]; }
+    for (int i = 0; i < n; i++) { x[first + i] = nx[i]; y[first + i] = ny[i]; perm[first + i] = np[i]; }
+    free(nx); free(ny); free(np); free(s1); free(s2);
+    int a = H->ncl;
+    orc_split(x, y, perm, first, first + nA - 1, nleaf, H);
+    int b = H->ncl;
+    orc_split(x, y, perm, first + nA, last, nleaf, H);
+    H->cl[me].son1 = a; H->cl[me].son2 = b;
+}
+
+static void orc_bbox(const orc *o, const orc_hmat *H, int k, double *b)
+{
+    b[0] = 1e300; b[1] = -1e300; b[2] = 1e300; b[3] = -1e300;
+    for (int p = H->cl[k].first; p <= H->cl[k].last; p++) {
+        int e = H->perm[p];
+        b[0] = fmin(b[0], o->elem[2 * e]); b[1] = fmax(b[1], o->elem[2 * e]);
+        b[2] = fmin(b[2], o->elem[2 * e + 1]); b[3] = fmax(b[3], o->elem[2 * e + 1]);
+    }
+}
+
+/* block_cluster_tree.f90:342-476 (admissibility eta*dist >= max(diam)) */
+static void orc_blocks(const orc *o, orc_hmat *H, double eta, int r, int c)
+{
+    double R[4], C[4];
+    orc_bbox(o, H, r, R);
+    orc_bbox(o, H, c, C);
+    double dr = sqrt((R[1] - R[0]) * (R[1] - R[0]) + (R[3] - R[2]) * (R[3] - R[2]));
+    double dc = sqrt((C[1] - C[0]) * (C[1] - C[0]) + (C[3] - C[2]) * (C[3] - C[2]));
+    double d = 0.0;
+    d = d + pow(fmax(0.0, R[0] - C[1]), 2) + pow(fmax(0.0, C[0] - R[1]), 2);
+    d = d + pow(fmax(0.0, R[2] - C[3]), 2) + pow(fmax(0.0, C[2] - R[3]), 2);
+    d = sqrt(d);
+    orc_clus cr = H->cl[r], cc = H->cl[c];
+    int dense;
+    if (eta * d >= fmax(dr, dc)) dense = 0;
+    else if (cr.son1 >= 0 && cc.son1 >= 0) {
+        orc_blocks(o, H, eta, cr.son1, cc.son1); orc_blocks(o, H, eta, cr.son1, cc.son2);
+        orc_blocks(o, H, eta, cr.son2, cc.son1); orc_blocks(o, H, eta, cr.son2, cc.son2);
+        return;
+    } else dense = 1;
+    if (H->nlv == H->cap) {
+        H->cap *= 2;
+        H->lv[0] = (orc_leaf *)realloc(H->lv[0], sizeof(orc_leaf) * H->cap);
+        H->lv[1] = (orc_leaf *)realloc(H->lv[1], sizeof(orc_leaf) * H->cap);
+    }
+    for (int q = 0; q < 2; q++) {
+        orc_leaf *L = &H->lv[q][H->nlv];
+        memset(L, 0, sizeof(*L));
+        L->r0 = cr.first; L->nr = cr.last - cr.first + 1; L->c0 = cc.first; L->nc = cc.last - cc.first + 1;
+        L->dense = dense;
+    }
+    H->nlv++;
+}
+
+/* compute_full_ACA: src/hmatrix/ACA_algorithm.f90:665-826, on the fully
+ * evaluated block; pivot = first maximum of |R| in column-major order,
+ * stop when |pivot| <= 10.0**(-14) (a default-real literal) or
+ * ||R||_F <= eps*||A||_F; more than 20 terms is the reference's STOP. */
+static int orc_full_aca(int m, int n, double *R, double eps, int maxr, double *A, double *B)
+{
+    double nA = 0.0;
+    for (int64_t q = 0; q < (int64_t)m * n; q++) nA += R[q] * R[q];
+    nA = sqrt(nA);
+    int rank = 0;
+    for (int k = 1; k <= (m < n ? m : n); k++) {
+        if (k > maxr) return -1;
+        int pi = 0, pj = 0;
+        double best = -1.0;
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < m; i++) {
+                double v = fabs(R[(int64_t)j * m + i]);
+                if (v > best) { best = v; pi = i; pj = j; }
+            }
+        if (best <= (double)1e-14f) return k - 1;
+        double piv = R[(int64_t)pj * m + pi];
+        for (int i = 0; i < m; i++) A[(int64_t)(k - 1) * m + i] = R[(int64_t)pj * m + i];
+        for (int j = 0; j < n; j++) B[(int64_t)(k - 1) * n + j] = R[(int64_t)j * m + pi] / piv;
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < m; i++)
+                R[(int64_t)j * m + i] = R[(int64_t)j * m + i] - A[(int64_t)(k - 1) * m + i] * B[(int64_t)(k - 1) * n + j];
+        double nR = 0.0;
+        for (int64_t q = 0; q < (int64_t)m * n; q++) nR += R[q] * R[q];
+        nR = sqrt(nR);
+        rank = k;
+        if (nR <= eps * nA) return k;
+    }
+    return rank;
+}
+
+static void orc_hmat_free(orc_hmat *H)
+{
+    if (!H) return;
+    for (int q = 0; q < 2; q++) {
+        if (!H->lv[q]) continue;
+        for (int b = 0; b < H->nlv; b++) { free(H->lv[q][b].A); free(H->lv[q][b].B); free(H->lv[q][b].F); }
+        free(H->lv[q]);
+    }
+    free(H->perm); free(H->cl); free(H);
+}
+
+/* initiate_hmat: src/hmatrix/initialisation_hmat.f90:13-100 (no
+ * recompression: it only lowers the ranks, within eps). Returns 0, or -1
+ * when an ACA needed more than 20 terms. */
+int orc_hmat_build(orc *o, int nleaf, double eta, double eps)
+{
+    int N = (int)o->N;
+    orc_hmat *H = (orc_hmat *)calloc(1, sizeof(orc_hmat));
+    H->N = N;
+    H->perm = (int *)malloc(sizeof(int) * N);
+    H->cl = (orc_clus *)malloc(sizeof(orc_clus) * 2 * N);
+    double *x = (double *)malloc(8 * N), *y = (double *)malloc(8 * N);
+    for (int i = 0; i < N; i++) { x[i] = o->elem[2 * i]; y[i] = o->elem[2 * i + 1]; H->perm[i] = i; }
+    orc_split(x, y, H->perm, 0, N - 1, nleaf, H);
+    free(x); free(y);
+    H->cap = 64;
+    H->lv[0] = (orc_leaf *)malloc(sizeof(orc_leaf) * H->cap);
+    H->lv[1] = (orc_leaf *)malloc(sizeof(orc_leaf) * H->cap);
+    orc_blocks(o, H, eta, 0, 0);
+    int ncomp = o->mode == DFN_MODE_II ? 2 : 1;
+    for (int q = 0; q < ncomp; q++) {
+        int which = o->mode == DFN_MODE_II ? 1 + q : 0;
+        for (int b = 0; b < H->nlv; b++) {
+            orc_leaf *L = &H->lv[q][b];
+            double *R = (double *)malloc(sizeof(double) * (size_t)L->nr * L->nc);
+            for (int j = 0; j < L->nc; j++)
+                for (int i = 0; i < L->nr; i++)
+                    R[(int64_t)j * L->nr + i] = orc_kernel_entry(o, H->perm[L->r0 + i], H->perm[L->c0 + j], which);
+            if (L->dense) { L->F = R; continue; }
+            L->A = (double *)malloc(sizeof(double) * (size_t)L->nr * 20);
+            L->B = (double *)malloc(sizeof(double) * (size_t)L->nc * 20);
+            double *Rc = (double *)malloc(sizeof(double) * (size_t)L->nr * L->nc);
+            memcpy(Rc, R, sizeof(double) * (size_t)L->nr * L->nc);
+            int r = orc_full_aca(L->nr, L->nc, Rc, eps, 20, L->A, L->B);
+            free(Rc);
+            if (r < 0) { H->failed = 1; L->dense = 1; L->F = R; continue; }
+            L->rank = r;
+            free(R);
+        }
+    }
+    orc_hmat_free((orc_hmat *)o->hmat);
+    o->hmat = H;
+    o->kernel_impl = 2;
+    return H->failed ? -1 : 0;
+}
+
+/* hmatII/hmatIII + Hgemv_right: y_perm = H x_perm, then back to element
+ * order and the prefactor (src/kernel_calculation/hmatrixModeII.f90:46-69). */
+static void orc_hmat_kv(const orc *o, const double *slip, double *sT, double *sN)
+{
+    const orc_hmat *H = (const orc_hmat *)o->hmat;
+    int N = H->N, ncomp = o->mode == DFN_MODE_II ? 2 : 1;
+    double *x = (double *)malloc(8 * N), *y = (double *)malloc(8 * N), *z = (double *)malloc(8 * 64);
+    for (int p = 0; p < N; p++) x[p] = slip[H->perm[p]];
+    for (int q = 0; q < ncomp; q++) {
+        for (int p = 0; p < N; p++) y[p] = 0.0;
+        for (int b = 0; b < H->nlv; b++) {
+            const orc_leaf *L = &H->lv[q][b];
+            if (L->dense) {
+                for (int i = 0; i < L->nr; i++) {
+                    double s = 0.0;
+                    for (int j = 0; j < L->nc; j++) s += L->F[(int64_t)j * L->nr + i] * x[L->c0 + j];
+                    y[L->r0 + i] += s;
+                }
+            } else {
+                for (int k = 0; k < L->rank; k++) {
+                    double s = 0.0;
+                    for (int j = 0; j < L->nc; j++) s += L->B[(int64_t)k * L->nc + j] * x[L->c0 + j];
+                    z[k] = s;
+                }
+                for (int i = 0; i < L->nr; i++) {
+                    double s = 0.0;
+                    for (int k = 0; k < L->rank; k++) s += L->A[(int64_t)k * L->nr + i] * z[k];
+                    y[L->r0 + i] += s;
+                }
+            }
+        }
+        double *out = q == 0 ? sT : sN;
+        double pref = o->mode == DFN_MODE_II ? o->mu / PI_F90 * (1.0 - o->cs * o->cs / (o->cp * o->cp))
+                                             : o->mu / (2.0 * PI_F90);
+        for (int p = 0; p < N; p++) out[H->perm[p]] = pref * y[p];
+    }
+    if (ncomp == 1 && sN) memset(sN, 0, 8 * N);
+    free(x); free(y); free(z);
+}
+
+void orc_hmat_perm(const orc *o, int *perm)
+{
+    const orc_hmat *H = (const orc_hmat *)o->hmat;
+    if (H) memcpy(perm, H->perm, sizeof(int) * H->N);
+}
+
+void orc_hmat_stats(const orc *o, int64_t *st)
+{
+    const orc_hmat *H = (const orc_hmat *)o->hmat;
+    st[0] = st[1] = st[2] = st[3] = 0;
+    if (!H) return;
+    st[0] = H->nlv;
+    for (int b = 0; b < H->nlv; b++) {
+        if (H->lv[0][b].dense) st[1]++;
+        else if (H->lv[0][b].rank > st[2]) st[2] = H->lv[0][b].rank;
+    }
+    st[3] = H->ncl;
+}
+
 void orc_get_state(const orc *o, double *Y, double *P, double *scal)
 {
     if (Y) memcpy(Y, o->Y, 8 * 3 * o->N);

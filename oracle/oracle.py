@@ -56,6 +56,9 @@ def load():
         "orc_get_loads": (None, [V, dp, dp, ctypes.POINTER(ctypes.c_ubyte)]),
         "orc_get_last_stress": (None, [V, dp, dp, dp]),
         "orc_counters": (None, [V, ctypes.POINTER(i64)]),
+        "orc_hmat_build": (cint, [V, cint, dbl, dbl]),
+        "orc_hmat_perm": (None, [V, ctypes.POINTER(ctypes.c_int)]),
+        "orc_hmat_stats": (None, [V, ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -101,6 +104,21 @@ class Oracle:
 
     def use_direct(self):
         self.lib.orc_set_kernel_impl(self.o, 0)
+
+    def use_hmatrix(self, leaf=100, eta=3.0, eps=1e-8):
+        """The reference's H-matrix (full-pivot ACA on evaluated blocks);
+        returns False when an ACA needed more than 20 terms (the reference stops)."""
+        return self.lib.orc_hmat_build(self.o, int(leaf), float(eta), float(eps)) == 0
+
+    def hmat_perm(self):
+        perm = np.empty(self.N, dtype=np.int32)
+        self.lib.orc_hmat_perm(self.o, perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return perm
+
+    def hmat_stats(self):
+        st = (ctypes.c_int64 * 4)()
+        self.lib.orc_hmat_stats(self.o, st)
+        return dict(zip(["leaves", "dense_leaves", "max_rank", "clusters"], list(st)))
 
     def entry(self, k, l, which):
         return self.lib.orc_kernel_entry(self.o, int(k), int(l), int(which))
