@@ -72,6 +72,18 @@ def load():
         "dfn_launch_count": (i64, [P]),
         "dfn_profile_kv": (i32, [P, i32]),
         "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
+        "dfn_get_report": (i32, [P, i32, ctypes.POINTER(DfnReport)]),
+        "dfn_set_mlp": (i32, [P, ctypes.POINTER(ctypes.c_float)]),
+        "dfn_record": (i32, [P, i64]),
+        "dfn_record_read": (i32, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64,
+                                  ctypes.POINTER(i64)]),
+        "dfn_mlp_train": (i32, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64,
+                                ctypes.POINTER(ctypes.c_float), i32, i32, ctypes.c_float, ctypes.c_uint64,
+                                ctypes.POINTER(ctypes.c_float)]),
+        "dfn_mlp_loss_grad": (i32, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64,
+                                    ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_float)]),
+        "dfn_velocity": (i32, [P, dp]),
         "dfn_hmat_stats": (i32, [P, ctypes.POINTER(i64)]),
         "dfn_hmat_perm": (i32, [P, ctypes.POINTER(i32)]),
         "dfn_create_batch":(i32, [ctypes.POINTER(DfnProblem), i32, ctypes.POINTER(DfnOptions), ctypes.POINTER(P)]),

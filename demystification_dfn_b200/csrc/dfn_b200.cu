@@ -13,6 +13,7 @@
 #include "../../include/dfn_b200.h"
 #include "dfn_device.cuh"
 #include "hmat_device.cuh"
+#include "newton.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -114,6 +115,14 @@ struct dfn_handle {
     double *hz = nullptr, *hout = nullptr;
     std::vector<int> hranks;              // rank of every low-rank leaf (report)
     int64_t hdense_vals = 0, hlr_vals = 0, hblocks = 0;
+    // Newton formulation and the learned guess
+    int form = 0, guess = 0, newton_maxit = 50;
+    double newton_tol = 1e-13;
+    double *tau0 = nullptr, *wlast = nullptr, *vnow = nullptr;
+    float *mlp = nullptr;
+    float *rec_x = nullptr, *rec_t = nullptr;
+    unsigned long long *rec_n = nullptr;
+    long long rec_cap = 0;
     // K.V launch timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -244,13 +253,18 @@ static FricParams fric_params(dfn_handle *h, int64_t nelem)
     f.fake = h->fake; f.partT = h->partT; f.partN = h->partN; f.SigT = h->SigT; f.SigN = h->SigN;
     f.Ptemp = h->Ptemp; f.Pdot = h->Pdot_s; f.y = h->Y; f.ytmp = h->ytmp; f.kbuf = h->kbuf; f.yscal = h->yscal;
     f.yout = h->yout; f.ctl = h->ctl;
+    f.form = h->form; f.guess = h->guess; f.maxit = h->newton_maxit; f.tol = h->newton_tol; f.off_explicit = 0.0;
+    f.tau0 = h->tau0; f.wlast = h->wlast; f.vnow = h->vnow; f.mlp = h->mlp;
+    f.rec_x = h->rec_x; f.rec_t = h->rec_t; f.rec_n = h->rec_n; f.rec_cap = h->rec_cap;
     return f;
 }
 
-static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t nelem)
+static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t nelem, double off_explicit = 0.0)
 {
     FricParams f = fric_params(h, nelem);
-    friction_kernel<<<(unsigned)((nelem + 255) / 256), 256, 0, h->stream>>>(f, stage, sys, mask);
+    f.off_explicit = off_explicit;
+    const size_t smem = (h->form == DFN_FORM_NEWTON && h->guess == DFN_GUESS_MLP) ? MLP_NPAR * sizeof(float) : 0;
+    friction_kernel<<<(unsigned)((nelem + 255) / 256), 256, smem, h->stream>>>(f, stage, sys, mask);
     h->launches++;
     CKL();
     return DFN_OK;
@@ -374,6 +388,7 @@ static void fill_report(const StepCtl &c, dfn_report *r)
     r->it_count = c.it_count; r->attempts = c.attempts; r->rejected = c.rejected; r->rhs_evals = c.rhs_evals;
     r->cg_iterations = c.cg_iters; r->probe_halvings = c.halvings; r->time = c.time; r->t_try = c.t_try;
     r->last_hdid = c.hdid; r->status = c.status; r->pad = 0; r->stage_cg_failures = c.stage_noconv;
+    r->newton_solves = c.newton_solves; r->newton_iters = c.newton_iters; r->newton_fail = c.newton_fail;
 }
 
 // ---------------------------------------------------------------------------
@@ -578,7 +593,8 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
+    void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
@@ -679,6 +695,10 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     h->mode = probs[0].fracture_mode; h->store = opt.kernel_storage;
     h->pressure = opt.pressure_solver; h->gemv_impl = opt.gemv_impl;
     h->max_attempts = opt.max_attempts > 0 ? opt.max_attempts : 64;
+    h->form = opt.formulation == DFN_FORM_NEWTON ? DFN_FORM_NEWTON : DFN_FORM_V;
+    h->guess = (opt.newton_guess >= 0 && opt.newton_guess <= 2) ? opt.newton_guess : 0;
+    h->newton_maxit = opt.newton_maxit > 0 ? opt.newton_maxit : 50;
+    h->newton_tol = opt.newton_tol > 0 ? opt.newton_tol : 1e-13;
     const int bpc = bytes_per_col(h->mode, h->store);
     const int64_t CW = GEMV_CHUNK_BYTES / bpc;
     // static_kernel selects the dense kernel ("direct") or the H-matrix
@@ -716,6 +736,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         I.mu_2cs = p.mu / (2.0 * p.cs);
         I.porosity = p.porosity; I.dyn_visc = p.dyn_viscosity; I.comp = p.fluid_comp + p.rock_comp;
         I.tol = p.tol_solver;
+        I.t0 = p.time0;
         eoff += I.N;
         if (!h->hmat) kvec += I.N * I.Np * bpc / 16;
         poff += I.nchunk * I.N;
@@ -788,6 +809,20 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         CKC(cudaGetLastError());
     }
     HCOPY(h->inst_of, inst_of.data(), Nt);
+    DALLOC(h->mlp, MLP_NPAR);
+    CKC(cudaMemset(h->mlp, 0, sizeof(float) * MLP_NPAR));
+    DALLOC(h->rec_n, 1);
+    CKC(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
+    if (h->form == DFN_FORM_NEWTON) {
+        DALLOC(h->tau0, Nt); DALLOC(h->wlast, Nt); DALLOC(h->vnow, Nt);
+        CKC(cudaMemset(h->vnow, 0, sizeof(double) * Nt));
+        HCOPY(h->fake, fake.data(), Nt);
+        newton_init_kernel<<<blocks_of(Nt, 256), 256, 0, h->stream>>>(Nt, h->inst_of, h->inst, h->a, h->b, h->f0,
+                                                                       h->V0, h->fake, h->P, h->Y, h->tau0,
+                                                                       h->wlast);
+        h->launches++;
+        CKC(cudaGetLastError());
+    }
     HCOPY(h->fake, fake.data(), Nt);
 
     // decoupled pressure segments from the face permeabilities
@@ -964,7 +999,7 @@ int32_t dfn_friction_law(dfn_handle *h, double x, int64_t nv, const double *Y, d
     CK(cudaMemcpyAsync(h->ytmp, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
     TRY(launch_pressure(h, M_ALL, 2, 0, 1, x, 1));
     TRY(launch_gemv(h, M_ALL, h->ytmp, 3, true));
-    TRY(launch_friction(h, 0, 0, M_ALL, N));
+    TRY(launch_friction(h, 0, 0, M_ALL, N, x));
     CK(cudaMemcpyAsync(Ydot, h->kbuf, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, h->stream));
     TRY(sync_ctl(h));
     int st = h->h_ctl[0].status;
@@ -1047,6 +1082,15 @@ int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, d
     if (time) *time = h->h_ctl[i].time;
     if (t_try) *t_try = h->h_ctl[i].t_try;
     if (it_count) *it_count = h->h_ctl[i].it_count;
+    return DFN_OK;
+}
+
+int32_t dfn_get_report(dfn_handle *h, int32_t i, dfn_report *rep)
+{
+    if (!h || !rep || i < 0 || i >= h->B) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    TRY(sync_ctl(h));
+    fill_report(h->h_ctl[i], rep);
     return DFN_OK;
 }
 
@@ -1201,6 +1245,173 @@ int32_t dfn_compute_P_noalloc(int64_t N, double dt, double time, const double *d
     CK(cudaStreamSynchronize(s));
     *ier = (c.status == 1) ? 1 : 0;
     if (c.status != 0 && c.status != 1) return c.status;
+    return DFN_OK;
+}
+
+int32_t dfn_set_mlp(dfn_handle *h, const float *weights)
+{
+    if (!h || !weights) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaMemcpy(h->mlp, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice));
+    return DFN_OK;
+}
+
+int32_t dfn_record(dfn_handle *h, int64_t capacity)
+{
+    if (!h || capacity < 0) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->rec_x) { cudaFree(h->rec_x); h->rec_x = nullptr; }
+    if (h->rec_t) { cudaFree(h->rec_t); h->rec_t = nullptr; }
+    h->rec_cap = 0;
+    CK(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
+    if (capacity > 0) {
+        CK(cudaMalloc((void **)&h->rec_x, sizeof(float) * MLP_IN * capacity));
+        CK(cudaMalloc((void **)&h->rec_t, sizeof(float) * capacity));
+        h->rec_cap = capacity;
+    }
+    return DFN_OK;
+}
+
+int32_t dfn_record_read(dfn_handle *h, float *x, float *t, int64_t max, int64_t *count)
+{
+    if (!h || !count) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned long long n = 0;
+    CK(cudaMemcpy(&n, h->rec_n, sizeof(n), cudaMemcpyDeviceToHost));
+    int64_t m = std::min<int64_t>((int64_t)n, h->rec_cap);
+    m = std::min<int64_t>(m, max);
+    if (m > 0 && x) CK(cudaMemcpy(x, h->rec_x, sizeof(float) * MLP_IN * m, cudaMemcpyDeviceToHost));
+    if (m > 0 && t) CK(cudaMemcpy(t, h->rec_t, sizeof(float) * m, cudaMemcpyDeviceToHost));
+    *count = m;
+    return DFN_OK;
+}
+
+// Gradient (and optionally an Adam step) over samples [0, n) of device
+// arrays in batches; returns the summed squared error.
+static int mlp_pass(const float *dX, const float *dT, int64_t n, int64_t n_total, float *dW, float *dm, float *dv,
+                    float *dg, float *dgp, float *dlp, float *dls, int step, float lr, float *loss_sum,
+                    cudaStream_t s)
+{
+    const int nblk = (int)((n + MLP_SB - 1) / MLP_SB);
+    const size_t smem = sizeof(MlpSmem);
+    CK(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mlp_grad_kernel<<<nblk, 256, smem, s>>>(dX, dT, n, n_total, dW, dgp, dlp);
+    CKL();
+    mlp_reduce_adam_kernel<<<(MLP_NPAR + 255) / 256, 256, 0, s>>>(dgp, nblk, dW, dm, dv, dg, step, lr);
+    CKL();
+    sum_kernel<<<1, 32, 0, s>>>(dlp, nblk, dls);
+    CKL();
+    float l = 0.0f;
+    CK(cudaMemcpyAsync(&l, dls, sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *loss_sum = l;
+    return DFN_OK;
+}
+
+struct MlpBuffers {
+    float *X = nullptr, *T = nullptr, *W = nullptr, *m = nullptr, *v = nullptr, *g = nullptr, *gp = nullptr,
+          *lp = nullptr, *ls = nullptr;
+    ~MlpBuffers()
+    {
+        float *p[] = {X, T, W, m, v, g, gp, lp, ls};
+        for (float *q : p)
+            if (q) cudaFree(q);
+    }
+};
+
+static int mlp_alloc(MlpBuffers &b, int64_t n, int64_t batch)
+{
+    const int64_t nblk = (batch + MLP_SB - 1) / MLP_SB;
+    CK(cudaMalloc((void **)&b.X, sizeof(float) * MLP_IN * std::max<int64_t>(n, 1)));
+    CK(cudaMalloc((void **)&b.T, sizeof(float) * std::max<int64_t>(n, 1)));
+    CK(cudaMalloc((void **)&b.W, sizeof(float) * MLP_NPAR));
+    CK(cudaMalloc((void **)&b.m, sizeof(float) * MLP_NPAR));
+    CK(cudaMalloc((void **)&b.v, sizeof(float) * MLP_NPAR));
+    CK(cudaMalloc((void **)&b.g, sizeof(float) * MLP_NPAR));
+    CK(cudaMalloc((void **)&b.gp, sizeof(float) * MLP_NPAR * nblk));
+    CK(cudaMalloc((void **)&b.lp, sizeof(float) * nblk));
+    CK(cudaMalloc((void **)&b.ls, sizeof(float)));
+    CK(cudaMemset(b.m, 0, sizeof(float) * MLP_NPAR));
+    CK(cudaMemset(b.v, 0, sizeof(float) * MLP_NPAR));
+    return DFN_OK;
+}
+
+int32_t dfn_mlp_loss_grad(const float *x, const float *t, int64_t n, const float *weights, float *loss, float *grad)
+{
+    if (!x || !t || n < 1 || !weights || !loss || !grad) return DFN_ERR_ARG;
+    MlpBuffers b;
+    TRY(mlp_alloc(b, n, n));
+    CK(cudaMemcpy(b.X, x, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.T, t, sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.W, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice));
+    float ls = 0.0f;
+    TRY(mlp_pass(b.X, b.T, n, n, b.W, b.m, b.v, b.g, b.gp, b.lp, b.ls, 1, 0.0f, &ls, nullptr));
+    *loss = ls / (float)n;
+    CK(cudaMemcpy(grad, b.g, sizeof(float) * MLP_NPAR, cudaMemcpyDeviceToHost));
+    return DFN_OK;
+}
+
+int32_t dfn_mlp_train(const float *x, const float *t, int64_t n, float *weights, int32_t epochs, int32_t batch,
+                      float lr, uint64_t seed, float *loss)
+{
+    if (!x || !t || n < 1 || !weights || epochs < 1 || batch < 1 || !(lr > 0)) return DFN_ERR_ARG;
+    // seeded shuffle of the samples (host), then epochs over fixed minibatches
+    std::vector<int64_t> order(n);
+    for (int64_t i = 0; i < n; i++) order[i] = i;
+    uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+    for (int64_t i = n - 1; i > 0; i--) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        const int64_t j = (int64_t)((st >> 33) % (uint64_t)(i + 1));
+        std::swap(order[i], order[j]);
+    }
+    std::vector<float> xs((size_t)MLP_IN * n), ts(n);
+    for (int64_t i = 0; i < n; i++) {
+        for (int q = 0; q < MLP_IN; q++) xs[(size_t)i * MLP_IN + q] = x[order[i] * MLP_IN + q];
+        ts[i] = t[order[i]];
+    }
+    MlpBuffers b;
+    TRY(mlp_alloc(b, n, batch));
+    CK(cudaMemcpy(b.X, xs.data(), sizeof(float) * xs.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.T, ts.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.W, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice));
+    int step = 0;
+    for (int ep = 0; ep < epochs; ep++) {
+        double esum = 0.0;
+        for (int64_t s0 = 0; s0 < n; s0 += batch) {
+            const int64_t m = std::min<int64_t>(batch, n - s0);
+            float ls = 0.0f;
+            TRY(mlp_pass(b.X + s0 * MLP_IN, b.T + s0, m, m, b.W, b.m, b.v, nullptr, b.gp, b.lp, b.ls, ++step, lr,
+                         &ls, nullptr));
+            esum += ls;
+        }
+        if (loss && ep == 0) loss[0] = (float)(esum / n);
+        if (loss && ep == epochs - 1) loss[1] = (float)(esum / n);
+    }
+    CK(cudaMemcpy(weights, b.W, sizeof(float) * MLP_NPAR, cudaMemcpyDeviceToHost));
+    return DFN_OK;
+}
+
+int32_t dfn_velocity(dfn_handle *h, double *V)
+{
+    if (!h || !V) return DFN_ERR_ARG;
+    TRY(single_only(h));
+    const int64_t N = h->hinst[0].N;
+    CK(cudaSetDevice(h->dev));
+    if (h->form != DFN_FORM_NEWTON) {
+        CK(cudaMemcpy(V, h->Y, sizeof(double) * N, cudaMemcpyDeviceToHost));
+        return DFN_OK;
+    }
+    // stresses of the committed slip, pressure at dt = 0 (the committed P),
+    // then the friction law for V
+    TRY(reset_status0(h));
+    CK(cudaMemcpyAsync(h->ytmp, h->Y, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, h->stream));
+    TRY(launch_pressure(h, M_ALL, 2, 0, 1, 0.0, 1));
+    TRY(launch_gemv(h, M_ALL, h->ytmp, 3, true));
+    TRY(launch_friction(h, 0, 0, M_ALL, N, 0.0));
+    CK(cudaMemcpyAsync(V, h->vnow, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync_ctl(h));
     return DFN_OK;
 }
 

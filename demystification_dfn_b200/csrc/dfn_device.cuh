@@ -22,6 +22,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "newton_core.cuh"
+
 #define DFN_PI 3.141592653589793238
 
 // ---------------------------------------------------------------------------
@@ -45,6 +47,7 @@ struct StepCtl {
     int pfail_mask;   // bit s: pressure system s of this attempt hit the CG cap
     int pad2;
     long long stage_noconv;  // stage pressure solves that hit the CG cap
+    long long newton_solves, newton_iters, newton_fail;  // Newton formulation counters
 };
 
 // Cash-Karp tableau, src/ode_solver/ode_bs.f90:200-210.
@@ -324,6 +327,7 @@ struct Inst {
     int64_t soff, nsrc;  // its injection sources
     double prefT, mu_2cs;
     double porosity, dyn_visc, comp, tol;
+    double t0;        // time at which the slip is zero (Newton formulation)
 };
 
 __device__ __forceinline__ bool takes_part(const StepCtl *ctl, int i, int mask)
@@ -937,7 +941,64 @@ struct FricParams {
     double *kbuf;                 // per instance [6][3N] at 18*eoff
     double *yscal, *yout;         // [3N] at 3*eoff
     StepCtl *ctl;
+    // Newton formulation
+    int form;                     // 0 = V formulation, 1 = Newton
+    int guess;                    // DFN_GUESS_*
+    int maxit;
+    double tol;
+    double off_explicit;          // stage-0 offset of the evaluation from the step start
+    const double *tau0;           // [Ntot] shear traction at slip 0
+    double *wlast;                // [Ntot] last solution, warm start
+    double *vnow;                 // [Ntot] V of this evaluation
+    const float *mlp;             // DFN_MLP_PARAMS weights (global)
+    float *rec_x, *rec_t;         // recorded solves
+    unsigned long long *rec_n;
+    long long rec_cap;
 };
+
+// Newton formulation of one element: stresses from slip, V from the
+// friction law (newton_core.cuh), derivatives of slip and log-state. The
+// normal-stress slot of the state holds sigmaN at slip 0 (derivative 0).
+__device__ __forceinline__ void newton_rhs(const FricParams &f, const float *mlpW, int64_t e, int mode, double eta,
+                                           double tt, double slip_unused, double psi, double sig0, double T,
+                                           double Nn, double Pt, double &dV, double &dpsi, double &dsig, int &iters,
+                                           int &ok)
+{
+    (void)slip_unused;
+    const double a = f.a[e], b = f.b[e], V0 = f.V0[e], Dc = f.Dc[e];
+    const double tau = f.tau0[e] + T + f.sload[e] * tt;
+    const double sig = ((mode == 2) ? sig0 + Nn : sig0) + f.nload[e] * tt;
+    const double s = -(sig + Pt);
+    const double lnA = log(2.0 * V0) - (f.f0[e] + b * psi) / a;
+    const double w0 = tau / (s * a);
+    double w = w0;
+    float x[MLP_IN];
+    if (f.guess == 1 || f.rec_cap > 0) mlp_features(tau, psi, s, Pt, a, b, w0, x);
+    if (f.guess == 1) w = w0 + 10.0 * (double)mlp_forward(mlpW, x);
+    else if (f.guess == 2 && f.wlast[e] != 0.0) w = f.wlast[e];
+    iters = 0;
+    ok = 1;
+    if (f.fake[e] || !(s > 0.0)) {
+        dV = 0.0; dpsi = 0.0; dsig = 0.0;
+        ok = f.fake[e] ? 1 : 0;
+        return;
+    }
+    w = newton_w(tau, s, a, lnA, eta, w, f.tol, f.maxit, iters, ok);
+    f.wlast[e] = w;
+    const double V = v_of_w(w, lnA);
+    f.vnow[e] = V;
+    dV = V;                                        // d slip / dt
+    dpsi = V0 / Dc * exp(-psi) - fabs(V) / Dc;     // aging law, as the reference
+    dsig = 0.0;
+    if (ok && f.rec_cap > 0) {
+        const unsigned long long q = atomicAdd(f.rec_n, 1ull);
+        if ((long long)q < f.rec_cap) {
+#pragma unroll
+            for (int i = 0; i < MLP_IN; i++) f.rec_x[q * MLP_IN + i] = x[i];
+            f.rec_t[q] = (float)((w - w0) / 10.0);
+        }
+    }
+}
 
 __device__ __forceinline__ void rsf_rhs(const FricParams &f, int mode, int64_t e, double mu_2cs, double V, double psi,
                                         double sig, double T, double Nn, double Pt, double Pd, double &dV,
@@ -971,8 +1032,17 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
 // sys: pressure system of this evaluation; mask: phases that take part.
 __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
 {
+    extern __shared__ float fric_smem[];
+    const float *mlpW = f.mlp;
+    if (f.form == 1 && f.guess == 1) {
+        // the learned guess: weights to shared memory for the whole block
+        for (int p = threadIdx.x; p < MLP_NPAR; p += blockDim.x) fric_smem[p] = f.mlp[p];
+        __syncthreads();
+        mlpW = fric_smem;
+    }
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int myi = -1;
+    int nit = 0, nsolve = 0, nfail = 0;
     double emax = 0.0;
     if (e < f.Ntot) {
         const int i = f.inst_of[e];
@@ -1000,7 +1070,17 @@ __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
         const double Pt = f.Ptemp[6 * I.eoff + (int64_t)sys * N + k];
         const double Pd = f.Pdot[6 * I.eoff + (int64_t)sys * N + k];
         double dV, dpsi, dsig;
-        rsf_rhs(f, f.mode, e, I.mu_2cs, V, psi, sig, T, Nn, Pt, Pd, dV, dpsi, dsig);
+        if (f.form == 1) {
+            const double off = (stage == 0) ? f.off_explicit
+                                            : (stage == 1 ? 0.0 : add_(ctl->x, mul_(ck_a(stage), ctl->h)));
+            const double tt = (ctl->time - I.t0) + off;
+            int ok = 1;
+            newton_rhs(f, mlpW, e, f.mode, I.mu_2cs, tt, V, psi, sig, T, Nn, Pt, dV, dpsi, dsig, nit, ok);
+            nsolve = f.fake[e] ? 0 : 1;
+            nfail = ok ? 0 : 1;
+        } else {
+            rsf_rhs(f, f.mode, e, I.mu_2cs, V, psi, sig, T, Nn, Pt, Pd, dV, dpsi, dsig);
+        }
         double *kb = f.kbuf + 18 * I.eoff;
         const int slot = (stage == 0) ? 0 : stage - 1;
         double *ks = kb + (int64_t)slot * S;
@@ -1051,6 +1131,52 @@ __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
             atomic_max_pos(&f.ctl[myi].errmax_bits, emax);
         }
     }
+    if (f.form == 1) {
+        // Newton counters: warp sums when the warp lies in one instance
+        const unsigned full = 0xffffffffu;
+        const int i0 = __shfl_sync(full, myi, 0);
+        if (__all_sync(full, myi == i0)) {
+            int a = nit, b = nsolve, c = nfail;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a += __shfl_xor_sync(full, a, o);
+                b += __shfl_xor_sync(full, b, o);
+                c += __shfl_xor_sync(full, c, o);
+            }
+            if ((threadIdx.x & 31) == 0 && i0 >= 0) {
+                atomicAdd((unsigned long long *)&f.ctl[i0].newton_iters, (unsigned long long)a);
+                atomicAdd((unsigned long long *)&f.ctl[i0].newton_solves, (unsigned long long)b);
+                if (c) atomicAdd((unsigned long long *)&f.ctl[i0].newton_fail, (unsigned long long)c);
+            }
+        } else if (myi >= 0) {
+            atomicAdd((unsigned long long *)&f.ctl[myi].newton_iters, (unsigned long long)nit);
+            atomicAdd((unsigned long long *)&f.ctl[myi].newton_solves, (unsigned long long)nsolve);
+            if (nfail) atomicAdd((unsigned long long *)&f.ctl[myi].newton_fail, (unsigned long long)nfail);
+        }
+    }
+}
+
+// tau0 of the Newton formulation: the shear traction for which the initial
+// V satisfies the friction law at slip 0; then the slip state is zeroed.
+__global__ void newton_init_kernel(int64_t Ntot, const int *inst_of, const Inst *inst, const double *a,
+                                   const double *b, const double *f0, const double *V0, const unsigned char *fake,
+                                   const double *P, double *Y, double *tau0, double *wlast)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= Ntot) return;
+    const Inst &I = inst[inst_of[e]];
+    const int64_t N = I.N, k = e - I.eoff;
+    double *y = Y + 3 * I.eoff;
+    const double V = y[k], psi = y[N + k], sig = y[2 * N + k];
+    double t0 = 0.0, w = 0.0;
+    if (!fake[e]) {
+        const double C = exp((f0[e] + b[e] * psi) / a[e]);
+        w = asinh(V * C / (2.0 * V0[e]));
+        t0 = I.mu_2cs * V - (sig + P[e]) * a[e] * w;
+    }
+    tau0[e] = t0;
+    wlast[e] = w;
+    y[k] = 0.0;
 }
 
 // Element-wise kernels over all instances; k == 0 of an instance also
@@ -1129,6 +1255,9 @@ __global__ void step_begin_kernel(StepCtl *ctl, const Inst *inst, int B, const d
             if (c.time < tb && c.time + c.t_try > tb) c.t_try = 10.0;
         }
     }
+    // runs to a target time (dfn_solve_batch with t_end > 0; the reference
+    // stops by step count only) land on it: the last step is shortened
+    if (c.t_end > 0.0 && c.time + c.t_try > c.t_end) c.t_try = c.t_end - c.time;
 }
 
 __global__ void set_h_kernel(StepCtl *ctl, int B)
@@ -1179,7 +1308,7 @@ __global__ void finish_kernel(StepCtl *ctl, int B, double t_cap)
     if (tn > t_cap) tn = t_cap;
     c.t_try = tn;
     c.steps_done += 1;
-    bool done = (c.steps_done >= c.target_steps) || (c.t_end > 0.0 && c.time >= c.t_end);
+    bool done = (c.steps_done >= c.target_steps) || (c.t_end > 0.0 && c.time >= c.t_end * (1.0 - 1e-14));
     c.phase = done ? PH_DONE : PH_NEW;
 }
 

@@ -18,13 +18,15 @@ from .simulation import make_options
 
 class Ensemble:
     def __init__(self, problems, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
-                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0):
+                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0,
+                 newton_tol=0.0):
         self.lib = _lib.load()
         self.arrays = [p if isinstance(p, ProblemArrays) else build_arrays(p) for p in problems]
         if not self.arrays:
             raise ValueError("an ensemble needs at least one problem")
         self.B = len(self.arrays)
-        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps)
+        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
+                           formulation, guess, newton_maxit, newton_tol)
         self._cs = [to_c(a) for a in self.arrays]
         arr = (DfnProblem * self.B)(*self._cs)
         self._arr = arr
@@ -79,6 +81,27 @@ class Ensemble:
         _lib.check(self.lib.dfn_get_state_instance(self.h, int(i), ptr(Y), ptr(P), ctypes.byref(t),
                                                    ctypes.byref(tt), ctypes.byref(it)), self.lib)
         return {"Y": Y, "P": P, "time": t.value, "t_try": tt.value, "it_count": it.value}
+
+    def report(self, i):
+        rep = DfnReport()
+        _lib.check(self.lib.dfn_get_report(self.h, int(i), ctypes.byref(rep)), self.lib)
+        return rep.as_dict()
+
+    def set_mlp(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        _lib.check(self.lib.dfn_set_mlp(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.lib)
+
+    def record(self, capacity):
+        _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)
+
+    def record_read(self, max_samples):
+        x = np.empty((int(max_samples), 6), dtype=np.float32)
+        t = np.empty(int(max_samples), dtype=np.float32)
+        n = ctypes.c_int64()
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.lib.dfn_record_read(self.h, x.ctypes.data_as(fp), t.ctypes.data_as(fp), int(max_samples),
+                                            ctypes.byref(n)), self.lib)
+        return x[:n.value], t[:n.value]
 
     def time_kernel(self, reps=10):
         ms = ctypes.c_double()

@@ -186,8 +186,10 @@ class DfnProblem(ctypes.Structure):
 class DfnOptions(ctypes.Structure):
     _fields_ = [("kernel_storage", ctypes.c_int32), ("pressure_solver", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
-                ("gemv_impl", ctypes.c_int32), ("hmat_leaf", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("hmat_eta", ctypes.c_double), ("hmat_eps", ctypes.c_double)]
+                ("gemv_impl", ctypes.c_int32), ("hmat_leaf", ctypes.c_int32), ("formulation", ctypes.c_int32),
+                ("hmat_eta", ctypes.c_double), ("hmat_eps", ctypes.c_double),
+                ("newton_guess", ctypes.c_int32), ("newton_maxit", ctypes.c_int32),
+                ("newton_tol", ctypes.c_double)]
 
 
 class DfnReport(ctypes.Structure):
@@ -195,7 +197,8 @@ class DfnReport(ctypes.Structure):
                 ("rhs_evals", ctypes.c_int64), ("cg_iterations", ctypes.c_int64),
                 ("probe_halvings", ctypes.c_int64), ("time", ctypes.c_double), ("t_try", ctypes.c_double),
                 ("last_hdid", ctypes.c_double), ("status", ctypes.c_int32), ("pad", ctypes.c_int32),
-                ("stage_cg_failures", ctypes.c_int64)]
+                ("stage_cg_failures", ctypes.c_int64), ("newton_solves", ctypes.c_int64),
+                ("newton_iters", ctypes.c_int64), ("newton_fail", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}

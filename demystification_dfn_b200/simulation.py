@@ -28,12 +28,20 @@ PRESSURE = {"cg": 0, "tridiag": 1, "cg_exact": 2}
 GEMV = {"tma": 0, "ldg": 1}
 
 
+FORMULATION = {"v": 0, "newton": 1}
+GUESS = {"analytic": 0, "mlp": 1, "warm": 2}
+
+
 def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64, hmat_leaf=0,
-                 hmat_eta=0.0, hmat_eps=0.0):
+                 hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0, newton_tol=0.0):
     """dfn_options; the H-matrix parameters default (0) to the reference's
     nleaf=100, eta=3, eps_ACA=1e-8 (src/variables.f90:122-124)."""
     opt = DfnOptions()
     lib.dfn_default_options(ctypes.byref(opt))
+    opt.formulation = FORMULATION[formulation]
+    opt.newton_guess = GUESS[guess]
+    opt.newton_maxit = int(newton_maxit)
+    opt.newton_tol = float(newton_tol)
     opt.kernel_storage = STORAGE[storage]
     opt.pressure_solver = PRESSURE[pressure]
     opt.device = int(device)
@@ -47,11 +55,14 @@ def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_a
 
 class Simulation:
     def __init__(self, problem, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
-                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0):
+                 hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0,
+                 newton_tol=0.0):
         self.lib = _lib.load()
         self.arrays = problem if isinstance(problem, ProblemArrays) else build_arrays(problem)
         self.N = self.arrays.N
-        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps)
+        opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
+                           formulation, guess, newton_maxit, newton_tol)
+        self.formulation = formulation
         self.options = {"storage": storage, "pressure": pressure, "gemv": gemv}
         self._c = to_c(self.arrays)
         h = ctypes.c_void_p()
@@ -159,6 +170,39 @@ class Simulation:
         ms = ctypes.c_double()
         _lib.check(self.lib.dfn_time_kernel(self.h, int(reps), ctypes.byref(ms)), self.lib)
         return ms.value
+
+    # -- learned Newton guess ------------------------------------------------
+    def set_mlp(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        _lib.check(self.lib.dfn_set_mlp(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.lib)
+
+    def record(self, capacity):
+        _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)
+
+    def record_read(self, max_samples):
+        x = np.empty((int(max_samples), 6), dtype=np.float32)
+        t = np.empty(int(max_samples), dtype=np.float32)
+        n = ctypes.c_int64()
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.lib.dfn_record_read(self.h, x.ctypes.data_as(fp), t.ctypes.data_as(fp), int(max_samples),
+                                            ctypes.byref(n)), self.lib)
+        return x[:n.value], t[:n.value]
+
+    def report(self):
+        rep = DfnReport()
+        _lib.check(self.lib.dfn_get_report(self.h, 0, ctypes.byref(rep)), self.lib)
+        return rep.as_dict()
+
+    def velocity(self):
+        V = np.empty(self.N)
+        _lib.check(self.lib.dfn_velocity(self.h, ptr(V)), self.lib)
+        return V
+
+    def solve_to(self, t_end):
+        """Advance to simulated time t_end (the last step lands on it)."""
+        reps = (DfnReport * 1)()
+        _lib.check(self.lib.dfn_solve_batch(self.h, 0, float(t_end), reps), self.lib)
+        return reps[0].as_dict()
 
     def hmat_stats(self):
         st = (ctypes.c_int64 * 8)()

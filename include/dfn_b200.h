@@ -96,10 +96,40 @@ typedef struct dfn_options {
     /* H-matrix parameters for static_kernel = hmatrix (0 = the reference's
      * defaults nleaf=100, eta=3, eps_ACA=1e-8, src/variables.f90:122-124) */
     int32_t hmat_leaf;
-    int32_t reserved;
+    /* DFN_FORM_V integrates V as the reference does; DFN_FORM_NEWTON
+     * integrates slip and psi and solves the friction law for V by Newton
+     * at every stage (no counterpart in the reference, see below). */
+    int32_t formulation;
     double hmat_eta;
     double hmat_eps;
+    int32_t newton_guess;     /* DFN_GUESS_* initial guess of the Newton solve */
+    int32_t newton_maxit;     /* Newton iteration cap (0 = 50) */
+    double newton_tol;        /* |residual| <= tol * (|tau| + sigma_eff*a*|w|) (0 = 1e-13) */
 } dfn_options;
+
+/* Newton formulation (options.formulation = DFN_FORM_NEWTON). The state is
+ * Y = [slip | psi | sigmaN0] (the third block keeps its initial value; its
+ * derivative is zero). Shear and normal traction are algebraic:
+ *   tau   = tau0 + K_T.slip + shear_loading_dot*(t - time0)
+ *   sigma = sigmaN0 + K_N.slip + normal_loading_dot*(t - time0)
+ * with tau0 chosen so that the initial V satisfies the friction law. Each
+ * stage solves tau - eta*V + (sigma+P)*a*asinh(V*C/(2 V0)) = 0 for V in
+ * w = asinh(V*C/(2 V0)), C = exp((f0 + b psi)/a), eta = mu/(2 cs); the
+ * derivative of this law in time is the reference's dV/dt
+ * (src/friction/RateStateAgingModeII.f90:54-68). */
+enum { DFN_FORM_V = 0, DFN_FORM_NEWTON = 1 };
+/* Initial guesses: ANALYTIC neglects radiation damping (w0 = tau/(sigma_eff a),
+ * exact when eta*V << tau); MLP adds the correction predicted by the learned
+ * network (dfn_set_mlp); WARM starts from the last solution of the element. */
+enum { DFN_GUESS_ANALYTIC = 0, DFN_GUESS_MLP = 1, DFN_GUESS_WARM = 2 };
+/* The learned guess: an FP32 MLP 6 -> 64 -> 64 -> 1 with SiLU activations.
+ * Weights, flat, in this order: W1[6][64], b1[64], W2[64][64], b2[64],
+ * W3[64], b3[1]. Inputs, from tau, psi, sigma_eff = -(sigmaN + P), P, a, b:
+ *   x = [w0/100, psi/30, ln(sigma_eff)/20 - 0.85, P/sigma_eff, 100a - 1, 100b - 1]
+ * with w0 = tau/(sigma_eff a); output y, guess w = w0 + 10 y. */
+#define DFN_MLP_PARAMS 4673
+#define DFN_MLP_IN 6
+#define DFN_MLP_HIDDEN 64
 
 /* Per-call report of the solve driver. */
 typedef struct dfn_report {
@@ -116,6 +146,9 @@ typedef struct dfn_report {
     int32_t pad;
     int64_t stage_cg_failures; /* stage pressure solves that hit the CG cap (the stage then uses the last
                                   CG iterate; the reference would use an uninitialised P_temp) */
+    int64_t newton_solves;     /* element Newton solves (Newton formulation) */
+    int64_t newton_iters;      /* Newton iterations summed over the solves */
+    int64_t newton_fail;       /* solves that hit the iteration cap */
 } dfn_report;
 
 typedef struct dfn_handle dfn_handle;
@@ -188,6 +221,8 @@ int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, dou
 int32_t dfn_solve_batch(dfn_handle *h, int64_t n_steps, double t_end, dfn_report *reps);
 int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, double *time, double *t_try,
                                int64_t *it_count);
+/* Counters and status of network i since the handle was created. */
+int32_t dfn_get_report(dfn_handle *h, int32_t i, dfn_report *rep);
 
 /* State access. Y has 3N entries. */
 int32_t dfn_get_state(dfn_handle *h, double *Y, double *P, double *time, double *t_try,
@@ -239,6 +274,32 @@ int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const 
                               int64_t nb_source, const int64_t *d_src_fault, const int64_t *d_src_element,
                               const double *d_src_Q, const double *d_src_t_beg, const double *d_src_t_end,
                               double *d_P_temp, double *d_P_dot, int32_t *ier, void *stream);
+
+/* ---- learned Newton guess (no counterpart in the reference) ------------- */
+/* Sets the MLP weights (DFN_MLP_PARAMS floats, host memory) used by
+ * DFN_GUESS_MLP. */
+int32_t dfn_set_mlp(dfn_handle *h, const float *weights);
+/* Records converged Newton solves: for every solve, the 6 MLP inputs and the
+ * training target (w* - w0)/10, FP32, in a device buffer of `capacity`
+ * samples (capacity 0 stops recording). dfn_record_read copies up to `max`
+ * samples to host memory (x: 6 per sample, t: 1) and returns the count. */
+int32_t dfn_record(dfn_handle *h, int64_t capacity);
+int32_t dfn_record_read(dfn_handle *h, float *x, float *t, int64_t max, int64_t *count);
+/* Trains the MLP on the GPU with the library's own forward/backward kernels
+ * (Adam, mean squared error, minibatches drawn in a seeded order) on n
+ * samples in host memory; weights (in/out) are DFN_MLP_PARAMS floats.
+ * loss[0]/loss[1] receive the mean loss of the first and the last epoch.
+ * Standalone: no handle, runs on the current device. */
+int32_t dfn_mlp_train(const float *x, const float *t, int64_t n, float *weights, int32_t epochs, int32_t batch,
+                      float lr, uint64_t seed, float *loss);
+/* Mean-squared-error loss and its gradient over n samples (host buffers),
+ * computed by the same device kernels as training; grad has
+ * DFN_MLP_PARAMS floats. */
+int32_t dfn_mlp_loss_grad(const float *x, const float *t, int64_t n, const float *weights, float *loss,
+                          float *grad);
+/* Slip rate of network 0 at its current state (Newton formulation: solves
+ * the friction law; V formulation: copies V). */
+int32_t dfn_velocity(dfn_handle *h, double *V);
 
 /* ---- H-matrix introspection (static_kernel = hmatrix) ------------------ */
 /* stats[0..7]: leaves, dense leaves, low-rank leaves, max rank, mean rank x 1000,
