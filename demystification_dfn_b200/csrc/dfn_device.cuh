@@ -974,14 +974,23 @@ __device__ __forceinline__ void newton_rhs(const FricParams &f, const float *mlp
     double w = w0;
     float x[MLP_IN];
     if (f.guess == 1 || f.rec_cap > 0) mlp_features(tau, psi, s, Pt, a, b, w0, x);
-    if (f.guess == 1) w = w0 + 10.0 * (double)mlp_forward(mlpW, x);
-    else if (f.guess == 2 && f.wlast[e] != 0.0) w = f.wlast[e];
     iters = 0;
     ok = 1;
     if (f.fake[e] || !(s > 0.0)) {
         dV = 0.0; dpsi = 0.0; dsig = 0.0;
         ok = f.fake[e] ? 1 : 0;
         return;
+    }
+    if (f.guess == 1) {
+        // the learned guess is judged by the FP64 residual: Newton starts
+        // from whichever of the analytic and the learned guess fits better
+        const double wm = w0 + 10.0 * (double)mlp_forward(mlpW, x);
+        double ev0, ev1, d0, d1;
+        eta_v(w0, lnA, eta, ev0, d0);
+        eta_v(wm, lnA, eta, ev1, d1);
+        if (fabs(tau - ev1 - s * a * wm) < fabs(tau - ev0 - s * a * w0)) w = wm;
+    } else if (f.guess == 2 && f.wlast[e] != 0.0) {
+        w = f.wlast[e];
     }
     w = newton_w(tau, s, a, lnA, eta, w, f.tol, f.maxit, iters, ok);
     f.wlast[e] = w;

@@ -120,7 +120,9 @@ typedef struct dfn_options {
 enum { DFN_FORM_V = 0, DFN_FORM_NEWTON = 1 };
 /* Initial guesses: ANALYTIC neglects radiation damping (w0 = tau/(sigma_eff a),
  * exact when eta*V << tau); MLP adds the correction predicted by the learned
- * network (dfn_set_mlp); WARM starts from the last solution of the element. */
+ * network (dfn_set_mlp) and Newton starts from whichever of the two guesses
+ * has the smaller FP64 residual; WARM starts from the last solution of the
+ * element. Convergence is always decided on the FP64 residual. */
 enum { DFN_GUESS_ANALYTIC = 0, DFN_GUESS_MLP = 1, DFN_GUESS_WARM = 2 };
 /* The learned guess: an FP32 MLP 6 -> 64 -> 64 -> 1 with SiLU activations.
  * Weights, flat, in this order: W1[6][64], b1[64], W2[64][64], b2[64],

@@ -63,11 +63,15 @@ def test_newton_formulation_reproduces_initial_velocity():
 
 @pytest.mark.gpu
 def test_newton_formulation_matches_v_formulation():
-    """Both formulations integrate the same physics; at the same final time
-    (runs land on t_end) slip rate and log-state agree to 1e-6."""
+    """Without pore-pressure forcing both formulations integrate the same ODE
+    (the V formulation is the time derivative of the friction law); at the
+    same final time (runs land on t_end) slip rate and log-state agree to
+    1e-6. With a diffusing pressure they differ at O(h): the reference's
+    V formulation uses the secant (P_temp - P)/dt for dP/dt and the pressure
+    at t_try for its first stage, the Newton formulation uses P_temp itself."""
     from demystification_dfn_b200.simulation import Simulation
 
-    p = _net()
+    p = _net(dP=0.0)
     t_end = 5000.0
     with Simulation(p, formulation="v", pressure="tridiag") as a, \
             Simulation(p, formulation="newton", pressure="tridiag") as b:
@@ -100,8 +104,9 @@ def test_learned_guess_saves_newton_iterations():
         out = []
         for _ in range(n):
             Y = Y0.copy()
-            # slip perturbations drive the stress (and V) over many decades
-            Y[:N] = rng.normal(0.0, 10 ** rng.uniform(-4, -1), N)
+            # slip perturbations drive the stress (and V) over many decades,
+            # up to fast slip (~1 m/s) where radiation damping matters
+            Y[:N] = rng.normal(0.0, 10 ** rng.uniform(-5, -2.6), N)
             Y[:N][s.arrays.fake_mask] = 0.0
             Y[N:2 * N] += rng.normal(0.0, 0.5, N)
             out.append(Y)
@@ -109,10 +114,10 @@ def test_learned_guess_saves_newton_iterations():
 
     with Simulation(p, formulation="newton", pressure="tridiag") as s:
         s.record(200000)
-        for Y in states(s, 300):
+        for Y in states(s, 1500):
             s.friction_law(1.0, Y)
         x, t = s.record_read(200000)
-    assert len(t) > 10000
+    assert len(t) > 20000
     w, loss = learned.train(x, t, epochs=40, batch=2048, lr=2e-3, seed=0)
     assert loss[1] < loss[0]
     test_states = None
@@ -129,6 +134,7 @@ def test_learned_guess_saves_newton_iterations():
             after = s.report()
             res[guess] = (after["newton_iters"] - before["newton_iters"],
                           after["newton_solves"] - before["newton_solves"], outs)
+            assert after["newton_fail"] == before["newton_fail"], guess
     ia, na, oa = res["analytic"]
     im, nm, om = res["mlp"]
     assert na == nm
