@@ -82,6 +82,8 @@ struct dfn_handle {
     int64_t *seg_start = nullptr;
     int *seg_inst = nullptr;
     int64_t nseg = 0, nseg0 = 0;
+    int *long_seg = nullptr;              // segments longer than TRI_SHORT_MAX
+    int64_t nlong = 0, nlong0 = 0;
     int64_t nsrc_tot = 0, part_tot = 0;
     // geometry and parameters (concatenated)
     double *node = nullptr, *elem = nullptr, *ds = nullptr, *tan = nullptr, *nrm = nullptr, *permx = nullptr;
@@ -239,6 +241,15 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
         pressure_tridiag_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
                                                              h->seg_start, h->seg_inst, nseg, h->Ptemp, h->Pdot_s,
                                                              h->pwork);
+        const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
+        if (nlong > 0) {
+            h->launches++;
+            CKL();
+            dim3 lgrid((unsigned)nlong, (unsigned)nsys);
+            pressure_tridiag_long_kernel<<<lgrid, TRI_NT, 0, h->stream>>>(
+                h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit, h->seg_start, h->seg_inst, h->long_seg,
+                h->Ptemp, h->Pdot_s, h->pwork);
+        }
     }
     h->launches++;
     CKL();
@@ -595,7 +606,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
-                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->node, h->elem, h->ds, h->tan,
+                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
                     h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
@@ -846,6 +857,18 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         DALLOC(h->seg_inst, sinst.size());
         HCOPY(h->seg_start, seg.data(), seg.size());
         HCOPY(h->seg_inst, sinst.data(), sinst.size());
+        // long segments go to the CTA-parallel solve; networks in order, so
+        // those of network 0 come first
+        std::vector<int> lg;
+        for (int64_t q = 0; q < h->nseg; q++) {
+            if (seg[q + 1] - seg[q] > TRI_SHORT_MAX) lg.push_back((int)q);
+            if (q + 1 == h->nseg0) h->nlong0 = (int64_t)lg.size();
+        }
+        h->nlong = (int64_t)lg.size();
+        if (h->nlong) {
+            DALLOC(h->long_seg, lg.size());
+            HCOPY(h->long_seg, lg.data(), lg.size());
+        }
     }
 
     if (h->hmat) {

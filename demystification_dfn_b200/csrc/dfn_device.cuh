@@ -641,6 +641,13 @@ __device__ __forceinline__ double block_max(double v, double *red)
     return red[32];
 }
 
+// Segments of more than TRI_SHORT_MAX elements are solved by a CTA of TRI_NT
+// threads (pressure_tridiag_long_kernel), rows in registers up to TRI_MAXM
+// rows per thread; shorter ones by one thread each.
+#define TRI_SHORT_MAX 48
+#define TRI_NT 256
+#define TRI_MAXM 16
+
 // System s of a pressure launch gets its dt from the controller:
 //   kind 0: dt = ctl->t_try (probe / first RHS), halving on non-convergence
 //   kind 1: dt = ctl->x + A_{s+1} * ctl->h   (stage s+1, s = 1..5)
@@ -896,6 +903,7 @@ __global__ void pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl
     const int64_t N = I.N;
     const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
     const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+    if (k1 - k0 > TRI_SHORT_MAX) return;                       // pressure_tridiag_long_kernel
     double *cp = work + 24 * I.eoff + (int64_t)sys * 4 * N;   // modified super-diagonal
     double *dp = cp + N;                                       // modified right-hand side
     double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
@@ -922,6 +930,214 @@ __global__ void pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl
         if (!isfinite(xk)) bad = true;
     }
     if (bad) atomicCAS(&ctl[i].status, 0, 4);
+}
+
+// ---------------------------------------------------------------------------
+// Long segments: the Thomas recurrences of one segment evaluated by a CTA.
+//
+// Thread t owns rows [t*m, t*m + m) of the segment (m = ceil(L / TRI_NT)).
+// The three sequential recurrences of the Thomas algorithm are each a scan
+// over an associative operator, so the CTA computes the value entering every
+// thread's rows with a two-level (warp shuffle + shared memory) scan of the
+// per-thread compositions and each thread then reruns the exact recurrence
+// over its own rows:
+//   c_k = A3_k / (A2_k - A1_k c_{k-1})       a Moebius map of c_{k-1}: the
+//        2x2 matrix [[0, A3], [-A1, A2]] acting on (p, q), c = p/q; products
+//        are rescaled by their largest entry (the ratio is unchanged);
+//   d_k = (r_k - A1_k d_{k-1}) / den_k        affine in d_{k-1};
+//   x_k = d_k - c_k x_{k+1}                   affine in x_{k+1}, scanned from
+//        the end of the segment.
+// The system is an M-matrix (diagonally dominant, A1, A3 <= 0), so |c| < 1
+// and every composed map is contracting; the result equals the sequential
+// solve to rounding. Rows live in registers for m <= TRI_MAXM, otherwise in
+// the global work area of the system.
+struct Mob { double a, b, c, d; };   // [[a, b], [c, d]]
+struct Aff { double a, b; };         // x -> a x + b
+
+__device__ __forceinline__ Mob mob_id() { return {1.0, 0.0, 0.0, 1.0}; }
+__device__ __forceinline__ Aff aff_id() { return {1.0, 0.0}; }
+// outer o applied after inner i
+__device__ __forceinline__ Mob compose(const Mob &o, const Mob &i)
+{
+    Mob r{o.a * i.a + o.b * i.c, o.a * i.b + o.b * i.d, o.c * i.a + o.d * i.c, o.c * i.b + o.d * i.d};
+    const double s = fmax(fmax(fabs(r.a), fabs(r.b)), fmax(fabs(r.c), fabs(r.d)));
+    if (s > 0.0 && isfinite(s)) {
+        const double q = 1.0 / s;
+        r.a *= q; r.b *= q; r.c *= q; r.d *= q;
+    }
+    return r;
+}
+__device__ __forceinline__ Aff compose(const Aff &o, const Aff &i) { return {o.a * i.a, o.a * i.b + o.b}; }
+__device__ __forceinline__ Mob shfl_up(const Mob &v, int d)
+{
+    return {__shfl_up_sync(0xffffffffu, v.a, d), __shfl_up_sync(0xffffffffu, v.b, d),
+            __shfl_up_sync(0xffffffffu, v.c, d), __shfl_up_sync(0xffffffffu, v.d, d)};
+}
+__device__ __forceinline__ Aff shfl_up(const Aff &v, int d)
+{
+    return {__shfl_up_sync(0xffffffffu, v.a, d), __shfl_up_sync(0xffffffffu, v.b, d)};
+}
+__device__ __forceinline__ Aff shfl_down(const Aff &v, int d)
+{
+    return {__shfl_down_sync(0xffffffffu, v.a, d), __shfl_down_sync(0xffffffffu, v.b, d)};
+}
+
+// Exclusive forward scan over the CTA (thread 0 first): returns the
+// composition of the maps of threads 0..t-1 (identity for t = 0).
+template <typename T>
+__device__ __forceinline__ T cta_scan_excl(T v, T ident, T *sm)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = TRI_NT / 32;
+    for (int d = 1; d < 32; d <<= 1) {
+        T o = shfl_up(v, d);
+        if (lane >= d) v = compose(v, o);
+    }
+    __syncthreads();
+    if (lane == 31) sm[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T acc = ident;
+        for (int q = 0; q < nw; q++) {
+            T tot = sm[q];
+            sm[q] = acc;               // prefix of the warps before q
+            acc = compose(tot, acc);
+        }
+    }
+    __syncthreads();
+    T prev = shfl_up(v, 1);
+    const T wp = sm[w];
+    return (lane == 0) ? wp : compose(prev, wp);
+}
+
+// Exclusive backward scan for affine maps: the composition of the maps of
+// threads t+1..NT-1, the last thread's applied first (identity for the last).
+__device__ __forceinline__ Aff cta_scan_excl_back(Aff v, Aff *sm)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = TRI_NT / 32;
+    for (int d = 1; d < 32; d <<= 1) {
+        Aff o = shfl_down(v, d);
+        if (lane + d < 32) v = compose(v, o);
+    }
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Aff acc = aff_id();
+        for (int q = nw - 1; q >= 0; q--) {
+            Aff tot = sm[q];
+            sm[q] = acc;               // composition of the warps after q
+            acc = compose(tot, acc);
+        }
+    }
+    __syncthreads();
+    Aff next = shfl_down(v, 1);
+    const Aff ws = sm[w];
+    return (lane == 31) ? ws : compose(next, ws);
+}
+
+// f(j) for the rows j < nr of this thread, in order (REV: reverse order);
+// with MAXM > 0 the loop is unrolled so that register arrays stay registers.
+template <int MAXM, bool REV, typename F>
+__device__ __forceinline__ void tri_rows(int nr, F f)
+{
+    if constexpr (MAXM > 0) {
+#pragma unroll
+        for (int q = 0; q < MAXM; q++) {
+            const int j = REV ? MAXM - 1 - q : q;
+            if (j < nr) f(j);
+        }
+    } else {
+        for (int q = 0; q < nr; q++) f(REV ? nr - 1 - q : q);
+    }
+}
+
+template <int MAXM>
+__device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int64_t k0, int64_t k1, double *Pt,
+                                            double *Pd, double *gw, int64_t N, Mob *smm, Aff *sma, int &bad)
+{
+    const int64_t L = k1 - k0;
+    const int64_t m = (L + TRI_NT - 1) / TRI_NT;
+    const int64_t r0 = (int64_t)threadIdx.x * m;
+    const int nr = (int)max((int64_t)0, min(m, L - r0));
+    constexpr int R = (MAXM > 0) ? MAXM : 1;
+    double reg[4][R];
+    // row q of element j of this thread: A1, den (A2 on input), c (A3 on
+    // input), d (right-hand side on input)
+    auto at = [&](int q, int j) -> double & {
+        if constexpr (MAXM > 0) return reg[q][j];
+        else return gw[(int64_t)q * N + k0 + r0 + j];
+    };
+    tri_rows<MAXM, false>(nr, [&](int j) {
+        const int64_t k = k0 + r0 + j;
+        double A1, A2, A3;
+        prow(p, k, dt, A1, A2, A3);
+        if (k == k0) A1 = 0.0;
+        if (k == k1 - 1) A3 = 0.0;
+        at(0, j) = A1; at(1, j) = A2; at(2, j) = A3;
+        at(3, j) = add_(p.P[k], psource(p, k, dt));
+    });
+    // c recurrence
+    Mob T = mob_id();
+    tri_rows<MAXM, false>(nr, [&](int j) { T = compose(Mob{0.0, at(2, j), -at(0, j), at(1, j)}, T); });
+    const Mob E = cta_scan_excl(T, mob_id(), smm);
+    double c = (threadIdx.x == 0) ? 0.0 : E.b / E.d;
+    tri_rows<MAXM, false>(nr, [&](int j) {
+        const double den = at(1, j) - at(0, j) * c;
+        c = at(2, j) / den;
+        at(1, j) = den; at(2, j) = c;
+    });
+    // d recurrence
+    Aff F = aff_id();
+    tri_rows<MAXM, false>(nr, [&](int j) { F = compose(Aff{-at(0, j) / at(1, j), at(3, j) / at(1, j)}, F); });
+    double d = cta_scan_excl(F, aff_id(), sma).b;
+    tri_rows<MAXM, false>(nr, [&](int j) {
+        d = (at(3, j) - at(0, j) * d) / at(1, j);
+        at(3, j) = d;
+    });
+    // back substitution
+    Aff G = aff_id();
+    tri_rows<MAXM, true>(nr, [&](int j) { G = compose(Aff{-at(2, j), at(3, j)}, G); });
+    double x = cta_scan_excl_back(G, sma).b;
+    tri_rows<MAXM, true>(nr, [&](int j) {
+        const int64_t k = k0 + r0 + j;
+        x = at(3, j) - at(2, j) * x;
+        Pt[k] = x;
+        Pd[k] = (dt < 1e-9) ? 0.0 : (x - p.P[k]) / dt;
+        if (!isfinite(x)) bad = 1;
+    });
+}
+
+// grid (long segments of the launch, systems); blockDim = TRI_NT.
+__global__ void __launch_bounds__(TRI_NT, 1) pressure_tridiag_long_kernel(PressGlobal g, const Inst *inst,
+                                                                          StepCtl *ctl, int mask, int kind, int sys0,
+                                                                          double dt_explicit,
+                                                                          const int64_t *seg_start,
+                                                                          const int *seg_inst, const int *long_seg,
+                                                                          double *Ptemp, double *Pdot, double *work)
+{
+    __shared__ Mob smm[TRI_NT / 32];
+    __shared__ Aff sma[TRI_NT / 32];
+    __shared__ int sbad;
+    const int sg = long_seg[blockIdx.x];
+    const int i = seg_inst[sg];
+    if (!takes_part(ctl, i, mask)) return;       // uniform over the CTA
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.y;
+    const int64_t N = I.N;
+    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
+    const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
+    double *gw = work + 24 * I.eoff + (int64_t)sys * 4 * N;
+    if (threadIdx.x == 0) sbad = 0;
+    int bad = 0;
+    if (k1 - k0 <= (int64_t)TRI_NT * TRI_MAXM)
+        tri_segment<TRI_MAXM>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
+    else
+        tri_segment<0>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
+    if (bad) atomicOr(&sbad, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && sbad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
 // ---------------------------------------------------------------------------

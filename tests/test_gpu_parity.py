@@ -117,6 +117,28 @@ def test_pressure_tridiag_is_exact(dt):
         assert rel(gP, ex) < 1e-12
 
 
+@pytest.mark.parametrize("case", ["fault4000", "fault6000", "mixed"])
+@pytest.mark.parametrize("dt", [0.5, 300.0, 86400.0])
+def test_pressure_tridiag_long_segments_are_exact(case, dt):
+    """Segments longer than 48 elements go to the CTA-parallel (scan) Thomas
+    solve: rows in registers up to 4096 elements, in global memory above;
+    the mixed network has segments on both sides of the 48-element split."""
+    if case == "mixed":
+        p = networks.fault_network(n_faults=6, box=3000.0, length_range=(300.0, 1500.0), seed=3, q_kgs=20.0)
+    else:
+        n = int(case[5:])
+        p = networks.single_fault(n_el=n, length=10.0 * n, mode="modeII")
+    o = Oracle(p)
+    with Simulation(p, pressure="tridiag") as s:
+        gP, gd, gi = s.compute_P(dt)
+        assert gi == 0
+        ex = o.pressure_exact(dt)
+        assert rel(gP, ex) < 1e-12
+        # P_dot = (P_new - P)/dt carries the error of P_new divided by dt
+        P0 = s.arrays.P
+        assert np.abs(gd - (ex - P0) / dt).max() <= 1e-11 * np.abs(ex).max() / dt
+
+
 @pytest.mark.parametrize("mode", ["modeII", "modeIII"])
 def test_friction_law_matches_oracle(mode):
     p = net(seed=7, n=4, mode=mode, tol=1e-6)
