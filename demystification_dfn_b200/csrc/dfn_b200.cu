@@ -121,7 +121,7 @@ struct dfn_handle {
     int form = 0, guess = 0, newton_maxit = 50;
     double newton_tol = 1e-13;
     double *tau0 = nullptr, *wlast = nullptr, *vnow = nullptr;
-    float *mlp = nullptr;
+    MlpTC *mlp = nullptr;                 // tensor-core image of the learned guess
     float *rec_x = nullptr, *rec_t = nullptr;
     unsigned long long *rec_n = nullptr;
     long long rec_cap = 0;
@@ -262,7 +262,7 @@ static FricParams fric_params(dfn_handle *h, int64_t nelem)
     f.Ntot = nelem; f.mode = h->mode; f.inst = h->inst; f.inst_of = h->inst_of;
     f.a = h->a; f.b = h->b; f.Dc = h->Dc; f.f0 = h->f0; f.V0 = h->V0; f.nload = h->nload; f.sload = h->sload;
     f.fake = h->fake; f.partT = h->partT; f.partN = h->partN; f.SigT = h->SigT; f.SigN = h->SigN;
-    f.Ptemp = h->Ptemp; f.Pdot = h->Pdot_s; f.y = h->Y; f.ytmp = h->ytmp; f.kbuf = h->kbuf; f.yscal = h->yscal;
+    f.Ptemp = h->Ptemp; f.Pdot = h->Pdot_s; f.Pc = h->P; f.y = h->Y; f.ytmp = h->ytmp; f.kbuf = h->kbuf; f.yscal = h->yscal;
     f.yout = h->yout; f.ctl = h->ctl;
     f.form = h->form; f.guess = h->guess; f.maxit = h->newton_maxit; f.tol = h->newton_tol; f.off_explicit = 0.0;
     f.tau0 = h->tau0; f.wlast = h->wlast; f.vnow = h->vnow; f.mlp = h->mlp;
@@ -274,8 +274,11 @@ static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t 
 {
     FricParams f = fric_params(h, nelem);
     f.off_explicit = off_explicit;
-    const size_t smem = (h->form == DFN_FORM_NEWTON && h->guess == DFN_GUESS_MLP) ? MLP_NPAR * sizeof(float) : 0;
-    friction_kernel<<<(unsigned)((nelem + 255) / 256), 256, smem, h->stream>>>(f, stage, sys, mask);
+    const unsigned grid = (unsigned)((nelem + 255) / 256);
+    if (h->form == DFN_FORM_NEWTON && h->guess == DFN_GUESS_MLP)
+        friction_kernel<true><<<grid, 256, sizeof(MlpTC), h->stream>>>(f, stage, sys, mask);
+    else
+        friction_kernel<false><<<grid, 256, 0, h->stream>>>(f, stage, sys, mask);
     h->launches++;
     CKL();
     return DFN_OK;
@@ -296,7 +299,12 @@ static int run_attempt(dfn_handle *h, int mask)
                                                                          mask);
     h->launches++;
     CKL();
-    TRY(launch_pressure(h, mask, 1, 1, 5, 0.0, h->B));
+    // the Newton formulation interpolates the stage pressure in time and
+    // needs only the full-step system (c = 1)
+    if (h->form == DFN_FORM_NEWTON)
+        TRY(launch_pressure(h, mask, 1, 4, 1, 0.0, h->B));
+    else
+        TRY(launch_pressure(h, mask, 1, 1, 5, 0.0, h->B));
     for (int s = 2; s <= 6; s++) {
         TRY(launch_gemv(h, mask, h->ytmp, 3, false));
         TRY(launch_friction(h, s, s - 1, mask, h->Ntot));
@@ -707,7 +715,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     h->pressure = opt.pressure_solver; h->gemv_impl = opt.gemv_impl;
     h->max_attempts = opt.max_attempts > 0 ? opt.max_attempts : 64;
     h->form = opt.formulation == DFN_FORM_NEWTON ? DFN_FORM_NEWTON : DFN_FORM_V;
-    h->guess = (opt.newton_guess >= 0 && opt.newton_guess <= 2) ? opt.newton_guess : 0;
+    h->guess = (opt.newton_guess >= 0 && opt.newton_guess <= 3) ? opt.newton_guess : 0;
     h->newton_maxit = opt.newton_maxit > 0 ? opt.newton_maxit : 50;
     h->newton_tol = opt.newton_tol > 0 ? opt.newton_tol : 1e-13;
     const int bpc = bytes_per_col(h->mode, h->store);
@@ -820,8 +828,8 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         CKC(cudaGetLastError());
     }
     HCOPY(h->inst_of, inst_of.data(), Nt);
-    DALLOC(h->mlp, MLP_NPAR);
-    CKC(cudaMemset(h->mlp, 0, sizeof(float) * MLP_NPAR));
+    CKC(cudaMalloc((void **)&h->mlp, kMlpImgBytes));
+    CKC(cudaMemset(h->mlp, 0, kMlpImgBytes));
     DALLOC(h->rec_n, 1);
     CKC(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
     if (h->form == DFN_FORM_NEWTON) {
@@ -1275,7 +1283,20 @@ int32_t dfn_set_mlp(dfn_handle *h, const float *weights)
 {
     if (!h || !weights) return DFN_ERR_ARG;
     CK(cudaSetDevice(h->dev));
-    CK(cudaMemcpy(h->mlp, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice));
+    // FP32 weights in, the kernels' FP16 tensor-core image out
+    float *w = nullptr;
+    CK(cudaMalloc((void **)&w, sizeof(float) * MLP_NPAR));
+    cudaError_t e = cudaMemcpyAsync(w, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        mlp_image_kernel<<<1, 256, 0, h->stream>>>(w, h->mlp);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(w);
+    if (e != cudaSuccess) {
+        set_err("dfn_set_mlp", e, __FILE__, __LINE__);
+        return DFN_ERR_CUDA;
+    }
     return DFN_OK;
 }
 
@@ -1373,6 +1394,21 @@ int32_t dfn_mlp_loss_grad(const float *x, const float *t, int64_t n, const float
     TRY(mlp_pass(b.X, b.T, n, n, b.W, b.m, b.v, b.g, b.gp, b.lp, b.ls, 1, 0.0f, &ls, nullptr));
     *loss = ls / (float)n;
     CK(cudaMemcpy(grad, b.g, sizeof(float) * MLP_NPAR, cudaMemcpyDeviceToHost));
+    return DFN_OK;
+}
+
+int32_t dfn_mlp_infer(const float *x, int64_t n, const float *weights, float *y)
+{
+    if (!x || n < 1 || !weights || !y) return DFN_ERR_ARG;
+    MlpBuffers b;
+    CK(cudaMalloc((void **)&b.X, sizeof(float) * MLP_IN * n));
+    CK(cudaMalloc((void **)&b.T, sizeof(float) * n));
+    CK(cudaMalloc((void **)&b.W, sizeof(float) * MLP_NPAR));
+    CK(cudaMemcpy(b.X, x, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.W, weights, sizeof(float) * MLP_NPAR, cudaMemcpyHostToDevice));
+    mlp_infer_kernel<<<(unsigned)((n + 255) / 256), 256, sizeof(MlpTC)>>>(b.X, n, b.W, b.T);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(y, b.T, sizeof(float) * n, cudaMemcpyDeviceToHost));
     return DFN_OK;
 }
 

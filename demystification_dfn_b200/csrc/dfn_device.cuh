@@ -1152,6 +1152,7 @@ struct FricParams {
     const double *partT, *partN;  // per instance [nchunk][N] at poff
     double *SigT, *SigN;          // stress rates of this evaluation
     const double *Ptemp, *Pdot;   // per instance [6][N] at 6*eoff
+    const double *Pc;             // committed pressure [Ntot]
     const double *y;              // state at the step start, [3N] at 3*eoff
     double *ytmp;                 // ytemp of this stage (in) / next stage (out)
     double *kbuf;                 // per instance [6][3N] at 18*eoff
@@ -1166,7 +1167,7 @@ struct FricParams {
     const double *tau0;           // [Ntot] shear traction at slip 0
     double *wlast;                // [Ntot] last solution, warm start
     double *vnow;                 // [Ntot] V of this evaluation
-    const float *mlp;             // DFN_MLP_PARAMS weights (global)
+    const MlpTC *mlp;             // tensor-core image of the learned guess (global)
     float *rec_x, *rec_t;         // recorded solves
     unsigned long long *rec_n;
     long long rec_cap;
@@ -1175,54 +1176,96 @@ struct FricParams {
 // Newton formulation of one element: stresses from slip, V from the
 // friction law (newton_core.cuh), derivatives of slip and log-state. The
 // normal-stress slot of the state holds sigmaN at slip 0 (derivative 0).
-__device__ __forceinline__ void newton_rhs(const FricParams &f, const float *mlpW, int64_t e, int mode, double eta,
-                                           double tt, double slip_unused, double psi, double sig0, double T,
-                                           double Nn, double Pt, double &dV, double &dpsi, double &dsig, int &iters,
-                                           int &ok)
-{
-    (void)slip_unused;
-    const double a = f.a[e], b = f.b[e], V0 = f.V0[e], Dc = f.Dc[e];
-    const double tau = f.tau0[e] + T + f.sload[e] * tt;
-    const double sig = ((mode == 2) ? sig0 + Nn : sig0) + f.nload[e] * tt;
-    const double s = -(sig + Pt);
-    const double lnA = log(2.0 * V0) - (f.f0[e] + b * psi) / a;
-    const double w0 = tau / (s * a);
-    double w = w0;
+// First half: stresses of the stage, the bounded analytic start and its
+// residual, the network inputs where the start misses the tolerance.
+struct NPre {
+    double tau, s, lnA, wa, ga;
+    int kind;          // 0 fake element, 1 no frictional strength, 2 solve
+    bool wa_ok;        // the analytic start meets the tolerance
+    bool need;         // the network is evaluated for this element
     float x[MLP_IN];
-    if (f.guess == 1 || f.rec_cap > 0) mlp_features(tau, psi, s, Pt, a, b, w0, x);
+};
+
+__device__ __forceinline__ void newton_pre(const FricParams &f, int64_t e, int mode, double eta, double tt,
+                                           double psi, double sig0, double T, double Nn, double Pt, NPre &q)
+{
+    const double a = f.a[e], b = f.b[e], V0 = f.V0[e];
+    q.tau = f.tau0[e] + T + f.sload[e] * tt;
+    const double sig = ((mode == 2) ? sig0 + Nn : sig0) + f.nload[e] * tt;
+    q.s = -(sig + Pt);
+    q.wa_ok = true;
+    q.need = false;
+    q.kind = f.fake[e] ? 0 : (q.s > 0.0 ? 2 : 1);
+    if (q.kind != 2) return;
+    const double s = q.s, tau = q.tau;
+    q.lnA = log(2.0 * V0) - (f.f0[e] + b * psi) / a;
+    // g(w) = tau - eta V(w) - s a w is decreasing, concave for w > 0 (convex
+    // for w < 0); the friction-only root w0 and the radiation-only root wr
+    // both lie beyond the root on the same side, so the one nearer zero is a
+    // start from which Newton approaches the root monotonically.
+    const double w0 = tau / (s * a);
+    const double wr = w_radiation(tau, eta, q.lnA);
+    q.wa = (f.guess != 3 && fabs(wr) < fabs(w0)) ? wr : w0;
+    q.ga = 0.0;
+    // residual of the analytic start; where it meets the tolerance (slow
+    // slip, radiation damping negligible) Newton takes no step and the
+    // network is neither evaluated nor trained on the solve
+    if (f.guess == 1 || f.rec_cap > 0) {
+        double eva, da;
+        eta_v(q.wa, q.lnA, eta, eva, da);
+        q.ga = fabs(tau - eva - s * a * q.wa);
+        q.wa_ok = q.ga <= f.tol * (fabs(tau) + s * a * fabs(q.wa) + 1e-300);
+        if (!q.wa_ok) mlp_features(q.wa, w0, wr, psi, s, Pt, a, b, q.x);
+        q.need = (f.guess == 1) && !q.wa_ok;
+    }
+}
+
+// Second half: the solve from the chosen start, the slip rate and the
+// derivatives [dslip, dpsi, dsigma0]; ym is the network's output.
+__device__ __forceinline__ void newton_post(const FricParams &f, int64_t e, double eta, double psi, const NPre &q,
+                                            float ym, double &dV, double &dpsi, double &dsig, int &iters, int &ok)
+{
     iters = 0;
     ok = 1;
-    if (f.fake[e] || !(s > 0.0)) {
-        dV = 0.0; dpsi = 0.0; dsig = 0.0;
-        ok = f.fake[e] ? 1 : 0;
+    dsig = 0.0;
+    if (q.kind == 0) {
+        dV = 0.0; dpsi = 0.0;
         return;
     }
-    if (f.guess == 1) {
-        // the learned guess is judged by the FP64 residual: Newton starts
-        // from whichever of the analytic and the learned guess fits better
-        const double wm = w0 + 10.0 * (double)mlp_forward(mlpW, x);
-        double ev0, ev1, d0, d1;
-        eta_v(w0, lnA, eta, ev0, d0);
-        eta_v(wm, lnA, eta, ev1, d1);
-        if (fabs(tau - ev1 - s * a * wm) < fabs(tau - ev0 - s * a * w0)) w = wm;
-    } else if (f.guess == 2 && f.wlast[e] != 0.0) {
-        w = f.wlast[e];
+    const double a = f.a[e], V0 = f.V0[e], Dc = f.Dc[e];
+    double V;
+    if (q.kind == 1) {
+        // effective normal stress not compressive: no frictional strength,
+        // the traction is balanced by radiation damping alone
+        V = q.tau / eta;
+    } else {
+        double w = q.wa;
+        if (q.need) {
+            // the learned guess is judged by the FP64 residual: Newton
+            // starts from whichever of the two guesses fits better
+            const double wm = q.wa + 10.0 * (double)ym;
+            double ev1, d1;
+            eta_v(wm, q.lnA, eta, ev1, d1);
+            if (fabs(q.tau - ev1 - q.s * a * wm) < q.ga) w = wm;
+        }
+        if (f.guess == 2 && f.wlast[e] != 0.0) w = f.wlast[e];
+        w = newton_w(q.tau, q.s, a, q.lnA, eta, w, f.tol, f.maxit, iters, ok);
+        f.wlast[e] = w;
+        V = v_of_w(w, q.lnA);
+        // recorded: converged solves the analytic start does not settle,
+        // the only ones that evaluate the network when it is deployed
+        if (ok && !q.wa_ok && f.rec_cap > 0) {
+            const unsigned long long r = atomicAdd(f.rec_n, 1ull);
+            if ((long long)r < f.rec_cap) {
+#pragma unroll
+                for (int i = 0; i < MLP_IN; i++) f.rec_x[r * MLP_IN + i] = q.x[i];
+                f.rec_t[r] = (float)((w - q.wa) / 10.0);
+            }
+        }
     }
-    w = newton_w(tau, s, a, lnA, eta, w, f.tol, f.maxit, iters, ok);
-    f.wlast[e] = w;
-    const double V = v_of_w(w, lnA);
     f.vnow[e] = V;
     dV = V;                                        // d slip / dt
     dpsi = V0 / Dc * exp(-psi) - fabs(V) / Dc;     // aging law, as the reference
-    dsig = 0.0;
-    if (ok && f.rec_cap > 0) {
-        const unsigned long long q = atomicAdd(f.rec_n, 1ull);
-        if ((long long)q < f.rec_cap) {
-#pragma unroll
-            for (int i = 0; i < MLP_IN; i++) f.rec_x[q * MLP_IN + i] = x[i];
-            f.rec_t[q] = (float)((w - w0) / 10.0);
-        }
-    }
 }
 
 __device__ __forceinline__ void rsf_rhs(const FricParams &f, int mode, int64_t e, double mu_2cs, double V, double psi,
@@ -1255,16 +1298,13 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
 //        2..5 = k_s, then ytemp of stage s+1 in place
 //        6 = k6, then yout, yerr and the max-norm contribution
 // sys: pressure system of this evaluation; mask: phases that take part.
+// LEARNED: Newton formulation with the learned guess (a separate
+// instantiation keeps the tensor-core inference's registers out of the
+// other variants).
+template <bool LEARNED>
 __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
 {
-    extern __shared__ float fric_smem[];
-    const float *mlpW = f.mlp;
-    if (f.form == 1 && f.guess == 1) {
-        // the learned guess: weights to shared memory for the whole block
-        for (int p = threadIdx.x; p < MLP_NPAR; p += blockDim.x) fric_smem[p] = f.mlp[p];
-        __syncthreads();
-        mlpW = fric_smem;
-    }
+    extern __shared__ __align__(16) unsigned char fric_smem[];
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int myi = -1;
     int nit = 0, nsolve = 0, nfail = 0;
@@ -1273,11 +1313,18 @@ __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
         const int i = f.inst_of[e];
         if (takes_part(f.ctl, i, mask)) myi = i;
     }
+    // phase 1: stresses, stage state and pressure; for the Newton
+    // formulation the analytic start and the network inputs
+    double T = 0.0, Nn = 0.0, V = 0.0, psi = 0.0, sig = 0.0, Pt = 0.0, Pd = 0.0;
+    NPre q;
+    q.kind = 0;
+    q.need = false;
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i++) q.x[i] = 0.0f;
     if (myi >= 0) {
         const Inst &I = f.inst[myi];
-        const int64_t N = I.N, k = e - I.eoff, S = 3 * N;
-        StepCtl *ctl = f.ctl + myi;
-        double T = 0.0, Nn = 0.0;
+        const int64_t N = I.N, k = e - I.eoff;
+        const StepCtl *ctl = f.ctl + myi;
         const double *pT = f.partT + I.poff + k;
         for (int64_t c = 0; c < I.nchunk; c++) T += pT[c * N];
         T = I.prefT * T;
@@ -1288,19 +1335,50 @@ __global__ void friction_kernel(FricParams f, int stage, int sys, int mask)
         }
         f.SigT[e] = T;
         f.SigN[e] = Nn;
-        const double *yi = f.y + 3 * I.eoff;
-        double *yt = f.ytmp + 3 * I.eoff;
-        const double *yin = (stage == 1) ? yi : yt;
-        const double V = yin[k], psi = yin[N + k], sig = yin[2 * N + k];
-        const double Pt = f.Ptemp[6 * I.eoff + (int64_t)sys * N + k];
-        const double Pd = f.Pdot[6 * I.eoff + (int64_t)sys * N + k];
-        double dV, dpsi, dsig;
+        const double *yin = (stage == 1) ? f.y + 3 * I.eoff : f.ytmp + 3 * I.eoff;
+        V = yin[k]; psi = yin[N + k]; sig = yin[2 * N + k];
+        Pt = f.Ptemp[6 * I.eoff + (int64_t)sys * N + k];
+        Pd = f.Pdot[6 * I.eoff + (int64_t)sys * N + k];
+        if (f.form == 1 && stage >= 1) {
+            // Newton formulation: the stress balance uses P itself, so the
+            // stage pressure must be smooth in the stage time. It is linear
+            // between the committed P (c = 0) and the implicit-Euler P over
+            // the whole step (system 4, c = 1), which is what is committed.
+            const double p0 = f.Pc[I.eoff + k];
+            const double c = (stage == 1) ? 0.0 : ck_a(stage);
+            Pt = add_(p0, mul_(c, f.Ptemp[6 * I.eoff + 4 * N + k] - p0));
+        }
         if (f.form == 1) {
             const double off = (stage == 0) ? f.off_explicit
                                             : (stage == 1 ? 0.0 : add_(ctl->x, mul_(ck_a(stage), ctl->h)));
             const double tt = (ctl->time - I.t0) + off;
+            newton_pre(f, e, f.mode, I.mu_2cs, tt, psi, sig, T, Nn, Pt, q);
+        }
+    }
+    // the learned guess: the network's image goes to shared memory only in
+    // blocks where some element needs it, and runs only in those warps
+    float ym = 0.0f;
+    if constexpr (LEARNED) {
+        MlpTC &S = *reinterpret_cast<MlpTC *>(fric_smem);
+        if (__syncthreads_or(q.need)) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(f.mlp);
+            uint4 *dst = reinterpret_cast<uint4 *>(fric_smem);
+            for (int p = threadIdx.x; p < (int)(sizeof(MlpTC) / 16); p += blockDim.x) dst[p] = src[p];
+            __syncthreads();
+            if (__any_sync(0xffffffffu, q.need)) ym = mlp_warp_tc(S, q.x);
+        }
+    }
+    // phase 2: derivatives and the Cash-Karp stage arithmetic
+    if (myi >= 0) {
+        const Inst &I = f.inst[myi];
+        const int64_t N = I.N, k = e - I.eoff, S = 3 * N;
+        StepCtl *ctl = f.ctl + myi;
+        const double *yi = f.y + 3 * I.eoff;
+        double *yt = f.ytmp + 3 * I.eoff;
+        double dV, dpsi, dsig;
+        if (f.form == 1) {
             int ok = 1;
-            newton_rhs(f, mlpW, e, f.mode, I.mu_2cs, tt, V, psi, sig, T, Nn, Pt, dV, dpsi, dsig, nit, ok);
+            newton_post(f, e, I.mu_2cs, psi, q, ym, dV, dpsi, dsig, nit, ok);
             nsolve = f.fake[e] ? 0 : 1;
             nfail = ok ? 0 : 1;
         } else {

@@ -106,6 +106,26 @@ __global__ void __launch_bounds__(256) mlp_grad_kernel(const float *__restrict__
 }
 
 // Sum of the block partials (fixed order); with lr > 0 also one Adam step.
+// The FP16 tensor-core image of the FP32 weights (one block).
+__global__ void mlp_image_kernel(const float *__restrict__ W, MlpTC *img) { mlp_tc_stage(*img, W); }
+
+// Inference of n rows by the friction kernel's tensor-core path; every lane
+// of every warp takes part (rows past n are zero inputs, not stored).
+__global__ void __launch_bounds__(256) mlp_infer_kernel(const float *__restrict__ X, int64_t n,
+                                                        const float *__restrict__ W, float *__restrict__ Y)
+{
+    extern __shared__ __align__(16) unsigned char infer_smem[];
+    MlpTC &S = *reinterpret_cast<MlpTC *>(infer_smem);
+    mlp_tc_stage(S, W);
+    __syncthreads();
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    float x[MLP_IN];
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i++) x[i] = (r < n) ? X[r * MLP_IN + i] : 0.0f;
+    const float y = mlp_warp_tc(S, x);
+    if (r < n) Y[r] = y;
+}
+
 __global__ void mlp_reduce_adam_kernel(const float *__restrict__ gpart, int nblk, float *W, float *m, float *v,
                                        float *gout, int step, float lr)
 {

@@ -95,7 +95,7 @@ class Ensemble:
         _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)
 
     def record_read(self, max_samples):
-        x = np.empty((int(max_samples), 6), dtype=np.float32)
+        x = np.empty((int(max_samples), 7), dtype=np.float32)
         t = np.empty(int(max_samples), dtype=np.float32)
         n = ctypes.c_int64()
         fp = ctypes.POINTER(ctypes.c_float)

@@ -16,8 +16,8 @@ import numpy as np
 
 from . import _lib
 
-N_IN, N_H = 6, 64
-N_PARAMS = N_IN * N_H + N_H + N_H * N_H + N_H + N_H + 1   # 4673
+N_IN, N_H = 7, 64
+N_PARAMS = N_IN * N_H + N_H + N_H * N_H + N_H + N_H + 1   # 4737
 
 
 def _fp(a):
@@ -38,7 +38,7 @@ def init_weights(seed=0):
 
 
 def train(x, t, weights=None, epochs=20, batch=4096, lr=2e-3, seed=0):
-    """Train on (x [n,6], t [n]) with the GPU kernels; returns (weights, loss first/last epoch)."""
+    """Train on (x [n,7], t [n]) with the GPU kernels; returns (weights, loss first/last epoch)."""
     lib = _lib.load()
     x = np.ascontiguousarray(x, dtype=np.float32)
     t = np.ascontiguousarray(t, dtype=np.float32)
@@ -59,3 +59,14 @@ def loss_grad(x, t, weights):
     g = np.zeros(N_PARAMS, dtype=np.float32)
     _lib.check(lib.dfn_mlp_loss_grad(_fp(x), _fp(t), len(t), _fp(w), _fp(loss), _fp(g)), lib)
     return float(loss[0]), g
+
+
+def infer(x, weights):
+    """Network outputs for rows x [n, 7] by the friction kernel's inference
+    path (FP16 tensor-core MMAs, FP32 accumulation)."""
+    lib = _lib.load()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    y = np.zeros(len(x), dtype=np.float32)
+    _lib.check(lib.dfn_mlp_infer(_fp(x), len(x), _fp(w), _fp(y)), lib)
+    return y

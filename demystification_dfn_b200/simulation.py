@@ -29,7 +29,7 @@ GEMV = {"tma": 0, "ldg": 1}
 
 
 FORMULATION = {"v": 0, "newton": 1}
-GUESS = {"analytic": 0, "mlp": 1, "warm": 2}
+GUESS = {"analytic": 0, "mlp": 1, "warm": 2, "quasistatic": 3}
 
 
 def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64, hmat_leaf=0,
@@ -180,7 +180,7 @@ class Simulation:
         _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)
 
     def record_read(self, max_samples):
-        x = np.empty((int(max_samples), 6), dtype=np.float32)
+        x = np.empty((int(max_samples), 7), dtype=np.float32)
         t = np.empty(int(max_samples), dtype=np.float32)
         n = ctypes.c_int64()
         fp = ctypes.POINTER(ctypes.c_float)

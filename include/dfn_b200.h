@@ -118,19 +118,31 @@ typedef struct dfn_options {
  * derivative of this law in time is the reference's dV/dt
  * (src/friction/RateStateAgingModeII.f90:54-68). */
 enum { DFN_FORM_V = 0, DFN_FORM_NEWTON = 1 };
-/* Initial guesses: ANALYTIC neglects radiation damping (w0 = tau/(sigma_eff a),
- * exact when eta*V << tau); MLP adds the correction predicted by the learned
- * network (dfn_set_mlp) and Newton starts from whichever of the two guesses
- * has the smaller FP64 residual; WARM starts from the last solution of the
- * element. Convergence is always decided on the FP64 residual. */
-enum { DFN_GUESS_ANALYTIC = 0, DFN_GUESS_MLP = 1, DFN_GUESS_WARM = 2 };
-/* The learned guess: an FP32 MLP 6 -> 64 -> 64 -> 1 with SiLU activations.
- * Weights, flat, in this order: W1[6][64], b1[64], W2[64][64], b2[64],
- * W3[64], b3[1]. Inputs, from tau, psi, sigma_eff = -(sigmaN + P), P, a, b:
- *   x = [w0/100, psi/30, ln(sigma_eff)/20 - 0.85, P/sigma_eff, 100a - 1, 100b - 1]
- * with w0 = tau/(sigma_eff a); output y, guess w = w0 + 10 y. */
-#define DFN_MLP_PARAMS 4673
-#define DFN_MLP_IN 6
+/* Initial guesses (w = asinh(V C / 2 V0), C = exp((f0 + b psi)/a)):
+ * QUASISTATIC neglects radiation damping, w0 = tau/(sigma_eff a), exact when
+ * eta*V << tau; ANALYTIC takes whichever of w0 and the radiation-only root
+ * wr (eta V(wr) = tau) is nearer zero: both bound the root from the same
+ * side, so Newton converges monotonically from it; MLP adds the correction
+ * predicted by the learned network (dfn_set_mlp) to the ANALYTIC start and
+ * Newton starts from whichever of the two has the smaller FP64 residual (the
+ * network is evaluated only where the ANALYTIC start misses the tolerance);
+ * WARM starts from the last solution of the element. Convergence is always
+ * decided on the FP64 residual. With sigma_eff <= 0 there is no frictional
+ * strength and V = tau/eta without a solve. */
+enum { DFN_GUESS_ANALYTIC = 0, DFN_GUESS_MLP = 1, DFN_GUESS_WARM = 2, DFN_GUESS_QUASISTATIC = 3 };
+/* The learned guess: an MLP 7 -> 64 -> 64 -> 1 with SiLU activations,
+ * trained in FP32; the friction kernel evaluates it with FP16 tensor-core
+ * MMAs and FP32 accumulation. Weights, flat, in this order: W1[7][64],
+ * b1[64], W2[64][64], b2[64], W3[64], b3[1]. Inputs, from tau, psi,
+ * sigma_eff = -(sigmaN + P), P, a, b:
+ *   x = [wa/100, psi/30, ln(sigma_eff)/20 - 0.85, P/(sigma_eff + |P|),
+ *        100a - 1, 100b - 1, clamp(|wr| - |w0|, -30, 30)/10]
+ * with wa the ANALYTIC start; output y, guess w = wa + 10 y. Recorded
+ * training samples (dfn_record) are these inputs and the target
+ * (w* - wa)/10 of converged solves whose ANALYTIC start missed the
+ * tolerance. */
+#define DFN_MLP_PARAMS 4737
+#define DFN_MLP_IN 7
 #define DFN_MLP_HIDDEN 64
 
 /* Per-call report of the solve driver. */
@@ -282,9 +294,10 @@ int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const 
  * DFN_GUESS_MLP. */
 int32_t dfn_set_mlp(dfn_handle *h, const float *weights);
 /* Records converged Newton solves: for every solve, the 6 MLP inputs and the
- * training target (w* - w0)/10, FP32, in a device buffer of `capacity`
+ * training target (w* - wa)/10, FP32, in a device buffer of `capacity`
  * samples (capacity 0 stops recording). dfn_record_read copies up to `max`
- * samples to host memory (x: 6 per sample, t: 1) and returns the count. */
+ * samples to host memory (x: DFN_MLP_IN per sample, t: 1) and returns the
+ * count. */
 int32_t dfn_record(dfn_handle *h, int64_t capacity);
 int32_t dfn_record_read(dfn_handle *h, float *x, float *t, int64_t max, int64_t *count);
 /* Trains the MLP on the GPU with the library's own forward/backward kernels
@@ -299,6 +312,10 @@ int32_t dfn_mlp_train(const float *x, const float *t, int64_t n, float *weights,
  * DFN_MLP_PARAMS floats. */
 int32_t dfn_mlp_loss_grad(const float *x, const float *t, int64_t n, const float *weights, float *loss,
                           float *grad);
+/* Network outputs y[n] for n input rows (host buffers) by the inference path
+ * of the friction kernel: one warp per 32 rows, FP16 tensor-core MMAs with
+ * FP32 accumulation. */
+int32_t dfn_mlp_infer(const float *x, int64_t n, const float *weights, float *y);
 /* Slip rate of network 0 at its current state (Newton formulation: solves
  * the friction law; V formulation: copies V). */
 int32_t dfn_velocity(dfn_handle *h, double *V);

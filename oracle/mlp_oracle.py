@@ -1,6 +1,6 @@
 """numpy FP64 oracle of the learned-guess MLP (test infrastructure only).
 
-Forward pass and backward pass of the 6 -> 64 -> 64 -> 1 SiLU network with
+Forward pass and backward pass of the 7 -> 64 -> 64 -> 1 SiLU network with
 the flat weight layout of include/dfn_b200.h, and the mean squared error.
 The network has no counterpart in the reference; this oracle checks the
 GPU training kernels' loss and gradients (and is itself checked against
@@ -8,7 +8,7 @@ finite differences in tests/test_oracle.py).
 """
 import numpy as np
 
-N_IN, N_H = 6, 64
+N_IN, N_H = 7, 64
 
 
 def unpack(w):
