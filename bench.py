@@ -130,6 +130,172 @@ def cpu_baseline(problem, threads, budget_s=20.0):
     return steps, dt
 
 
+def _timed(stream, fn):
+    import torch
+
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a0.record(stream)
+    out = fn()
+    a1.record(stream)
+    torch.cuda.synchronize()
+    return out, a0.elapsed_time(a1)
+
+
+def leg_single_fault(args, local, stream):
+    """One straight 40 km fault, 4000 x 10 m elements, mode II dense FP64
+    kernel (256 MB), injection at the centre, tol 1e-8; CG (the reference's
+    solver) and the exact tridiagonal pressure solve."""
+    from demystification_dfn_b200 import networks
+    from demystification_dfn_b200.simulation import Simulation
+
+    p = networks.single_fault()
+    out = {"workload": "single fault 40 km, 4000 elements, mode II, 50 kg/s injection, tol 1e-8"}
+    for pressure in ("cg", "tridiag"):
+        s = Simulation(p, pressure=pressure, device=local, gemv=args.gemv)
+        s.set_stream(stream.cuda_stream)
+        s.solve_steps(3)
+        n = 200
+        rep, ms = _timed(stream, lambda: s.solve_steps(n))
+        out[pressure] = {"steps_per_s": n / (ms / 1e3), "kv_ms": s.time_kernel(20), "kv_bytes": s.kernel_bytes,
+                         "simulated_s": rep["time"], "cg_iterations": rep["cg_iterations"],
+                         "probe_halvings": rep["probe_halvings"]}
+        s.close()
+    return out
+
+
+def leg_hmatrix(args, local, stream):
+    """4000 seeded faults in 20 km x 20 km (~82k elements), H-matrix with
+    leaf 64, eta 2, ACA 1e-6, FP32 factors, FP64 sums."""
+    from demystification_dfn_b200 import networks
+    from demystification_dfn_b200.simulation import Simulation
+
+    hbm, _ = peaks()
+    p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
+    t0 = time.perf_counter()
+    s = Simulation(p, storage="fp32", pressure=args.pressure, device=local, gemv=args.gemv, hmat_leaf=64,
+                   hmat_eta=2.0, hmat_eps=1e-6)
+    build_s = time.perf_counter() - t0
+    s.set_stream(stream.cuda_stream)
+    st = s.hmat_stats()
+    s.solve_steps(3)
+    s.profile_kv(True)
+    n = 10
+    rep, ms = _timed(stream, lambda: s.solve_steps(n))
+    kms, kn = s.profile_kv_read()
+    s.profile_kv(False)
+    kavg = kms / max(kn, 1)
+    gbs = s.kernel_bytes / (kavg / 1e3) / 1e9
+    dense_equiv = 2 * s.N * s.N * 4
+    out = {"workload": "4000 faults 20x20 km, H-matrix leaf 64 eta 2 ACA 1e-6, FP32 factors", "n_elements": s.N,
+           "build_s": build_s, "stats": st, "steps_per_s": n / (ms / 1e3), "kv_avg_ms": kavg,
+           "kv_bytes": s.kernel_bytes, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
+           "compression_vs_dense_fp32": s.kernel_bytes / dense_equiv, "simulated_s": rep["time"]}
+    s.close()
+    return out
+
+
+def leg_learned(args, local, stream):
+    """Newton slip formulation with the learned initial guess.
+
+    Record the Newton solves that the analytic start does not settle on
+    training networks (ensemble seeds 0-7, 120 faults each), train the MLP on
+    the GPU, then deploy it on held-out seeds 64-71 up to the same simulated
+    time as (i) the FP64 Newton run with the analytic start, the reference of
+    this formulation, (ii) FP32 storage with the analytic start and (iii)
+    FP32 storage with the learned guess; (ii') FP32 with the quasi-static
+    start (radiation damping neglected) shows what the bounded analytic start
+    already saves. The FP64 V formulation (the reference's own ODE) is run
+    beside it for its step count and its slip rates at the same time."""
+    from demystification_dfn_b200 import learned, networks
+    from demystification_dfn_b200.ensemble import Ensemble
+    from demystification_dfn_b200.layout import build_arrays
+    from demystification_dfn_b200.simulation import Simulation
+
+    kw = dict(n_faults=120)
+    t_end, max_steps = 2.0e6, 6000
+    train_nets = [networks.ensemble_member(s, **kw) for s in range(8)]
+    test_nets = [networks.ensemble_member(s, **kw) for s in range(64, 72)]
+    cap = 4_000_000
+    ens = Ensemble(train_nets, storage="fp32", pressure="tridiag", device=local, formulation="newton")
+    ens.set_stream(stream.cuda_stream)
+    ens.record(cap)
+    ens.solve(n_steps=max_steps, t_end=t_end, check=False)
+    x, t = ens.record_read(cap)
+    ens.close()
+    t0 = time.perf_counter()
+    w, loss = learned.train(x, t, epochs=20, batch=4096, lr=2e-3, seed=0)
+    out = {"workload": "8 held-out networks (ensemble seeds 64-71, 120 faults, injection + diffusion), "
+                       "to t = %.0e s" % t_end,
+           "train_samples": int(len(t)), "train_loss_first_last": [float(loss[0]), float(loss[1])],
+           "train_s": time.perf_counter() - t0, "networks": len(test_nets)}
+    runs = (("newton_fp64_analytic", "newton", "analytic", "fp64"),
+            ("newton_fp32_quasistatic", "newton", "quasistatic", "fp32"),
+            ("newton_fp32_analytic", "newton", "analytic", "fp32"),
+            ("newton_fp32_mlp", "newton", "mlp", "fp32"),
+            ("v_fp64", "v", "analytic", "fp64"))
+    ref = None
+    for name, form, guess, store in runs:
+        e = Ensemble(test_nets, storage=store, pressure="tridiag", device=local, formulation=form, guess=guess)
+        e.set_stream(stream.cuda_stream)
+        if guess == "mlp":
+            e.set_mlp(w)
+        out["elements"] = int(sum(e.n_elements))
+        reps, ms = _timed(stream, lambda: e.solve(n_steps=max_steps, t_end=t_end, check=False))
+        steps = sum(r["it_count"] for r in reps)
+        res = {"ms_to_t_end": ms, "accepted_steps": int(steps), "steps_per_s": steps / (ms / 1e3),
+               "newton_solves": int(sum(r["newton_solves"] for r in reps)),
+               "newton_iterations": int(sum(r["newton_iters"] for r in reps)),
+               "newton_fail": int(sum(r["newton_fail"] for r in reps)),
+               "reached_t_end": sum(1 for r in reps if abs(r["time"] - t_end) <= 1e-9 * t_end),
+               "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
+                                 for s in sorted({r["status"] for r in reps})}}
+        states = [e.state(i) for i in range(len(test_nets))]
+        e.close()
+        # slip (Newton state) and slip rate of every network at t_end
+        fin = []
+        for i, p in enumerate(test_nets):
+            st = states[i]
+            if abs(st["time"] - t_end) > 1e-9 * t_end:
+                fin.append(None)
+                continue
+            if form == "v":
+                fin.append((None, st["Y"][:len(st["P"])]))
+                continue
+            with Simulation(p, storage="fp32", pressure="tridiag", device=local, formulation="newton") as s:
+                s.set_stream(stream.cuda_stream)
+                s.set_state(st["Y"], st["P"], st["time"], st["t_try"], st["it_count"])
+                fin.append((st["Y"][:s.N].copy(), s.velocity()))
+        if ref is None:
+            ref = fin
+            res["max_V_at_t_end"] = max(float(np.abs(f[1]).max()) for f in fin if f is not None)
+        else:
+            es, ev = 0.0, 0.0
+            for i, p in enumerate(test_nets):
+                if fin[i] is None or ref[i] is None:
+                    continue
+                real = ~build_arrays(p).fake_mask
+                if fin[i][0] is not None:
+                    d, dr = fin[i][0][real], ref[i][0][real]
+                    es = max(es, float(np.abs(d - dr).max() / max(np.abs(dr).max(), 1e-300)))
+                v, vr = fin[i][1][real], ref[i][1][real]
+                ev = max(ev, float(np.abs(v - vr).max() / np.abs(vr).max()))
+            if form != "v":
+                res["max_rel_err_slip_vs_newton_fp64"] = es
+            res["max_rel_err_V_vs_newton_fp64"] = ev
+        out[name] = res
+    m = out["newton_fp32_mlp"]
+    per = lambda r: r["newton_iterations"] / max(r["newton_solves"], 1)
+    for base in ("quasistatic", "analytic"):
+        b = out["newton_fp32_" + base]
+        if b["newton_iterations"]:
+            out["newton_iterations_per_solve_saved_vs_" + base] = 1.0 - per(m) / per(b)
+    out["time_to_t_end_v_fp64_over_newton_fp32_mlp"] = out["v_fp64"]["ms_to_t_end"] / m["ms_to_t_end"]
+    out["time_to_t_end_newton_fp64_over_newton_fp32_mlp"] = (out["newton_fp64_analytic"]["ms_to_t_end"]
+                                                              / m["ms_to_t_end"])
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -179,6 +345,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
     ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,learned,cpu",
+                    help="comma list of the extra legs to run")
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -268,7 +436,8 @@ def main():
     e2e_value = world * e2e_steps / float(te.item())
 
     extras = {}
-    if rank == 0 and not args.no_extras:
+    legs = set() if args.no_extras else set(args.legs.split(","))
+    if rank == 0 and "precision" in legs:
         # mixed-precision storage of the same network (same steps, same start)
         for store in ("fp32", "bf16x2"):
             if store == args.storage:
@@ -294,7 +463,7 @@ def main():
                              "compared_after": f"{args.warmup}+{args.steps} accepted steps from the same start"}
             s2.close()
 
-    if rank == 0 and args.ensemble > 0 and not args.no_extras:
+    if rank == 0 and args.ensemble > 0 and "ensemble" in legs:
         # batched ensemble: many networks of uneven size in one handle, one
         # launch per kernel for the whole batch, per-network step control
         from demystification_dfn_b200 import networks
@@ -341,12 +510,19 @@ def main():
             ens.close()
         extras["ensemble"] = ens_out
 
+    if rank == 0 and "single_fault" in legs:
+        extras["single_fault"] = leg_single_fault(args, local, stream)
+    if rank == 0 and "hmatrix" in legs:
+        extras["hmatrix"] = leg_hmatrix(args, local, stream)
+    if rank == 0 and "learned" in legs:
+        extras["learned_newton"] = leg_learned(args, local, stream)
+
     if rank == 0:
         hbm, src = peaks()
         kv_avg = kv_ms / max(kv_n, 1)
         achieved = kv_bytes / (kv_avg / 1e3) / 1e9
         cpu = None
-        if not args.no_extras:
+        if "cpu" in legs:
             threads = os.cpu_count() or 1
             steps_c, dt_c = cpu_baseline(make_problem(0, args.n_faults), threads, args.cpu_budget)
             cpu = {"value": steps_c / dt_c, "unit": "steps/s", "cores": threads, "kind": "port",
@@ -375,7 +551,7 @@ def main():
                                            "time")},
         }
         if extras:
-            line["mixed_precision"] = extras
+            line["extras"] = extras
         print(json.dumps(line))
     sim.close()
     if world > 1:
