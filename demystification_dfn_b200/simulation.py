@@ -279,5 +279,8 @@ class Simulation:
             from .hdf5 import write_output
 
             os.makedirs(output_dir, exist_ok=True)
-            write_output(os.path.join(output_dir, "output%07d" % it), buf, freq, self.N)
+            # rows past the saved ones repeat the previous file's, as the
+            # reference's persistent save arrays do
+            self._ring = write_output(os.path.join(output_dir, "output%07d" % it), buf, freq, self.N,
+                                      stale=getattr(self, "_ring", None))
         buf.clear()

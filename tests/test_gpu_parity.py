@@ -8,6 +8,8 @@ Tolerances (relative to the largest magnitude of the compared quantity):
   to well below 1e3 * tol_solver Pa
 * whole RK45 steps: slip rate and log-state within 1e-8 (the parity target)
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -254,3 +256,30 @@ def test_reference_shipped_problems(tag, steps):
         assert rel(g["Y"][:N], r["Y"][:N]) < 1e-8
         assert rel(g["Y"][N:2 * N], r["Y"][N:2 * N]) < 1e-8
         assert rel(g["P"], r["P"]) < 1e-8
+
+
+def test_solve_writes_reference_output_files(tmp_path):
+    """Simulation.solve with an output directory: save_data every stride_time
+    steps, an output%07d file every freq_writing_file saved rows and a last
+    one at max_it (src/solver.f90:180-201), holding the same snapshots as a
+    run that keeps them in memory."""
+    from demystification_dfn_b200.hdf5 import read_output
+
+    p = net(seed=12, n=3, tol=1e-6)
+    with Simulation(p) as s:
+        mem = s.solve(max_it=25, stride_time=2, freq_writing_file=5)
+    with Simulation(p) as s:
+        s.solve(max_it=25, stride_time=2, freq_writing_file=5, output_dir=str(tmp_path))
+    files = sorted(os.listdir(tmp_path))
+    # saved at it_count 1, 3, ..., 25: 13 rows -> files after rows 5, 10 and the last 3
+    assert files == ["output0000009", "output0000019", "output0000025"]
+    rows = []
+    for f in files:
+        o = read_output(str(tmp_path / f))
+        rows += [{k: o[k][r] for k in ("V", "theta", "P", "time")} for r in range(5)]
+    rows = rows[:13]
+    assert len(mem) == 13
+    for a, b in zip(mem, rows):
+        assert a["time"] == b["time"]
+        for k in ("V", "theta", "P"):
+            assert np.array_equal(a[k], b[k]), k

@@ -41,3 +41,71 @@ def test_reader_matches_golden_on_shipped_files():
         a, b = build_arrays(p), build_arrays(q)
         for k in ("node", "a", "b", "V", "theta", "sigmaN", "P", "permeability", "src_Q"):
             assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+# --- writer -----------------------------------------------------------------
+
+def _same_tree(a, b, path=""):
+    assert set(a) == set(b), path
+    for k in a:
+        if isinstance(a[k], dict):
+            _same_tree(a[k], b[k], path + k + "/")
+            continue
+        va, vb = np.asarray(a[k]), np.asarray(b[k])
+        if va.dtype.kind in "OUS":
+            assert str(a[k]) == str(b[k]), path + k
+        else:
+            assert va.dtype.kind == vb.dtype.kind, path + k
+            assert np.array_equal(va.reshape(-1), vb.reshape(-1)), path + k
+
+
+@pytest.mark.parametrize("tag", ["bp6", "network"])
+def test_config_writer_round_trip_of_reference_configs(tmp_path, tag):
+    """Problem from the shipped config -> DemystiFicatioN.write -> reader:
+    the same datasets (names, groups, integer/float kinds, values)."""
+    from demystification_dfn_b200.hdf5 import config_tree, read_file
+
+    p = refconfigs.problem(tag)
+    path = p.write(str(tmp_path) + "/case/")
+    assert path.endswith("case/config") and os.path.exists(path)
+    t = read_file(path)
+    _same_tree(t, config_tree(p))
+    # every dataset the reference's reader opens is present (configuration.f90:70-379)
+    assert t["fault1"]["node"].shape == (p.faults[0].nb_node, 2)
+    q = read_config(path)
+    a, b = build_arrays(p), build_arrays(q)
+    for k in ("node", "a", "b", "Dc", "V", "theta", "sigmaN", "P", "permeability", "src_Q", "src_index"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_config_writer_many_faults_uses_multilevel_group_btree(tmp_path):
+    """800 faults: the root group has 802 links, more than one B-tree node of
+    symbol-table nodes holds, so the group B-tree gets a second level."""
+    from demystification_dfn_b200 import networks
+    from demystification_dfn_b200.hdf5 import read_file
+
+    p = networks.fault_network(n_faults=800, seed=0)
+    path = p.write(str(tmp_path) + "/")
+    t = read_file(path)
+    assert len(t) == 802 and t["fault800"]["nb_element"] == p.faults[799].nb_element
+    a, b = build_arrays(p), build_arrays(read_config(path))
+    for k in ("node", "a", "b", "V", "theta", "P"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_output_writer_layout_and_stale_rows(tmp_path):
+    """output%07d: six (nb_element, freq) fields and time (freq); a short
+    last file keeps the previous file's rows past its own."""
+    from demystification_dfn_b200.hdf5 import OUTPUT_FIELDS, read_file, read_output, write_output
+
+    rng = np.random.default_rng(0)
+    N, F = 7, 4
+    snaps = [dict({k: rng.normal(size=N) for k in OUTPUT_FIELDS}, time=float(i)) for i in range(6)]
+    ring = write_output(str(tmp_path / "output0000004"), snaps[:4], F, N)
+    raw = read_file(str(tmp_path / "output0000004"))
+    assert raw["V"].shape == (N, F) and raw["time"].shape == (F,)
+    assert np.array_equal(raw["V"][:, 2], snaps[2]["V"])
+    write_output(str(tmp_path / "output0000006"), snaps[4:], F, N, stale=ring)
+    o = read_output(str(tmp_path / "output0000006"))
+    assert np.array_equal(o["time"], [4.0, 5.0, 2.0, 3.0])
+    assert np.array_equal(o["P"][1], snaps[5]["P"]) and np.array_equal(o["P"][3], snaps[3]["P"])
