@@ -85,6 +85,7 @@ def load():
                                     ctypes.POINTER(ctypes.c_float)]),
         "dfn_mlp_infer": (i32, [ctypes.POINTER(ctypes.c_float), i64, ctypes.POINTER(ctypes.c_float),
                                 ctypes.POINTER(ctypes.c_float)]),
+        "dfn_set_graphs": (i32, [P, i32]),
         "dfn_velocity": (i32, [P, dp]),
         "dfn_hmat_stats": (i32, [P, ctypes.POINTER(i64)]),
         "dfn_hmat_perm": (i32, [P, ctypes.POINTER(i32)]),

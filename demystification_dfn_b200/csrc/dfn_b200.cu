@@ -71,6 +71,13 @@ struct dfn_handle {
     int dev = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // CUDA graph of kGraphRounds rounds of the solve loop, replayed on the
+    // handle's stream (captured on cap_stream: capture needs a stream other
+    // than the legacy default one a caller may have set)
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int64_t graph_kernels = 0;
+    bool use_graphs = true;
     int B = 1;                    // networks in the batch
     int mode = 2, store = 0, pressure = 0, gemv_impl = 0, max_attempts = 64;
     int64_t Ntot = 0;             // elements of all networks
@@ -364,6 +371,61 @@ static int put_ctl(dfn_handle *h)
 // Advances every network by `nsteps` accepted steps, or until its time
 // reaches t_end (> 0). Rounds are launched in groups; the controllers are
 // read between groups only.
+static const int64_t kGraphRounds = 8;
+
+static void drop_graph(dfn_handle *h)
+{
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+}
+
+// Capture kGraphRounds rounds into an executable graph. Every kernel of a
+// round reads the step controllers on the device, so the same graph serves
+// every later replay; rounds of networks that are done are no-ops.
+static int build_graph(dfn_handle *h)
+{
+    cudaStream_t saved = h->stream;
+    const int64_t l0 = h->launches;
+    cudaGraph_t g = nullptr;
+    h->stream = h->cap_stream;
+    cudaError_t e = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal);
+    int st = (e == cudaSuccess) ? DFN_OK : DFN_ERR_CUDA;
+    for (int64_t r = 0; r < kGraphRounds && st == DFN_OK; r++) st = run_round(h);
+    cudaError_t e2 = cudaStreamEndCapture(h->cap_stream, &g);
+    h->stream = saved;
+    h->graph_kernels = h->launches - l0;
+    h->launches = l0;
+    if (st == DFN_OK && e2 == cudaSuccess && g) {
+        e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+        if (e != cudaSuccess) {
+            h->graph_exec = nullptr;
+            st = DFN_ERR_CUDA;
+        }
+    } else if (st == DFN_OK) {
+        st = DFN_ERR_CUDA;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();   // a failed capture leaves nothing behind: direct launches follow
+    return st;
+}
+
+// n rounds: whole graphs while possible (not while K.V launches are being
+// timed one by one), then single launches.
+static int run_rounds(dfn_handle *h, int64_t n)
+{
+    if (h->use_graphs && !h->prof && n >= kGraphRounds) {
+        if (!h->graph_exec && build_graph(h) != DFN_OK) h->use_graphs = false;
+        if (h->graph_exec) {
+            for (; n >= kGraphRounds; n -= kGraphRounds) {
+                CK(cudaGraphLaunch(h->graph_exec, h->stream));
+                h->launches += h->graph_kernels;
+            }
+        }
+    }
+    for (int64_t r = 0; r < n; r++) TRY(run_round(h));
+    return DFN_OK;
+}
+
 static int solve_impl(dfn_handle *h, int64_t nsteps, double t_end)
 {
     arm_kernel<<<blocks_of(h->B, 128), 128, 0, h->stream>>>(h->ctl, h->B, (long long)nsteps, t_end,
@@ -372,7 +434,7 @@ static int solve_impl(dfn_handle *h, int64_t nsteps, double t_end)
     CKL();
     int64_t group = (t_end > 0.0) ? 8 : std::max<int64_t>(nsteps, 1);
     for (int64_t guard = 0; guard < 1000000; guard++) {
-        for (int64_t r = 0; r < group; r++) TRY(run_round(h));
+        TRY(run_rounds(h, group));
         TRY(sync_ctl(h));
         int64_t remaining = 0;
         bool active = false;
@@ -625,6 +687,8 @@ int32_t dfn_destroy(dfn_handle *h)
     for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return DFN_OK;
@@ -710,6 +774,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     CKC(cudaSetDevice(h->dev));
     CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
+    CKC(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
     h->B = count;
     h->mode = probs[0].fracture_mode; h->store = opt.kernel_storage;
     h->pressure = opt.pressure_solver; h->gemv_impl = opt.gemv_impl;
@@ -949,6 +1014,16 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
 int32_t dfn_create(const dfn_problem *p, const dfn_options *opt, dfn_handle **out)
 {
     return dfn_create_batch(p, 1, opt, out);
+}
+
+int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)
+{
+    if (!h) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->use_graphs = enable != 0;
+    drop_graph(h);
+    return DFN_OK;
 }
 
 int32_t dfn_set_stream(dfn_handle *h, void *s)
@@ -1308,6 +1383,7 @@ int32_t dfn_record(dfn_handle *h, int64_t capacity)
     if (h->rec_x) { cudaFree(h->rec_x); h->rec_x = nullptr; }
     if (h->rec_t) { cudaFree(h->rec_t); h->rec_t = nullptr; }
     h->rec_cap = 0;
+    drop_graph(h);        // the friction launches carry the recording buffers
     CK(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
     if (capacity > 0) {
         CK(cudaMalloc((void **)&h->rec_x, sizeof(float) * MLP_IN * capacity));

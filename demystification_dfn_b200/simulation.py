@@ -90,6 +90,11 @@ class Simulation:
     def set_stream(self, stream_handle: int):
         _lib.check(self.lib.dfn_set_stream(self.h, ctypes.c_void_p(stream_handle)), self.lib)
 
+    def set_graphs(self, enable: bool):
+        """Replay the solve loop's rounds as a CUDA graph (default) or launch
+        every kernel on its own; results are identical."""
+        _lib.check(self.lib.dfn_set_graphs(self.h, 1 if enable else 0), self.lib)
+
     @property
     def kernel_bytes(self):
         return int(self.lib.dfn_kernel_bytes(self.h))

@@ -180,6 +180,14 @@ void dfn_default_options(dfn_options *opt);
  * assembles the kernel matrices on the device and sets time/t_try/it_count
  * as solve() does at entry (src/solver.f90:47-56). */
 int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle **out);
+/* Solve loops (dfn_solve_steps, dfn_solve_batch) replay a CUDA graph of 8
+ * rounds of the solve() loop when at least 8 rounds remain (on by default;
+ * captured at the first such call, on a private stream, and replayed on the
+ * handle's stream). Results are identical either way; enable = 0 launches
+ * every kernel on its own. While dfn_profile_kv is on, kernels are launched
+ * one by one so that each K.V launch is timed. No counterpart in the
+ * reference (a host loop of subroutine calls). */
+int32_t dfn_set_graphs(dfn_handle *h, int32_t enable);
 /* A batch of independent networks in one handle (no counterpart in the
  * reference, which runs one network per process). All networks share the
  * fracture mode and the options; each keeps its own state, step size,

@@ -93,3 +93,21 @@ def test_mode3_batch():
     with Ensemble(ps, pressure="cg", storage="fp32") as ens:
         reps = ens.solve(n_steps=10)
         assert all(r["status"] == 0 and r["it_count"] == 10 for r in reps)
+
+
+@pytest.mark.parametrize("pressure", ["cg", "tridiag"])
+def test_graph_replay_matches_single_launches_bitwise(pressure):
+    """The solve loop replayed as CUDA graphs of 8 rounds gives the state of
+    the same rounds launched one by one, bit for bit, for a batch run to a
+    step count (graphs, then single rounds for the remainder) and to t_end."""
+    ps = [networks.small_network(seed=s, n_faults=3 + s % 3, tol=1e-7) for s in range(4)]
+    out = []
+    for graphs in (True, False):
+        with Ensemble(ps, pressure=pressure) as ens:
+            ens.set_graphs(graphs)
+            ens.solve(n_steps=21)
+            ens.solve(t_end=ens.state(0)["time"] * 3.0)
+            out.append([ens.state(i) for i in range(len(ps))])
+    for a, b in zip(*out):
+        assert a["it_count"] == b["it_count"] and a["time"] == b["time"]
+        assert np.array_equal(a["Y"], b["Y"]) and np.array_equal(a["P"], b["P"])
