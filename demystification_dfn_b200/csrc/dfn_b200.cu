@@ -91,6 +91,8 @@ struct dfn_handle {
     int64_t nseg = 0, nseg0 = 0;
     int *long_seg = nullptr;              // segments longer than TRI_SHORT_MAX
     int64_t nlong = 0, nlong0 = 0;
+    int *short_seg = nullptr;             // the others
+    int64_t nshort = 0, nshort0 = 0;
     int64_t nsrc_tot = 0, part_tot = 0;
     // geometry and parameters (concatenated)
     double *node = nullptr, *elem = nullptr, *ds = nullptr, *tan = nullptr, *nrm = nullptr, *permx = nullptr;
@@ -243,15 +245,19 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
                                                                h->Ptemp, h->Pdot_s, h->pwork,
                                                                h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0);
     } else {
-        const int64_t nseg = (ninst == h->B) ? h->nseg : h->nseg0;
-        dim3 grid((unsigned)((nseg + 127) / 128), (unsigned)nsys);
-        pressure_tridiag_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
-                                                             h->seg_start, h->seg_inst, nseg, h->Ptemp, h->Pdot_s,
-                                                             h->pwork);
+        const int64_t nshort = (ninst == h->B) ? h->nshort : h->nshort0;
         const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
+        if (nshort > 0) {
+            dim3 grid((unsigned)((nshort + 7) / 8), (unsigned)nsys);
+            pressure_tridiag_kernel<<<grid, 256, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0,
+                                                                 dt_explicit, h->seg_start, h->seg_inst,
+                                                                 h->short_seg, nshort, h->Ptemp, h->Pdot_s, h->pwork);
+            if (nlong > 0) {
+                h->launches++;
+                CKL();
+            }
+        }
         if (nlong > 0) {
-            h->launches++;
-            CKL();
             dim3 lgrid((unsigned)nlong, (unsigned)nsys);
             pressure_tridiag_long_kernel<<<lgrid, TRI_NT, 0, h->stream>>>(
                 h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit, h->seg_start, h->seg_inst, h->long_seg,
@@ -676,7 +682,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
-                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->node, h->elem, h->ds, h->tan,
+                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
                     h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
@@ -932,15 +938,24 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         HCOPY(h->seg_inst, sinst.data(), sinst.size());
         // long segments go to the CTA-parallel solve; networks in order, so
         // those of network 0 come first
-        std::vector<int> lg;
+        std::vector<int> lg, sh;
         for (int64_t q = 0; q < h->nseg; q++) {
             if (seg[q + 1] - seg[q] > TRI_SHORT_MAX) lg.push_back((int)q);
-            if (q + 1 == h->nseg0) h->nlong0 = (int64_t)lg.size();
+            else sh.push_back((int)q);
+            if (q + 1 == h->nseg0) {
+                h->nlong0 = (int64_t)lg.size();
+                h->nshort0 = (int64_t)sh.size();
+            }
         }
         h->nlong = (int64_t)lg.size();
+        h->nshort = (int64_t)sh.size();
         if (h->nlong) {
             DALLOC(h->long_seg, lg.size());
             HCOPY(h->long_seg, lg.data(), lg.size());
+        }
+        if (h->nshort) {
+            DALLOC(h->short_seg, sh.size());
+            HCOPY(h->short_seg, sh.data(), sh.size());
         }
     }
 

@@ -641,10 +641,12 @@ __device__ __forceinline__ double block_max(double v, double *red)
     return red[32];
 }
 
-// Segments of more than TRI_SHORT_MAX elements are solved by a CTA of TRI_NT
-// threads (pressure_tridiag_long_kernel), rows in registers up to TRI_MAXM
-// rows per thread; shorter ones by one thread each.
-#define TRI_SHORT_MAX 48
+// Segments of at most TRI_SHORT_MAX elements are solved by one warp each
+// (pressure_tridiag_kernel, up to TRI_WMAXM rows per lane), longer ones by a
+// CTA of TRI_NT threads (pressure_tridiag_long_kernel), rows in registers up
+// to TRI_MAXM rows per thread.
+#define TRI_SHORT_MAX 64
+#define TRI_WMAXM 2
 #define TRI_NT 256
 #define TRI_MAXM 16
 
@@ -889,58 +891,16 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
 // thread per decoupled segment (a maximal run of elements joined by nonzero
 // face permeability; the fake elements between faults are segments of one).
 // seg_start holds global element indices; segments never cross instances.
-__global__ void pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl, int mask, int kind, int sys0,
-                                        double dt_explicit, const int64_t *seg_start, const int *seg_inst,
-                                        int64_t nseg, double *Ptemp, double *Pdot, double *work)
-{
-    const int64_t sg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (sg >= nseg) return;
-    const int i = seg_inst[sg];
-    if (!takes_part(ctl, i, mask)) return;
-    const Inst I = inst[i];
-    const PressParams p = press_params(g, I, i, ctl);
-    const int sys = sys0 + blockIdx.y;
-    const int64_t N = I.N;
-    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
-    const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
-    if (k1 - k0 > TRI_SHORT_MAX) return;                       // pressure_tridiag_long_kernel
-    double *cp = work + 24 * I.eoff + (int64_t)sys * 4 * N;   // modified super-diagonal
-    double *dp = cp + N;                                       // modified right-hand side
-    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
-    double cprev = 0.0, dprev = 0.0;
-    for (int64_t k = k0; k < k1; k++) {
-        double A1, A2, A3;
-        prow(p, k, dt, A1, A2, A3);
-        if (k == k0) A1 = 0.0;
-        if (k == k1 - 1) A3 = 0.0;
-        double rhs = add_(p.P[k], psource(p, k, dt));
-        double den = A2 - A1 * cprev;
-        double c = A3 / den;
-        double d = (rhs - A1 * dprev) / den;
-        cp[k] = c; dp[k] = d;
-        cprev = c; dprev = d;
-    }
-    double xn = 0.0;
-    bool bad = false;
-    for (int64_t k = k1 - 1; k >= k0; k--) {
-        double xk = dp[k] - cp[k] * xn;
-        xn = xk;
-        Pt[k] = xk;
-        Pd[k] = (dt < 1e-9) ? 0.0 : (xk - p.P[k]) / dt;
-        if (!isfinite(xk)) bad = true;
-    }
-    if (bad) atomicCAS(&ctl[i].status, 0, 4);
-}
-
 // ---------------------------------------------------------------------------
-// Long segments: the Thomas recurrences of one segment evaluated by a CTA.
+// The Thomas recurrences of one segment evaluated by a group of NTG threads
+// (a warp for short segments, a CTA for long ones).
 //
-// Thread t owns rows [t*m, t*m + m) of the segment (m = ceil(L / TRI_NT)).
+// Thread t owns rows [t*m, t*m + m) of the segment (m = ceil(L / NTG)).
 // The three sequential recurrences of the Thomas algorithm are each a scan
-// over an associative operator, so the CTA computes the value entering every
-// thread's rows with a two-level (warp shuffle + shared memory) scan of the
-// per-thread compositions and each thread then reruns the exact recurrence
-// over its own rows:
+// over an associative operator, so the group computes the value entering
+// every thread's rows with a scan of the per-thread compositions (warp
+// shuffles, plus shared memory across the warps of a CTA) and each thread
+// then reruns the exact recurrence over its own rows:
 //   c_k = A3_k / (A2_k - A1_k c_{k-1})       a Moebius map of c_{k-1}: the
 //        2x2 matrix [[0, A3], [-A1, A2]] acting on (p, q), c = p/q; products
 //        are rescaled by their largest entry (the ratio is unchanged);
@@ -982,15 +942,19 @@ __device__ __forceinline__ Aff shfl_down(const Aff &v, int d)
     return {__shfl_down_sync(0xffffffffu, v.a, d), __shfl_down_sync(0xffffffffu, v.b, d)};
 }
 
-// Exclusive forward scan over the CTA (thread 0 first): returns the
+// Exclusive forward scan over the group (thread 0 first): returns the
 // composition of the maps of threads 0..t-1 (identity for t = 0).
-template <typename T>
-__device__ __forceinline__ T cta_scan_excl(T v, T ident, T *sm)
+template <int NTG, typename T>
+__device__ __forceinline__ T grp_scan_excl(T v, T ident, T *sm)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = TRI_NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = NTG / 32;
     for (int d = 1; d < 32; d <<= 1) {
         T o = shfl_up(v, d);
         if (lane >= d) v = compose(v, o);
+    }
+    if constexpr (NTG == 32) {
+        T prev = shfl_up(v, 1);
+        return (lane == 0) ? ident : prev;
     }
     __syncthreads();
     if (lane == 31) sm[w] = v;
@@ -1010,13 +974,18 @@ __device__ __forceinline__ T cta_scan_excl(T v, T ident, T *sm)
 }
 
 // Exclusive backward scan for affine maps: the composition of the maps of
-// threads t+1..NT-1, the last thread's applied first (identity for the last).
-__device__ __forceinline__ Aff cta_scan_excl_back(Aff v, Aff *sm)
+// threads t+1..NTG-1, the last thread's applied first (identity for the last).
+template <int NTG>
+__device__ __forceinline__ Aff grp_scan_excl_back(Aff v, Aff *sm)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = TRI_NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = NTG / 32;
     for (int d = 1; d < 32; d <<= 1) {
         Aff o = shfl_down(v, d);
         if (lane + d < 32) v = compose(v, o);
+    }
+    if constexpr (NTG == 32) {
+        Aff next = shfl_down(v, 1);
+        return (lane == 31) ? aff_id() : next;
     }
     __syncthreads();
     if (lane == 0) sm[w] = v;
@@ -1051,13 +1020,14 @@ __device__ __forceinline__ void tri_rows(int nr, F f)
     }
 }
 
-template <int MAXM>
+template <int NTG, int MAXM>
 __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int64_t k0, int64_t k1, double *Pt,
                                             double *Pd, double *gw, int64_t N, Mob *smm, Aff *sma, int &bad)
 {
     const int64_t L = k1 - k0;
-    const int64_t m = (L + TRI_NT - 1) / TRI_NT;
-    const int64_t r0 = (int64_t)threadIdx.x * m;
+    const int tid = (NTG == 32) ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+    const int64_t m = (L + NTG - 1) / NTG;
+    const int64_t r0 = (int64_t)tid * m;
     const int nr = (int)max((int64_t)0, min(m, L - r0));
     constexpr int R = (MAXM > 0) ? MAXM : 1;
     double reg[4][R];
@@ -1079,8 +1049,8 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     // c recurrence
     Mob T = mob_id();
     tri_rows<MAXM, false>(nr, [&](int j) { T = compose(Mob{0.0, at(2, j), -at(0, j), at(1, j)}, T); });
-    const Mob E = cta_scan_excl(T, mob_id(), smm);
-    double c = (threadIdx.x == 0) ? 0.0 : E.b / E.d;
+    const Mob E = grp_scan_excl<NTG>(T, mob_id(), smm);
+    double c = (tid == 0) ? 0.0 : E.b / E.d;
     tri_rows<MAXM, false>(nr, [&](int j) {
         const double den = at(1, j) - at(0, j) * c;
         c = at(2, j) / den;
@@ -1089,7 +1059,7 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     // d recurrence
     Aff F = aff_id();
     tri_rows<MAXM, false>(nr, [&](int j) { F = compose(Aff{-at(0, j) / at(1, j), at(3, j) / at(1, j)}, F); });
-    double d = cta_scan_excl(F, aff_id(), sma).b;
+    double d = grp_scan_excl<NTG>(F, aff_id(), sma).b;
     tri_rows<MAXM, false>(nr, [&](int j) {
         d = (at(3, j) - at(0, j) * d) / at(1, j);
         at(3, j) = d;
@@ -1097,7 +1067,7 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     // back substitution
     Aff G = aff_id();
     tri_rows<MAXM, true>(nr, [&](int j) { G = compose(Aff{-at(2, j), at(3, j)}, G); });
-    double x = cta_scan_excl_back(G, sma).b;
+    double x = grp_scan_excl_back<NTG>(G, sma).b;
     tri_rows<MAXM, true>(nr, [&](int j) {
         const int64_t k = k0 + r0 + j;
         x = at(3, j) - at(2, j) * x;
@@ -1105,6 +1075,31 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
         Pd[k] = (dt < 1e-9) ? 0.0 : (x - p.P[k]) / dt;
         if (!isfinite(x)) bad = 1;
     });
+}
+
+// Short segments, one warp each: grid (ceil(segments / 8), systems),
+// blockDim 256; seg_list holds the launch's short segments.
+__global__ void __launch_bounds__(256) pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
+                                                               int mask, int kind, int sys0, double dt_explicit,
+                                                               const int64_t *seg_start, const int *seg_inst,
+                                                               const int *seg_list, int64_t nlist, double *Ptemp,
+                                                               double *Pdot, double *work)
+{
+    const int64_t q = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= nlist) return;                      // whole warp
+    const int sg = seg_list[q];
+    const int i = seg_inst[sg];
+    if (!takes_part(ctl, i, mask)) return;       // whole warp
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.y;
+    const int64_t N = I.N;
+    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
+    const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
+    int bad = 0;
+    tri_segment<32, TRI_WMAXM>(p, dt, k0, k1, Pt, Pd, nullptr, N, nullptr, nullptr, bad);
+    if (bad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
 // grid (long segments of the launch, systems); blockDim = TRI_NT.
@@ -1132,9 +1127,9 @@ __global__ void __launch_bounds__(TRI_NT, 1) pressure_tridiag_long_kernel(PressG
     if (threadIdx.x == 0) sbad = 0;
     int bad = 0;
     if (k1 - k0 <= (int64_t)TRI_NT * TRI_MAXM)
-        tri_segment<TRI_MAXM>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
+        tri_segment<TRI_NT, TRI_MAXM>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
     else
-        tri_segment<0>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
+        tri_segment<TRI_NT, 0>(p, dt, k0, k1, Pt, Pd, gw, N, smm, sma, bad);
     if (bad) atomicOr(&sbad, 1);
     __syncthreads();
     if (threadIdx.x == 0 && sbad) atomicCAS(&ctl[i].status, 0, 4);
