@@ -14,6 +14,8 @@
 #include "dfn_device.cuh"
 #include "hmat_device.cuh"
 #include "newton.cuh"
+#include "tc_gemm.cuh"
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -109,6 +111,12 @@ struct dfn_handle {
     void *K = nullptr;
     size_t K_bytes = 0;
     int64_t kv_bytes = 0;         // algorithmic bytes of one K.V over the batch
+    // shared-geometry batch on tensor cores (DFN_STORE_BF16X2_TC)
+    bool tc = false;
+    int tc_bn = 0, tc_nmt = 0, tc_split = 1, tc_kps = 0, tc_nkb = 0;
+    int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
+    __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each
+    CUtensorMap tc_map[4];
     StepCtl *ctl = nullptr;
     StepCtl *h_ctl = nullptr;     // pinned mirror, B entries
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -208,6 +216,65 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
     return DFN_OK;
 }
 
+// Shared-geometry K.V on tensor cores: V of every network to BF16 hi/lo rows,
+// then one GEMM over (128-row tile, reduction split) work units.
+template <int BN>
+static void tc_launch_bn(dfn_handle *h, const TcOut &o)
+{
+    tc_gemm_kernel<BN><<<(unsigned)(h->tc_nmt * h->tc_split), TC_THREADS, tc_smem_bytes(BN), h->stream>>>(
+        h->tc_map[0], h->tc_map[1], h->tc_map[2], h->tc_map[3], o, h->err_flag);
+}
+
+static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
+{
+    const Inst &I = h->hinst[0];
+    const int64_t nb = (int64_t)h->tc_bn * h->tc_kpad;
+    tc_pack_v_kernel<<<blocks_of(nb, 256), 256, 0, h->stream>>>(Vbase, vmul, I.N, h->B, h->tc_bn, h->tc_kpad,
+                                                                h->tc_B, h->tc_B + nb);
+    h->launches++;
+    CKL();
+    TcOut o;
+    o.partT = h->partT; o.partN = h->partN; o.inst = h->inst; o.N = I.N; o.mrows = h->tc_mrows; o.R = h->B;
+    o.kb_per_split = h->tc_kps; o.nkb = h->tc_nkb; o.nmt = h->tc_nmt;
+    switch (h->tc_bn) {
+    case 16: tc_launch_bn<16>(h, o); break;
+    case 32: tc_launch_bn<32>(h, o); break;
+    case 64: tc_launch_bn<64>(h, o); break;
+    case 128: tc_launch_bn<128>(h, o); break;
+    default: tc_launch_bn<256>(h, o); break;
+    }
+    return DFN_OK;
+}
+
+// 2D tensor map of a row-major BF16 matrix [rows][kpad], boxes of 64 x box_rows,
+// 128-byte swizzle (the tcgen05 K-major operand layout).
+static int tc_encode(CUtensorMap *m, const void *ptr, int64_t rows, int64_t kpad, int box_rows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            g_err = "cuTensorMapEncodeTiled is not available";
+            return DFN_ERR_CUDA;
+        }
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(kpad * 2)};
+    cuuint32_t box[2] = {TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        g_err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return DFN_ERR_CUDA;
+    }
+    return DFN_OK;
+}
+
 // K.V of all networks (only0 = false) or of network 0 (only0 = true);
 // V of network i is Vbase[vmul*eoff_i + l].
 static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, bool only0)
@@ -218,6 +285,8 @@ static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, b
     const int64_t ntiles = only0 ? h->ntiles0 : h->ntiles;
     if (h->hmat) {
         TRY(launch_hmat(h, mask, Vbase, vmul, only0));
+    } else if (h->tc) {
+        TRY(launch_tc(h, Vbase, vmul));
     } else if (h->gemv_impl == 0) {
         gemv_tma_fn fn = pick_gemv_tma(h->mode, h->store);
         fn<<<(unsigned)ntiles, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(
@@ -682,7 +751,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
-                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->node, h->elem, h->ds, h->tan,
+                    h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
                     h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
@@ -762,7 +831,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     *out = nullptr;
     dfn_options opt;
     if (opt_in) opt = *opt_in; else dfn_default_options(&opt);
-    if (opt.kernel_storage < 0 || opt.kernel_storage > 2) { g_err = "bad kernel_storage"; return DFN_ERR_ARG; }
+    if (opt.kernel_storage < 0 || opt.kernel_storage > 3) { g_err = "bad kernel_storage"; return DFN_ERR_ARG; }
     if (opt.pressure_solver < 0 || opt.pressure_solver > 2) { g_err = "bad pressure_solver"; return DFN_ERR_ARG; }
     for (int i = 0; i < count; i++) {
         TRY(check_problem(&probs[i]));
@@ -806,6 +875,42 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         return DFN_ERR_UNSUPPORTED;
     }
     h->ncomp = (h->mode == DFN_MODE_II) ? 2 : 1;
+    h->tc = h->store == DFN_STORE_BF16X2_TC;
+    if (h->tc) {
+        const dfn_problem &p0 = probs[0];
+        std::string why;
+        if (h->hmat) why = "the H-matrix path has its own storage";
+        if (count > 256) why = "at most 256 networks share one tensor-core kernel matrix";
+        for (int i = 1; i < count && why.empty(); i++) {
+            const dfn_problem &q = probs[i];
+            if (q.nb_element != p0.nb_element || q.nb_fault != p0.nb_fault || q.fracture_mode != p0.fracture_mode ||
+                q.mu != p0.mu || q.cp != p0.cp || q.cs != p0.cs ||
+                memcmp(q.node, p0.node, sizeof(double) * 2 * (p0.nb_element + 1)) != 0)
+                why = "networks of a tensor-core batch must share nb_element, nodes, fracture mode and mu, cp, cs";
+        }
+        if (!why.empty()) {
+            g_err = why;
+            dfn_destroy(h);
+            return DFN_ERR_ARG;
+        }
+        const int64_t N0 = p0.nb_element;
+        h->tc_mrows = h->ncomp * N0;
+        h->tc_nmt = (int)((h->tc_mrows + TC_BM - 1) / TC_BM);
+        h->tc_mpad = (int64_t)h->tc_nmt * TC_BM;
+        h->tc_nkb = (int)((N0 + TC_BK - 1) / TC_BK);
+        h->tc_kpad = (int64_t)h->tc_nkb * TC_BK;
+        h->tc_bn = count <= 16 ? 16 : count <= 32 ? 32 : count <= 64 ? 64 : count <= 128 ? 128 : 256;
+        // reduction splits: the fewest that fill whole waves of the SMs well
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+        double best = -1.0;
+        for (int s = 1; s <= 8 && s <= h->tc_nkb; s++) {
+            const int64_t units = (int64_t)h->tc_nmt * s;
+            const double eff = (double)units / (double)(((units + sms - 1) / sms) * sms);
+            if (eff > best + 0.05) { best = eff; h->tc_split = s; }
+        }
+        h->tc_kps = (h->tc_nkb + h->tc_split - 1) / h->tc_split;
+    }
 
     // instance table
     int64_t eoff = 0, kvec = 0, poff = 0, soff = 0;
@@ -814,9 +919,9 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         const dfn_problem &p = probs[i];
         Inst &I = h->hinst[i];
         I.N = p.nb_element;
-        I.Np = h->hmat ? I.N : ((I.N + CW - 1) / CW) * CW;
+        I.Np = (h->hmat || h->tc) ? I.N : ((I.N + CW - 1) / CW) * CW;
         I.eoff = eoff;
-        I.nchunk = h->hmat ? 1 : I.Np / CW;
+        I.nchunk = h->hmat ? 1 : (h->tc ? h->tc_split : I.Np / CW);
         I.kvec = kvec;
         I.poff = poff;
         I.soff = soff;
@@ -828,10 +933,10 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         I.tol = p.tol_solver;
         I.t0 = p.time0;
         eoff += I.N;
-        if (!h->hmat) kvec += I.N * I.Np * bpc / 16;
+        if (!h->hmat && !h->tc) kvec += I.N * I.Np * bpc / 16;
         poff += I.nchunk * I.N;
         soff += I.nsrc;
-        if (!h->hmat) h->kv_bytes += I.N * I.N * bpc;
+        if (!h->hmat && !h->tc) h->kv_bytes += I.N * I.N * bpc;
     }
     const int64_t Nt = eoff;
     h->Ntot = Nt;
@@ -966,9 +1071,42 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
             return st;
         }
     }
+    if (h->tc) {
+        // one kernel matrix for the batch: BF16 hi and lo, rows padded to
+        // 128, reduction to 64 with zeros; V rows of all networks likewise
+        const int64_t na = h->tc_mpad * h->tc_kpad, nb = (int64_t)h->tc_bn * h->tc_kpad;
+        DALLOC(h->tc_A, 2 * na);
+        DALLOC(h->tc_B, 2 * nb);
+        CKC(cudaMemsetAsync(h->tc_A, 0, sizeof(__nv_bfloat16) * 2 * na, h->stream));
+        CKC(cudaMemsetAsync(h->tc_B, 0, sizeof(__nv_bfloat16) * 2 * nb, h->stream));
+        const Inst &I = h->hinst[0];
+        dim3 grid((unsigned)I.N, (unsigned)((I.N + 255) / 256));
+        if (h->mode == 2)
+            tc_assemble_kernel<2><<<grid, 256, 0, h->stream>>>(I.N, h->tc_kpad, h->node, h->elem, h->tan, h->nrm,
+                                                              h->tc_A, h->tc_A + na);
+        else
+            tc_assemble_kernel<3><<<grid, 256, 0, h->stream>>>(I.N, h->tc_kpad, h->node, h->elem, h->tan, h->nrm,
+                                                              h->tc_A, h->tc_A + na);
+        h->launches++;
+        CKC(cudaGetLastError());
+        h->kv_bytes = 4 * h->tc_mrows * I.N;   // hi + lo, 2 bytes each, per stored entry
+        int st = tc_encode(&h->tc_map[0], h->tc_A, h->tc_mpad, h->tc_kpad, TC_BM);
+        if (st == DFN_OK) st = tc_encode(&h->tc_map[1], h->tc_A + na, h->tc_mpad, h->tc_kpad, TC_BM);
+        if (st == DFN_OK) st = tc_encode(&h->tc_map[2], h->tc_B, h->tc_bn, h->tc_kpad, h->tc_bn);
+        if (st == DFN_OK) st = tc_encode(&h->tc_map[3], h->tc_B + nb, h->tc_bn, h->tc_kpad, h->tc_bn);
+        if (st != DFN_OK) {
+            dfn_destroy(h);
+            return st;
+        }
+        CKC(cudaFuncSetAttribute(tc_gemm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(16)));
+        CKC(cudaFuncSetAttribute(tc_gemm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(32)));
+        CKC(cudaFuncSetAttribute(tc_gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(64)));
+        CKC(cudaFuncSetAttribute(tc_gemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(128)));
+        CKC(cudaFuncSetAttribute(tc_gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(256)));
+    }
     // dense kernel matrices, one per network
     h->K_bytes = (size_t)std::max<int64_t>(kvec, 1) * 16;
-    if (!h->hmat) {
+    if (!h->hmat && !h->tc) {
         cudaError_t e = cudaMalloc(&h->K, h->K_bytes);
         if (e != cudaSuccess) {
             set_err("cudaMalloc K", e, __FILE__, __LINE__);
@@ -977,7 +1115,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
     }
     std::vector<int4> tiles;
-    for (int i = 0; i < count && !h->hmat; i++) {
+    for (int i = 0; i < count && !h->hmat && !h->tc; i++) {
         const Inst &I = h->hinst[i];
         const int64_t e0 = I.eoff;
         void *Ki = static_cast<unsigned char *>(h->K) + I.kvec * 16;
@@ -1068,6 +1206,41 @@ int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_sT, dou
                                                                  h->partN, d_sT, d_sN);
     h->launches++;
     CKL();
+    return DFN_OK;
+}
+
+int32_t dfn_kernel_batch(dfn_handle *h, const double *slip, double *sT, double *sN)
+{
+    if (!h || !slip || !sT) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    const int64_t Nt = h->Ntot;
+    double *d = nullptr;
+    CK(cudaMalloc((void **)&d, sizeof(double) * 3 * Nt));
+    int st = DFN_OK;
+    cudaError_t e = cudaMemcpyAsync(d, slip, sizeof(double) * Nt, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) st = launch_gemv(h, M_ALL, d, 1, false);
+    for (int i = 0; i < h->B && e == cudaSuccess && st == DFN_OK; i++) {
+        const Inst &I = h->hinst[i];
+        kv_finish_kernel<<<blocks_of(I.N, 256), 256, 0, h->stream>>>(I.N, h->mode, (int)I.nchunk, I.prefT,
+                                                                     h->partT + I.poff, h->partN + I.poff,
+                                                                     d + Nt + I.eoff, d + 2 * Nt + I.eoff);
+        h->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && st == DFN_OK)
+        e = cudaMemcpyAsync(sT, d + Nt, sizeof(double) * Nt, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && st == DFN_OK && sN)
+        e = cudaMemcpyAsync(sN, d + 2 * Nt, sizeof(double) * Nt, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        set_err("dfn_kernel_batch", e, __FILE__, __LINE__);
+        return DFN_ERR_CUDA;
+    }
+    if (st != DFN_OK) return st;
+    int flag = 0;
+    CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) { g_err = "a K.V kernel gave up waiting on its pipeline"; return DFN_ERR_CUDA; }
     return DFN_OK;
 }
 

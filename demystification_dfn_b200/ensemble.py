@@ -71,6 +71,17 @@ class Ensemble:
     def n_elements(self):
         return [a.N for a in self.arrays]
 
+    def kernel(self, slips):
+        """K.V of every network: list of slip vectors in, lists of shear and
+        normal stress rates out (dfn_kernel_batch)."""
+        v = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64) for s in slips]))
+        if len(v) != sum(self.n_elements):
+            raise ValueError("one slip vector per network, of its nb_element")
+        sT, sN = np.empty_like(v), np.empty_like(v)
+        _lib.check(self.lib.dfn_kernel_batch(self.h, ptr(v), ptr(sT), ptr(sN)), self.lib)
+        cut = np.cumsum(self.n_elements)[:-1]
+        return np.split(sT, cut), np.split(sN, cut)
+
     def solve(self, n_steps=0, t_end=0.0, check=True):
         """Advance every network by n_steps accepted steps, or to time t_end."""
         reps = (DfnReport * self.B)()

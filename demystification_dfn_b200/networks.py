@@ -209,3 +209,34 @@ def small_network(seed=0, n_faults=4, mode="modeII", **kw):
     kw.setdefault("box", 600.0)
     kw.setdefault("length_range", (40.0, 160.0))
     return fault_network(n_faults=n_faults, seed=seed, mode=mode, **kw)
+
+
+def shared_geometry_ensemble(count, base=None, seed=0, noise=0.10, **kw):
+    """``count`` realisations of one fault network (same faults, nodes and
+    elastic constants, so one kernel matrix serves all of them): each member
+    redraws the per-fault a and b (lognormal ``noise``), the initial slip
+    rates and the fault that carries the pore-pressure step, from its own
+    seed. ``base`` defaults to :func:`fault_network` with ``seed`` and ``kw``."""
+    import copy
+
+    if base is None:
+        base = fault_network(seed=seed, **kw)
+    members = []
+    for m in range(count):
+        rng = np.random.default_rng(100_000 + 7919 * seed + m)
+        p = copy.deepcopy(base)
+        p.hyperparameter.simulation_name = f"{base.hyperparameter.simulation_name}_member{m}"
+        dP = max(float(np.max(f.P)) for f in base.faults)
+        stepped = int(rng.integers(len(p.faults)))
+        for i, f in enumerate(p.faults):
+            n = f.nb_element
+            f.a[:] = np.mean(f.a) * np.exp(rng.normal(0.0, noise))
+            f.b[:] = np.mean(f.b) * np.exp(rng.normal(0.0, noise))
+            V = np.mean(f.V) * np.exp(rng.normal(0.0, noise, n))
+            f.V[:] = V
+            f.theta[:] = np.log(f.V0 / V)
+            f.P[:] = 0.0
+            if i == stepped:
+                f.P[: max(1, n // 2)] = dP
+        members.append(p)
+    return members

@@ -47,7 +47,12 @@ typedef enum dfn_status {
 
 enum { DFN_MODE_II = 2, DFN_MODE_III = 3 };                    /* hyperparameter/fracture_mode */
 enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter/static_kernel */
-enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2 }; /* stored K entries */
+/* Stored K entries. DFN_STORE_BF16X2_TC: for a batch whose networks share
+ * one geometry (same nb_element, nodes, fracture mode and elastic constants;
+ * up to 256 networks), K is stored once as BF16 hi + lo matrices and the
+ * K.V of all networks of a stage is one tcgen05 tensor-core GEMM (BF16
+ * products, FP32 accumulation). No counterpart in the reference. */
+enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_BF16X2_TC = 3 };
 /* Pressure solver: DFN_PRESSURE_CG is the reference's CG with tree-reduced
  * dot products; DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
  * does, reproducing its rounding and iteration counts bit for bit (slower
@@ -204,6 +209,12 @@ int64_t dfn_nb_element(const dfn_handle *h);
 int64_t dfn_kernel_bytes(const dfn_handle *h);
 
 /* ---- operators (host buffers) ---------------------------------------- */
+/* K.V of every network of a batch: slip, sT and sN hold the networks'
+ * vectors back to back (host memory, sum of nb_element doubles each; sN may
+ * be NULL). Allocates a device buffer per call (a utility, not a stage of the
+ * solve loop). No counterpart in the reference, whose kernel_ptr serves one
+ * network (src/variables.f90:17-26). */
+int32_t dfn_kernel_batch(dfn_handle *h, const double *slip, double *sT, double *sN);
 /* Replaces kernel_ptr => directII/directIII/hmatII/hmatIII,
  * interface src/variables.f90:17-26: stressT/stressN = K.slip (stress rates
  * when slip holds V). stressN may be NULL in mode III. */
