@@ -296,6 +296,78 @@ def leg_learned(args, local, stream):
     return out
 
 
+def leg_tensor_core(args, local, stream):
+    """Shared-geometry ensemble on tensor cores: 64 realisations of the
+    800-fault network (per-member a, b, initial V and stepped fault), K.V of
+    all members as one tcgen05 GEMM per stage (BF16 hi+lo, FP32
+    accumulation), against single-network FP64 runs of two members to the
+    same simulated time (V formulation and Newton slip formulation)."""
+    from demystification_dfn_b200 import networks
+    from demystification_dfn_b200.ensemble import Ensemble
+    from demystification_dfn_b200.simulation import Simulation
+
+    hbm, _ = peaks()
+    tc_peak = 1653.7
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        tc_peak = float(json.load(open(pk)).get("bf16_tflops", tc_peak))
+    base = make_problem(0, args.n_faults)
+    R = 64
+    members = networks.shared_geometry_ensemble(R, base=base, seed=0)
+    out = {"workload": f"{R} realisations of the {len(base.faults)}-fault network sharing one kernel matrix",
+           "members": R}
+    t_end = 200.0
+    for form in ("v", "newton"):
+        e = Ensemble(members, storage="bf16x2_tc", pressure=args.pressure, device=local, formulation=form)
+        e.set_stream(stream.cuda_stream)
+        N = e.n_elements[0]
+        e.solve(n_steps=3, check=False)
+        e.profile_kv(True)
+        n = 20
+        reps, ms = _timed(stream, lambda: e.solve(n_steps=n, check=False))
+        kms, kn = e.profile_kv_read()
+        e.profile_kv(False)
+        kavg = kms / max(kn, 1)
+        flops = 3 * 2 * (2 * N) * N * R      # three BF16 products per entry, mode II rows
+        res = {"network_steps_per_s": R * n / (ms / 1e3), "ms_per_round": ms / n, "kv_avg_ms": kavg,
+               "kv_bytes": e.kernel_bytes, "kv_GBps": e.kernel_bytes / (kavg / 1e3) / 1e9,
+               "kv_frac_of_measured_hbm": e.kernel_bytes / (kavg / 1e3) / 1e9 / hbm,
+               "tensor_TFLOPs": flops / (kavg / 1e3) / 1e12,
+               "tensor_frac_of_measured_bf16": flops / (kavg / 1e3) / 1e12 / tc_peak,
+               "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
+                                 for s in sorted({r["status"] for r in reps})}}
+        e.close()
+        # accuracy: the same members to t_end, batch on tensor cores vs FP64 alone
+        e = Ensemble(members[:2], storage="bf16x2_tc", pressure=args.pressure, device=local, formulation=form)
+        e.set_stream(stream.cuda_stream)
+        e.solve(t_end=t_end, check=False)
+        errs = {}
+        for i in range(2):
+            a = e.state(i)
+            with Simulation(members[i], pressure=args.pressure, device=local, formulation=form) as s:
+                s.set_stream(stream.cuda_stream)
+                s.solve_to(t_end)
+                b = s.state()
+                Vb = s.velocity()
+            Na = len(a["P"])
+            if form == "v":
+                Va = a["Y"][:Na]
+            else:
+                with Simulation(members[i], pressure=args.pressure, device=local, formulation=form) as s2:
+                    s2.set_state(a["Y"], a["P"], a["time"], a["t_try"], a["it_count"])
+                    Va = s2.velocity()
+                d, dr = a["Y"][:Na], b["Y"][:Na]
+                errs["slip"] = max(errs.get("slip", 0.0), float(np.abs(d - dr).max() / np.abs(dr).max()))
+            errs["V"] = max(errs.get("V", 0.0), float(np.abs(Va - Vb).max() / np.abs(Vb).max()))
+            pa, pb = a["Y"][Na:2 * Na], b["Y"][Na:2 * Na]
+            errs["psi"] = max(errs.get("psi", 0.0), float(np.abs(pa - pb).max() / np.abs(pb).max()))
+        e.close()
+        res["max_rel_err_vs_fp64_single_network_at_t_end"] = errs
+        res["t_end_s"] = t_end
+        out[form] = res
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -345,7 +417,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
     ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
-    ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,learned,cpu",
+    ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,tensor_core,learned,cpu",
                     help="comma list of the extra legs to run")
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
@@ -514,6 +586,8 @@ def main():
         extras["single_fault"] = leg_single_fault(args, local, stream)
     if rank == 0 and "hmatrix" in legs:
         extras["hmatrix"] = leg_hmatrix(args, local, stream)
+    if rank == 0 and "tensor_core" in legs:
+        extras["tensor_core"] = leg_tensor_core(args, local, stream)
     if rank == 0 and "learned" in legs:
         extras["learned_newton"] = leg_learned(args, local, stream)
 
