@@ -15,7 +15,6 @@
 #include "hmat_device.cuh"
 #include "newton.cuh"
 #include "tc_gemm.cuh"
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -115,8 +114,7 @@ struct dfn_handle {
     bool tc = false;
     int tc_bn = 0, tc_nmt = 0, tc_split = 1, tc_kps = 0, tc_nkb = 0;
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
-    __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each
-    CUtensorMap tc_map[4];
+    __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
     StepCtl *h_ctl = nullptr;     // pinned mirror, B entries
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -221,8 +219,9 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
 template <int BN>
 static void tc_launch_bn(dfn_handle *h, const TcOut &o)
 {
+    const int64_t na = h->tc_mpad * h->tc_kpad, nb = (int64_t)h->tc_bn * h->tc_kpad;
     tc_gemm_kernel<BN><<<(unsigned)(h->tc_nmt * h->tc_split), TC_THREADS, tc_smem_bytes(BN), h->stream>>>(
-        h->tc_map[0], h->tc_map[1], h->tc_map[2], h->tc_map[3], o, h->err_flag);
+        h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o, h->err_flag);
 }
 
 static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
@@ -242,35 +241,6 @@ static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
     case 64: tc_launch_bn<64>(h, o); break;
     case 128: tc_launch_bn<128>(h, o); break;
     default: tc_launch_bn<256>(h, o); break;
-    }
-    return DFN_OK;
-}
-
-// 2D tensor map of a row-major BF16 matrix [rows][kpad], boxes of 64 x box_rows,
-// 128-byte swizzle (the tcgen05 K-major operand layout).
-static int tc_encode(CUtensorMap *m, const void *ptr, int64_t rows, int64_t kpad, int box_rows)
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
-    if (!enc) {
-        void *fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn) {
-            g_err = "cuTensorMapEncodeTiled is not available";
-            return DFN_ERR_CUDA;
-        }
-        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(kpad * 2)};
-    cuuint32_t box[2] = {TC_BK, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-        g_err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
-        return DFN_ERR_CUDA;
     }
     return DFN_OK;
 }
@@ -1090,14 +1060,6 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         h->launches++;
         CKC(cudaGetLastError());
         h->kv_bytes = 4 * h->tc_mrows * I.N;   // hi + lo, 2 bytes each, per stored entry
-        int st = tc_encode(&h->tc_map[0], h->tc_A, h->tc_mpad, h->tc_kpad, TC_BM);
-        if (st == DFN_OK) st = tc_encode(&h->tc_map[1], h->tc_A + na, h->tc_mpad, h->tc_kpad, TC_BM);
-        if (st == DFN_OK) st = tc_encode(&h->tc_map[2], h->tc_B, h->tc_bn, h->tc_kpad, h->tc_bn);
-        if (st == DFN_OK) st = tc_encode(&h->tc_map[3], h->tc_B + nb, h->tc_bn, h->tc_kpad, h->tc_bn);
-        if (st != DFN_OK) {
-            dfn_destroy(h);
-            return st;
-        }
         CKC(cudaFuncSetAttribute(tc_gemm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(16)));
         CKC(cudaFuncSetAttribute(tc_gemm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(32)));
         CKC(cudaFuncSetAttribute(tc_gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(64)));

@@ -12,13 +12,21 @@
 // K step into one FP32 accumulator in TMEM (the lo x lo term is below the
 // BF16 rounding of the others).
 //
+// Layout in HBM: K (hi and lo) and the packed V rows are stored tile by
+// tile (128 x 64 for K, BN x 64 for V, tiles of one row block consecutive
+// along the reduction), each tile already in the 128-byte-swizzled order the
+// tensor cores read from shared memory (16-byte chunk c of row r at chunk
+// position c ^ (r mod 8) within 1024-byte groups of 8 rows). A stage is then
+// four contiguous bulk copies (16 KiB for a K tile), which streams HBM at
+// full page locality instead of 128-byte row pieces 2N bytes apart.
+//
 // Work unit: one 128-row tile of K and one split of the reduction range (the
 // splits spread the 128-row tiles over the 148 SMs; their partial sums go to
 // part[s][row] and the friction kernel adds them in a fixed order, so the
 // result is deterministic). One CTA of 4 warps per unit:
-//   warp 0, one lane   TMA producer: 2D tiled copies (128-byte swizzle) of
-//                      Khi, Klo (128 x 64) and Vhi, Vlo (BN x 64) per stage
-//                      into a ring of 2-4 stages, completed on mbarriers;
+//   warp 0, one lane   producer: cp.async.bulk copies of the Khi, Klo and
+//                      Vhi, Vlo tiles of a stage into a ring of 2-4 stages,
+//                      completed on mbarriers;
 //   warp 1, one lane   MMA issuer: 4 x 3 tcgen05.mma per stage, then
 //                      tcgen05.commit to the stage's "empty" mbarrier;
 //   all 4 warps        epilogue: tcgen05.ld of the warp's 32 TMEM lanes
@@ -27,7 +35,6 @@
 // producer waits (bounded) for the copies it issued, TMEM is freed and the
 // CTA returns.
 #pragma once
-#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -40,6 +47,12 @@ __host__ __device__ constexpr size_t tc_stage_bytes(int bn) { return (size_t)2 *
 // ring depth that keeps the stages within 192 KiB of shared memory
 __host__ __device__ constexpr int tc_stages(int bn) { return bn <= 64 ? 4 : (bn <= 128 ? 3 : 2); }
 __host__ __device__ constexpr size_t tc_smem_bytes(int bn) { return tc_stages(bn) * tc_stage_bytes(bn) + 1024 + 256; }
+
+// Element offset of (row r, column j < 64) inside a swizzled tile of 128-byte rows.
+__host__ __device__ inline int64_t tc_swz(int64_t r, int64_t j)
+{
+    return (r >> 3) * 512 + (r & 7) * 64 + ((((j >> 3) ^ (r & 7))) << 3) + (j & 7);
+}
 
 struct TcOut {
     double *partT, *partN;     // per network at inst[r].poff: [splits][N]
@@ -71,13 +84,6 @@ __host__ __device__ constexpr uint32_t tc_idesc(int bn)
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
-__device__ __forceinline__ void tc_tma_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                 ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-                 : "memory");
-}
-
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
 {
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -93,8 +99,8 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar)
 
 template <int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, TcOut out,
+    tc_gemm_kernel(const __nv_bfloat16 *__restrict__ Ah, const __nv_bfloat16 *__restrict__ Al,
+                   const __nv_bfloat16 *__restrict__ Bh, const __nv_bfloat16 *__restrict__ Bl, TcOut out,
                    int *err_flag)
 {
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "N of an M=128 MMA is a multiple of 16 up to 256");
@@ -142,11 +148,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (*(volatile int *)abort_flag) break;
             unsigned char *st = ring + s * tc_stage_bytes(BN);
             mbar_expect_tx(&full[s], TX);
-            const int kx = (kb0 + i) * TC_BK, my = mt * TC_BM;
-            tc_tma_2d(st, &mAh, kx, my, &full[s]);
-            tc_tma_2d(st + A_BYTES, &mAl, kx, my, &full[s]);
-            tc_tma_2d(st + 2 * A_BYTES, &mBh, kx, 0, &full[s]);
-            tc_tma_2d(st + 2 * A_BYTES + B_BYTES, &mBl, kx, 0, &full[s]);
+            const int64_t kb = kb0 + i;
+            const int64_t at = ((int64_t)mt * out.nkb + kb) * (TC_BM * TC_BK), bt = kb * (BN * TC_BK);
+            tma_bulk_g2s(st, Ah + at, A_BYTES, &full[s]);
+            tma_bulk_g2s(st + A_BYTES, Al + at, A_BYTES, &full[s]);
+            tma_bulk_g2s(st + 2 * A_BYTES, Bh + bt, B_BYTES, &full[s]);
+            tma_bulk_g2s(st + 2 * A_BYTES + B_BYTES, Bl + bt, B_BYTES, &full[s]);
             issued = i + 1;
         }
         // the copies this thread issued complete before the CTA may exit
@@ -222,8 +229,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                      "r"((uint32_t)(BN < 32 ? 32 : BN)));
 }
 
-// V of the R networks of a stage -> BF16 hi/lo rows [rpad][kpad] (zero
-// padded); V of network r is Vbase[vmul * r * N + l].
+// V of the R networks of a stage -> BF16 hi/lo, swizzled tiles of rpad rows
+// per 64 reduction elements (zero padded); V of network r is
+// Vbase[vmul * r * N + l]. One thread per (row, element).
 __global__ void tc_pack_v_kernel(const double *__restrict__ Vbase, int vmul, int64_t N, int R, int rpad,
                                  int64_t kpad, __nv_bfloat16 *__restrict__ Bh, __nv_bfloat16 *__restrict__ Bl)
 {
@@ -234,12 +242,19 @@ __global__ void tc_pack_v_kernel(const double *__restrict__ Vbase, int vmul, int
     double x = (r < R && l < N) ? Vbase[(int64_t)vmul * r * N + l] : 0.0;
     const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
     const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
-    Bh[idx] = h;
-    Bl[idx] = lo;
+    const int64_t o = (l / TC_BK) * ((int64_t)rpad * TC_BK) + tc_swz(r, l % TC_BK);
+    Bh[o] = h;
+    Bl[o] = lo;
 }
 
-// Kernel matrix of the shared geometry as BF16 hi/lo rows [mpad][kpad]:
-// shear rows 0..N-1, normal rows N..2N-1 (mode II); padding stays zero.
+// Kernel matrix of the shared geometry as BF16 hi/lo swizzled tiles (row
+// block mt, reduction block kb at tile mt * nkb + kb): shear rows 0..N-1,
+// normal rows N..2N-1 (mode II); padding stays zero.
+__device__ __forceinline__ int64_t tc_a_index(int64_t m, int64_t l, int64_t nkb)
+{
+    return ((m / TC_BM) * nkb + l / TC_BK) * (TC_BM * TC_BK) + tc_swz(m % TC_BM, l % TC_BK);
+}
+
 template <int MODE>
 __global__ void tc_assemble_kernel(int64_t N, int64_t kpad, const double *__restrict__ node,
                                    const double *__restrict__ elem, const double *__restrict__ tan,
@@ -254,13 +269,14 @@ __global__ void tc_assemble_kernel(int64_t N, int64_t kpad, const double *__rest
     double T = 0.0, Nn = 0.0;
     if (MODE == 3) T = entry_mode3(e1, e2, tan[2 * k], tan[2 * k + 1], xl, yl, xr, yr);
     else entry_mode2(e1, e2, nrm[2 * k], nrm[2 * k + 1], xl, yl, xr, yr, nrm[2 * l], nrm[2 * l + 1], T, Nn);
+    const int64_t nkb = kpad / TC_BK;
     __nv_bfloat16 h, lo;
     split_bf16(T, h, lo);
-    Ah[k * kpad + l] = h;
-    Al[k * kpad + l] = lo;
+    Ah[tc_a_index(k, l, nkb)] = h;
+    Al[tc_a_index(k, l, nkb)] = lo;
     if (MODE == 2) {
         split_bf16(Nn, h, lo);
-        Ah[(N + k) * kpad + l] = h;
-        Al[(N + k) * kpad + l] = lo;
+        Ah[tc_a_index(N + k, l, nkb)] = h;
+        Al[tc_a_index(N + k, l, nkb)] = lo;
     }
 }
