@@ -315,11 +315,13 @@ def leg_tensor_core(args, local, stream):
     R = 64
     members = networks.shared_geometry_ensemble(R, base=base, seed=0)
     out = {"workload": f"{R} realisations of the {len(base.faults)}-fault network sharing one kernel matrix",
-           "members": R}
+           "members": R, "pressure_solver": "tridiag (exact implicit step)"}
     t_end = 200.0
+    pressure = "tridiag"
     for form in ("v", "newton"):
-        e = Ensemble(members, storage="bf16x2_tc", pressure=args.pressure, device=local, formulation=form)
+        e = Ensemble(members, storage="bf16x2_tc", pressure=pressure, device=local, formulation=form)
         e.set_stream(stream.cuda_stream)
+        res_tune = e.autotune()
         N = e.n_elements[0]
         e.solve(n_steps=3, check=False)
         e.profile_kv(True)
@@ -335,16 +337,17 @@ def leg_tensor_core(args, local, stream):
                "tensor_TFLOPs": flops / (kavg / 1e3) / 1e12,
                "tensor_frac_of_measured_bf16": flops / (kavg / 1e3) / 1e12 / tc_peak,
                "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
-                                 for s in sorted({r["status"] for r in reps})}}
+                                 for s in sorted({r["status"] for r in reps})},
+               "autotune": res_tune}
         e.close()
         # accuracy: the same members to t_end, batch on tensor cores vs FP64 alone
-        e = Ensemble(members[:2], storage="bf16x2_tc", pressure=args.pressure, device=local, formulation=form)
+        e = Ensemble(members[:2], storage="bf16x2_tc", pressure=pressure, device=local, formulation=form)
         e.set_stream(stream.cuda_stream)
         e.solve(t_end=t_end, check=False)
         errs = {}
         for i in range(2):
             a = e.state(i)
-            with Simulation(members[i], pressure=args.pressure, device=local, formulation=form) as s:
+            with Simulation(members[i], pressure=pressure, device=local, formulation=form) as s:
                 s.set_stream(stream.cuda_stream)
                 s.solve_to(t_end)
                 b = s.state()
@@ -353,7 +356,7 @@ def leg_tensor_core(args, local, stream):
             if form == "v":
                 Va = a["Y"][:Na]
             else:
-                with Simulation(members[i], pressure=args.pressure, device=local, formulation=form) as s2:
+                with Simulation(members[i], pressure=pressure, device=local, formulation=form) as s2:
                     s2.set_state(a["Y"], a["P"], a["time"], a["t_try"], a["it_count"])
                     Va = s2.velocity()
                 d, dr = a["Y"][:Na], b["Y"][:Na]

@@ -86,6 +86,7 @@ def load():
         "dfn_mlp_infer": (i32, [ctypes.POINTER(ctypes.c_float), i64, ctypes.POINTER(ctypes.c_float),
                                 ctypes.POINTER(ctypes.c_float)]),
         "dfn_set_graphs": (i32, [P, i32]),
+        "dfn_autotune": (i32, [P, ctypes.c_void_p]),
         "dfn_kernel_batch": (i32, [P, dp, dp, dp]),
         "dfn_velocity": (i32, [P, dp]),
         "dfn_hmat_stats": (i32, [P, ctypes.POINTER(i64)]),

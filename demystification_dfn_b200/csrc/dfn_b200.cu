@@ -94,6 +94,7 @@ struct dfn_handle {
     int64_t nlong = 0, nlong0 = 0;
     int *short_seg = nullptr;             // the others
     int64_t nshort = 0, nshort0 = 0;
+    bool tri_thread = false;              // short segments: one thread (true) or one warp each
     int64_t nsrc_tot = 0, part_tot = 0;
     // geometry and parameters (concatenated)
     double *node = nullptr, *elem = nullptr, *ds = nullptr, *tan = nullptr, *nrm = nullptr, *permx = nullptr;
@@ -286,7 +287,17 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
     } else {
         const int64_t nshort = (ninst == h->B) ? h->nshort : h->nshort0;
         const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
-        if (nshort > 0) {
+        if (nshort > 0 && h->tri_thread) {
+            dim3 grid((unsigned)((nshort + 127) / 128), (unsigned)nsys);
+            pressure_tridiag_thread_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0,
+                                                                        dt_explicit, h->seg_start, h->seg_inst,
+                                                                        h->short_seg, nshort, h->Ptemp, h->Pdot_s,
+                                                                        h->pwork);
+            if (nlong > 0) {
+                h->launches++;
+                CKL();
+            }
+        } else if (nshort > 0) {
             dim3 grid((unsigned)((nshort + 7) / 8), (unsigned)nsys);
             pressure_tridiag_kernel<<<grid, 256, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0,
                                                                  dt_explicit, h->seg_start, h->seg_inst,
@@ -1024,6 +1035,10 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
         h->nlong = (int64_t)lg.size();
         h->nshort = (int64_t)sh.size();
+        // default launch shape of the short segments (dfn_autotune measures
+        // instead): warps while the segments fill few waves of warps, threads
+        // once there are tens of thousands
+        h->tri_thread = h->nshort >= 16384;
         if (h->nlong) {
             DALLOC(h->long_seg, lg.size());
             HCOPY(h->long_seg, lg.data(), lg.size());
@@ -1129,6 +1144,58 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
 int32_t dfn_create(const dfn_problem *p, const dfn_options *opt, dfn_handle **out)
 {
     return dfn_create_batch(p, 1, opt, out);
+}
+
+// Times the interchangeable launch shapes on this handle's own data and
+// keeps the fastest: K.V through TMA bulk copies or 128-bit loads (bitwise
+// identical results), and, with the tridiagonal pressure solve, short
+// segments one thread or one warp each (equal to rounding). The timing
+// launches write only per-attempt work buffers; the state is untouched.
+int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
+{
+    if (!h) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    dfn_tuning r;
+    memset(&r, 0, sizeof(r));
+    const bool prof = h->prof;
+    h->prof = false;
+    auto time_it = [&](auto &&launch, int reps, double &ms) -> int {
+        TRY(launch());   // warm-up
+        CK(cudaEventRecord(h->ev0, h->stream));
+        for (int q = 0; q < reps; q++) TRY(launch());
+        CK(cudaEventRecord(h->ev1, h->stream));
+        CK(cudaEventSynchronize(h->ev1));
+        float f = 0.0f;
+        CK(cudaEventElapsedTime(&f, h->ev0, h->ev1));
+        ms = f / reps;
+        return DFN_OK;
+    };
+    r.gemv_impl = h->gemv_impl;
+    if (!h->hmat && !h->tc) {
+        const int keep = h->gemv_impl;
+        for (int impl = 0; impl < 2; impl++) {
+            h->gemv_impl = impl;
+            TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, r.ms[impl]));
+        }
+        h->gemv_impl = (r.ms[1] < r.ms[0]) ? 1 : 0;
+        r.gemv_impl = h->gemv_impl;
+        (void)keep;
+    }
+    r.tri_thread = h->tri_thread ? 1 : 0;
+    if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {
+        for (int v = 0; v < 2; v++) {
+            h->tri_thread = v == 1;
+            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, r.ms[2 + v]));
+        }
+        h->tri_thread = r.ms[3] < r.ms[2];
+        r.tri_thread = h->tri_thread ? 1 : 0;
+    }
+    h->prof = prof;
+    drop_graph(h);
+    CK(cudaStreamSynchronize(h->stream));
+    if (t) *t = r;
+    return DFN_OK;
 }
 
 int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)

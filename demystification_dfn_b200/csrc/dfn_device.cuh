@@ -903,7 +903,8 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
 // then reruns the exact recurrence over its own rows:
 //   c_k = A3_k / (A2_k - A1_k c_{k-1})       a Moebius map of c_{k-1}: the
 //        2x2 matrix [[0, A3], [-A1, A2]] acting on (p, q), c = p/q; products
-//        are rescaled by their largest entry (the ratio is unchanged);
+//        are rescaled by a power of two near their largest entry (exact; the
+//        ratio is unchanged);
 //   d_k = (r_k - A1_k d_{k-1}) / den_k        affine in d_{k-1};
 //   x_k = d_k - c_k x_{k+1}                   affine in x_{k+1}, scanned from
 //        the end of the segment.
@@ -916,15 +917,20 @@ struct Aff { double a, b; };         // x -> a x + b
 
 __device__ __forceinline__ Mob mob_id() { return {1.0, 0.0, 0.0, 1.0}; }
 __device__ __forceinline__ Aff aff_id() { return {1.0, 0.0}; }
+// 2^-e for s in [2^e, 2^(e+1)) (normal s), else 1: an exact rescaling.
+__device__ __forceinline__ double pow2_inv(double s)
+{
+    const long long bits = __double_as_longlong(s);
+    const int ex = (int)((bits >> 52) & 0x7FF);
+    if (ex == 0 || ex >= 2046) return 1.0;
+    return __longlong_as_double((long long)(2046 - ex) << 52);
+}
 // outer o applied after inner i
 __device__ __forceinline__ Mob compose(const Mob &o, const Mob &i)
 {
     Mob r{o.a * i.a + o.b * i.c, o.a * i.b + o.b * i.d, o.c * i.a + o.d * i.c, o.c * i.b + o.d * i.d};
-    const double s = fmax(fmax(fabs(r.a), fabs(r.b)), fmax(fabs(r.c), fabs(r.d)));
-    if (s > 0.0 && isfinite(s)) {
-        const double q = 1.0 / s;
-        r.a *= q; r.b *= q; r.c *= q; r.d *= q;
-    }
+    const double q = pow2_inv(fmax(fmax(fabs(r.a), fabs(r.b)), fmax(fabs(r.c), fabs(r.d))));
+    r.a *= q; r.b *= q; r.c *= q; r.d *= q;
     return r;
 }
 __device__ __forceinline__ Aff compose(const Aff &o, const Aff &i) { return {o.a * i.a, o.a * i.b + o.b}; }
@@ -1031,7 +1037,7 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     const int nr = (int)max((int64_t)0, min(m, L - r0));
     constexpr int R = (MAXM > 0) ? MAXM : 1;
     double reg[4][R];
-    // row q of element j of this thread: A1, den (A2 on input), c (A3 on
+    // row q of element j of this thread: A1, 1/den (A2 on input), c (A3 on
     // input), d (right-hand side on input)
     auto at = [&](int q, int j) -> double & {
         if constexpr (MAXM > 0) return reg[q][j];
@@ -1052,29 +1058,83 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     const Mob E = grp_scan_excl<NTG>(T, mob_id(), smm);
     double c = (tid == 0) ? 0.0 : E.b / E.d;
     tri_rows<MAXM, false>(nr, [&](int j) {
-        const double den = at(1, j) - at(0, j) * c;
-        c = at(2, j) / den;
-        at(1, j) = den; at(2, j) = c;
+        const double rden = 1.0 / (at(1, j) - at(0, j) * c);
+        c = at(2, j) * rden;
+        at(1, j) = rden; at(2, j) = c;
     });
     // d recurrence
     Aff F = aff_id();
-    tri_rows<MAXM, false>(nr, [&](int j) { F = compose(Aff{-at(0, j) / at(1, j), at(3, j) / at(1, j)}, F); });
+    tri_rows<MAXM, false>(nr, [&](int j) { F = compose(Aff{-at(0, j) * at(1, j), at(3, j) * at(1, j)}, F); });
     double d = grp_scan_excl<NTG>(F, aff_id(), sma).b;
     tri_rows<MAXM, false>(nr, [&](int j) {
-        d = (at(3, j) - at(0, j) * d) / at(1, j);
+        d = (at(3, j) - at(0, j) * d) * at(1, j);
         at(3, j) = d;
     });
     // back substitution
     Aff G = aff_id();
     tri_rows<MAXM, true>(nr, [&](int j) { G = compose(Aff{-at(2, j), at(3, j)}, G); });
     double x = grp_scan_excl_back<NTG>(G, sma).b;
+    const double rdt = (dt < 1e-9) ? 0.0 : 1.0 / dt;
     tri_rows<MAXM, true>(nr, [&](int j) {
         const int64_t k = k0 + r0 + j;
         x = at(3, j) - at(2, j) * x;
         Pt[k] = x;
-        Pd[k] = (dt < 1e-9) ? 0.0 : (x - p.P[k]) / dt;
+        Pd[k] = (x - p.P[k]) * rdt;
         if (!isfinite(x)) bad = 1;
     });
+}
+
+// Short segments, one thread each (the sequential Thomas algorithm): for
+// launches with many more segments than a wave of warps, where the scans'
+// instructions would outweigh the latency they hide. grid (ceil(segments /
+// 128), systems), blockDim 128.
+__global__ void __launch_bounds__(128) pressure_tridiag_thread_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
+                                                                      int mask, int kind, int sys0,
+                                                                      double dt_explicit, const int64_t *seg_start,
+                                                                      const int *seg_inst, const int *seg_list,
+                                                                      int64_t nlist, double *Ptemp, double *Pdot,
+                                                                      double *work)
+{
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= nlist) return;
+    const int sg = seg_list[q];
+    const int i = seg_inst[sg];
+    if (!takes_part(ctl, i, mask)) return;
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.y;
+    const int64_t N = I.N;
+    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
+    const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+    double *cp = work + 24 * I.eoff + (int64_t)sys * 4 * N;   // modified super-diagonal
+    double *dp = cp + N;                                       // modified right-hand side
+    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
+    double cprev = 0.0, dprev = 0.0;
+#pragma unroll 4
+    for (int64_t k = k0; k < k1; k++) {
+        double A1, A2, A3;
+        prow(p, k, dt, A1, A2, A3);
+        if (k == k0) A1 = 0.0;
+        if (k == k1 - 1) A3 = 0.0;
+        const double rhs = add_(p.P[k], psource(p, k, dt));
+        const double rden = 1.0 / (A2 - A1 * cprev);
+        const double c = A3 * rden;
+        const double d = (rhs - A1 * dprev) * rden;
+        cp[k] = c; dp[k] = d;
+        cprev = c; dprev = d;
+    }
+    const double rdt = (dt < 1e-9) ? 0.0 : 1.0 / dt;
+    double xn = 0.0;
+    bool bad = false;
+#pragma unroll 4
+    for (int64_t k = k1 - 1; k >= k0; k--) {
+        const double xk = dp[k] - cp[k] * xn;
+        xn = xk;
+        Pt[k] = xk;
+        Pd[k] = (xk - p.P[k]) * rdt;
+        if (!isfinite(xk)) bad = true;
+    }
+    if (bad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
 // Short segments, one warp each: grid (ceil(segments / 8), systems),

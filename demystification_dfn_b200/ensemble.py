@@ -54,6 +54,17 @@ class Ensemble:
     def set_stream(self, stream_handle: int):
         _lib.check(self.lib.dfn_set_stream(self.h, ctypes.c_void_p(stream_handle)), self.lib)
 
+    def autotune(self):
+        """Time the interchangeable launch shapes (K.V copy path, short-segment
+        pressure solve) on this handle's data and keep the fastest."""
+        class _T(ctypes.Structure):
+            _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32),
+                        ("ms", ctypes.c_double * 4)]
+        t = _T()
+        _lib.check(self.lib.dfn_autotune(self.h, ctypes.byref(t)), self.lib)
+        return {"gemv_impl": ["tma", "ldg"][t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
+                "ms": {"kv_tma": t.ms[0], "kv_ldg": t.ms[1], "pressure_warp": t.ms[2], "pressure_thread": t.ms[3]}}
+
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch
         every kernel on its own; results are identical."""

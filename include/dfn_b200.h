@@ -185,6 +185,22 @@ void dfn_default_options(dfn_options *opt);
  * assembles the kernel matrices on the device and sets time/t_try/it_count
  * as solve() does at entry (src/solver.f90:47-56). */
 int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle **out);
+/* Autotuner: times the interchangeable launch shapes on the handle's own
+ * data and keeps the fastest. K.V: TMA bulk copies or 128-bit loads
+ * (gemv_impl 0/1, bitwise identical results); tridiagonal pressure: short
+ * segments (<= 64 elements) solved by one thread each (sequential Thomas) or
+ * one warp each (scans), equal to rounding. ms[] = milliseconds per launch of
+ * K.V TMA, K.V LDG, pressure by warps, pressure by threads (0 = not timed).
+ * Without a call, K.V uses options.gemv_impl and the short segments use
+ * threads once a launch has at least 16384 of them. No counterpart in the
+ * reference. */
+typedef struct dfn_tuning {
+    int32_t gemv_impl;
+    int32_t tri_thread;
+    double ms[4];
+} dfn_tuning;
+int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
+
 /* Solve loops (dfn_solve_steps, dfn_solve_batch) replay a CUDA graph of 8
  * rounds of the solve() loop when at least 8 rounds remain (on by default;
  * captured at the first such call, on a private stream, and replayed on the

@@ -111,3 +111,27 @@ def test_graph_replay_matches_single_launches_bitwise(pressure):
     for a, b in zip(*out):
         assert a["it_count"] == b["it_count"] and a["time"] == b["time"]
         assert np.array_equal(a["Y"], b["Y"]) and np.array_equal(a["P"], b["P"])
+
+
+def test_autotune_keeps_results():
+    """The autotuner picks among launch shapes with equal results: the K.V
+    copy path is bitwise neutral, the short-segment pressure solve (thread or
+    warp per segment) equal to rounding."""
+    ps = members()
+    out = {}
+    for pressure in ("cg", "tridiag"):
+        for tune in (False, True):
+            with Ensemble(ps, pressure=pressure) as ens:
+                if tune:
+                    t = ens.autotune()
+                    assert t["gemv_impl"] in ("tma", "ldg") and t["ms"]["kv_tma"] > 0 and t["ms"]["kv_ldg"] > 0
+                    if pressure == "tridiag":
+                        assert t["ms"]["pressure_warp"] > 0 and t["ms"]["pressure_thread"] > 0
+                ens.solve(n_steps=12)
+                out[(pressure, tune)] = [ens.state(i) for i in range(len(ps))]
+    for a, b in zip(out[("cg", False)], out[("cg", True)]):
+        assert np.array_equal(a["Y"], b["Y"]) and a["time"] == b["time"]
+    for a, b in zip(out[("tridiag", False)], out[("tridiag", True)]):
+        N = len(a["P"])
+        assert abs(a["time"] - b["time"]) <= 1e-10 * b["time"]
+        assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-9 * np.abs(b["Y"][:N]).max()
