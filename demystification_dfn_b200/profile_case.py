@@ -1,0 +1,57 @@
+"""Small, fixed workloads for profiling one kernel under ncu.
+
+    python -m demystification_dfn_b200.profile_case tc_kv [R]
+        R realisations (default 64) of the 800-fault network sharing one
+        kernel matrix: three K.V launches of the tensor-core GEMM (2.05 GB of
+        BF16 hi + lo entries per launch).
+    python -m demystification_dfn_b200.profile_case tc_round [cg|tridiag]
+        the same batch, six solve rounds launched one by one (launch list of
+        a round: GEMM, pressure, friction, step control).
+    python -m demystification_dfn_b200.profile_case ensemble_round
+        eight 120-fault networks (FP32 storage, tridiagonal pressure), forty
+        solve rounds launched one by one.
+
+Each case exits 0 after printing one line, so the same command can run once
+without ncu and then under it.
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+
+def main(argv):
+    from . import networks
+    from .ensemble import Ensemble
+
+    case = argv[0] if argv else "tc_kv"
+    if case == "tc_kv":
+        R = int(argv[1]) if len(argv) > 1 else 64
+        base = networks.fault_network(n_faults=800, seed=0)
+        e = Ensemble(networks.shared_geometry_ensemble(R, base=base, seed=0), storage="bf16x2_tc")
+        rng = np.random.default_rng(0)
+        N = e.n_elements[0]
+        for _ in range(3):
+            e.kernel([rng.normal(size=N) for _ in range(R)])
+    elif case == "tc_round":
+        pressure = argv[1] if len(argv) > 1 else "tridiag"
+        base = networks.fault_network(n_faults=800, seed=0)
+        e = Ensemble(networks.shared_geometry_ensemble(64, base=base, seed=0), storage="bf16x2_tc",
+                     pressure=pressure)
+        e.set_graphs(False)
+        e.solve(n_steps=6, check=False)
+    elif case == "ensemble_round":
+        e = Ensemble([networks.ensemble_member(s, n_faults=120) for s in range(64, 72)], storage="fp32",
+                     pressure="tridiag")
+        e.set_graphs(False)
+        e.solve(n_steps=40, check=False)
+    else:
+        raise SystemExit(f"unknown case {case!r}")
+    e.close()
+    print("ok", case)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
