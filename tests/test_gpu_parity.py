@@ -283,3 +283,30 @@ def test_solve_writes_reference_output_files(tmp_path):
         assert a["time"] == b["time"]
         for k in ("V", "theta", "P"):
             assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("mode", ["modeII", "modeIII"])
+def test_event_onset_matches_oracle(mode):
+    """A velocity-weakening fault (a = 0.010 < b = 0.015) loaded by a 200 kg/s
+    injection reaches seismic slip rates within ~70 steps: the first accepted
+    step with max V > 1e-3 m/s comes at the same step and, in simulated time,
+    within 1e-6 of the simulated span (the north-star event-onset target)."""
+    p = networks.single_fault(n_el=200, length=2000.0, a=0.010, b=0.015, Dc=1e-3, q_kgs=200.0, tol=1e-6,
+                              mode=mode)
+    o = Oracle(p, threads=4)
+    o.use_dense()
+
+    def onset(step, state):
+        for k in range(1, 400):
+            step()
+            s = state()
+            N = len(s["P"])
+            if np.abs(s["Y"][:N]).max() > 1e-3:
+                return k, s["time"]
+        return None, None
+
+    ko, to = onset(lambda: o.solve_steps(1), o.state)
+    with Simulation(p, pressure="cg_exact") as s:
+        kg, tg = onset(lambda: s.solve_steps(1), s.state)
+    assert ko is not None and kg == ko
+    assert abs(tg - to) <= 1e-6 * to
