@@ -538,15 +538,22 @@ def main():
                              "compared_after": f"{args.warmup}+{args.steps} accepted steps from the same start"}
             s2.close()
 
-    if rank == 0 and args.ensemble > 0 and "ensemble" in legs:
+    if args.ensemble > 0 and "ensemble" in legs:
         # batched ensemble: many networks of uneven size in one handle, one
-        # launch per kernel for the whole batch, per-network step control
+        # launch per kernel for the whole batch, per-network step control;
+        # with several ranks each rank takes its share of the networks
+        # (placed by K.V bytes) and the throughput is the job's
         from demystification_dfn_b200 import networks
         from demystification_dfn_b200.ensemble import Ensemble
+        from demystification_dfn_b200.layout import build_arrays
+        from demystification_dfn_b200.sharding import reduce_timing, shard_by_work
 
-        members = networks.ensemble(args.ensemble)
+        allm = networks.ensemble(args.ensemble)
+        sizes = [build_arrays(p).N for p in allm]
+        members = [allm[i] for i in shard_by_work(sizes, world, rank)]
         hbm, _ = peaks()
-        ens_out = {"networks": len(members), "steps_per_network": args.ensemble_steps}
+        ens_out = {"networks": len(allm), "steps_per_network": args.ensemble_steps, "ranks": world,
+                   "placement": "networks sharded over ranks by K.V bytes"}
         for store in ("fp64", "fp32", "bf16x2"):
             ens = Ensemble(members, storage=store, pressure=args.pressure, device=local, gemv=args.gemv)
             ens.set_stream(stream.cuda_stream)
@@ -559,13 +566,15 @@ def main():
             a1.record(stream)
             torch.cuda.synchronize()
             kms, kn = ens.profile_kv_read()
-            ms_e = a0.elapsed_time(a1)
+            ms_local = a0.elapsed_time(a1)
+            ms_e, work = reduce_timing(ms_local, len(members) * args.ensemble_steps,
+                                       dist=dist if world > 1 else None, device="cuda")
             done = sum(1 for r in reps if r["status"] == 0)
             kavg = kms / max(kn, 1)
             gbs = ens.kernel_bytes / (kavg / 1e3) / 1e9
-            ens_out[store] = {"steps_per_s": len(members) * args.ensemble_steps / (ms_e / 1e3),
+            ens_out[store] = {"steps_per_s": work / (ms_e / 1e3),
                               "ms_per_round_avg": ms_e / max(kn // 6, 1), "networks_ok": done,
-                              "elements_total": int(sum(ens.n_elements)), "kv_bytes": ens.kernel_bytes,
+                              "elements_on_rank0": int(sum(ens.n_elements)), "kv_bytes_rank0": ens.kernel_bytes,
                               "kv_avg_ms": kavg, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
                               "rejected": int(sum(r["rejected"] for r in reps)),
                               "probe_halvings": int(sum(r["probe_halvings"] for r in reps)),
@@ -605,6 +614,10 @@ def main():
             cpu = {"value": steps_c / dt_c, "unit": "steps/s", "cores": threads, "kind": "port",
                    "sample": f"{steps_c} accepted steps of the same network from its initial state "
                              f"({dt_c:.1f} s), matrix-free directII as in the reference"}
+            # one core: the reference's own build is serial
+            s1, d1 = cpu_baseline(make_problem(0, args.n_faults), 1, args.cpu_budget / 2)
+            cpu["value_1core"] = s1 / d1
+            cpu["sample_1core"] = f"{s1} accepted steps on 1 thread ({d1:.1f} s)"
         line = {
             "metric": "RK45 accepted steps/s", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
