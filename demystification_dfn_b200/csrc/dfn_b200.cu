@@ -107,6 +107,7 @@ struct dfn_handle {
     double *Y = nullptr, *P = nullptr, *Pdot = nullptr, *yout = nullptr, *yscal = nullptr, *ytmp = nullptr;
     double *kbuf = nullptr, *SigT = nullptr, *SigN = nullptr, *partT = nullptr, *partN = nullptr;
     double *Ptemp = nullptr, *Pdot_s = nullptr, *pwork = nullptr, *vin = nullptr, *vout = nullptr, *snap = nullptr;
+    double *pcoef = nullptr;              // CG row coefficients [6][3N] per network
     int *err_flag = nullptr;
     void *K = nullptr;
     size_t K_bytes = 0;
@@ -283,7 +284,7 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
         dim3 grid((unsigned)nsys, (unsigned)ninst);
         pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
                                                                h->Ptemp, h->Pdot_s, h->pwork,
-                                                               h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0);
+                                                               h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0, h->pcoef);
     } else {
         const int64_t nshort = (ninst == h->B) ? h->nshort : h->nshort0;
         const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
@@ -736,7 +737,7 @@ int32_t dfn_destroy(dfn_handle *h)
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
                     h->yscal, h->ytmp, h->kbuf, h->SigT, h->SigN, h->partT, h->partN, h->Ptemp, h->Pdot_s,
-                    h->pwork, h->vin, h->vout, h->snap, h->err_flag, h->K, h->ctl};
+                    h->pwork, h->pcoef, h->vin, h->vout, h->snap, h->err_flag, h->K, h->ctl};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -934,6 +935,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     DALLOC(h->ytmp, 3 * Nt); DALLOC(h->kbuf, 18 * Nt); DALLOC(h->SigT, Nt); DALLOC(h->SigN, Nt);
     DALLOC(h->partT, poff); DALLOC(h->partN, poff);
     DALLOC(h->Ptemp, 6 * Nt); DALLOC(h->Pdot_s, 6 * Nt); DALLOC(h->pwork, 24 * Nt);
+    if (h->pressure != DFN_PRESSURE_TRIDIAG) DALLOC(h->pcoef, 18 * Nt);
     DALLOC(h->vin, 3 * h->hinst[0].N); DALLOC(h->vout, 3 * h->hinst[0].N); DALLOC(h->snap, 5 * Nt);
     DALLOC(h->err_flag, 1); DALLOC(h->ctl, count);
     DALLOC(h->src_fault, soff); DALLOC(h->src_elem, soff); DALLOC(h->src_Q, soff); DALLOC(h->src_tb, soff);

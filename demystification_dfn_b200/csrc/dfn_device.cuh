@@ -641,6 +641,29 @@ __device__ __forceinline__ double block_max(double v, double *red)
     return red[32];
 }
 
+// Sum of a and max of b over the CTA in one pass (red: 66 doubles).
+__device__ __forceinline__ void block_sum_max(double a, double b, double *red, double &sa, double &mb)
+{
+    a = warp_sum(a);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) { red[w] = a; red[33 + w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        double t = (lane < (blockDim.x >> 5)) ? red[lane] : 0.0;
+        double u = (lane < (blockDim.x >> 5)) ? red[33 + lane] : 0.0;
+        t = warp_sum(t);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) u = fmax(u, __shfl_xor_sync(0xffffffffu, u, o));
+        if (lane == 0) { red[32] = t; red[65] = u; }
+    }
+    __syncthreads();
+    sa = red[32];
+    mb = red[65];
+}
+
 // Segments of at most TRI_SHORT_MAX elements are solved by one warp each
 // (pressure_tridiag_kernel, up to TRI_WMAXM rows per lane), longer ones by a
 // CTA of TRI_NT threads (pressure_tridiag_long_kernel), rows in registers up
@@ -678,6 +701,17 @@ __device__ __forceinline__ double pmatvec_row(const PressParams &p, int64_t k, d
     double m;
     if (k == 0) m = add_(mul_(A2, v[0]), mul_(A3, v[1]));
     else if (k == p.N - 1) m = add_(mul_(A1, v[k - 1]), mul_(A2, v[k]));
+    else m = add_(add_(mul_(A1, v[k - 1]), mul_(A2, v[k])), mul_(A3, v[k + 1]));
+    return __ddiv_rn(m, A2);
+}
+
+// The same row with the coefficients of prow taken from a cache (identical
+// operands and order, so identical results).
+__device__ __forceinline__ double pmatvec_row_c(int64_t k, int64_t N, double A1, double A2, double A3, const double *v)
+{
+    double m;
+    if (k == 0) m = add_(mul_(A2, v[0]), mul_(A3, v[1]));
+    else if (k == N - 1) m = add_(mul_(A1, v[k - 1]), mul_(A2, v[k]));
     else m = add_(add_(mul_(A1, v[k - 1]), mul_(A2, v[k])), mul_(A3, v[k + 1]));
     return __ddiv_rn(m, A2);
 }
@@ -722,17 +756,24 @@ __device__ __forceinline__ double seq_dot(const double *a, const double *b, int6
 // its iteration counts bit for bit (needed where a solve sits at the
 // 200-iteration cap or at the tolerance, since that decides t_try halving);
 // exact = 0 sums them with a tree reduction. Returns ier.
+// With cf (3N doubles, or null): the row coefficients, which do not change
+// during a solve, are computed once into cf, and the residual's sum of
+// squares and max-norm share one reduction (red: 66 doubles); the iterates
+// are the same as without.
 __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, double *pv, double *Mp, double *red,
-                        long long *iters, int exact)
+                        long long *iters, int exact, double *cf = nullptr)
 {
     const int64_t N = p.N;
     const int tid = threadIdx.x, nt = blockDim.x;
+    double *c1 = cf, *c2 = cf ? cf + N : nullptr, *c3 = cf ? cf + 2 * N : nullptr;
     // x = P, r = b1 - M x, p = r
     double lmax = 0.0, lrr = 0.0;
     for (int64_t k = tid; k < N; k += nt) {
         double A1, A2, A3;
         prow(p, k, dt, A1, A2, A3);
-        const double rk = add_(pb1(p, k, dt, A2), -pmatvec_row(p, k, dt, p.P));
+        if (cf) { c1[k] = A1; c2[k] = A2; c3[k] = A3; }
+        const double rk = add_(pb1(p, k, dt, A2), -(cf ? pmatvec_row_c(k, N, A1, A2, A3, p.P)
+                                                        : pmatvec_row(p, k, dt, p.P)));
         x[k] = p.P[k];
         r[k] = rk;
         pv[k] = rk;
@@ -749,7 +790,7 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
         it++;
         double lpap = 0.0;
         for (int64_t k = tid; k < N; k += nt) {
-            const double m = pmatvec_row(p, k, dt, pv);
+            const double m = cf ? pmatvec_row_c(k, N, c1[k], c2[k], c3[k], pv) : pmatvec_row(p, k, dt, pv);
             Mp[k] = m;
             lpap += pv[k] * m;
         }
@@ -763,12 +804,21 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
             lr1 += r1 * r1;
             lm = fmax(lm, fabs(r1));
         }
-        const double r1r1 = exact ? seq_dot(r, r, N, red) : block_sum(lr1, red);
+        double r1r1, mx;
+        if (exact) {
+            r1r1 = seq_dot(r, r, N, red);
+            mx = block_max(lm, red);
+        } else if (cf) {
+            block_sum_max(lr1, lm, red, r1r1, mx);
+        } else {
+            r1r1 = block_sum(lr1, red);
+            mx = block_max(lm, red);
+        }
         const double beta = r1r1 / rr;
         for (int64_t k = tid; k < N; k += nt) pv[k] = add_(r[k], mul_(beta, pv[k]));
         rr = r1r1;
         if (it > 200) { *iters += it; return 1; }
-        errmax = block_max(lm, red) / p.tol;
+        errmax = mx / p.tol;
     }
     *iters += it;
     return 0;
@@ -778,18 +828,18 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
 // the batched solver and the allocation-free entry point.
 __device__ void cg_system(const PressParams &p, StepCtl *ctl, int kind, int sys, double dt_explicit, double *Pt,
                           double *Pd, double *x, double *r, double *pv, double *Mp, double *red, long long *iters,
-                          int exact)
+                          int exact, double *cf = nullptr)
 {
     const int64_t N = p.N;
     double dt = sys_dt(ctl, kind, sys, dt_explicit);
-    int ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact);
+    int ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact, cf);
     if (kind == 0) {
         // probe: src/solver.f90:81-92, halve t_try until the solve converges
         int guard = 0;
         while (ier == 1 && guard < 1100) {
             dt = dt / 2.0;
             guard++;
-            ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact);
+            ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact, cf);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -870,9 +920,10 @@ __device__ __forceinline__ PressParams press_params(const PressGlobal &g, const 
 // 4*N_i per system; outputs Ptemp/Pdot at 6*eoff + sys*N_i.
 __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
                                                                  int mask, int kind, int sys0, double dt_explicit,
-                                                                 double *Ptemp, double *Pdot, double *work, int exact)
+                                                                 double *Ptemp, double *Pdot, double *work, int exact,
+                                                                 double *coef)
 {
-    __shared__ double red[33];
+    __shared__ double red[66];
     __shared__ long long iters;
     const int i = blockIdx.y;
     if (!takes_part(ctl, i, mask)) return;
@@ -884,7 +935,8 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
     if (threadIdx.x == 0) iters = 0;
     __syncthreads();
     cg_system(p, ctl + i, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
-              Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact);
+              Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact,
+              coef + 18 * I.eoff + (int64_t)sys * 3 * N);
 }
 
 // Exact solve of the unscaled tridiagonal system A x = P + source, one
