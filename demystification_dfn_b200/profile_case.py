@@ -7,6 +7,9 @@
     python -m demystification_dfn_b200.profile_case tc_round [cg|tridiag]
         the same batch, six solve rounds launched one by one (launch list of
         a round: GEMM, pressure, friction, step control).
+    python -m demystification_dfn_b200.profile_case hmatrix_kv
+        the 4000-fault network (N = 81 750) as an H-matrix (leaf 64, eta 2,
+        ACA 1e-6, FP32 factors): three K.V launches (three kernels each).
     python -m demystification_dfn_b200.profile_case ensemble_round
         eight 120-fault networks (FP32 storage, tridiagonal pressure), forty
         solve rounds launched one by one.
@@ -41,6 +44,14 @@ def main(argv):
                      pressure=pressure)
         e.set_graphs(False)
         e.solve(n_steps=6, check=False)
+    elif case == "hmatrix_kv":
+        from .simulation import Simulation
+
+        p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
+        e = Simulation(p, storage="fp32", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
+        rng = np.random.default_rng(0)
+        for _ in range(3):
+            e.kernel(rng.normal(size=e.N))
     elif case == "ensemble_round":
         e = Ensemble([networks.ensemble_member(s, n_faults=120) for s in range(64, 72)], storage="fp32",
                      pressure="tridiag")
