@@ -127,11 +127,13 @@ struct dfn_handle {
     int ncomp = 1;                        // 2 in mode II (shear and normal), 1 in mode III
     HBlk *hblk = nullptr;
     HTask *ht1 = nullptr, *ht2 = nullptr;
-    int64_t hn1 = 0, hn2 = 0, hn1_0 = 0, hn2_0 = 0;
+    int64_t hn1 = 0, hn2 = 0, hn1_0 = 0, hn2_0 = 0;   // low-rank column tasks, low-rank row tasks
+    int64_t hn3 = 0, hn3_0 = 0;                        // dense row tasks
+    HTask *ht3 = nullptr;
     void *hvals = nullptr;
     int *hperm = nullptr;
     int64_t *hrowptr = nullptr, *hslots = nullptr;
-    double *hz = nullptr, *hout = nullptr;
+    double *hz = nullptr, *hout = nullptr, *hxp = nullptr;
     std::vector<int> hranks;              // rank of every low-rank leaf (report)
     int64_t hdense_vals = 0, hlr_vals = 0, hblocks = 0;
     // Newton formulation and the learned guess
@@ -188,26 +190,41 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
 {
     const int64_t n1 = only0 ? h->hn1_0 : h->hn1, n2 = only0 ? h->hn2_0 : h->hn2;
     const int64_t ne = only0 ? h->hinst[0].N : h->Ntot;
+    hm_permute_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->inst_of, h->inst, h->ctl, mask, h->hperm,
+                                                                 Vbase, vmul, h->hxp);
+    h->launches++;
+    CKL();
     if (n1 > 0) {
         if (h->store == 0)
             hm_lowrank_kernel<double><<<(unsigned)n1, 256, 0, h->stream>>>(
-                h->ht1, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hperm, Vbase, vmul, h->hz);
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hz);
         else
             hm_lowrank_kernel<float><<<(unsigned)n1, 256, 0, h->stream>>>(
-                h->ht1, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hperm, Vbase, vmul, h->hz);
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hz);
         h->launches++;
         CKL();
     }
-    if (h->store == 0)
-        hm_rows_kernel<double><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
-                                                                    (const double *)h->hvals, h->hperm, Vbase, vmul,
-                                                                    h->hz, h->hout);
-    else
-        hm_rows_kernel<float><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
-                                                                   (const float *)h->hvals, h->hperm, Vbase, vmul,
-                                                                   h->hz, h->hout);
-    h->launches++;
-    CKL();
+    const int64_t n3 = only0 ? h->hn3_0 : h->hn3;
+    if (n3 > 0) {
+        if (h->store == 0)
+            hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
+                                                                         (const double *)h->hvals, h->hxp, h->hout);
+        else
+            hm_dense_kernel<float><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
+                                                                        (const float *)h->hvals, h->hxp, h->hout);
+        h->launches++;
+        CKL();
+    }
+    if (n2 > 0) {
+        if (h->store == 0)
+            hm_rows_kernel<double><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                        (const double *)h->hvals, h->hz, h->hout);
+        else
+            hm_rows_kernel<float><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                       (const float *)h->hvals, h->hz, h->hout);
+        h->launches++;
+        CKL();
+    }
     hm_gather_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->ncomp, h->inst_of, h->inst, h->ctl, mask,
                                                                 h->hperm, h->hrowptr, h->hslots, h->hout, h->partT,
                                                                 h->partN);
@@ -552,9 +569,12 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     CK(cudaMemcpy(nr.data(), h->nrm, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(nd.data(), h->node, sizeof(double) * 2 * (Nt + B), cudaMemcpyDeviceToHost));
 
+    // values per 16-byte vector of the stored type; factor rows padded to it
+    const int VW = h->store == DFN_STORE_FP64 ? 2 : 4;
+    auto rup = [VW](int64_t n) { return (n + VW - 1) / VW * VW; };
     std::vector<int> perm(Nt);
     std::vector<HBlk> blks;
-    std::vector<HTask> t1, t2;
+    std::vector<HTask> t1, t2, t3;
     std::vector<double> vals;
     int64_t zoff = 0, slot = 0;
     // row contributions: per component, per global position, slot indices
@@ -616,14 +636,29 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 hb.inst = i; hb.comp = c; hb.dense = H.dense; hb.rank = H.rank;
                 hb.r0 = L.r0; hb.nr = L.nr; hb.c0 = L.c0; hb.nc = L.nc;
                 hb.outoff = slot;
+                vals.resize(rup((int64_t)vals.size()), 0.0);   // 16-byte aligned start
                 hb.foff = (int64_t)vals.size();
                 if (H.dense) {
-                    vals.insert(vals.end(), H.F.begin(), H.F.end());
+                    // F row-major, rows padded with zeros
+                    hb.ld = (int)rup(L.nc);
+                    vals.resize(vals.size() + (size_t)L.nr * hb.ld, 0.0);
+                    for (int ii = 0; ii < L.nr; ii++)
+                        for (int jj = 0; jj < L.nc; jj++)
+                            vals[hb.foff + (size_t)ii * hb.ld + jj] = H.F[(size_t)ii * L.nc + jj];
                     h->hdense_vals += (int64_t)H.F.size();
                 } else {
-                    vals.insert(vals.end(), H.A.begin(), H.A.end());
+                    // A^T (rank x nr) and B^T (rank x nc), rank-major, rows padded
+                    hb.lda = (int)rup(L.nr);
+                    hb.ld = (int)rup(L.nc);
+                    vals.resize(vals.size() + (size_t)H.rank * hb.lda, 0.0);
+                    for (int q = 0; q < H.rank; q++)
+                        for (int ii = 0; ii < L.nr; ii++)
+                            vals[hb.foff + (size_t)q * hb.lda + ii] = H.A[(size_t)ii * H.rank + q];
                     hb.goff = (int64_t)vals.size();
-                    vals.insert(vals.end(), H.B.begin(), H.B.end());
+                    vals.resize(vals.size() + (size_t)H.rank * hb.ld, 0.0);
+                    for (int q = 0; q < H.rank; q++)
+                        for (int jj = 0; jj < L.nc; jj++)
+                            vals[hb.goff + (size_t)q * hb.ld + jj] = H.B[(size_t)jj * H.rank + q];
                     hb.zoff = zoff;
                     hb.ntask1 = (L.nc + HM_COLS - 1) / HM_COLS;
                     zoff += (int64_t)hb.ntask1 * H.rank;
@@ -635,7 +670,10 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 if (!H.dense)
                     for (int j = 0; j < hb.ntask1; j++)
                         t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
-                for (int r = 0; r < L.nr; r += HM_ROWS) t2.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
+                if (H.dense)
+                    for (int r = 0; r < L.nr; r += HM_ROWS) t3.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
+                else
+                    for (int r = 0; r < L.nr; r += HM_LROWS) t2.push_back(HTask{bi, r, std::min(HM_LROWS, L.nr - r), 0});
                 for (int r = 0; r < L.nr; r++) rows[(size_t)c * Nt + e0 + L.r0 + r].push_back(slot + r);
                 slot += L.nr;
             }
@@ -643,6 +681,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
         if (i == 0) {
             h->hn1_0 = (int64_t)t1.size();
             h->hn2_0 = (int64_t)t2.size();
+            h->hn3_0 = (int64_t)t3.size();
         }
     }
     // tasks must list network 0 first for the operator entry points; they
@@ -654,9 +693,10 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     }
     h->hn1 = (int64_t)t1.size();
     h->hn2 = (int64_t)t2.size();
+    h->hn3 = (int64_t)t3.size();
     h->hblocks = (int64_t)blks.size();
     const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
-    h->kv_bytes = (int64_t)(vals.size() * vsz);
+    h->kv_bytes = (h->hdense_vals + h->hlr_vals) * (int64_t)vsz;   // stored entries, padding excluded
     CK(cudaMalloc(&h->hvals, std::max<size_t>(vals.size(), 1) * vsz));
     if (h->store == DFN_STORE_FP64) {
         CK(cudaMemcpy(h->hvals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice));
@@ -669,7 +709,9 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     CK(cudaMalloc((void **)&h->ht1, std::max<size_t>(t1.size(), 1) * sizeof(HTask)));
     if (!t1.empty()) CK(cudaMemcpy(h->ht1, t1.data(), t1.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->ht2, std::max<size_t>(t2.size(), 1) * sizeof(HTask)));
-    CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    if (!t2.empty()) CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->ht3, std::max<size_t>(t3.size(), 1) * sizeof(HTask)));
+    if (!t3.empty()) CK(cudaMemcpy(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
     CK(cudaMemcpy(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hrowptr, sizeof(int64_t) * rowptr.size()));
@@ -677,6 +719,8 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
     CK(cudaMemcpy(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hz, sizeof(double) * std::max<int64_t>(zoff, 1)));
+    CK(cudaMalloc((void **)&h->hxp, sizeof(double) * (Nt + HM_XPAD)));
+    CK(cudaMemset(h->hxp, 0, sizeof(double) * (Nt + HM_XPAD)));
     CK(cudaMalloc((void **)&h->hout, sizeof(double) * std::max<int64_t>(slot, 1)));
     return DFN_OK;
 }
@@ -732,7 +776,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,

@@ -4,17 +4,20 @@
 //
 // The reference recurses over the block tree and calls ZGEMV on each leaf
 // with complex(8) storage (16 bytes per real entry). Here the leaves are a
-// flat list and every K.V is three launches over task lists:
-//   1. z_b = B_b^T x for every low-rank block b, split in column chunks
+// flat list and every K.V is five launches over task lists:
+//   0. xp = x in cluster order (one gather, so that the leaf kernels read
+//      their columns contiguously);
+//   1. z_b = B_b^T xp for every low-rank block b, split in column chunks
 //      (partial sums per chunk, added in fixed order in step 2);
-//   2. the rows of every leaf: F_b x (dense leaves) or A_b z_b (low-rank),
-//      one output slot per (leaf, row);
+//   2. the rows of every leaf: F_b xp (dense leaves) and A_b z_b (low-rank
+//      leaves), two launches, one output slot per (leaf, row);
 //   3. y(row) = sum of the row's slots in a fixed order, written in the
 //      original element order (y[perm[pos]]).
-// x is the slip-rate vector read through the cluster permutation. Factors are
-// stored row-major (F: nr x nc, A: nr x rank, B: nc x rank) in FP64 or FP32;
-// sums are FP64. Every launch is predicated on the network's phase like the
-// dense K.V, and covers all networks of a batch.
+// Factors are stored in FP64 or FP32 with rows padded to whole 16-byte
+// vectors and 16-byte aligned: dense F row-major (nr x ldf), low-rank A and
+// B transposed, rank-major (r x lda, r x ldb), so that every factor streams
+// as coalesced 16-byte loads. Sums are FP64. Every launch is predicated on
+// the network's phase like the dense K.V, and covers all networks of a batch.
 #pragma once
 #include "dfn_device.cuh"
 #include "hmat_build.h"
@@ -22,96 +25,158 @@
 struct HBlk {
     int inst, comp, dense, rank;
     int r0, nr, c0, nc;        // positions in cluster order (within the network)
-    int64_t foff;              // dense: F offset; low-rank: A offset (values)
-    int64_t goff;              // low-rank: B offset (values)
+    int64_t foff;              // dense: F offset; low-rank: A^T offset (values)
+    int64_t goff;              // low-rank: B^T offset (values)
     int64_t zoff;              // low-rank: first z partial (ntask1 x rank doubles)
     int64_t outoff;            // first output slot of the leaf's rows
     int ntask1;                // column chunks of the low-rank product
+    int ld;                    // padded row length: dense F, or low-rank B^T
+    int lda;                   // low-rank A^T padded row length
     int pad;
 };
 
 struct HTask { int blk, start, count, chunk; };
 
 constexpr int HM_COLS = 1024;  // columns per step-1 task
-constexpr int HM_ROWS = 64;    // rows per step-2 task
+constexpr int HM_ROWS = 64;    // rows per step-2 task of a dense leaf
+constexpr int HM_LROWS = 256;  // rows per step-2 task of a low-rank leaf
+constexpr int HM_XPAD = 8;     // zero doubles after xp (padded columns read them)
 
+template <typename T> struct HVec;
+template <> struct HVec<float> {
+    using V = float4;
+    static constexpr int W = 4;
+    __device__ static void unpack(const float4 &v, double *o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+};
+template <> struct HVec<double> {
+    using V = double2;
+    static constexpr int W = 2;
+    __device__ static void unpack(const double2 &v, double *o) { o[0] = v.x; o[1] = v.y; }
+};
+
+// xp[eoff + pos] = x of network i at its element perm[pos]
+__global__ void hm_permute_kernel(int64_t Ntot, const int *__restrict__ inst_of, const Inst *__restrict__ inst,
+                                  const StepCtl *__restrict__ ctl, int mask, const int *__restrict__ perm,
+                                  const double *__restrict__ Vbase, int vmul, double *__restrict__ xp)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= Ntot) return;
+    const int i = inst_of[e];
+    if (!takes_part(ctl, i, mask)) return;
+    const Inst &I = inst[i];
+    xp[e] = Vbase[(int64_t)vmul * I.eoff + perm[e]];
+}
+
+// z partial of one column chunk: warp w takes rank rows q = w, w+8, ...;
+// lanes stream the row's columns in 16-byte vectors.
 template <typename T>
 __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
                                                          const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                          int mask, const T *__restrict__ vals,
-                                                         const int *__restrict__ perm, const double *__restrict__ Vbase,
-                                                         int vmul, double *__restrict__ zpart)
+                                                         const double *__restrict__ xp, double *__restrict__ zpart)
 {
-    __shared__ double red[8][hmat::kMaxRank];
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
     const HTask t = tasks[blockIdx.x];
     const HBlk b = blks[t.blk];
     if (!takes_part(ctl, b.inst, mask)) return;
     const Inst &I = inst[b.inst];
-    const double *V = Vbase + (int64_t)vmul * I.eoff;
-    const int *pm = perm + I.eoff;
-    // warp w takes columns start+w, start+w+8, ...; lane q accumulates rank
-    // components q and q+32 (the r values of a column are contiguous)
-    static_assert(hmat::kMaxRank <= 64, "two rank components per lane");
-    const int r = b.rank;
+    const double *x = xp + I.eoff + b.c0 + t.start;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double acc0 = 0.0, acc1 = 0.0;
-    for (int l = t.start + w; l < t.start + t.count; l += 8) {
-        const double x = V[pm[b.c0 + l]];
-        const T *row = vals + b.goff + (int64_t)l * r;
-        if (lane < r) acc0 = fma((double)row[lane], x, acc0);
-        if (lane + 32 < r) acc1 = fma((double)row[lane + 32], x, acc1);
-    }
-    red[w][lane] = acc0;
-    red[w][lane + 32] = acc1;
-    __syncthreads();
-    if (threadIdx.x < r) {
+    const int nv = (t.count + W - 1) / W;    // vectors of the chunk (padding columns are zero)
+    for (int q = w; q < b.rank; q += 8) {
+        const VT *row = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld + t.start);
         double s = 0.0;
-        for (int ww = 0; ww < 8; ww++) s += red[ww][threadIdx.x];
-        zpart[b.zoff + (int64_t)t.chunk * r + threadIdx.x] = s;
+        for (int v = lane; v < nv; v += 32) {
+            double f[W];
+            HVec<T>::unpack(row[v], f);
+#pragma unroll
+            for (int j = 0; j < W; j++) s = fma(f[j], x[v * W + j], s);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) zpart[b.zoff + (int64_t)t.chunk * b.rank + q] = s;
     }
 }
 
+// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
+// xp; four rows per half-warp in flight (their loads issued together).
+template <typename T>
+__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
+                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
+                                                       int mask, const T *__restrict__ vals,
+                                                       const double *__restrict__ xp, double *__restrict__ out)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    constexpr int U = 4;
+    const HTask t = tasks[blockIdx.x];
+    const HBlk b = blks[t.blk];
+    if (!takes_part(ctl, b.inst, mask)) return;
+    const Inst &I = inst[b.inst];
+    const double *x = xp + I.eoff + b.c0;
+    const int hl = threadIdx.x & 15, w = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
+    const int nv = (b.nc + W - 1) / W;
+    const VT zero{};
+    // the loop runs the same trips in both half-warps (shuffles below)
+    for (int wb = w * 2 * U; wb < t.count; wb += 8 * 2 * U) {
+        const int i0 = wb + half * U;
+        double s[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) s[u] = 0.0;
+        for (int v = hl; v < nv; v += 16) {
+            double xv[W];
+#pragma unroll
+            for (int j = 0; j < W; j++) xv[j] = x[v * W + j];
+            VT fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int row = t.start + i0 + u;
+                fv[u] = (i0 + u < t.count) ? reinterpret_cast<const VT *>(vals + b.foff + (int64_t)row * b.ld)[v]
+                                           : zero;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                double a[W];
+                HVec<T>::unpack(fv[u], a);
+#pragma unroll
+                for (int j = 0; j < W; j++) s[u] = fma(a[j], xv[j], s[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+            if (hl == 0 && i0 + u < t.count) out[b.outoff + t.start + i0 + u] = s[u];
+        }
+    }
+}
+
+// Rows of low-rank leaves: one thread per row, sum over the rank of
+// A^T[q][row] z[q] (coalesced across the threads for each q).
 template <typename T>
 __global__ void __launch_bounds__(256) hm_rows_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                       int mask, const T *__restrict__ vals,
-                                                      const int *__restrict__ perm, const double *__restrict__ Vbase,
-                                                      int vmul, const double *__restrict__ zpart,
-                                                      double *__restrict__ out)
+                                                      const double *__restrict__ zpart, double *__restrict__ out)
 {
     __shared__ double z[hmat::kMaxRank];
     const HTask t = tasks[blockIdx.x];
     const HBlk b = blks[t.blk];
     if (!takes_part(ctl, b.inst, mask)) return;
-    const Inst &I = inst[b.inst];
-    if (b.dense) {
-        const double *V = Vbase + (int64_t)vmul * I.eoff;
-        const int *pm = perm + I.eoff;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        for (int i = w; i < t.count; i += 8) {
-            const int row = t.start + i;
-            const T *f = vals + b.foff + (int64_t)row * b.nc;
-            double s = 0.0;
-            for (int l = lane; l < b.nc; l += 32) s = fma((double)f[l], V[pm[b.c0 + l]], s);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) out[b.outoff + row] = s;
-        }
-    } else {
-        const int r = b.rank;
-        if (threadIdx.x < r) {
-            double s = 0.0;
-            for (int j = 0; j < b.ntask1; j++) s += zpart[b.zoff + (int64_t)j * r + threadIdx.x];
-            z[threadIdx.x] = s;
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < t.count; i += blockDim.x) {
-            const int row = t.start + i;
-            const T *a = vals + b.foff + (int64_t)row * r;
-            double s = 0.0;
-            for (int q = 0; q < r; q++) s = fma((double)a[q], z[q], s);
-            out[b.outoff + row] = s;
-        }
+    const int r = b.rank;
+    if (threadIdx.x < r) {
+        double s = 0.0;
+        for (int j = 0; j < b.ntask1; j++) s += zpart[b.zoff + (int64_t)j * r + threadIdx.x];
+        z[threadIdx.x] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < t.count; i += blockDim.x) {
+        const int row = t.start + i;
+        const T *a = vals + b.foff + row;
+        double s = 0.0;
+        for (int q = 0; q < r; q++) s = fma((double)a[(int64_t)q * b.lda], z[q], s);
+        out[b.outoff + row] = s;
     }
 }
 
