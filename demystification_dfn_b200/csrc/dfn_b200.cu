@@ -130,6 +130,8 @@ struct dfn_handle {
     int64_t hn1 = 0, hn2 = 0, hn1_0 = 0, hn2_0 = 0;   // low-rank column tasks, low-rank row tasks
     int64_t hn3 = 0, hn3_0 = 0;                        // dense row tasks
     HTask *ht3 = nullptr;
+    int64_t hn4 = 0, hn4_0 = 0;                        // low-rank leaves done whole
+    int *hl4 = nullptr;
     void *hvals = nullptr;
     int *hperm = nullptr;
     int64_t *hrowptr = nullptr, *hslots = nullptr;
@@ -205,6 +207,17 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         CKL();
     }
     const int64_t n3 = only0 ? h->hn3_0 : h->hn3;
+    const int64_t n4 = only0 ? h->hn4_0 : h->hn4;
+    if (n4 > 0) {
+        if (h->store == 0)
+            hm_lowrank_fused_kernel<double><<<(unsigned)n4, 256, 0, h->stream>>>(
+                h->hl4, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+        else
+            hm_lowrank_fused_kernel<float><<<(unsigned)n4, 256, 0, h->stream>>>(
+                h->hl4, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        h->launches++;
+        CKL();
+    }
     if (n3 > 0) {
         if (h->store == 0)
             hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
@@ -575,6 +588,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     std::vector<int> perm(Nt);
     std::vector<HBlk> blks;
     std::vector<HTask> t1, t2, t3;
+    std::vector<int> l4;
     std::vector<double> vals;
     int64_t zoff = 0, slot = 0;
     // row contributions: per component, per global position, slot indices
@@ -667,13 +681,15 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 }
                 const int bi = (int)blks.size();
                 blks.push_back(hb);
-                if (!H.dense)
+                if (H.dense) {
+                    for (int r = 0; r < L.nr; r += HM_ROWS) t3.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
+                } else if (L.nc <= HM_COLS) {
+                    l4.push_back(bi);   // whole leaf in one CTA
+                } else {
                     for (int j = 0; j < hb.ntask1; j++)
                         t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
-                if (H.dense)
-                    for (int r = 0; r < L.nr; r += HM_ROWS) t3.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
-                else
                     for (int r = 0; r < L.nr; r += HM_LROWS) t2.push_back(HTask{bi, r, std::min(HM_LROWS, L.nr - r), 0});
+                }
                 for (int r = 0; r < L.nr; r++) rows[(size_t)c * Nt + e0 + L.r0 + r].push_back(slot + r);
                 slot += L.nr;
             }
@@ -682,6 +698,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
             h->hn1_0 = (int64_t)t1.size();
             h->hn2_0 = (int64_t)t2.size();
             h->hn3_0 = (int64_t)t3.size();
+            h->hn4_0 = (int64_t)l4.size();
         }
     }
     // tasks must list network 0 first for the operator entry points; they
@@ -694,6 +711,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     h->hn1 = (int64_t)t1.size();
     h->hn2 = (int64_t)t2.size();
     h->hn3 = (int64_t)t3.size();
+    h->hn4 = (int64_t)l4.size();
     h->hblocks = (int64_t)blks.size();
     const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
     h->kv_bytes = (h->hdense_vals + h->hlr_vals) * (int64_t)vsz;   // stored entries, padding excluded
@@ -710,6 +728,8 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     if (!t1.empty()) CK(cudaMemcpy(h->ht1, t1.data(), t1.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->ht2, std::max<size_t>(t2.size(), 1) * sizeof(HTask)));
     if (!t2.empty()) CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hl4, std::max<size_t>(l4.size(), 1) * sizeof(int)));
+    if (!l4.empty()) CK(cudaMemcpy(h->hl4, l4.data(), l4.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->ht3, std::max<size_t>(t3.size(), 1) * sizeof(HTask)));
     if (!t3.empty()) CK(cudaMemcpy(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
@@ -776,7 +796,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,

@@ -152,6 +152,48 @@ __global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__
     }
 }
 
+// Low-rank leaves of at most HM_COLS columns, whole: z = B^T xp into shared
+// memory (warp per rank row), then the rows y = A z (thread per row); one
+// CTA per leaf, no partial sums in global memory.
+template <typename T>
+__global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__restrict__ leaves,
+                                                               const HBlk *__restrict__ blks,
+                                                               const Inst *__restrict__ inst,
+                                                               const StepCtl *__restrict__ ctl, int mask,
+                                                               const T *__restrict__ vals,
+                                                               const double *__restrict__ xp, double *__restrict__ out)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    __shared__ double z[hmat::kMaxRank];
+    const HBlk b = blks[leaves[blockIdx.x]];
+    if (!takes_part(ctl, b.inst, mask)) return;
+    const Inst &I = inst[b.inst];
+    const double *x = xp + I.eoff + b.c0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nv = (b.nc + W - 1) / W;
+    for (int q = w; q < b.rank; q += 8) {
+        const VT *row = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld);
+        double s = 0.0;
+        for (int v = lane; v < nv; v += 32) {
+            double f[W];
+            HVec<T>::unpack(row[v], f);
+#pragma unroll
+            for (int j = 0; j < W; j++) s = fma(f[j], x[v * W + j], s);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) z[q] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < b.nr; i += blockDim.x) {
+        const T *a = vals + b.foff + i;
+        double s = 0.0;
+        for (int q = 0; q < b.rank; q++) s = fma((double)a[(int64_t)q * b.lda], z[q], s);
+        out[b.outoff + i] = s;
+    }
+}
+
 // Rows of low-rank leaves: one thread per row, sum over the rank of
 // A^T[q][row] z[q] (coalesced across the threads for each q).
 template <typename T>
