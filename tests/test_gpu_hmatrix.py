@@ -90,3 +90,40 @@ def test_hmat_batch_equals_single():
             with Simulation(p, **kw) as s:
                 s.solve_steps(8)
                 assert np.array_equal(ens.state(i)["Y"], s.state()["Y"])
+
+
+def test_loaded_network_event_onset_hmatrix():
+    """Config-3 physics at test size: a velocity-weakening network under
+    tectonic shear loading (0.05 Pa/s) reaches seismic slip (max V > 1e-3
+    m/s) after ~1.2 simulated years and ~500 adaptive steps. The GPU
+    H-matrix (partial-pivot ACA + recompression, FP64 factors) and the
+    oracle's restatement of the reference's H-matrix (full-pivot ACA) agree
+    to the ACA tolerance, not bit for bit, so the onset times agree to 1e-3;
+    FP32 factors follow FP64 factors to 1e-4."""
+    p = networks.fault_network(n_faults=6, box=3000.0, length_range=(300.0, 1200.0), seed=3, dP=0.0,
+                               kernel="hmatrix", tol=1e-6)
+    for f in p.faults:
+        f.shear_loading_dot[:] = 0.05
+    o = Oracle(p, threads=4)
+    assert o.use_hmatrix(leaf=32, eta=2.0, eps=1e-6)
+
+    def onset(step, state):
+        for k in range(1, 3000):
+            step()
+            s = state()
+            N = len(s["P"])
+            if np.abs(s["Y"][:N]).max() > 1e-3:
+                return k, s["time"]
+        return None, None
+
+    ko, to = onset(lambda: o.solve_steps(1), o.state)
+    assert ko is not None
+    res = {}
+    for store in ("fp64", "fp32"):
+        with Simulation(p, storage=store, pressure="cg", hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6) as s:
+            res[store] = onset(lambda: s.solve_steps(1), s.state)
+    kg, tg = res["fp64"]
+    kf, tf = res["fp32"]
+    assert kg is not None and kf is not None
+    assert abs(tg - to) <= 1e-3 * to
+    assert abs(tf - tg) <= 1e-4 * tg
