@@ -115,6 +115,7 @@ struct dfn_handle {
     // shared-geometry batch on tensor cores (DFN_STORE_BF16X2_TC)
     bool tc = false;
     int tc_bn = 0, tc_nmt = 0, tc_split = 1, tc_kps = 0, tc_nkb = 0;
+    bool tc_shallow = false;              // 2-stage ring instead of the deepest (autotuner)
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -252,8 +253,13 @@ template <int BN>
 static void tc_launch_bn(dfn_handle *h, const TcOut &o)
 {
     const int64_t na = h->tc_mpad * h->tc_kpad, nb = (int64_t)h->tc_bn * h->tc_kpad;
-    tc_gemm_kernel<BN><<<(unsigned)(h->tc_nmt * h->tc_split), TC_THREADS, tc_smem_bytes(BN), h->stream>>>(
-        h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o, h->err_flag);
+    const unsigned grid = (unsigned)(h->tc_nmt * h->tc_split);
+    if (h->tc_shallow && tc_stages(BN) > 2)
+        tc_gemm_kernel<BN, 2><<<grid, TC_THREADS, tc_smem_bytes(BN, 2), h->stream>>>(
+            h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o, h->err_flag);
+    else
+        tc_gemm_kernel<BN, tc_stages(BN)><<<grid, TC_THREADS, tc_smem_bytes(BN, tc_stages(BN)), h->stream>>>(
+            h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o, h->err_flag);
 }
 
 static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
@@ -1141,11 +1147,11 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         h->launches++;
         CKC(cudaGetLastError());
         h->kv_bytes = 4 * h->tc_mrows * I.N;   // hi + lo, 2 bytes each, per stored entry
-        CKC(cudaFuncSetAttribute(tc_gemm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(16)));
-        CKC(cudaFuncSetAttribute(tc_gemm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(32)));
-        CKC(cudaFuncSetAttribute(tc_gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(64)));
-        CKC(cudaFuncSetAttribute(tc_gemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(128)));
-        CKC(cudaFuncSetAttribute(tc_gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(256)));
+#define TC_SMEM_ATTR(BN, ST) \
+    CKC(cudaFuncSetAttribute(tc_gemm_kernel<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(BN, ST)))
+        TC_SMEM_ATTR(16, 4); TC_SMEM_ATTR(32, 4); TC_SMEM_ATTR(64, 4); TC_SMEM_ATTR(128, 3); TC_SMEM_ATTR(256, 2);
+        TC_SMEM_ATTR(16, 2); TC_SMEM_ATTR(32, 2); TC_SMEM_ATTR(64, 2); TC_SMEM_ATTR(128, 2);
+#undef TC_SMEM_ATTR
     }
     // dense kernel matrices, one per network
     h->K_bytes = (size_t)std::max<int64_t>(kvec, 1) * 16;
@@ -1247,6 +1253,17 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         h->gemv_impl = (r.ms[1] < r.ms[0]) ? 1 : 0;
         r.gemv_impl = h->gemv_impl;
         (void)keep;
+    }
+    if (h->tc && tc_stages(h->tc_bn) > 2) {
+        double ms2[2];
+        for (int v = 0; v < 2; v++) {
+            h->tc_shallow = v == 1;
+            TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, ms2[v]));
+        }
+        h->tc_shallow = ms2[1] < ms2[0];
+        r.ms[0] = ms2[0];
+        r.ms[1] = ms2[1];
+        r.gemv_impl = h->tc_shallow ? 1 : 0;
     }
     r.tri_thread = h->tri_thread ? 1 : 0;
     if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {

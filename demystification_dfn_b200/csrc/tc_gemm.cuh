@@ -44,9 +44,11 @@
 #define TC_THREADS 128
 
 __host__ __device__ constexpr size_t tc_stage_bytes(int bn) { return (size_t)2 * TC_BM * TC_BK * 2 + (size_t)2 * bn * TC_BK * 2; }
-// ring depth that keeps the stages within 192 KiB of shared memory
+// deepest ring that keeps the stages within 192 KiB of shared memory (one
+// CTA per SM); the autotuner may pick a 2-stage ring instead (two CTAs per
+// SM for BN <= 64, one's fill and epilogue overlapping the other's stream)
 __host__ __device__ constexpr int tc_stages(int bn) { return bn <= 64 ? 4 : (bn <= 128 ? 3 : 2); }
-__host__ __device__ constexpr size_t tc_smem_bytes(int bn) { return tc_stages(bn) * tc_stage_bytes(bn) + 1024 + 256; }
+__host__ __device__ constexpr size_t tc_smem_bytes(int bn, int stages) { return stages * tc_stage_bytes(bn) + 1024 + 256; }
 
 // Element offset of (row r, column j < 64) inside a swizzled tile of 128-byte rows.
 __host__ __device__ inline int64_t tc_swz(int64_t r, int64_t j)
@@ -97,14 +99,14 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar)
                  : "memory");
 }
 
-template <int BN>
+template <int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm_kernel(const __nv_bfloat16 *__restrict__ Ah, const __nv_bfloat16 *__restrict__ Al,
                    const __nv_bfloat16 *__restrict__ Bh, const __nv_bfloat16 *__restrict__ Bl, TcOut out,
                    int *err_flag)
 {
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "N of an M=128 MMA is a multiple of 16 up to 256");
-    constexpr int STAGES = tc_stages(BN);
+    static_assert(STAGES >= 2 && STAGES * tc_stage_bytes(BN) <= 196608, "ring within 192 KiB");
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     // 1024-byte alignment of the stage ring (128-byte swizzle atoms)
     unsigned char *ring = reinterpret_cast<unsigned char *>(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);

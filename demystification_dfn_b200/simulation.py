@@ -63,6 +63,7 @@ class Simulation:
         opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
                            formulation, guess, newton_maxit, newton_tol)
         self.formulation = formulation
+        self._storage = storage
         self.options = {"storage": storage, "pressure": pressure, "gemv": gemv}
         self._c = to_c(self.arrays)
         h = ctypes.c_void_p()
@@ -98,8 +99,13 @@ class Simulation:
                         ("ms", ctypes.c_double * 4)]
         t = _T()
         _lib.check(self.lib.dfn_autotune(self.h, ctypes.byref(t)), self.lib)
-        return {"gemv_impl": ["tma", "ldg"][t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
-                "ms": {"kv_tma": t.ms[0], "kv_ldg": t.ms[1], "pressure_warp": t.ms[2], "pressure_thread": t.ms[3]}}
+        if self._storage == "bf16x2_tc":
+            names = ("tc_ring_deep", "tc_ring_2stage")
+        else:
+            names = ("tma", "ldg")
+        return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
+                "ms": {"kv_" + names[0]: t.ms[0], "kv_" + names[1]: t.ms[1], "pressure_warp": t.ms[2],
+                       "pressure_thread": t.ms[3]}}
 
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch

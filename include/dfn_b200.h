@@ -191,9 +191,13 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * segments (<= 64 elements) solved by one thread each (sequential Thomas) or
  * one warp each (scans), equal to rounding. ms[] = milliseconds per launch of
  * K.V TMA, K.V LDG, pressure by warps, pressure by threads (0 = not timed).
- * Without a call, K.V uses options.gemv_impl and the short segments use
- * threads once a launch has at least 16384 of them. No counterpart in the
- * reference. */
+ * For DFN_STORE_BF16X2_TC handles the two K.V choices are instead the
+ * tensor-core GEMM with its deepest shared-memory ring (one CTA per SM,
+ * gemv_impl 0) or a 2-stage ring (two CTAs per SM, gemv_impl 1), timed in
+ * ms[0] and ms[1]; both give identical results.
+ * Without a call, K.V uses options.gemv_impl (the deepest ring for
+ * tensor-core handles) and the short segments use threads once a launch has
+ * at least 16384 of them. No counterpart in the reference. */
 typedef struct dfn_tuning {
     int32_t gemv_impl;
     int32_t tri_thread;

@@ -79,3 +79,20 @@ def test_tensor_core_storage_needs_shared_geometry():
     ps = [networks.small_network(seed=s, n_faults=3) for s in (1, 2)]
     with pytest.raises(_lib.DfnError):
         Ensemble(ps, storage="bf16x2_tc")
+
+
+def test_tensor_core_autotune_keeps_results():
+    """Both shared-memory rings of the GEMM give the same sums in the same
+    order: K.V after the autotuner's choice equals K.V before, bit for bit."""
+    ps = _members(40)
+    rng = np.random.default_rng(4)
+    with Ensemble(ps, storage="bf16x2_tc") as e:
+        N = e.n_elements[0]
+        slips = [rng.normal(size=N) for _ in ps]
+        a, _ = e.kernel(slips)
+        t = e.autotune()
+        assert t["gemv_impl"] in ("tc_ring_deep", "tc_ring_2stage")
+        assert t["ms"]["kv_tc_ring_deep"] > 0 and t["ms"]["kv_tc_ring_2stage"] > 0
+        b, _ = e.kernel(slips)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
