@@ -572,7 +572,7 @@ static void fill_report(const StepCtl &c, dfn_report *r)
 // as the dense assembly (entry_mode2/entry_mode3).
 struct HostLeaf {
     int dense, rank;
-    std::vector<double> F, A, B;   // row-major F (nr x nc), A (nr x rank), B (nc x rank)
+    std::vector<double> A, B;   // low-rank factors, A (nr x rank), B (nc x rank)
 };
 
 static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_options &opt)
@@ -595,6 +595,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     std::vector<HBlk> blks;
     std::vector<HTask> t1, t2, t3;
     std::vector<int> l4;
+    int64_t dense_off = 0;   // values of the dense region (first in the device array)
     std::vector<double> vals;
     int64_t zoff = 0, slot = 0;
     // row contributions: per component, per global position, slot indices
@@ -631,12 +632,9 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                     if (rank >= 0) rank = hmat::recompress(L.nr, L.nc, rank, eps, A, Bm);
                     if (rank > hmat::kMaxRank) rank = -1;
                 }
-                if (rank < 0) {   // dense leaf, or low-rank leaf whose ACA did not converge
-                    H.dense = 1;
+                if (rank < 0) {   // dense leaf, or low-rank leaf whose ACA did not converge:
+                    H.dense = 1;  // entries evaluated on the device after upload
                     H.rank = 0;
-                    H.F.resize((size_t)L.nr * L.nc);
-                    for (int ii = 0; ii < L.nr; ii++)
-                        for (int jj = 0; jj < L.nc; jj++) H.F[(size_t)ii * L.nc + jj] = ent(ii, jj);
                 } else {
                     H.dense = 0;
                     H.rank = rank;
@@ -656,17 +654,16 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 hb.inst = i; hb.comp = c; hb.dense = H.dense; hb.rank = H.rank;
                 hb.r0 = L.r0; hb.nr = L.nr; hb.c0 = L.c0; hb.nc = L.nc;
                 hb.outoff = slot;
-                vals.resize(rup((int64_t)vals.size()), 0.0);   // 16-byte aligned start
-                hb.foff = (int64_t)vals.size();
                 if (H.dense) {
-                    // F row-major, rows padded with zeros
+                    // F row-major, rows padded with zeros, in the dense region
+                    // (filled on the device)
                     hb.ld = (int)rup(L.nc);
-                    vals.resize(vals.size() + (size_t)L.nr * hb.ld, 0.0);
-                    for (int ii = 0; ii < L.nr; ii++)
-                        for (int jj = 0; jj < L.nc; jj++)
-                            vals[hb.foff + (size_t)ii * hb.ld + jj] = H.F[(size_t)ii * L.nc + jj];
-                    h->hdense_vals += (int64_t)H.F.size();
+                    hb.foff = dense_off;
+                    dense_off += rup((int64_t)L.nr * hb.ld);
+                    h->hdense_vals += (int64_t)L.nr * L.nc;
                 } else {
+                    vals.resize(rup((int64_t)vals.size()), 0.0);   // 16-byte aligned start
+                    hb.foff = (int64_t)vals.size();
                     // A^T (rank x nr) and B^T (rank x nc), rank-major, rows padded
                     hb.lda = (int)rup(L.nr);
                     hb.ld = (int)rup(L.nc);
@@ -721,12 +718,18 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     h->hblocks = (int64_t)blks.size();
     const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
     h->kv_bytes = (h->hdense_vals + h->hlr_vals) * (int64_t)vsz;   // stored entries, padding excluded
-    CK(cudaMalloc(&h->hvals, std::max<size_t>(vals.size(), 1) * vsz));
+    // device values: [dense leaves | low-rank factors]
+    for (HBlk &hb : blks)
+        if (!hb.dense) { hb.foff += dense_off; hb.goff += dense_off; }
+    const size_t ntot = (size_t)dense_off + vals.size();
+    CK(cudaMalloc(&h->hvals, std::max<size_t>(ntot, 1) * vsz));
+    CK(cudaMemsetAsync(h->hvals, 0, (size_t)dense_off * vsz, h->stream));   // padding of the dense rows
     if (h->store == DFN_STORE_FP64) {
-        CK(cudaMemcpy(h->hvals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(static_cast<double *>(h->hvals) + dense_off, vals.data(), vals.size() * 8,
+                      cudaMemcpyHostToDevice));
     } else {
         std::vector<float> f(vals.begin(), vals.end());
-        CK(cudaMemcpy(h->hvals, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(static_cast<float *>(h->hvals) + dense_off, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc((void **)&h->hblk, std::max<size_t>(blks.size(), 1) * sizeof(HBlk)));
     CK(cudaMemcpy(h->hblk, blks.data(), blks.size() * sizeof(HBlk), cudaMemcpyHostToDevice));
@@ -744,6 +747,19 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     CK(cudaMemcpy(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
     CK(cudaMemcpy(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice));
+    if (!t3.empty()) {
+        if (h->store == DFN_STORE_FP64)
+            hm_fill_dense_kernel<double><<<(unsigned)t3.size(), 256, 0, h->stream>>>(
+                h->ht3, h->hblk, h->inst, h->mode, h->hperm, h->node, h->elem, h->tan, h->nrm,
+                static_cast<double *>(h->hvals));
+        else
+            hm_fill_dense_kernel<float><<<(unsigned)t3.size(), 256, 0, h->stream>>>(
+                h->ht3, h->hblk, h->inst, h->mode, h->hperm, h->node, h->elem, h->tan, h->nrm,
+                static_cast<float *>(h->hvals));
+        h->launches++;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+    }
     CK(cudaMalloc((void **)&h->hz, sizeof(double) * std::max<int64_t>(zoff, 1)));
     CK(cudaMalloc((void **)&h->hxp, sizeof(double) * (Nt + HM_XPAD)));
     CK(cudaMemset(h->hxp, 0, sizeof(double) * (Nt + HM_XPAD)));

@@ -222,6 +222,42 @@ __global__ void __launch_bounds__(256) hm_rows_kernel(const HTask *__restrict__ 
     }
 }
 
+// Setup: the entries of the dense leaves, evaluated on the device (the same
+// formulas as the dense assembly), rows [start, start+count) of a task.
+template <typename T>
+__global__ void __launch_bounds__(256) hm_fill_dense_kernel(const HTask *__restrict__ tasks,
+                                                            const HBlk *__restrict__ blks,
+                                                            const Inst *__restrict__ inst, int mode,
+                                                            const int *__restrict__ perm,
+                                                            const double *__restrict__ node,
+                                                            const double *__restrict__ elem,
+                                                            const double *__restrict__ tan,
+                                                            const double *__restrict__ nrm, T *__restrict__ vals)
+{
+    const HTask t = tasks[blockIdx.x];
+    const HBlk b = blks[t.blk];
+    const Inst &I = inst[b.inst];
+    const int64_t e0 = I.eoff;
+    const double *E = elem + 2 * e0, *Tn = tan + 2 * e0, *R = nrm + 2 * e0, *D = node + 2 * (e0 + b.inst);
+    const int *pm = perm + e0;
+    const int64_t n = (int64_t)t.count * b.nc;
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+        const int i = t.start + (int)(q / b.nc), j = (int)(q % b.nc);
+        const int64_t k = pm[b.r0 + i], l = pm[b.c0 + j];
+        double v;
+        if (mode == 3) {
+            v = entry_mode3(E[2 * k], E[2 * k + 1], Tn[2 * k], Tn[2 * k + 1], D[2 * l], D[2 * l + 1], D[2 * l + 2],
+                            D[2 * l + 3]);
+        } else {
+            double kt, kn;
+            entry_mode2(E[2 * k], E[2 * k + 1], R[2 * k], R[2 * k + 1], D[2 * l], D[2 * l + 1], D[2 * l + 2],
+                        D[2 * l + 3], R[2 * l], R[2 * l + 1], kt, kn);
+            v = b.comp == 0 ? kt : kn;
+        }
+        vals[b.foff + (int64_t)i * b.ld + j] = (T)v;
+    }
+}
+
 // y(pos) = sum of the slots of row pos (fixed order), stored at the
 // original element index in the K.V result arrays (partials with one chunk).
 __global__ void hm_gather_kernel(int64_t Ntot, int ncomp, const int *__restrict__ inst_of,
