@@ -317,7 +317,10 @@ def leg_tensor_core(args, local, stream):
     800-fault network (per-member a, b, initial V and stepped fault), K.V of
     all members as one tcgen05 GEMM per stage (BF16 hi+lo, FP32
     accumulation), against single-network FP64 runs of two members to the
-    same simulated time (V formulation and Newton slip formulation)."""
+    same simulated time: V formulation, Newton slip formulation, and the
+    Newton formulation with the learned initial guess (trained on solves
+    recorded from eight members of the same batch) -- the batched
+    mixed-precision learned-guess form."""
     from demystification_dfn_b200 import networks
     from demystification_dfn_b200.ensemble import Ensemble
     from demystification_dfn_b200.simulation import Simulation
@@ -334,9 +337,24 @@ def leg_tensor_core(args, local, stream):
            "members": R, "pressure_solver": "tridiag (exact implicit step)"}
     t_end = 200.0
     pressure = "tridiag"
-    for form in ("v", "newton"):
-        e = Ensemble(members, storage="bf16x2_tc", pressure=pressure, device=local, formulation=form)
+    from demystification_dfn_b200 import learned
+
+    rec = Ensemble(members[:8], storage="bf16x2_tc", pressure=pressure, device=local, formulation="newton")
+    rec.set_stream(stream.cuda_stream)
+    rec.record(2_000_000)
+    rec.solve(n_steps=60, check=False)
+    xr, tr = rec.record_read(2_000_000)
+    rec.close()
+    weights = learned.train(xr, tr, epochs=20, batch=4096, lr=2e-3, seed=0)[0] if len(tr) >= 4096 else None
+    out["learned_train_samples"] = int(len(tr))
+    runs = [("v", "v", "analytic"), ("newton", "newton", "analytic")]
+    if weights is not None:
+        runs.append(("newton_learned", "newton", "mlp"))
+    for name, form, guess in runs:
+        e = Ensemble(members, storage="bf16x2_tc", pressure=pressure, device=local, formulation=form, guess=guess)
         e.set_stream(stream.cuda_stream)
+        if guess == "mlp":
+            e.set_mlp(weights)
         res_tune = e.autotune()
         N = e.n_elements[0]
         e.solve(n_steps=3, check=False)
@@ -357,8 +375,11 @@ def leg_tensor_core(args, local, stream):
                "autotune": res_tune}
         e.close()
         # accuracy: the same members to t_end, batch on tensor cores vs FP64 alone
-        e = Ensemble(members[:2], storage="bf16x2_tc", pressure=pressure, device=local, formulation=form)
+        e = Ensemble(members[:2], storage="bf16x2_tc", pressure=pressure, device=local, formulation=form,
+                     guess=guess)
         e.set_stream(stream.cuda_stream)
+        if guess == "mlp":
+            e.set_mlp(weights)
         e.solve(t_end=t_end, check=False)
         errs = {}
         for i in range(2):
@@ -383,7 +404,9 @@ def leg_tensor_core(args, local, stream):
         e.close()
         res["max_rel_err_vs_fp64_single_network_at_t_end"] = errs
         res["t_end_s"] = t_end
-        out[form] = res
+        res["newton_iterations_per_solve"] = (sum(r["newton_iters"] for r in reps) /
+                                              max(sum(r["newton_solves"] for r in reps), 1))
+        out[name] = res
     return out
 
 
