@@ -716,6 +716,16 @@ __device__ __forceinline__ double pmatvec_row_c(int64_t k, int64_t N, double A1,
     return __ddiv_rn(m, A2);
 }
 
+// The Jacobi-scaled row with the off-diagonal coefficients divided by the
+// diagonal once per solve (s1 = A1/A2, s3 = A3/A2): equal to pmatvec_row up
+// to rounding, without a division per element and iteration.
+__device__ __forceinline__ double pmatvec_row_s(int64_t k, int64_t N, double s1, double s3, const double *v)
+{
+    if (k == 0) return fma(s3, v[1], v[0]);
+    if (k == N - 1) return fma(s1, v[k - 1], v[k]);
+    return fma(s1, v[k - 1], fma(s3, v[k + 1], v[k]));
+}
+
 // b1(k) = P(k)/diag(k) plus the injection terms, each added separately as
 // in src/fluid_diffusion.f90:45-64.
 __device__ __forceinline__ double pb1(const PressParams &p, int64_t k, double dt, double diag)
@@ -771,7 +781,10 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
     for (int64_t k = tid; k < N; k += nt) {
         double A1, A2, A3;
         prow(p, k, dt, A1, A2, A3);
-        if (cf) { c1[k] = A1; c2[k] = A2; c3[k] = A3; }
+        if (cf) {
+            if (exact) { c1[k] = A1; c2[k] = A2; c3[k] = A3; }
+            else { c1[k] = A1 / A2; c3[k] = A3 / A2; }
+        }
         const double rk = add_(pb1(p, k, dt, A2), -(cf ? pmatvec_row_c(k, N, A1, A2, A3, p.P)
                                                         : pmatvec_row(p, k, dt, p.P)));
         x[k] = p.P[k];
@@ -790,7 +803,9 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
         it++;
         double lpap = 0.0;
         for (int64_t k = tid; k < N; k += nt) {
-            const double m = cf ? pmatvec_row_c(k, N, c1[k], c2[k], c3[k], pv) : pmatvec_row(p, k, dt, pv);
+            const double m = !cf ? pmatvec_row(p, k, dt, pv)
+                                 : (exact ? pmatvec_row_c(k, N, c1[k], c2[k], c3[k], pv)
+                                          : pmatvec_row_s(k, N, c1[k], c3[k], pv));
             Mp[k] = m;
             lpap += pv[k] * m;
         }
