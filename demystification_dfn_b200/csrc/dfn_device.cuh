@@ -831,6 +831,8 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
         }
         const double beta = r1r1 / rr;
         for (int64_t k = tid; k < N; k += nt) pv[k] = add_(r[k], mul_(beta, pv[k]));
+        // the next stencil reads the neighbours' pv: all updates first
+        __syncthreads();
         rr = r1r1;
         if (it > 200) { *iters += it; return 1; }
         errmax = mx / p.tol;
