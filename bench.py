@@ -423,6 +423,34 @@ def leg_tensor_core(args, local, stream):
     return out
 
 
+def leg_span(args, local, stream):
+    """The benchmark network over the configuration's span (0.1 simulated
+    year) from its initial state, FP64 plain path, in chunks of 500 accepted
+    steps until the span is reached or 120 s of wall time have passed."""
+    from demystification_dfn_b200 import _lib
+    from demystification_dfn_b200.layout import DfnReport
+    from demystification_dfn_b200.networks import YEAR
+    from demystification_dfn_b200.simulation import Simulation
+
+    span = 0.1 * YEAR
+    s = Simulation(make_problem(0, args.n_faults), storage="fp64", pressure=args.pressure, device=local,
+                   gemv=args.gemv)
+    s.set_stream(stream.cuda_stream)
+    reps = (DfnReport * 1)()
+    t0 = time.perf_counter()
+    while True:
+        _lib.check(s.lib.dfn_solve_batch(s.h, 500, float(span), reps), s.lib)
+        rep = reps[0].as_dict()
+        done = rep["time"] >= span * (1 - 1e-12)
+        if done or rep["status"] != 0 or time.perf_counter() - t0 > 120.0:
+            break
+    wall = time.perf_counter() - t0
+    out = {"span_s": span, "reached_s": rep["time"], "accepted_steps": int(rep["it_count"]), "wall_s": wall,
+           "status": int(rep["status"]), "complete": bool(done)}
+    s.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -472,7 +500,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
     ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
-    ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,tensor_core,learned,cpu",
+    ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,tensor_core,span,learned,cpu",
                     help="comma list of the extra legs to run")
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
@@ -652,6 +680,8 @@ def main():
         extras["hmatrix"] = leg_hmatrix(args, local, stream)
     if rank == 0 and "tensor_core" in legs:
         extras["tensor_core"] = leg_tensor_core(args, local, stream)
+    if rank == 0 and "span" in legs:
+        extras["span"] = leg_span(args, local, stream)
     if rank == 0 and "learned" in legs:
         extras["learned_newton"] = leg_learned(args, local, stream)
 
