@@ -451,6 +451,39 @@ def leg_span(args, local, stream):
     return out
 
 
+def leg_ensemble_span(args, local, stream, storage="fp32", wall_limit=240.0):
+    """The 64-network ensemble over its whole span (1 simulated year), FP32
+    storage, one handle, in chunks of 1000 accepted steps per network until
+    every network has reached the span or the wall-time limit has passed.
+    Not in the default legs (about three minutes)."""
+    from demystification_dfn_b200 import networks
+    from demystification_dfn_b200.ensemble import Ensemble
+    from demystification_dfn_b200.networks import YEAR
+
+    members = networks.ensemble(64)
+    e = Ensemble(members, storage=storage, pressure=args.pressure, device=local, gemv=args.gemv)
+    e.set_stream(stream.cuda_stream)
+    tune = e.autotune()
+    t0 = time.perf_counter()
+    while True:
+        reps = e.solve(n_steps=1000, t_end=YEAR, check=False)
+        times = np.array([r["time"] for r in reps])
+        live = [r for r in reps if r["status"] == 0 and r["time"] < YEAR * (1 - 1e-12)]
+        if not live or time.perf_counter() - t0 > wall_limit:
+            break
+    wall = time.perf_counter() - t0
+    steps = int(sum(r["it_count"] for r in reps))
+    out = {"networks": len(members), "storage": storage, "span_s": YEAR, "wall_s": wall,
+           "networks_complete": int(sum(1 for r in reps if r["time"] >= YEAR * (1 - 1e-12))),
+           "min_reached_s": float(times.min()), "median_reached_s": float(np.median(times)),
+           "accepted_steps_total": steps, "network_steps_per_s": steps / wall,
+           "rejected_total": int(sum(r["rejected"] for r in reps)),
+           "status_counts": {str(st): sum(1 for r in reps if r["status"] == st) for st in sorted({r["status"] for r in reps})},
+           "short_segments": tune["short_segments"], "kv_impl": tune["gemv_impl"]}
+    e.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -501,7 +534,8 @@ def main():
     ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,tensor_core,span,learned,cpu",
-                    help="comma list of the extra legs to run")
+                    help="comma list of the extra legs to run (ensemble_span, the 64 networks over 1 "
+                         "simulated year, is available but not in the default list)")
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -682,6 +716,8 @@ def main():
         extras["tensor_core"] = leg_tensor_core(args, local, stream)
     if rank == 0 and "span" in legs:
         extras["span"] = leg_span(args, local, stream)
+    if rank == 0 and "ensemble_span" in legs:
+        extras["ensemble_span"] = leg_ensemble_span(args, local, stream)
     if rank == 0 and "learned" in legs:
         extras["learned_newton"] = leg_learned(args, local, stream)
 

@@ -117,3 +117,22 @@ def check(status, lib=None):
         lib = lib or load()
         raise DfnError(status, (lib.dfn_last_error() or b"").decode())
     return status
+
+
+class DfnTuning(ctypes.Structure):
+    _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32), ("ms", ctypes.c_double * 6)]
+
+
+def autotune(lib, h, storage):
+    """dfn_autotune on handle h; names the K.V shapes of the handle's storage."""
+    t = DfnTuning()
+    check(lib.dfn_autotune(h, ctypes.byref(t)), lib)
+    if storage == "bf16x2_tc":
+        names = ("tc_persistent", "tc_ring_deep", "tc_ring_2stage")
+        ms = {"kv_tc_persistent": t.ms[0], "kv_tc_ring_deep": t.ms[1], "kv_tc_ring_2stage": t.ms[4]}
+    else:
+        names = ("tma", "ldg")
+        ms = {"kv_tma": t.ms[0], "kv_ldg": t.ms[1]}
+    ms["pressure_warp"] = t.ms[2]
+    ms["pressure_thread"] = t.ms[3]
+    return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp", "ms": ms}

@@ -115,7 +115,8 @@ struct dfn_handle {
     // shared-geometry batch on tensor cores (DFN_STORE_BF16X2_TC)
     bool tc = false;
     int tc_bn = 0, tc_nmt = 0, tc_split = 1, tc_kps = 0, tc_nkb = 0;
-    bool tc_shallow = false;              // 2-stage ring instead of the deepest (autotuner)
+    int tc_variant = 0;                   // 0 persistent, 1 unit per CTA deepest ring, 2 unit per CTA 2-stage ring
+    int sms = 148;                        // streaming multiprocessors of the device
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -253,8 +254,16 @@ template <int BN>
 static void tc_launch_bn(dfn_handle *h, const TcOut &o)
 {
     const int64_t na = h->tc_mpad * h->tc_kpad, nb = (int64_t)h->tc_bn * h->tc_kpad;
-    const unsigned grid = (unsigned)(h->tc_nmt * h->tc_split);
-    if (h->tc_shallow && tc_stages(BN) > 2)
+    const unsigned units = (unsigned)(h->tc_nmt * h->tc_split);
+    if (h->tc_variant == 0) {
+        const unsigned grid = std::min(units, (unsigned)h->sms);
+        tc_gemm_persistent_kernel<BN, tc_stages(BN)><<<grid, TC_PTHREADS, tc_smem_bytes(BN, tc_stages(BN)),
+                                                       h->stream>>>(h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o,
+                                                                    h->err_flag);
+        return;
+    }
+    const unsigned grid = units;
+    if (h->tc_variant == 2 && tc_stages(BN) > 2)
         tc_gemm_kernel<BN, 2><<<grid, TC_THREADS, tc_smem_bytes(BN, 2), h->stream>>>(
             h->tc_A, h->tc_A + na, h->tc_B, h->tc_B + nb, o, h->err_flag);
     else
@@ -272,7 +281,7 @@ static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
     CKL();
     TcOut o;
     o.partT = h->partT; o.partN = h->partN; o.inst = h->inst; o.N = I.N; o.mrows = h->tc_mrows; o.R = h->B;
-    o.kb_per_split = h->tc_kps; o.nkb = h->tc_nkb; o.nmt = h->tc_nmt;
+    o.kb_per_split = h->tc_kps; o.nkb = h->tc_nkb; o.nmt = h->tc_nmt; o.nsplit = h->tc_split;
     switch (h->tc_bn) {
     case 16: tc_launch_bn<16>(h, o); break;
     case 32: tc_launch_bn<32>(h, o); break;
@@ -921,6 +930,8 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     h->B = count;
     h->mode = probs[0].fracture_mode; h->store = opt.kernel_storage;
     h->pressure = opt.pressure_solver; h->gemv_impl = opt.gemv_impl;
+    if (cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->sms <= 0)
+        h->sms = 148;
     h->max_attempts = opt.max_attempts > 0 ? opt.max_attempts : 64;
     h->form = opt.formulation == DFN_FORM_NEWTON ? DFN_FORM_NEWTON : DFN_FORM_V;
     h->guess = (opt.newton_guess >= 0 && opt.newton_guess <= 3) ? opt.newton_guess : 0;
@@ -969,8 +980,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         h->tc_kpad = (int64_t)h->tc_nkb * TC_BK;
         h->tc_bn = count <= 16 ? 16 : count <= 32 ? 32 : count <= 64 ? 64 : count <= 128 ? 128 : 256;
         // reduction splits: the fewest that fill whole waves of the SMs well
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+        const int sms = h->sms;
         double best = -1.0;
         for (int s = 1; s <= 8 && s <= h->tc_nkb; s++) {
             const int64_t units = (int64_t)h->tc_nmt * s;
@@ -1168,6 +1178,17 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         TC_SMEM_ATTR(16, 4); TC_SMEM_ATTR(32, 4); TC_SMEM_ATTR(64, 4); TC_SMEM_ATTR(128, 3); TC_SMEM_ATTR(256, 2);
         TC_SMEM_ATTR(16, 2); TC_SMEM_ATTR(32, 2); TC_SMEM_ATTR(64, 2); TC_SMEM_ATTR(128, 2);
 #undef TC_SMEM_ATTR
+#define TC_SMEM_ATTR(BN, ST)                                                                                       \
+    CKC(cudaFuncSetAttribute(tc_gemm_persistent_kernel<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                             (int)tc_smem_bytes(BN, ST)))
+        TC_SMEM_ATTR(16, 4); TC_SMEM_ATTR(32, 4); TC_SMEM_ATTR(64, 4); TC_SMEM_ATTR(128, 3); TC_SMEM_ATTR(256, 2);
+#undef TC_SMEM_ATTR
+        if (opt.gemv_impl < 0 || opt.gemv_impl > 2) {
+            g_err = "gemv_impl of a tensor-core handle is 0 (persistent), 1 (deepest ring) or 2 (2-stage ring)";
+            dfn_destroy(h);
+            return DFN_ERR_ARG;
+        }
+        h->tc_variant = opt.gemv_impl;
     }
     // dense kernel matrices, one per network
     h->K_bytes = (size_t)std::max<int64_t>(kvec, 1) * 16;
@@ -1270,16 +1291,23 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         r.gemv_impl = h->gemv_impl;
         (void)keep;
     }
-    if (h->tc && tc_stages(h->tc_bn) > 2) {
-        double ms2[2];
-        for (int v = 0; v < 2; v++) {
-            h->tc_shallow = v == 1;
-            TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, ms2[v]));
+    if (h->tc) {
+        // persistent -> ms[0], unit per CTA with the deepest ring -> ms[1],
+        // unit per CTA with a 2-stage ring -> ms[4] (when that is another shape)
+        const int nv = tc_stages(h->tc_bn) > 2 ? 3 : 2;
+        double msv[3] = {0.0, 0.0, 0.0};
+        for (int v = 0; v < nv; v++) {
+            h->tc_variant = v;
+            TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, msv[v]));
         }
-        h->tc_shallow = ms2[1] < ms2[0];
-        r.ms[0] = ms2[0];
-        r.ms[1] = ms2[1];
-        r.gemv_impl = h->tc_shallow ? 1 : 0;
+        int best = 0;
+        for (int v = 1; v < nv; v++)
+            if (msv[v] < msv[best]) best = v;
+        h->tc_variant = best;
+        r.ms[0] = msv[0];
+        r.ms[1] = msv[1];
+        r.ms[4] = msv[2];
+        r.gemv_impl = best;
     }
     r.tri_thread = h->tri_thread ? 1 : 0;
     if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {

@@ -65,6 +65,7 @@ struct TcOut {
     int kb_per_split;          // reduction stages per split
     int nkb;                   // reduction stages in total
     int nmt;                   // 128-row tiles
+    int nsplit;                // reduction splits (work units = nmt * nsplit)
 };
 
 // Shared-memory matrix descriptor (tcgen05): K-major operand, 128-byte
@@ -97,6 +98,62 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+
+// Bounded wait that also gives up once another role of the CTA raised the
+// abort flag.
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, const int *abort_flag)
+{
+    for (int it = 0; it < (1 << 22); it++) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(smem_u32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if ((it & 63) == 63 && *(volatile const int *)abort_flag) return false;
+    }
+    return false;
+}
+
+// Epilogue of one work unit for one warp: TMEM lanes 32q..32q+31 (rows of
+// the 128-row tile) x BN columns (networks), read from accumulator columns
+// starting at tmem_acc, stored as part[split][row] of each network; zeros
+// when the unit had no reduction stages (have = false).
+template <int BN>
+__device__ __forceinline__ void tc_store_unit(uint32_t tmem_acc, const TcOut &out, int mt, int split, int q, int lane,
+                                              bool have)
+{
+    const int64_t row = (int64_t)mt * TC_BM + q * 32 + lane;
+    const bool shear = row < out.N;
+    const int64_t k = shear ? row : row - out.N;
+    const bool live = row < out.mrows;
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t v[16];
+        if (have) {
+            const uint32_t taddr = tmem_acc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                           "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int r = c0 + j;
+            if (live && r < out.R) {
+                double *dst = (shear ? out.partT : out.partN) + out.inst[r].poff + (int64_t)split * out.N + k;
+                *dst = (double)__uint_as_float(v[j]);
+            }
+        }
+    }
 }
 
 template <int BN, int STAGES>
@@ -193,34 +250,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     const bool good = ok && !*(volatile int *)abort_flag;
     if (good || nk == 0) {
-        const int64_t row = (int64_t)mt * TC_BM + warp * 32 + lane;
-        const bool shear = row < out.N;
-        const int64_t k = shear ? row : row - out.N;
-        const bool live = row < out.mrows;
-#pragma unroll
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            uint32_t v[16];
-            if (nk > 0) {
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-                               "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                             : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            } else {
-#pragma unroll
-                for (int j = 0; j < 16; j++) v[j] = 0u;
-            }
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const int r = c0 + j;
-                if (live && r < out.R) {
-                    double *dst = (shear ? out.partT : out.partN) + out.inst[r].poff + (int64_t)split * out.N + k;
-                    *dst = (double)__uint_as_float(v[j]);
-                }
-            }
-        }
+        tc_store_unit<BN>(tmem, out, mt, split, warp, lane, nk > 0);
     } else if (threadIdx.x == 0) {
         atomicExch(err_flag, 1);
     }
@@ -229,6 +259,159 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"((uint32_t)(BN < 32 ? 32 : BN)));
+}
+
+// Persistent form of the same GEMM: one CTA per SM walks the work units
+// u = blockIdx.x, blockIdx.x + gridDim.x, ... (unit u = row tile u % nmt,
+// split u / nmt, as above). The producer streams the stages of consecutive
+// units through the ring without a break, the MMA issuer alternates between
+// two TMEM accumulators (2 x BN columns), and four epilogue warps drain one
+// accumulator while the MMAs of the next unit fill the other, so the per-unit
+// start-up (TMEM allocation, barrier set-up, first copy latency) and the
+// epilogue leave the HBM stream. Every unit is summed exactly as in
+// tc_gemm_kernel: the results are identical bit for bit.
+//   warp 0, one lane   producer;  warp 1, one lane   MMA issuer;
+//   warps 2-5          epilogue (TMEM lane quarter warp % 4).
+#define TC_PTHREADS 192
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(TC_PTHREADS, 1)
+    tc_gemm_persistent_kernel(const __nv_bfloat16 *__restrict__ Ah, const __nv_bfloat16 *__restrict__ Al,
+                              const __nv_bfloat16 *__restrict__ Bh, const __nv_bfloat16 *__restrict__ Bl, TcOut out,
+                              int *err_flag)
+{
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "N of an M=128 MMA is a multiple of 16 up to 256");
+    static_assert(STAGES >= 2 && STAGES * tc_stage_bytes(BN) <= 196608, "ring within 192 KiB");
+    constexpr uint32_t TCOLS = 2 * BN < 32 ? 32 : 2 * BN;   // two accumulators, a power of two >= 32
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    unsigned char *ring = reinterpret_cast<unsigned char *>(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + STAGES * tc_stage_bytes(BN));
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;    // accumulator a holds a finished unit
+    uint64_t *tempty = tfull + 2;        // accumulator a has been read out
+    uint64_t *done = tempty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int units = out.nmt * out.nsplit;
+    constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2;
+    constexpr uint32_t TX = 2 * A_BYTES + 2 * B_BYTES;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int a = 0; a < 2; a++) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 4); }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: stage g of this CTA goes to ring slot g % STAGES
+            uint32_t g = 0;
+            bool stop = false;
+            for (int u = blockIdx.x; u < units && !stop; u += gridDim.x) {
+                const int mt = u % out.nmt, split = u / out.nmt;
+                const int kb0 = split * out.kb_per_split, kb1 = min(kb0 + out.kb_per_split, out.nkb);
+                for (int kb = kb0; kb < kb1; kb++, g++) {
+                    const uint32_t s = g % STAGES, use = g / STAGES;
+                    if (use > 0 && !tc_wait(&empty[s], (use - 1) & 1, abort_flag)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    unsigned char *st = ring + s * tc_stage_bytes(BN);
+                    mbar_expect_tx(&full[s], TX);
+                    const int64_t at = ((int64_t)mt * out.nkb + kb) * (TC_BM * TC_BK), bt = (int64_t)kb * (BN * TC_BK);
+                    tma_bulk_g2s(st, Ah + at, A_BYTES, &full[s]);
+                    tma_bulk_g2s(st + A_BYTES, Al + at, A_BYTES, &full[s]);
+                    tma_bulk_g2s(st + 2 * A_BYTES, Bh + bt, B_BYTES, &full[s]);
+                    tma_bulk_g2s(st + 2 * A_BYTES + B_BYTES, Bl + bt, B_BYTES, &full[s]);
+                }
+            }
+            // the copies this thread issued complete before the CTA may exit
+            for (uint32_t i = (g > STAGES ? g - STAGES : 0); i < g; i++)
+                if (!mbar_wait(&full[i % STAGES], (i / STAGES) & 1)) *abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: unit j of this CTA accumulates in TMEM columns (j & 1) * BN
+            const uint32_t idesc = tc_idesc(BN);
+            uint32_t g = 0;
+            bool stop = false;
+            int j = 0;
+            for (int u = blockIdx.x; u < units && !stop; u += gridDim.x, j++) {
+                const int split = u / out.nmt;
+                const int kb0 = split * out.kb_per_split, kb1 = min(kb0 + out.kb_per_split, out.nkb);
+                const int a = j & 1;
+                const uint32_t acc = tmem + (uint32_t)(a * BN);
+                if (j >= 2 && !tc_wait(&tempty[a], ((j >> 1) - 1) & 1, abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int kb = kb0; kb < kb1; kb++, g++) {
+                    const uint32_t s = g % STAGES, use = g / STAGES;
+                    if (!tc_wait(&full[s], use & 1, abort_flag)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(ring + s * tc_stage_bytes(BN));
+                    const uint64_t ah = tc_desc(base), al = tc_desc(base + A_BYTES);
+                    const uint64_t bh = tc_desc(base + 2 * A_BYTES), bl = tc_desc(base + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 16; kk++) {
+                        const uint64_t o = (uint64_t)(kk * 32 >> 4);
+                        tc_mma(acc, ah + o, bh + o, idesc, (kb > kb0 || kk > 0) ? 1u : 0u);
+                        tc_mma(acc, ah + o, bl + o, idesc, 1u);
+                        tc_mma(acc, al + o, bh + o, idesc, 1u);
+                    }
+                    tc_commit(&empty[s]);
+                }
+                if (!stop) tc_commit(&tfull[a]);   // arrives once the unit's MMAs have completed
+            }
+            tc_commit(done);
+            if (!mbar_wait(done, 0)) *abort_flag = 1;
+        }
+    } else {
+        // epilogue warps
+        const int q = warp & 3;
+        int j = 0;
+        for (int u = blockIdx.x; u < units; u += gridDim.x, j++) {
+            const int mt = u % out.nmt, split = u / out.nmt;
+            const int kb0 = split * out.kb_per_split, kb1 = min(kb0 + out.kb_per_split, out.nkb);
+            const int a = j & 1;
+            bool ok = tc_wait(&tfull[a], (j >> 1) & 1, abort_flag);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) {
+                if (lane == 0) *(volatile int *)abort_flag = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            tc_store_unit<BN>(tmem + (uint32_t)(a * BN), out, mt, split, q, lane, kb1 > kb0);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[a]);
+        }
+    }
+    __syncwarp();
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0 && *(volatile int *)abort_flag) atomicExch(err_flag, 1);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
 }
 
 // V of the R networks of a stage -> BF16 hi/lo, swizzled tiles of rpad rows

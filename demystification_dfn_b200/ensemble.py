@@ -58,18 +58,7 @@ class Ensemble:
     def autotune(self):
         """Time the interchangeable launch shapes (K.V copy path, short-segment
         pressure solve) on this handle's data and keep the fastest."""
-        class _T(ctypes.Structure):
-            _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32),
-                        ("ms", ctypes.c_double * 4)]
-        t = _T()
-        _lib.check(self.lib.dfn_autotune(self.h, ctypes.byref(t)), self.lib)
-        if self._storage == "bf16x2_tc":
-            names = ("tc_ring_deep", "tc_ring_2stage")
-        else:
-            names = ("tma", "ldg")
-        return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
-                "ms": {"kv_" + names[0]: t.ms[0], "kv_" + names[1]: t.ms[1], "pressure_warp": t.ms[2],
-                       "pressure_thread": t.ms[3]}}
+        return _lib.autotune(self.lib, self.h, self._storage)
 
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch

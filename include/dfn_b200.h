@@ -97,7 +97,9 @@ typedef struct dfn_options {
     int32_t pressure_solver;  /* DFN_PRESSURE_* */
     int32_t device;           /* CUDA device ordinal */
     int32_t max_attempts;     /* RK attempts per step scheduled on the device before the host looks (>=1) */
-    int32_t gemv_impl;        /* 0 = TMA bulk-copy pipeline, 1 = direct 128-bit loads */
+    int32_t gemv_impl;        /* 0 = TMA bulk-copy pipeline, 1 = direct 128-bit loads;
+                                 tensor-core storage: 0 persistent GEMM, 1 / 2 one unit
+                                 per CTA with the deepest / a 2-stage ring */
     /* H-matrix parameters for static_kernel = hmatrix (0 = the reference's
      * defaults nleaf=100, eta=3, eps_ACA=1e-8, src/variables.f90:122-124) */
     int32_t hmat_leaf;
@@ -191,17 +193,19 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * segments (<= 64 elements) solved by one thread each (sequential Thomas) or
  * one warp each (scans), equal to rounding. ms[] = milliseconds per launch of
  * K.V TMA, K.V LDG, pressure by warps, pressure by threads (0 = not timed).
- * For DFN_STORE_BF16X2_TC handles the two K.V choices are instead the
- * tensor-core GEMM with its deepest shared-memory ring (one CTA per SM,
- * gemv_impl 0) or a 2-stage ring (two CTAs per SM, gemv_impl 1), timed in
- * ms[0] and ms[1]; both give identical results.
- * Without a call, K.V uses options.gemv_impl (the deepest ring for
- * tensor-core handles) and the short segments use threads once a launch has
- * at least 16384 of them. No counterpart in the reference. */
+ * For DFN_STORE_BF16X2_TC handles the K.V choices are instead the
+ * tensor-core GEMM as a persistent kernel (one CTA per SM walking the work
+ * units, epilogue overlapped with the next unit; gemv_impl 0, ms[0]), one
+ * unit per CTA with the deepest shared-memory ring (gemv_impl 1, ms[1]) or
+ * with a 2-stage ring (two CTAs per SM; gemv_impl 2, ms[4], timed when it
+ * differs from the deepest ring); all give identical results.
+ * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles)
+ * and the short segments use threads once a launch has at least 16384 of
+ * them. ms[5] is reserved (0). No counterpart in the reference. */
 typedef struct dfn_tuning {
     int32_t gemv_impl;
     int32_t tri_thread;
-    double ms[4];
+    double ms[6];
 } dfn_tuning;
 int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
 

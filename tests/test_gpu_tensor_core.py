@@ -82,8 +82,9 @@ def test_tensor_core_storage_needs_shared_geometry():
 
 
 def test_tensor_core_autotune_keeps_results():
-    """Both shared-memory rings of the GEMM give the same sums in the same
-    order: K.V after the autotuner's choice equals K.V before, bit for bit."""
+    """The persistent GEMM and the two unit-per-CTA rings sum every unit in
+    the same order: K.V after the autotuner's choice equals K.V before, bit
+    for bit."""
     ps = _members(40)
     rng = np.random.default_rng(4)
     with Ensemble(ps, storage="bf16x2_tc") as e:
@@ -91,8 +92,33 @@ def test_tensor_core_autotune_keeps_results():
         slips = [rng.normal(size=N) for _ in ps]
         a, _ = e.kernel(slips)
         t = e.autotune()
-        assert t["gemv_impl"] in ("tc_ring_deep", "tc_ring_2stage")
-        assert t["ms"]["kv_tc_ring_deep"] > 0 and t["ms"]["kv_tc_ring_2stage"] > 0
+        assert t["gemv_impl"] in ("tc_persistent", "tc_ring_deep", "tc_ring_2stage")
+        assert t["ms"]["kv_tc_persistent"] > 0 and t["ms"]["kv_tc_ring_deep"] > 0
+        assert t["ms"]["kv_tc_ring_2stage"] > 0   # BN = 64 has a deeper ring than two stages
         b, _ = e.kernel(slips)
         for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("count", [3, 40, 130])
+def test_tensor_core_shapes_identical(count):
+    """Each K.V shape of the GEMM (persistent, deepest ring, 2-stage ring),
+    chosen at creation, gives the same bits; batch sizes cover BN = 16, 64
+    and 256 (BN = 256 has no shallower ring: shapes 1 and 2 coincide)."""
+    # 250 faults, N of about 5000: more work units than SMs, so every
+    # persistent CTA walks several units and both TMEM accumulators
+    base = networks.fault_network(n_faults=250, box=3500.0, seed=2)
+    ps = networks.shared_geometry_ensemble(count, base=base, seed=count)
+    rng = np.random.default_rng(count)
+    outs = []
+    for gemv in ("tc_persistent", "tc_ring_deep", "tc_ring_2stage"):
+        with Ensemble(ps, storage="bf16x2_tc", gemv=gemv) as e:
+            N = e.n_elements[0]
+            if not outs:
+                slips = [rng.normal(size=N) for _ in ps]
+            outs.append(e.kernel(slips))
+    for o in outs[1:]:
+        for x, y in zip(outs[0][0], o[0]):
+            assert np.array_equal(x, y)
+        for x, y in zip(outs[0][1], o[1]):
             assert np.array_equal(x, y)
