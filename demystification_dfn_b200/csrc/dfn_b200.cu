@@ -117,6 +117,7 @@ struct dfn_handle {
     int tc_bn = 0, tc_nmt = 0, tc_split = 1, tc_kps = 0, tc_nkb = 0;
     int tc_variant = 0;                   // 0 persistent, 1 unit per CTA deepest ring, 2 unit per CTA 2-stage ring
     int sms = 148;                        // streaming multiprocessors of the device
+    int pcl = 0, pcl_n = 0, pcl_max = 0;  // cluster CG: CTAs per cluster, largest range, clusters at once
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -323,9 +324,32 @@ static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, b
 }
 
 // Pressure systems sys0..sys0+nsys-1 of the first `ninst` networks.
+static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl, int n, unsigned gx, unsigned gy,
+                       cudaStream_t stream)
+{
+    cfg = cudaLaunchConfig_t{};
+    cfg.gridDim = dim3(gx, gy);
+    cfg.blockDim = dim3(PCL_THREADS);
+    cfg.dynamicSmemBytes = pcl_smem_bytes(n);
+    cfg.stream = stream;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+}
+
 static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys, double dt_explicit, int ninst)
 {
-    if (h->pressure != DFN_PRESSURE_TRIDIAG) {
+    if (h->pressure == DFN_PRESSURE_CG && h->pcl > 0 && nsys * ninst <= h->pcl_max) {
+        // few systems: one cluster of CTAs per system, vectors in shared memory
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute at[1];
+        pcl_config(cfg, at, h->pcl, h->pcl_n, (unsigned)(nsys * h->pcl), (unsigned)ninst, h->stream);
+        CK(cudaLaunchKernelEx(&cfg, pressure_cg_cluster_kernel, h->pg, (const Inst *)h->inst, h->ctl, mask, kind,
+                              sys0, dt_explicit, h->Ptemp, h->Pdot_s));
+    } else if (h->pressure != DFN_PRESSURE_TRIDIAG) {
         dim3 grid((unsigned)nsys, (unsigned)ninst);
         pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
                                                                h->Ptemp, h->Pdot_s, h->pwork,
@@ -1234,6 +1258,35 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     PressGlobal &pg = h->pg;
     pg.P = h->P; pg.permx = h->permx; pg.ds = h->ds; pg.src_fault = h->src_fault; pg.src_elem = h->src_elem;
     pg.src_Q = h->src_Q; pg.src_tb = h->src_tb; pg.src_te = h->src_te;
+
+    // cluster CG (CG mode): the fewest CTAs per cluster (2, 4 or 8) whose
+    // ranges hold at most PCL_NTARGET elements, else 8 up to PCL_NMAX;
+    // systems under 2048 elements keep the one-CTA solver
+    if (h->pressure == DFN_PRESSURE_CG) {
+        int64_t nmax = 0;
+        for (int i = 0; i < count; i++) nmax = std::max<int64_t>(nmax, h->hinst[i].N);
+        int cl = 0;
+        if (nmax >= 2048) {
+            for (int c = 2; c <= 8 && !cl; c *= 2)
+                if ((nmax + c - 1) / c <= PCL_NTARGET) cl = c;
+            if (!cl && (nmax + 7) / 8 <= PCL_NMAX) cl = 8;
+        }
+        if (cl) {
+            const int n = (int)((nmax + cl - 1) / cl);
+            int nc = 0;
+            cudaLaunchConfig_t cfg;
+            cudaLaunchAttribute at[1];
+            pcl_config(cfg, at, cl, n, (unsigned)cl, 1, h->stream);
+            if (cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pcl_smem_bytes(n)) == cudaSuccess &&
+                cudaOccupancyMaxActiveClusters(&nc, pressure_cg_cluster_kernel, &cfg) == cudaSuccess && nc > 0) {
+                h->pcl = cl;
+                h->pcl_n = n;
+                h->pcl_max = nc;
+            }
+            cudaGetLastError();   // an unsupported shape leaves the one-CTA solver in place
+        }
+    }
 
     // controllers: solve() entry, src/solver.f90:50-56
     for (int i = 0; i < count; i++) {

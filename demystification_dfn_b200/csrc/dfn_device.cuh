@@ -20,6 +20,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cooperative_groups.h>
 #include <stdint.h>
 
 #include "newton_core.cuh"
@@ -954,6 +955,232 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
     cg_system(p, ctl + i, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
               Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact,
               coef + 18 * I.eoff + (int64_t)sys * 3 * N);
+}
+
+// ---------------------------------------------------------------------------
+// Cluster form of the Jacobi-scaled CG (exact = 0) for a few large systems.
+// The CL CTAs of a thread-block cluster split the elements of one system
+// into contiguous ranges of n elements (the last range may be shorter) and
+// keep every vector of the solve in shared memory; a range's neighbour
+// entries of the search direction and the CTAs' partial sums are read from
+// the other CTAs' shared memory (distributed shared memory). Per iteration:
+// two cluster barriers (one per reduction), no global-memory traffic. Each
+// CTA sums the CL partial sums with the same butterfly, so every CTA holds
+// the same scalars and takes the same branches. Iterates equal cg_solve's
+// (exact = 0 with cached coefficients) up to the order of the dot-product
+// sums.
+//
+// Race-freedom: a CTA's reduction slots and its r and direction entries are
+// read by other CTAs only between the two barriers that follow their write;
+// the direction is double-buffered by iteration parity, and the entry a
+// neighbour needs at a range boundary for the next iteration is computed
+// locally from the neighbour's r and current direction (both final after
+// the second barrier, rewritten only after the next iteration's first).
+#define PCL_THREADS 1024
+#define PCL_NTARGET 2048    // elements per CTA the cluster size aims at
+#define PCL_NMAX 3800       // elements per CTA that fit in shared memory
+
+// Dynamic shared memory of a cluster CTA with ranges of n elements: eight
+// slot doubles, five vectors of n and two direction buffers of n + 2.
+__host__ __device__ constexpr size_t pcl_smem_bytes(int n) { return ((size_t)7 * n + 12) * sizeof(double); }
+
+namespace cgrp = cooperative_groups;
+
+// Sum over the cluster: CTA tree sum, the CTA's partial into slot, cluster
+// barrier, then each warp sums the CL partials (bitwise the same result in
+// every lane, warp and CTA).
+__device__ __forceinline__ double cluster_sum(double v, double *red, double *slot)
+{
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    v = block_sum(v, red);
+    if (threadIdx.x == 0) *slot = v;
+    cl.sync();
+    const int lane = threadIdx.x & 31;
+    double t = (lane < (int)cl.num_blocks()) ? *cl.map_shared_rank(slot, lane) : 0.0;
+    return warp_sum(t);
+}
+// Sum of a and max of b over the cluster (slot: 2 doubles).
+__device__ __forceinline__ void cluster_sum_max(double a, double b, double *red, double *slot, double &sa, double &mb)
+{
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    block_sum_max(a, b, red, sa, mb);
+    if (threadIdx.x == 0) { slot[0] = sa; slot[1] = mb; }
+    cl.sync();
+    const int lane = threadIdx.x & 31;
+    const bool on = lane < (int)cl.num_blocks();
+    double t = on ? cl.map_shared_rank(slot, lane)[0] : 0.0;
+    double u = on ? cl.map_shared_rank(slot, lane)[1] : 0.0;
+    sa = warp_sum(t);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u = fmax(u, __shfl_xor_sync(0xffffffffu, u, o));
+    mb = u;
+}
+
+// Shared-memory vectors of one cluster CTA (range of n elements).
+struct PclVec {
+    double *s1, *s3, *x, *r, *Mp, *pv;   // pv: two buffers of n + 2 (halo at 0 and n + 1)
+    double *slot;                        // reduction slots: [0..1] sum/max, [2] sum
+};
+
+__device__ __forceinline__ PclVec pcl_vec(double *sm, int n)
+{
+    PclVec v;
+    v.slot = sm;
+    v.s1 = sm + 8; v.s3 = v.s1 + n; v.x = v.s3 + n; v.r = v.x + n; v.Mp = v.r + n; v.pv = v.Mp + n;
+    return v;
+}
+
+// One CG solve by the cluster; this CTA owns elements [k0, k0 + nk) of a
+// range of capacity n (ranges before the last are full). Returns ier, the
+// same in every CTA.
+__device__ int cg_solve_cluster(const PressParams &p, double dt, int64_t k0, int nk, int n, const PclVec &v,
+                                double *red, long long *iters)
+{
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    const int rank = (int)cl.block_rank(), ncl = (int)cl.num_blocks();
+    const int64_t N = p.N;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double *pc = v.pv;
+    double lmax = 0.0, lrr = 0.0;
+    for (int j = tid; j < nk; j += nt) {
+        const int64_t k = k0 + j;
+        double A1, A2, A3;
+        prow(p, k, dt, A1, A2, A3);
+        v.s1[j] = A1 / A2;
+        v.s3[j] = A3 / A2;
+        const double rk = add_(pb1(p, k, dt, A2), -pmatvec_row_c(k, N, A1, A2, A3, p.P));
+        v.x[j] = p.P[k];
+        v.r[j] = rk;
+        pc[j + 1] = rk;
+        lmax = fmax(lmax, fabs(rk));
+        lrr += rk * rk;
+    }
+    double rr, mx0;
+    cluster_sum_max(lrr, lmax, red, v.slot, rr, mx0);
+    // halo of the first direction (= r) from the neighbours
+    if (tid == 0 && rank > 0) pc[0] = cl.map_shared_rank(pc, rank - 1)[n];
+    if (tid == 32 && rank < ncl - 1) pc[nk + 1] = cl.map_shared_rank(pc, rank + 1)[1];
+    __syncthreads();
+    double errmax = mx0 / p.tol;
+    long long it = 0;
+    int cur = 0;
+    int ier = 0;
+    while (errmax >= 1.0) {
+        it++;
+        pc = v.pv + cur * (n + 2);
+        double lpap = 0.0;
+        for (int j = tid; j < nk; j += nt) {
+            const int64_t k = k0 + j;
+            double m;
+            if (k == 0) m = fma(v.s3[j], pc[j + 2], pc[j + 1]);
+            else if (k == N - 1) m = fma(v.s1[j], pc[j], pc[j + 1]);
+            else m = fma(v.s1[j], pc[j], fma(v.s3[j], pc[j + 2], pc[j + 1]));
+            v.Mp[j] = m;
+            lpap += pc[j + 1] * m;
+        }
+        const double pap = cluster_sum(lpap, red, v.slot + 2);
+        const double alpha = rr / pap;
+        double lr1 = 0.0, lm = 0.0;
+        for (int j = tid; j < nk; j += nt) {
+            v.x[j] = add_(v.x[j], mul_(alpha, pc[j + 1]));
+            const double r1 = add_(v.r[j], -mul_(alpha, v.Mp[j]));
+            v.r[j] = r1;
+            lr1 += r1 * r1;
+            lm = fmax(lm, fabs(r1));
+        }
+        double r1r1, mx;
+        cluster_sum_max(lr1, lm, red, v.slot, r1r1, mx);
+        const double beta = r1r1 / rr;
+        double *pn = v.pv + (cur ^ 1) * (n + 2);
+        for (int j = tid; j < nk; j += nt) pn[j + 1] = add_(v.r[j], mul_(beta, pc[j + 1]));
+        if (tid == 0 && rank > 0)
+            pn[0] = add_(cl.map_shared_rank(v.r, rank - 1)[n - 1], mul_(beta, cl.map_shared_rank(pc, rank - 1)[n]));
+        if (tid == 32 && rank < ncl - 1)
+            pn[nk + 1] = add_(cl.map_shared_rank(v.r, rank + 1)[0], mul_(beta, cl.map_shared_rank(pc, rank + 1)[1]));
+        __syncthreads();
+        cur ^= 1;
+        rr = r1r1;
+        if (it > 200) { ier = 1; break; }
+        errmax = mx / p.tol;
+    }
+    // the next solve (or the output) may reuse the slots and buffers only
+    // after every CTA has read this one's last partial sums
+    cl.sync();
+    *iters += it;
+    return ier;
+}
+
+// Batched cluster CG: cluster (system s, instance i) of CL CTAs along x.
+// Same systems, outputs and controller updates as pressure_cg_batch_kernel
+// with exact = 0. Instance i is split into ranges of ceil(N_i / CL)
+// elements (dynamic shared memory sized for the largest instance).
+__global__ void __launch_bounds__(PCL_THREADS, 1)
+    pressure_cg_cluster_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl, int mask, int kind, int sys0,
+                               double dt_explicit, double *Ptemp, double *Pdot)
+{
+    extern __shared__ __align__(16) double pcl_sm[];
+    __shared__ double red[66];
+    __shared__ long long iters;
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    const int ncl = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int i = blockIdx.y;
+    if (!takes_part(ctl, i, mask)) return;   // uniform over the cluster
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + (int)(blockIdx.x / ncl);
+    const int64_t N = I.N;
+    const int n = (int)((N + ncl - 1) / ncl);
+    const int64_t k0 = (int64_t)rank * n;
+    const int nk = (int)max((int64_t)0, min((int64_t)n, N - k0));
+    const PclVec v = pcl_vec(pcl_sm, n);
+    StepCtl *c = ctl + i;
+    if (threadIdx.x == 0) iters = 0;
+    __syncthreads();
+    double dt = sys_dt(c, kind, sys, dt_explicit);
+    int ier = cg_solve_cluster(p, dt, k0, nk, n, v, red, &iters);
+    int guard = 0;
+    if (kind == 0) {
+        // probe: src/solver.f90:81-92, halve t_try until the solve converges
+        while (ier == 1 && guard < 1100) {
+            dt = dt / 2.0;
+            guard++;
+            ier = cg_solve_cluster(p, dt, k0, nk, n, v, red, &iters);
+        }
+    }
+    // as cg_system: a stage solve that hits the cap still writes its last iterate
+    const int write = (ier == 0) || (kind == 1);
+    double mxx = 0.0;
+    if (write) {
+        double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
+        double lmx = 0.0;
+        for (int j = threadIdx.x; j < nk; j += blockDim.x) {
+            const int64_t k = k0 + j;
+            const double xk = v.x[j];
+            Pd[k] = (dt < 1e-9) ? 0.0 : (xk - p.P[k]) / dt;
+            Pt[k] = xk;
+            lmx = fmax(lmx, fabs(xk));
+        }
+        double unused;
+        cluster_sum_max(0.0, lmx, red, v.slot, unused, mxx);
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        if (kind == 0) {
+            c->t_try = dt;
+            c->halvings += guard;
+        }
+        if (write && !(mxx <= 1.7976931348623157e308)) atomicCAS(&c->status, 0, 4);
+        atomicAdd((unsigned long long *)&c->cg_iters, (unsigned long long)iters);
+        if (ier) {
+            if (kind == 1) {
+                atomicOr(&c->pfail_mask, 1 << sys);
+                atomicAdd((unsigned long long *)&c->stage_noconv, 1ull);
+            } else {
+                if (kind == 0) c->probe_ier = 1;
+                atomicCAS(&c->status, 0, 1);
+            }
+        }
+    }
+    cl.sync();   // no CTA leaves while another may still read its shared memory
 }
 
 // Exact solve of the unscaled tridiagonal system A x = P + source, one

@@ -54,7 +54,10 @@ enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter
  * products, FP32 accumulation). No counterpart in the reference. */
 enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_BF16X2_TC = 3 };
 /* Pressure solver: DFN_PRESSURE_CG is the reference's CG with tree-reduced
- * dot products; DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
+ * dot products (systems of 2048 elements or more, when a launch has few of
+ * them, are solved by a cluster of 2 to 8 CTAs holding the vectors in shared
+ * memory: a tree of another shape, so such a network's results can differ
+ * in rounding between a batch and a handle of its own); DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
  * does, reproducing its rounding and iteration counts bit for bit (slower
  * for large N); DFN_PRESSURE_TRIDIAG solves the same implicit step exactly. */
 enum { DFN_PRESSURE_CG = 0, DFN_PRESSURE_TRIDIAG = 1, DFN_PRESSURE_CG_EXACT = 2 };
