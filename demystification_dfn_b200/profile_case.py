@@ -4,6 +4,11 @@
         R realisations (default 64) of the 800-fault network sharing one
         kernel matrix: three K.V launches of the tensor-core GEMM (2.05 GB of
         BF16 hi + lo entries per launch).
+    python -m demystification_dfn_b200.profile_case tc_shapes [R ...]
+        for each R (default 64), the same batch: the autotuner's timing of the
+        three GEMM shapes (persistent, one unit per CTA with the deepest or a
+        2-stage ring), three calls, one JSON line per R; checks that K.V is
+        unchanged bit for bit across the calls.
     python -m demystification_dfn_b200.profile_case tc_round [cg|tridiag]
         the same batch, six solve rounds launched one by one (launch list of
         a round: GEMM, pressure, friction, step control).
@@ -37,6 +42,26 @@ def main(argv):
         N = e.n_elements[0]
         for _ in range(3):
             e.kernel([rng.normal(size=N) for _ in range(R)])
+    elif case == "tc_shapes":
+        import json
+
+        base = networks.fault_network(n_faults=800, seed=0)
+        for R in [int(x) for x in argv[1:]] or [64]:
+            e = Ensemble(networks.shared_geometry_ensemble(R, base=base, seed=0), storage="bf16x2_tc")
+            rng = np.random.default_rng(0)
+            N = e.n_elements[0]
+            slips = [rng.normal(size=N) for _ in range(R)]
+            a = e.kernel(slips)
+            tunes = [e.autotune() for _ in range(3)]
+            b = e.kernel(slips)
+            same = all(np.array_equal(x, y) for x, y in zip(a[0] + a[1], b[0] + b[1]))
+            ms = {k: v for k, v in tunes[-1]["ms"].items() if k.startswith("kv_")}
+            print(json.dumps({"R": R, "kv_bytes": e.kernel_bytes, "ms": ms, "pick": tunes[-1]["gemv_impl"],
+                              "unchanged": same}))
+            e.close()
+            if not same:
+                raise SystemExit("K.V changed across GEMM shapes")
+        e = None
     elif case == "tc_round":
         pressure = argv[1] if len(argv) > 1 else "tridiag"
         base = networks.fault_network(n_faults=800, seed=0)
@@ -59,7 +84,8 @@ def main(argv):
         e.solve(n_steps=40, check=False)
     else:
         raise SystemExit(f"unknown case {case!r}")
-    e.close()
+    if e is not None:
+        e.close()
     print("ok", case)
     return 0
 
