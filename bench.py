@@ -671,6 +671,7 @@ def main():
         for store in ("fp64", "fp32", "bf16x2"):
             ens = Ensemble(members, storage=store, pressure=args.pressure, device=local, gemv=args.gemv)
             ens.set_stream(stream.cuda_stream)
+            tune = ens.autotune()
             ens.solve(n_steps=3)
             torch.cuda.synchronize()
             ens.profile_kv(True)
@@ -693,6 +694,7 @@ def main():
                               "rejected": int(sum(r["rejected"] for r in reps)),
                               "probe_halvings": int(sum(r["probe_halvings"] for r in reps)),
                               "stage_cg_failures": int(sum(r["stage_cg_failures"] for r in reps)),
+                              "autotune": tune,
                               "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
                                                 for s in sorted({r["status"] for r in reps})}}
             if store == "fp64":

@@ -120,11 +120,13 @@ def check(status, lib=None):
 
 
 class DfnTuning(ctypes.Structure):
-    _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32), ("ms", ctypes.c_double * 6)]
+    _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32), ("ms", ctypes.c_double * 6),
+                ("cg_cluster", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
-def autotune(lib, h, storage):
-    """dfn_autotune on handle h; names the K.V shapes of the handle's storage."""
+def autotune(lib, h, storage, pressure):
+    """dfn_autotune on handle h; names the K.V shapes of the handle's storage
+    and the pressure shapes of its solver."""
     t = DfnTuning()
     check(lib.dfn_autotune(h, ctypes.byref(t)), lib)
     if storage == "bf16x2_tc":
@@ -133,6 +135,11 @@ def autotune(lib, h, storage):
     else:
         names = ("tma", "ldg")
         ms = {"kv_tma": t.ms[0], "kv_ldg": t.ms[1]}
-    ms["pressure_warp"] = t.ms[2]
-    ms["pressure_thread"] = t.ms[3]
-    return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp", "ms": ms}
+    if pressure == "cg":
+        ms["pressure_cg_cta"] = t.ms[2]
+        ms["pressure_cg_cluster"] = t.ms[3]
+    else:
+        ms["pressure_warp"] = t.ms[2]
+        ms["pressure_thread"] = t.ms[3]
+    return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
+            "cg_cluster": bool(t.cg_cluster), "ms": ms}

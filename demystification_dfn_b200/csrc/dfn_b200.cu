@@ -118,6 +118,7 @@ struct dfn_handle {
     int tc_variant = 0;                   // 0 persistent, 1 unit per CTA deepest ring, 2 unit per CTA 2-stage ring
     int sms = 148;                        // streaming multiprocessors of the device
     int pcl = 0, pcl_n = 0, pcl_max = 0;  // cluster CG: CTAs per cluster, largest range, clusters at once
+    int pcl_mode = -1;                    // -1: clusters when they all fit at once, 0: never, 1: always (autotuner)
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -342,7 +343,8 @@ static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl,
 
 static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys, double dt_explicit, int ninst)
 {
-    if (h->pressure == DFN_PRESSURE_CG && h->pcl > 0 && nsys * ninst <= h->pcl_max) {
+    const bool clusters = h->pcl > 0 && (h->pcl_mode == 1 || (h->pcl_mode < 0 && nsys * ninst <= h->pcl_max));
+    if (h->pressure == DFN_PRESSURE_CG && clusters) {
         // few systems: one cluster of CTAs per system, vectors in shared memory
         cudaLaunchConfig_t cfg;
         cudaLaunchAttribute at[1];
@@ -1363,6 +1365,17 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         r.gemv_impl = best;
     }
     r.tri_thread = h->tri_thread ? 1 : 0;
+    if (h->pressure == DFN_PRESSURE_CG && h->pcl > 0) {
+        for (int v = 0; v < 2; v++) {
+            h->pcl_mode = v;
+            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, r.ms[2 + v]));
+        }
+        h->pcl_mode = r.ms[3] < r.ms[2] ? 1 : 0;
+    }
+    r.cg_cluster = (h->pressure == DFN_PRESSURE_CG && h->pcl > 0 &&
+                    (h->pcl_mode == 1 || (h->pcl_mode < 0 && 5 * h->B <= h->pcl_max)))
+                       ? 1
+                       : 0;
     if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {
         for (int v = 0; v < 2; v++) {
             h->tri_thread = v == 1;

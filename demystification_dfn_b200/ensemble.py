@@ -26,6 +26,7 @@ class Ensemble:
             raise ValueError("an ensemble needs at least one problem")
         self.B = len(self.arrays)
         self._storage = storage
+        self._pressure = pressure
         opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
                            formulation, guess, newton_maxit, newton_tol)
         self._cs = [to_c(a) for a in self.arrays]
@@ -58,7 +59,7 @@ class Ensemble:
     def autotune(self):
         """Time the interchangeable launch shapes (K.V copy path, short-segment
         pressure solve) on this handle's data and keep the fastest."""
-        return _lib.autotune(self.lib, self.h, self._storage)
+        return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
 
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch

@@ -64,6 +64,7 @@ class Simulation:
                            formulation, guess, newton_maxit, newton_tol)
         self.formulation = formulation
         self._storage = storage
+        self._pressure = pressure
         self.options = {"storage": storage, "pressure": pressure, "gemv": gemv}
         self._c = to_c(self.arrays)
         h = ctypes.c_void_p()
@@ -94,7 +95,7 @@ class Simulation:
     def autotune(self):
         """Time the interchangeable launch shapes (K.V copy path, short-segment
         pressure solve) on this handle's data and keep the fastest."""
-        return _lib.autotune(self.lib, self.h, self._storage)
+        return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
 
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch

@@ -202,13 +202,20 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * unit per CTA with the deepest shared-memory ring (gemv_impl 1, ms[1]) or
  * with a 2-stage ring (two CTAs per SM; gemv_impl 2, ms[4], timed when it
  * differs from the deepest ring); all give identical results.
- * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles)
- * and the short segments use threads once a launch has at least 16384 of
- * them. ms[5] is reserved (0). No counterpart in the reference. */
+ * CG pressure (DFN_PRESSURE_CG) with systems of 2048 elements or more: the
+ * stage systems of the batch solved by one CTA each (ms[2]) or by a cluster
+ * of CTAs each (ms[3]); cg_cluster = 1 when the cluster form is kept. The
+ * two differ in the order of the dot-product sums (equal to rounding).
+ * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
+ * the short segments use threads once a launch has at least 16384 of them,
+ * and the CG uses clusters when all of a launch's clusters fit on the GPU at
+ * once. ms[5] is reserved (0). No counterpart in the reference. */
 typedef struct dfn_tuning {
     int32_t gemv_impl;
     int32_t tri_thread;
     double ms[6];
+    int32_t cg_cluster;
+    int32_t reserved;
 } dfn_tuning;
 int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
 

@@ -135,3 +135,25 @@ def test_autotune_keeps_results():
         N = len(a["P"])
         assert abs(a["time"] - b["time"]) <= 1e-10 * b["time"]
         assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-9 * np.abs(b["Y"][:N]).max()
+
+
+def test_autotune_cg_cluster_choice_equal_to_rounding():
+    """Networks of 2048 elements or more: the autotuner times the stage
+    pressure systems solved by one CTA each and by a cluster of CTAs each;
+    both forms stop at max|r| < tol_solver, so runs with either agree to the
+    solver tolerance (here after 6 steps: slip rate to 1e-6 relative)."""
+    ps = [networks.fault_network(n_faults=150, box=3000.0, seed=s, tol=1e-8) for s in (31, 32)]
+    out = []
+    for tune in (False, True):
+        with Ensemble(ps, pressure="cg") as ens:
+            if tune:
+                t = ens.autotune()
+                assert t["ms"]["pressure_cg_cta"] > 0 and t["ms"]["pressure_cg_cluster"] > 0
+                assert t["cg_cluster"] == (t["ms"]["pressure_cg_cluster"] < t["ms"]["pressure_cg_cta"])
+            reps = ens.solve(n_steps=6)
+            assert all(r["status"] == 0 for r in reps)
+            out.append([ens.state(i) for i in range(len(ps))])
+    for a, b in zip(*out):
+        N = len(a["P"])
+        assert abs(a["time"] - b["time"]) <= 1e-9 * a["time"]
+        assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-6 * np.abs(a["Y"][:N]).max()

@@ -83,6 +83,48 @@ def test_pressure_cg_matches_oracle(dt):
         assert np.abs(gP - ex).max() < 1e3 * 1e-6
 
 
+def _cluster_case(case):
+    # N >= 2048: the CG runs on a thread-block cluster of 2 (N = 4 000),
+    # 4 (N = 5 748) or 8 CTAs (N = 10 215, the last range one element shorter)
+    if case == "single4000":
+        return networks.single_fault(n_el=4000, length=40e3, mode="modeII", tol=1e-8)
+    if case == "net300":
+        return networks.fault_network(n_faults=300, box=4000.0, seed=5, tol=1e-8)
+    return networks.fault_network(n_faults=500, box=5500.0, seed=6, tol=1e-8)
+
+
+@pytest.mark.parametrize("case", ["single4000", "net300", "net500"])
+@pytest.mark.parametrize("dt", [10.0, 3600.0, 86400.0])
+def test_pressure_cg_cluster_matches_oracle(case, dt):
+    """The cluster CG (vectors in shared memory, reductions across the CTAs
+    of a cluster) stops at the same criterion max|r| < tol_solver as the
+    reference CG: both are within 1e3 * tol_solver Pa of each other and of
+    the exact implicit step, or both report non-convergence."""
+    p = _cluster_case(case)
+    o = Oracle(p)
+    with Simulation(p, pressure="cg") as s:
+        assert s.N >= 2048
+        gP, gd, gi = s.compute_P(dt)
+        oP, od, oi = o.compute_P(dt)
+        assert gi == oi
+        if oi == 0:
+            assert np.abs(gP - oP).max() < 1e3 * 1e-8
+            assert np.abs(gP - o.pressure_exact(dt)).max() < 1e3 * 1e-8
+            scale = max(np.abs(od).max(), 1e-300)
+            assert np.abs(gd - od).max() / scale < 1e-6
+
+
+def test_pressure_cg_cluster_nonconvergence_sets_ier():
+    p = networks.single_fault(n_el=4000, length=40e3, mode="modeIII", tol=1e-14)
+    with Simulation(p, pressure="cg") as s:
+        P0 = s.state()["P"]
+        _, _, ier = s.compute_P(86400.0)
+        assert ier == 1
+        _, _, ier2 = s.compute_P(1e-3)
+        assert ier2 in (0, 1)
+        assert np.array_equal(s.state()["P"], P0)
+
+
 @pytest.mark.parametrize("dt", [1.0, 100.0, 1000.0, 5000.0])
 def test_pressure_cg_exact_is_bitwise_reference_cg(dt):
     """Sequential dot products and the reference's operand order: the same
