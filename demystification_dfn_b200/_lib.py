@@ -121,7 +121,7 @@ def check(status, lib=None):
 
 class DfnTuning(ctypes.Structure):
     _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32), ("ms", ctypes.c_double * 6),
-                ("cg_cluster", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("cg_cluster", ctypes.c_int32), ("cg_cluster_ctas", ctypes.c_int32)]
 
 
 def autotune(lib, h, storage, pressure):
@@ -142,4 +142,4 @@ def autotune(lib, h, storage, pressure):
         ms["pressure_warp"] = t.ms[2]
         ms["pressure_thread"] = t.ms[3]
     return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
-            "cg_cluster": bool(t.cg_cluster), "ms": ms}
+            "cg_cluster": bool(t.cg_cluster), "cg_cluster_ctas": int(t.cg_cluster_ctas), "ms": ms}

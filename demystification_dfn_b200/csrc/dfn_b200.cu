@@ -119,6 +119,7 @@ struct dfn_handle {
     int sms = 148;                        // streaming multiprocessors of the device
     int pcl = 0, pcl_n = 0, pcl_max = 0;  // cluster CG: CTAs per cluster, largest range, clusters at once
     int pcl_mode = -1;                    // -1: clusters when they all fit at once, 0: never, 1: always (autotuner)
+    bool pcl_lean = false;                // x in global memory, M p recomputed (long ranges)
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -325,13 +326,13 @@ static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, b
 }
 
 // Pressure systems sys0..sys0+nsys-1 of the first `ninst` networks.
-static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl, int n, unsigned gx, unsigned gy,
-                       cudaStream_t stream)
+static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl, int n, bool lean, unsigned gx,
+                       unsigned gy, cudaStream_t stream)
 {
     cfg = cudaLaunchConfig_t{};
     cfg.gridDim = dim3(gx, gy);
     cfg.blockDim = dim3(PCL_THREADS);
-    cfg.dynamicSmemBytes = pcl_smem_bytes(n);
+    cfg.dynamicSmemBytes = pcl_smem_bytes(n, lean);
     cfg.stream = stream;
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cl;
@@ -348,9 +349,9 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
         // few systems: one cluster of CTAs per system, vectors in shared memory
         cudaLaunchConfig_t cfg;
         cudaLaunchAttribute at[1];
-        pcl_config(cfg, at, h->pcl, h->pcl_n, (unsigned)(nsys * h->pcl), (unsigned)ninst, h->stream);
+        pcl_config(cfg, at, h->pcl, h->pcl_n, h->pcl_lean, (unsigned)(nsys * h->pcl), (unsigned)ninst, h->stream);
         CK(cudaLaunchKernelEx(&cfg, pressure_cg_cluster_kernel, h->pg, (const Inst *)h->inst, h->ctl, mask, kind,
-                              sys0, dt_explicit, h->Ptemp, h->Pdot_s));
+                              sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, h->pcl_lean ? 1 : 0));
     } else if (h->pressure != DFN_PRESSURE_TRIDIAG) {
         dim3 grid((unsigned)nsys, (unsigned)ninst);
         pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
@@ -1261,33 +1262,47 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     pg.P = h->P; pg.permx = h->permx; pg.ds = h->ds; pg.src_fault = h->src_fault; pg.src_elem = h->src_elem;
     pg.src_Q = h->src_Q; pg.src_tb = h->src_tb; pg.src_te = h->src_te;
 
-    // cluster CG (CG mode): the fewest CTAs per cluster (2, 4 or 8) whose
-    // ranges hold at most PCL_NTARGET elements, else 8 up to PCL_NMAX;
-    // systems under 2048 elements keep the one-CTA solver
+    // cluster CG (CG mode): the fewest CTAs per cluster (2 to 16) whose
+    // ranges hold at most PCL_NTARGET elements, else the first of 8 roomy,
+    // 16 roomy, 16 lean, 8 lean whose ranges fit in shared memory, taking
+    // the first shape the device can schedule; systems under 2048 elements
+    // keep the one-CTA solver
     if (h->pressure == DFN_PRESSURE_CG) {
         int64_t nmax = 0;
         for (int i = 0; i < count; i++) nmax = std::max<int64_t>(nmax, h->hinst[i].N);
-        int cl = 0;
+        struct Shape { int cl; bool lean; };
+        std::vector<Shape> cand;
         if (nmax >= 2048) {
-            for (int c = 2; c <= 8 && !cl; c *= 2)
-                if ((nmax + c - 1) / c <= PCL_NTARGET) cl = c;
-            if (!cl && (nmax + 7) / 8 <= PCL_NMAX) cl = 8;
+            for (int c = 2; c <= 16; c *= 2)
+                if ((nmax + c - 1) / c <= PCL_NTARGET) cand.push_back({c, false});
+            const Shape more[4] = {{8, false}, {16, false}, {16, true}, {8, true}};
+            for (const Shape &sh : more)
+                if (pcl_smem_bytes((int)((nmax + sh.cl - 1) / sh.cl), sh.lean) <= (size_t)PCL_SMEM_CAP)
+                    cand.push_back(sh);
         }
-        if (cl) {
-            const int n = (int)((nmax + cl - 1) / cl);
+        // the attributes are per function, shared by every handle: set to
+        // the largest values any handle may use
+        const bool attrs =
+            cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                cudaSuccess &&
+            cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 PCL_SMEM_CAP) == cudaSuccess;
+        for (size_t q = 0; attrs && q < cand.size(); q++) {
+            const Shape &sh = cand[q];
+            const int n = (int)((nmax + sh.cl - 1) / sh.cl);
             int nc = 0;
             cudaLaunchConfig_t cfg;
             cudaLaunchAttribute at[1];
-            pcl_config(cfg, at, cl, n, (unsigned)cl, 1, h->stream);
-            if (cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)pcl_smem_bytes(n)) == cudaSuccess &&
-                cudaOccupancyMaxActiveClusters(&nc, pressure_cg_cluster_kernel, &cfg) == cudaSuccess && nc > 0) {
-                h->pcl = cl;
+            pcl_config(cfg, at, sh.cl, n, sh.lean, (unsigned)sh.cl, 1, h->stream);
+            if (cudaOccupancyMaxActiveClusters(&nc, pressure_cg_cluster_kernel, &cfg) == cudaSuccess && nc > 0) {
+                h->pcl = sh.cl;
                 h->pcl_n = n;
+                h->pcl_lean = sh.lean;
                 h->pcl_max = nc;
+                break;
             }
-            cudaGetLastError();   // an unsupported shape leaves the one-CTA solver in place
         }
+        cudaGetLastError();   // an unsupported shape leaves the one-CTA solver in place
     }
 
     // controllers: solve() entry, src/solver.f90:50-56
@@ -1372,6 +1387,7 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         }
         h->pcl_mode = r.ms[3] < r.ms[2] ? 1 : 0;
     }
+    r.cg_cluster_ctas = h->pressure == DFN_PRESSURE_CG ? h->pcl : 0;
     r.cg_cluster = (h->pressure == DFN_PRESSURE_CG && h->pcl > 0 &&
                     (h->pcl_mode == 1 || (h->pcl_mode < 0 && 5 * h->B <= h->pcl_max)))
                        ? 1

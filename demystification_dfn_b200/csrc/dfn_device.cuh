@@ -976,13 +976,22 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
 // neighbour needs at a range boundary for the next iteration is computed
 // locally from the neighbour's r and current direction (both final after
 // the second barrier, rewritten only after the next iteration's first).
+//
+// Layouts: "roomy" keeps x and M p in shared memory too; "lean" (ranges too
+// long for that) keeps x in the system's global work area and recomputes
+// M p in the second pass from the same operands (the same value), which
+// lets a cluster of 16 CTAs hold systems of up to about 92 000 elements.
 #define PCL_THREADS 1024
-#define PCL_NTARGET 2048    // elements per CTA the cluster size aims at
-#define PCL_NMAX 3800       // elements per CTA that fit in shared memory
+#define PCL_NTARGET 2048           // elements per CTA the cluster size aims at
+#define PCL_SMEM_CAP (226 * 1024)  // dynamic shared memory per CTA (the rest: static)
 
 // Dynamic shared memory of a cluster CTA with ranges of n elements: eight
-// slot doubles, five vectors of n and two direction buffers of n + 2.
-__host__ __device__ constexpr size_t pcl_smem_bytes(int n) { return ((size_t)7 * n + 12) * sizeof(double); }
+// slot doubles, s1, s3, r (and x, M p unless lean) of n each, two direction
+// buffers of n + 2.
+__host__ __device__ constexpr size_t pcl_smem_bytes(int n, bool lean)
+{
+    return ((size_t)(lean ? 5 : 7) * n + 12) * sizeof(double);
+}
 
 namespace cgrp = cooperative_groups;
 
@@ -1016,18 +1025,34 @@ __device__ __forceinline__ void cluster_sum_max(double a, double b, double *red,
     mb = u;
 }
 
-// Shared-memory vectors of one cluster CTA (range of n elements).
+// Vectors of one cluster CTA (range of n elements): shared memory, except
+// x in the lean layout (xg: this range's slice of the global work area).
 struct PclVec {
-    double *s1, *s3, *x, *r, *Mp, *pv;   // pv: two buffers of n + 2 (halo at 0 and n + 1)
+    double *s1, *s3, *x, *r, *Mp, *pv;   // pv: two buffers of n + 2 (halo at 0 and n + 1); Mp null when lean
     double *slot;                        // reduction slots: [0..1] sum/max, [2] sum
 };
 
-__device__ __forceinline__ PclVec pcl_vec(double *sm, int n)
+__device__ __forceinline__ PclVec pcl_vec(double *sm, int n, bool lean, double *xg)
 {
     PclVec v;
     v.slot = sm;
-    v.s1 = sm + 8; v.s3 = v.s1 + n; v.x = v.s3 + n; v.r = v.x + n; v.Mp = v.r + n; v.pv = v.Mp + n;
+    v.s1 = sm + 8; v.s3 = v.s1 + n; v.r = v.s3 + n; v.pv = v.r + n;
+    if (lean) {
+        v.x = xg;
+        v.Mp = nullptr;
+    } else {
+        v.x = v.pv + 2 * (n + 2);
+        v.Mp = v.x + n;
+    }
     return v;
+}
+
+// Row j of the Jacobi-scaled stencil on direction buffer pc (halo at 0).
+__device__ __forceinline__ double pcl_row(const PclVec &v, const double *pc, int j, int64_t k, int64_t N)
+{
+    if (k == 0) return fma(v.s3[j], pc[j + 2], pc[j + 1]);
+    if (k == N - 1) return fma(v.s1[j], pc[j], pc[j + 1]);
+    return fma(v.s1[j], pc[j], fma(v.s3[j], pc[j + 2], pc[j + 1]));
 }
 
 // One CG solve by the cluster; this CTA owns elements [k0, k0 + nk) of a
@@ -1070,12 +1095,8 @@ __device__ int cg_solve_cluster(const PressParams &p, double dt, int64_t k0, int
         pc = v.pv + cur * (n + 2);
         double lpap = 0.0;
         for (int j = tid; j < nk; j += nt) {
-            const int64_t k = k0 + j;
-            double m;
-            if (k == 0) m = fma(v.s3[j], pc[j + 2], pc[j + 1]);
-            else if (k == N - 1) m = fma(v.s1[j], pc[j], pc[j + 1]);
-            else m = fma(v.s1[j], pc[j], fma(v.s3[j], pc[j + 2], pc[j + 1]));
-            v.Mp[j] = m;
+            const double m = pcl_row(v, pc, j, k0 + j, N);
+            if (v.Mp) v.Mp[j] = m;
             lpap += pc[j + 1] * m;
         }
         const double pap = cluster_sum(lpap, red, v.slot + 2);
@@ -1083,7 +1104,8 @@ __device__ int cg_solve_cluster(const PressParams &p, double dt, int64_t k0, int
         double lr1 = 0.0, lm = 0.0;
         for (int j = tid; j < nk; j += nt) {
             v.x[j] = add_(v.x[j], mul_(alpha, pc[j + 1]));
-            const double r1 = add_(v.r[j], -mul_(alpha, v.Mp[j]));
+            const double m = v.Mp ? v.Mp[j] : pcl_row(v, pc, j, k0 + j, N);
+            const double r1 = add_(v.r[j], -mul_(alpha, m));
             v.r[j] = r1;
             lr1 += r1 * r1;
             lm = fmax(lm, fabs(r1));
@@ -1113,10 +1135,11 @@ __device__ int cg_solve_cluster(const PressParams &p, double dt, int64_t k0, int
 // Batched cluster CG: cluster (system s, instance i) of CL CTAs along x.
 // Same systems, outputs and controller updates as pressure_cg_batch_kernel
 // with exact = 0. Instance i is split into ranges of ceil(N_i / CL)
-// elements (dynamic shared memory sized for the largest instance).
+// elements (dynamic shared memory sized for the largest instance); lean:
+// x of system s in work + 24 eoff_i + 4 N_i s (the one-CTA solver's x).
 __global__ void __launch_bounds__(PCL_THREADS, 1)
     pressure_cg_cluster_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl, int mask, int kind, int sys0,
-                               double dt_explicit, double *Ptemp, double *Pdot)
+                               double dt_explicit, double *Ptemp, double *Pdot, double *work, int lean)
 {
     extern __shared__ __align__(16) double pcl_sm[];
     __shared__ double red[66];
@@ -1132,7 +1155,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 1)
     const int n = (int)((N + ncl - 1) / ncl);
     const int64_t k0 = (int64_t)rank * n;
     const int nk = (int)max((int64_t)0, min((int64_t)n, N - k0));
-    const PclVec v = pcl_vec(pcl_sm, n);
+    const PclVec v = pcl_vec(pcl_sm, n, lean != 0, work + 24 * I.eoff + (int64_t)sys * 4 * N + k0);
     StepCtl *c = ctl + i;
     if (threadIdx.x == 0) iters = 0;
     __syncthreads();

@@ -55,7 +55,7 @@ enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter
 enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_BF16X2_TC = 3 };
 /* Pressure solver: DFN_PRESSURE_CG is the reference's CG with tree-reduced
  * dot products (systems of 2048 elements or more, when a launch has few of
- * them, are solved by a cluster of 2 to 8 CTAs holding the vectors in shared
+ * them, are solved by a cluster of 2 to 16 CTAs holding the vectors in shared
  * memory: a tree of another shape, so such a network's results can differ
  * in rounding between a batch and a handle of its own); DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
  * does, reproducing its rounding and iteration counts bit for bit (slower
@@ -204,8 +204,10 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * differs from the deepest ring); all give identical results.
  * CG pressure (DFN_PRESSURE_CG) with systems of 2048 elements or more: the
  * stage systems of the batch solved by one CTA each (ms[2]) or by a cluster
- * of CTAs each (ms[3]); cg_cluster = 1 when the cluster form is kept. The
- * two differ in the order of the dot-product sums (equal to rounding).
+ * of CTAs each (ms[3]); cg_cluster = 1 when the cluster form is kept,
+ * cg_cluster_ctas = CTAs per cluster of this handle's cluster form (2 to
+ * 16; 0 when it has none). The two differ in the order of the dot-product
+ * sums (equal to rounding).
  * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
  * the short segments use threads once a launch has at least 16384 of them,
  * and the CG uses clusters when all of a launch's clusters fit on the GPU at
@@ -215,7 +217,7 @@ typedef struct dfn_tuning {
     int32_t tri_thread;
     double ms[6];
     int32_t cg_cluster;
-    int32_t reserved;
+    int32_t cg_cluster_ctas;
 } dfn_tuning;
 int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
 

@@ -114,6 +114,23 @@ def test_pressure_cg_cluster_matches_oracle(case, dt):
             assert np.abs(gd - od).max() / scale < 1e-6
 
 
+def test_pressure_cg_cluster_lean_layout_matches_oracle():
+    """70 000 elements: ranges of 4 375 elements on a cluster of 16 CTAs,
+    too long to keep x and M p in shared memory (x in the global work area,
+    M p recomputed). Where the device cannot schedule clusters of 16 the
+    one-CTA solver runs instead; the parity bound is the same."""
+    p = networks.single_fault(n_el=70000, length=700e3, mode="modeIII", tol=1e-8, kernel="hmatrix")
+    o = Oracle(p)
+    with Simulation(p, storage="fp32", pressure="cg", hmat_leaf=256, hmat_eta=2.0, hmat_eps=1e-4) as s:
+        for dt in (60.0, 20000.0):
+            gP, gd, gi = s.compute_P(dt)
+            oP, od, oi = o.compute_P(dt)
+            assert gi == oi == 0
+            assert np.abs(gP - oP).max() < 1e3 * 1e-8
+        ctas = s.autotune()["cg_cluster_ctas"]
+        assert ctas in (0, 16)
+
+
 def test_pressure_cg_cluster_nonconvergence_sets_ier():
     p = networks.single_fault(n_el=4000, length=40e3, mode="modeIII", tol=1e-14)
     with Simulation(p, pressure="cg") as s:
