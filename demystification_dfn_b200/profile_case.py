@@ -15,6 +15,10 @@
     python -m demystification_dfn_b200.profile_case hmatrix_kv
         the 4000-fault network (N = 81 750) as an H-matrix (leaf 64, eta 2,
         ACA 1e-6, FP32 factors): three K.V launches (three kernels each).
+    python -m demystification_dfn_b200.profile_case hmatrix_autotune
+        the same network with CG pressure: the autotuner's timing of the
+        stage pressure systems by one CTA each and by a cluster of CTAs each
+        (one JSON line).
     python -m demystification_dfn_b200.profile_case ensemble_round
         eight 120-fault networks (FP32 storage, tridiagonal pressure), forty
         solve rounds launched one by one.
@@ -77,6 +81,14 @@ def main(argv):
         rng = np.random.default_rng(0)
         for _ in range(3):
             e.kernel(rng.normal(size=e.N))
+    elif case == "hmatrix_autotune":
+        import json
+
+        from .simulation import Simulation
+
+        p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
+        e = Simulation(p, storage="fp32", pressure="cg", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
+        print(json.dumps(e.autotune()))
     elif case == "ensemble_round":
         e = Ensemble([networks.ensemble_member(s, n_faults=120) for s in range(64, 72)], storage="fp32",
                      pressure="tridiag")
