@@ -17,6 +17,7 @@
 #include "tc_gemm.cuh"
 
 #include <algorithm>
+#include <deque>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -608,7 +609,34 @@ static void fill_report(const StepCtl &c, dfn_report *r)
 // as the dense assembly (entry_mode2/entry_mode3).
 struct HostLeaf {
     int dense, rank;
-    std::vector<double> A, B;   // low-rank factors, A (nr x rank), B (nc x rank)
+    int64_t foff, goff;         // low-rank: A'^T and B'^T offsets in the low-rank value region
+};
+
+// Device buffer owned by the build (freed on every return path).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    int reserve(size_t b)
+    {
+        if (b <= bytes) return DFN_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&p, b) != cudaSuccess) return DFN_ERR_NOMEM;
+        bytes = b;
+        return DFN_OK;
+    }
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+struct LrSegment {
+    int64_t start, len;   // values of the low-rank region
+    DevBuf buf;
 };
 
 static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_options &opt)
@@ -618,11 +646,8 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     const double eps = opt.hmat_eps > 0 ? opt.hmat_eps : 1e-8;
     const int B = h->B, nc = h->ncomp;
     const int64_t Nt = h->Ntot;
-    std::vector<double> el(2 * Nt), tn(2 * Nt), nr(2 * Nt), nd(2 * (Nt + B));
+    std::vector<double> el(2 * Nt);   // midpoints: cluster tree and admissibility on the host
     CK(cudaMemcpy(el.data(), h->elem, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(tn.data(), h->tan, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(nr.data(), h->nrm, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(nd.data(), h->node, sizeof(double) * 2 * (Nt + B), cudaMemcpyDeviceToHost));
 
     // values per 16-byte vector of the stored type; factor rows padded to it
     const int VW = h->store == DFN_STORE_FP64 ? 2 : 4;
@@ -632,55 +657,112 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     std::vector<HTask> t1, t2, t3;
     std::vector<int> l4;
     int64_t dense_off = 0;   // values of the dense region (first in the device array)
-    std::vector<double> vals;
+    int64_t lr_off = 0;      // values of the low-rank region (after it)
+    const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
+    const size_t kAcaScratch = (size_t)2 << 30;   // device ACA scratch per batch of leaves
+    DevBuf scratch, flagbuf, leafbuf, rankbuf, placebuf, dperm;
+    std::deque<LrSegment> segs;
+    CK(cudaFuncSetAttribute(hm_aca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hm_aca_smem_bytes()));
     int64_t zoff = 0, slot = 0;
     // row contributions: per component, per global position, slot indices
     std::vector<std::vector<int64_t>> rows((size_t)nc * Nt);
     for (int i = 0; i < B; i++) {
         const Inst &I = h->hinst[i];
         const int64_t e0 = I.eoff, N = I.N;
-        const double *E = el.data() + 2 * e0, *T = tn.data() + 2 * e0, *R = nr.data() + 2 * e0,
-                     *D = nd.data() + 2 * (e0 + i);
+        const double *E = el.data() + 2 * e0;
         hmat::Tree tree = hmat::build_tree(E, (int)N, leaf);
         for (int64_t p = 0; p < N; p++) perm[e0 + p] = tree.perm[p];
+        TRY(dperm.reserve(sizeof(int) * (size_t)N));
+        CK(cudaMemcpy(dperm.p, tree.perm.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
         std::vector<hmat::Block> leaves;
         hmat::build_blocks(tree, hmat::boxes(tree, E), eta, 0, 0, leaves);
         for (int c = 0; c < nc; c++) {
-            auto entry = [&](int64_t k, int64_t l) -> double {
-                if (h->mode == DFN_MODE_III)
-                    return entry_mode3(E[2 * k], E[2 * k + 1], T[2 * k], T[2 * k + 1], D[2 * l], D[2 * l + 1],
-                                       D[2 * l + 2], D[2 * l + 3]);
-                double kt, kn;
-                entry_mode2(E[2 * k], E[2 * k + 1], R[2 * k], R[2 * k + 1], D[2 * l], D[2 * l + 1], D[2 * l + 2],
-                            D[2 * l + 3], R[2 * l], R[2 * l + 1], kt, kn);
-                return c == 0 ? kt : kn;
-            };
+            // admissible leaves: partial-pivot ACA and recompression on the
+            // device (hm_aca_kernel), in batches whose scratch stays within
+            // kAcaScratch; factors placed in leaf order into segments of the
+            // low-rank value region
             std::vector<HostLeaf> host(leaves.size());
-#pragma omp parallel for schedule(dynamic, 4)
-            for (int64_t b = 0; b < (int64_t)leaves.size(); b++) {
-                const hmat::Block &L = leaves[b];
-                HostLeaf &H = host[b];
-                auto ent = [&](int ii, int jj) { return entry(tree.perm[L.r0 + ii], tree.perm[L.c0 + jj]); };
-                int rank = -1;
-                std::vector<double> A, Bm;
-                if (!L.dense) {
-                    rank = hmat::aca_partial(L.nr, L.nc, ent, eps, hmat::kMaxRank, A, Bm);
-                    if (rank >= 0) rank = hmat::recompress(L.nr, L.nc, rank, eps, A, Bm);
-                    if (rank > hmat::kMaxRank) rank = -1;
+            std::vector<int> lr;
+            for (size_t b = 0; b < leaves.size(); b++) {
+                host[b] = HostLeaf{1, 0, 0, 0};
+                if (!leaves[b].dense) lr.push_back((int)b);
+            }
+            AcaGeom geo;
+            geo.mode = h->mode == DFN_MODE_III ? 3 : 2;
+            geo.comp = c;
+            geo.perm = static_cast<const int *>(dperm.p);
+            geo.E = h->elem + 2 * e0; geo.T = h->tan + 2 * e0; geo.R = h->nrm + 2 * e0; geo.D = h->node + 2 * (e0 + i);
+            for (size_t q0 = 0; q0 < lr.size();) {
+                std::vector<AcaLeaf> al;
+                int64_t soff = 0, foff = 0;
+                size_t q1 = q0;
+                while (q1 < lr.size()) {
+                    const hmat::Block &L = leaves[lr[q1]];
+                    const int64_t need = 2LL * (L.nr + L.nc) * HM_KMAX;
+                    if (!al.empty() && (size_t)(soff + need) * sizeof(double) > kAcaScratch) break;
+                    al.push_back(AcaLeaf{L.r0, L.c0, L.nr, L.nc, soff, foff});
+                    soff += need;
+                    foff += L.nr + L.nc;
+                    q1++;
                 }
-                if (rank < 0) {   // dense leaf, or low-rank leaf whose ACA did not converge:
-                    H.dense = 1;  // entries evaluated on the device after upload
-                    H.rank = 0;
-                } else {
+                TRY(scratch.reserve((size_t)soff * sizeof(double)));
+                TRY(flagbuf.reserve((size_t)foff));
+                TRY(leafbuf.reserve(al.size() * sizeof(AcaLeaf)));
+                TRY(rankbuf.reserve(al.size() * sizeof(int)));
+                TRY(placebuf.reserve(al.size() * sizeof(AcaPlace)));
+                CK(cudaMemcpyAsync(leafbuf.p, al.data(), al.size() * sizeof(AcaLeaf), cudaMemcpyHostToDevice,
+                                   h->stream));
+                CK(cudaMemsetAsync(flagbuf.p, 0, (size_t)foff, h->stream));
+                hm_aca_kernel<<<(unsigned)al.size(), HM_BT, hm_aca_smem_bytes(), h->stream>>>(
+                    static_cast<const AcaLeaf *>(leafbuf.p), geo, eps, static_cast<double *>(scratch.p),
+                    static_cast<char *>(flagbuf.p), static_cast<int *>(rankbuf.p));
+                h->launches++;
+                CK(cudaGetLastError());
+                std::vector<int> ranks(al.size());
+                CK(cudaMemcpyAsync(ranks.data(), rankbuf.p, al.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                                   h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                // offsets in leaf order (16-byte aligned starts, rows padded)
+                std::vector<AcaPlace> pl(al.size());
+                const int64_t seg0 = lr_off;
+                for (size_t t = 0; t < al.size(); t++) {
+                    HostLeaf &H = host[lr[q0 + t]];
+                    const int rk = ranks[t] > hmat::kMaxRank ? -1 : ranks[t];
+                    pl[t] = AcaPlace{0, 0, 0, 0, 0};
+                    if (rk < 0) continue;   // did not converge: stored dense
                     H.dense = 0;
-                    H.rank = rank;
-                    H.A.resize((size_t)L.nr * rank);
-                    H.B.resize((size_t)L.nc * rank);
-                    for (int q = 0; q < rank; q++) {
-                        for (int ii = 0; ii < L.nr; ii++) H.A[(size_t)ii * rank + q] = A[(size_t)q * L.nr + ii];
-                        for (int jj = 0; jj < L.nc; jj++) H.B[(size_t)jj * rank + q] = Bm[(size_t)q * L.nc + jj];
-                    }
+                    H.rank = rk;
+                    if (rk == 0) continue;  // zero block
+                    const int lda = (int)rup(al[t].nr), ld = (int)rup(al[t].nc);
+                    lr_off = rup(lr_off);
+                    H.foff = lr_off;
+                    lr_off += (int64_t)rk * lda;
+                    H.goff = lr_off;
+                    lr_off += (int64_t)rk * ld;
+                    pl[t] = AcaPlace{H.foff - seg0, H.goff - seg0, lda, ld, rk};
                 }
+                if (lr_off > seg0) {
+                    segs.emplace_back();
+                    LrSegment &sg = segs.back();
+                    sg.start = seg0;
+                    sg.len = lr_off - seg0;
+                    TRY(sg.buf.reserve((size_t)sg.len * vsz));
+                    CK(cudaMemsetAsync(sg.buf.p, 0, (size_t)sg.len * vsz, h->stream));
+                    CK(cudaMemcpyAsync(placebuf.p, pl.data(), pl.size() * sizeof(AcaPlace), cudaMemcpyHostToDevice,
+                                       h->stream));
+                    if (h->store == DFN_STORE_FP64)
+                        hm_aca_place_kernel<double><<<(unsigned)al.size(), 256, 0, h->stream>>>(
+                            static_cast<const AcaLeaf *>(leafbuf.p), static_cast<const AcaPlace *>(placebuf.p),
+                            static_cast<const double *>(scratch.p), static_cast<double *>(sg.buf.p));
+                    else
+                        hm_aca_place_kernel<float><<<(unsigned)al.size(), 256, 0, h->stream>>>(
+                            static_cast<const AcaLeaf *>(leafbuf.p), static_cast<const AcaPlace *>(placebuf.p),
+                            static_cast<const double *>(scratch.p), static_cast<float *>(sg.buf.p));
+                    h->launches++;
+                    CK(cudaGetLastError());
+                    CK(cudaStreamSynchronize(h->stream));   // scratch and place list are reused by the next batch
+                }
+                q0 = q1;
             }
             for (size_t b = 0; b < leaves.size(); b++) {
                 const hmat::Block &L = leaves[b];
@@ -698,24 +780,16 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                     dense_off += rup((int64_t)L.nr * hb.ld);
                     h->hdense_vals += (int64_t)L.nr * L.nc;
                 } else {
-                    vals.resize(rup((int64_t)vals.size()), 0.0);   // 16-byte aligned start
-                    hb.foff = (int64_t)vals.size();
-                    // A^T (rank x nr) and B^T (rank x nc), rank-major, rows padded
+                    // A'^T (rank x nr) and B'^T (rank x nc), rank-major, rows
+                    // padded, placed by the device build
                     hb.lda = (int)rup(L.nr);
                     hb.ld = (int)rup(L.nc);
-                    vals.resize(vals.size() + (size_t)H.rank * hb.lda, 0.0);
-                    for (int q = 0; q < H.rank; q++)
-                        for (int ii = 0; ii < L.nr; ii++)
-                            vals[hb.foff + (size_t)q * hb.lda + ii] = H.A[(size_t)ii * H.rank + q];
-                    hb.goff = (int64_t)vals.size();
-                    vals.resize(vals.size() + (size_t)H.rank * hb.ld, 0.0);
-                    for (int q = 0; q < H.rank; q++)
-                        for (int jj = 0; jj < L.nc; jj++)
-                            vals[hb.goff + (size_t)q * hb.ld + jj] = H.B[(size_t)jj * H.rank + q];
+                    hb.foff = H.foff;
+                    hb.goff = H.goff;
                     hb.zoff = zoff;
                     hb.ntask1 = (L.nc + HM_COLS - 1) / HM_COLS;
                     zoff += (int64_t)hb.ntask1 * H.rank;
-                    h->hlr_vals += (int64_t)(H.A.size() + H.B.size());
+                    h->hlr_vals += (int64_t)(L.nr + L.nc) * H.rank;
                     h->hranks.push_back(H.rank);
                 }
                 const int bi = (int)blks.size();
@@ -752,21 +826,18 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     h->hn3 = (int64_t)t3.size();
     h->hn4 = (int64_t)l4.size();
     h->hblocks = (int64_t)blks.size();
-    const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
     h->kv_bytes = (h->hdense_vals + h->hlr_vals) * (int64_t)vsz;   // stored entries, padding excluded
     // device values: [dense leaves | low-rank factors]
     for (HBlk &hb : blks)
         if (!hb.dense) { hb.foff += dense_off; hb.goff += dense_off; }
-    const size_t ntot = (size_t)dense_off + vals.size();
+    const size_t ntot = (size_t)(dense_off + lr_off);
     CK(cudaMalloc(&h->hvals, std::max<size_t>(ntot, 1) * vsz));
     CK(cudaMemsetAsync(h->hvals, 0, (size_t)dense_off * vsz, h->stream));   // padding of the dense rows
-    if (h->store == DFN_STORE_FP64) {
-        CK(cudaMemcpy(static_cast<double *>(h->hvals) + dense_off, vals.data(), vals.size() * 8,
-                      cudaMemcpyHostToDevice));
-    } else {
-        std::vector<float> f(vals.begin(), vals.end());
-        CK(cudaMemcpy(static_cast<float *>(h->hvals) + dense_off, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
-    }
+    for (LrSegment &sg : segs)
+        CK(cudaMemcpyAsync(static_cast<char *>(h->hvals) + (size_t)(dense_off + sg.start) * vsz, sg.buf.p,
+                           (size_t)sg.len * vsz, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    segs.clear();
     CK(cudaMalloc((void **)&h->hblk, std::max<size_t>(blks.size(), 1) * sizeof(HBlk)));
     CK(cudaMemcpy(h->hblk, blks.data(), blks.size() * sizeof(HBlk), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->ht1, std::max<size_t>(t1.size(), 1) * sizeof(HTask)));

@@ -1,5 +1,9 @@
-// hmat_build.h — host-side construction of the hierarchical (H-) matrix
-// representation of the kernel matrices (setup, run once per handle).
+// hmat_build.h — host-side part of the construction of the hierarchical
+// (H-) matrix representation of the kernel matrices (setup, run once per
+// handle): the cluster tree and the block partition. The low-rank factors
+// of the admissible blocks are computed on the device (hm_aca_kernel:
+// partial-pivot ACA, then QR + SVD recompression), the dense blocks are
+// filled on the device (hm_fill_dense_kernel).
 //
 // Restates the reference's construction (src/hmatrix/initialisation_hmat.f90:13-100):
 //  * cluster tree by bounding-box bisection of the element midpoints
@@ -10,21 +14,18 @@
 //  * block cluster tree with eta-admissibility eta*dist >= max(diam)
 //    (src/hmatrix/block_cluster_tree.f90:342-476): admissible pairs become
 //    low-rank leaves, non-admissible pairs split into the four son pairs
-//    when both clusters have sons, else become dense leaves;
-//  * low-rank factors A B^T of every admissible block, compressed by QR of
-//    A and B and an SVD of R_A R_B^T truncated at the first singular value
-//    <= eps*sigma_1 (kept), as src/hmatrix/H_matrix_recompression.f90:145-301,538-575.
-// Difference: the reference runs a full-pivot ACA on the fully evaluated
-// block (src/hmatrix/ACA_algorithm.f90:665-826, O(m n) kernel evaluations
-// per block); this construction runs the partial-pivot ACA
-// (O((m+n) k) evaluations, the reference's unused `ACA` routine, :12-260)
-// with the same relative Frobenius stopping tolerance. A block whose ACA
-// does not converge within kMaxRank is stored dense.
+//    when both clusters have sons, else become dense leaves.
+// Difference in the factors: the reference runs a full-pivot ACA on the
+// fully evaluated block (src/hmatrix/ACA_algorithm.f90:665-826, O(m n)
+// kernel evaluations per block); the device construction runs the
+// partial-pivot ACA (O((m+n) k) evaluations, the reference's unused `ACA`
+// routine, :12-260) with the same relative Frobenius stopping tolerance and
+// the recompression of src/hmatrix/H_matrix_recompression.f90:145-301,538-575.
+// A block whose ACA does not converge within kMaxRank is stored dense.
 #pragma once
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
-#include <functional>
 #include <vector>
 
 namespace hmat {
@@ -144,222 +145,6 @@ inline std::vector<BBox> boxes(const Tree &t, const double *elem)
         bb[k] = b;
     }
     return bb;
-}
-
-// ---------------------------------------------------------------------------
-// dense linear algebra on small column-major matrices
-
-// Householder QR of M (m x k, column-major, m >= k): returns R (k x k upper)
-// and overwrites M with Q (m x k, orthonormal columns).
-inline void qr_thin(std::vector<double> &M, int m, int k, std::vector<double> &R)
-{
-    std::vector<double> V(M), tau(k, 0.0);
-    for (int j = 0; j < k; j++) {
-        double nrm = 0;
-        for (int i = j; i < m; i++) nrm += V[j * m + i] * V[j * m + i];
-        nrm = std::sqrt(nrm);
-        if (nrm == 0) { tau[j] = 0; continue; }
-        const double a0 = V[j * m + j];
-        const double alpha = a0 > 0 ? -nrm : nrm;
-        V[j * m + j] = a0 - alpha;
-        double vn = 0;
-        for (int i = j; i < m; i++) vn += V[j * m + i] * V[j * m + i];
-        tau[j] = 2.0 / vn;
-        for (int c = j + 1; c < k; c++) {
-            double s = 0;
-            for (int i = j; i < m; i++) s += V[j * m + i] * V[c * m + i];
-            s *= tau[j];
-            for (int i = j; i < m; i++) V[c * m + i] -= s * V[j * m + i];
-        }
-    }
-    // R = upper triangle of H_{k-1} ... H_0 M
-    std::vector<double> W(M);
-    for (int j = 0; j < k; j++) {
-        if (tau[j] == 0) continue;
-        for (int c = j; c < k; c++) {
-            double s = 0;
-            for (int i = j; i < m; i++) s += V[j * m + i] * W[c * m + i];
-            s *= tau[j];
-            for (int i = j; i < m; i++) W[c * m + i] -= s * V[j * m + i];
-        }
-    }
-    R.assign(k * k, 0.0);
-    for (int c = 0; c < k; c++)
-        for (int r = 0; r <= c; r++) R[c * k + r] = W[c * m + r];
-    // Q = H_0 H_1 ... H_{k-1} applied to the first k unit vectors
-    M.assign((size_t)m * k, 0.0);
-    for (int c = 0; c < k; c++) M[c * m + c] = 1.0;
-    for (int j = k - 1; j >= 0; j--) {
-        if (tau[j] == 0) continue;
-        for (int c = 0; c < k; c++) {
-            double s = 0;
-            for (int i = j; i < m; i++) s += V[j * m + i] * M[c * m + i];
-            s *= tau[j];
-            for (int i = j; i < m; i++) M[c * m + i] -= s * V[j * m + i];
-        }
-    }
-}
-
-// One-sided Jacobi SVD of a square k x k matrix G (column-major):
-// G = U diag(S) W^T with S sorted descending.
-inline void svd_jacobi(const std::vector<double> &G, int k, std::vector<double> &U, std::vector<double> &S,
-                       std::vector<double> &W)
-{
-    U = G;
-    W.assign(k * k, 0.0);
-    for (int i = 0; i < k; i++) W[i * k + i] = 1.0;
-    for (int sweep = 0; sweep < 60; sweep++) {
-        double off = 0;
-        for (int p = 0; p < k - 1; p++)
-            for (int q = p + 1; q < k; q++) {
-                double a = 0, b = 0, g = 0;
-                for (int i = 0; i < k; i++) {
-                    a += U[p * k + i] * U[p * k + i];
-                    b += U[q * k + i] * U[q * k + i];
-                    g += U[p * k + i] * U[q * k + i];
-                }
-                if (std::fabs(g) <= 1e-300) continue;
-                off = std::max(off, std::fabs(g) / std::sqrt(a * b));
-                const double zeta = (b - a) / (2 * g);
-                const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
-                const double cs = 1 / std::sqrt(1 + t * t), sn = cs * t;
-                for (int i = 0; i < k; i++) {
-                    const double up = U[p * k + i], uq = U[q * k + i];
-                    U[p * k + i] = cs * up - sn * uq;
-                    U[q * k + i] = sn * up + cs * uq;
-                    const double wp = W[p * k + i], wq = W[q * k + i];
-                    W[p * k + i] = cs * wp - sn * wq;
-                    W[q * k + i] = sn * wp + cs * wq;
-                }
-            }
-        if (off < 1e-15) break;
-    }
-    S.assign(k, 0.0);
-    for (int j = 0; j < k; j++) {
-        double n = 0;
-        for (int i = 0; i < k; i++) n += U[j * k + i] * U[j * k + i];
-        n = std::sqrt(n);
-        S[j] = n;
-        if (n > 0)
-            for (int i = 0; i < k; i++) U[j * k + i] /= n;
-    }
-    std::vector<int> ord(k);
-    for (int i = 0; i < k; i++) ord[i] = i;
-    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return S[a] > S[b]; });
-    std::vector<double> U2(k * k), W2(k * k), S2(k);
-    for (int j = 0; j < k; j++) {
-        S2[j] = S[ord[j]];
-        for (int i = 0; i < k; i++) { U2[j * k + i] = U[ord[j] * k + i]; W2[j * k + i] = W[ord[j] * k + i]; }
-    }
-    U = U2; W = W2; S = S2;
-}
-
-// Partial-pivot ACA of the m x n block entry(i, j) (i, j local). Returns
-// the rank (0 for a zero block, -1 when it did not converge within maxr);
-// A (m x k) and B (n x k) column-major.
-inline int aca_partial(int m, int n, const std::function<double(int, int)> &entry, double eps, int maxr,
-                       std::vector<double> &A, std::vector<double> &B)
-{
-    A.clear(); B.clear();
-    std::vector<char> row_used(m, 0), col_used(n, 0);
-    double norm2 = 0.0;
-    int k = 0, i_star = 0, zero_rows = 0;
-    std::vector<double> row(n), col(m);
-    while (k < std::min(m, n)) {
-        if (k >= maxr) return -1;
-        row_used[i_star] = 1;
-        for (int j = 0; j < n; j++) {
-            double v = entry(i_star, j);
-            for (int q = 0; q < k; q++) v -= A[q * m + i_star] * B[q * n + j];
-            row[j] = v;
-        }
-        int j_star = -1;
-        double best = 0;
-        for (int j = 0; j < n; j++)
-            if (!col_used[j] && std::fabs(row[j]) > best) { best = std::fabs(row[j]); j_star = j; }
-        if (j_star < 0 || best <= 1e-300) {
-            // zero residual row: try another unused row
-            if (++zero_rows > 3) break;
-            int nxt = -1;
-            for (int i = 0; i < m; i++)
-                if (!row_used[i]) { nxt = i; break; }
-            if (nxt < 0) break;
-            i_star = nxt;
-            continue;
-        }
-        col_used[j_star] = 1;
-        const double piv = row[j_star];
-        for (int j = 0; j < n; j++) row[j] /= piv;
-        for (int i = 0; i < m; i++) {
-            double v = entry(i, j_star);
-            for (int q = 0; q < k; q++) v -= B[q * n + j_star] * A[q * m + i];
-            col[i] = v;
-        }
-        // ||S_k||_F^2 = ||S_{k-1}||^2 + 2 sum_q (a_q.a_k)(b_q.b_k) + |a_k|^2 |b_k|^2
-        double an = 0, bn = 0;
-        for (int i = 0; i < m; i++) an += col[i] * col[i];
-        for (int j = 0; j < n; j++) bn += row[j] * row[j];
-        double cross = 0;
-        for (int q = 0; q < k; q++) {
-            double aa = 0, bb = 0;
-            for (int i = 0; i < m; i++) aa += A[q * m + i] * col[i];
-            for (int j = 0; j < n; j++) bb += B[q * n + j] * row[j];
-            cross += aa * bb;
-        }
-        norm2 += 2 * cross + an * bn;
-        A.insert(A.end(), col.begin(), col.end());
-        B.insert(B.end(), row.begin(), row.end());
-        k++;
-        if (std::sqrt(an * bn) <= eps * std::sqrt(std::fabs(norm2))) return k;
-        int nxt = -1;
-        double bi = -1;
-        for (int i = 0; i < m; i++)
-            if (!row_used[i] && std::fabs(col[i]) > bi) { bi = std::fabs(col[i]); nxt = i; }
-        if (nxt < 0) return k;
-        i_star = nxt;
-    }
-    return k;
-}
-
-// Recompression of A B^T (m x k, n x k), H_matrix_recompression.f90:145-301:
-// QR of both factors, SVD of R_A R_B^T, truncation at the first singular
-// value <= eps * sigma_1 (inclusive). Returns the new rank.
-inline int recompress(int m, int n, int k, double eps, std::vector<double> &A, std::vector<double> &B)
-{
-    if (k == 0 || k >= std::min(m, n)) return k;
-    std::vector<double> Ra, Rb;
-    qr_thin(A, m, k, Ra);
-    qr_thin(B, n, k, Rb);
-    std::vector<double> G(k * k, 0.0);   // Ra * Rb^T
-    for (int c = 0; c < k; c++)
-        for (int r = 0; r < k; r++) {
-            double s = 0;
-            for (int q = 0; q < k; q++) s += Ra[q * k + r] * Rb[q * k + c];
-            G[c * k + r] = s;
-        }
-    std::vector<double> U, S, W;
-    svd_jacobi(G, k, U, S, W);
-    int r = 0;
-    for (int i = 0; i < k; i++) {
-        r = i + 1;
-        if (S[i] <= eps * S[0]) break;
-    }
-    std::vector<double> A2((size_t)m * r, 0.0), B2((size_t)n * r, 0.0);
-    for (int j = 0; j < r; j++) {
-        for (int i = 0; i < m; i++) {
-            double s = 0;
-            for (int q = 0; q < k; q++) s += A[q * m + i] * U[j * k + q];
-            A2[j * m + i] = s * S[j];
-        }
-        for (int i = 0; i < n; i++) {
-            double s = 0;
-            for (int q = 0; q < k; q++) s += B[q * n + i] * W[j * k + q];
-            B2[j * n + i] = s;
-        }
-    }
-    A.swap(A2);
-    B.swap(B2);
-    return r;
 }
 
 }  // namespace hmat

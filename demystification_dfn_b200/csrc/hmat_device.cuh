@@ -258,6 +258,394 @@ __global__ void __launch_bounds__(256) hm_fill_dense_kernel(const HTask *__restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Low-rank leaves built on the device: one 128-thread CTA per admissible
+// leaf runs the partial-pivot ACA (the reference's unused `ACA` routine,
+// src/hmatrix/ACA_algorithm.f90:12-260, with the relative Frobenius stopping
+// rule of its full-pivot ACA) and the recompression of
+// src/hmatrix/H_matrix_recompression.f90:145-301 (QR of both factors, SVD of
+// R_A R_B^T, truncation), in these steps:
+//   partial-pivot ACA: residual row at the pivot row, pivot column = the
+//     largest unused |entry| (lowest index on ties), scaled row into B, the
+//     residual column into A, ||S_k||_F^2 updated by 2 sum_q (a_q.a_k)(b_q.b_k)
+//     + |a_k|^2 |b_k|^2, stop at |a_k||b_k| <= eps ||S_k||_F, next pivot row
+//     = the largest unused |a_k(i)|; -1 beyond HM_KMAX terms (stored dense);
+//   recompression (when 0 < k < min(m, n)): Householder QR of A and B in
+//     place (reflectors below the diagonal, R above it, R's diagonal and the
+//     reflector scales in shared memory), one-sided Jacobi SVD of
+//     R_A R_B^T (k x k, shared memory; rotations of a sweep in parallel
+//     rounds of disjoint column pairs), truncation at the first singular
+//     value <= eps * sigma_1 (kept), A' = Q_A U_r S_r and B' = Q_B W_r formed
+//     by applying the reflectors to [U_r S_r; 0] and [W_r; 0].
+// Results: rank[b] (-1 dense, 0 zero block) and the factors A' (m x r) and
+// B' (n x r), column-major by rank, in the leaf's X regions of the scratch.
+// Sums are block reductions in a fixed order (deterministic).
+#define HM_KMAX 64
+#define HM_BT 128
+
+struct AcaLeaf {
+    int r0, c0, nr, nc;
+    int64_t soff;     // scratch doubles: A (nr x 64), B (nc x 64), XA (nr x 64), XB (nc x 64)
+    int64_t foff;     // char flags: nr row flags, nc column flags
+};
+
+// Dynamic shared memory of hm_aca_kernel: G/U and W (64 x 64 each) + small arrays.
+constexpr size_t hm_aca_smem_bytes() { return (size_t)(2 * HM_KMAX * HM_KMAX + 8 * HM_KMAX + 64) * sizeof(double); }
+
+__device__ __forceinline__ double hm_block_sum(double v, double *red)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < HM_BT / 32; q++) t += red[q];
+    return t;
+}
+
+// max |v| over the CTA with the lowest index on ties (idx -1: none > 0)
+__device__ __forceinline__ void hm_block_argmax(double v, int idx, double *redv, int *redi, double &best, int &bi)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi >= 0 && (idx < 0 || oi < idx))) { v = ov; idx = oi; }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) { redv[w] = v; redi[w] = idx; }
+    __syncthreads();
+    best = redv[0];
+    bi = redi[0];
+#pragma unroll
+    for (int q = 1; q < HM_BT / 32; q++)
+        if (redv[q] > best || (redv[q] == best && redi[q] >= 0 && (bi < 0 || redi[q] < bi))) { best = redv[q]; bi = redi[q]; }
+}
+
+struct AcaGeom {
+    int mode, comp;
+    const int *perm;                                  // cluster order of the network
+    const double *E, *T, *R, *D;                      // midpoints, tangents, normals, nodes of the network
+};
+
+__device__ __forceinline__ double aca_entry(const AcaGeom &g, int64_t k, int64_t l)
+{
+    if (g.mode == 3)
+        return entry_mode3(g.E[2 * k], g.E[2 * k + 1], g.T[2 * k], g.T[2 * k + 1], g.D[2 * l], g.D[2 * l + 1],
+                           g.D[2 * l + 2], g.D[2 * l + 3]);
+    double kt, kn;
+    entry_mode2(g.E[2 * k], g.E[2 * k + 1], g.R[2 * k], g.R[2 * k + 1], g.D[2 * l], g.D[2 * l + 1], g.D[2 * l + 2],
+                g.D[2 * l + 3], g.R[2 * l], g.R[2 * l + 1], kt, kn);
+    return g.comp == 0 ? kt : kn;
+}
+
+// Householder QR of M (m x k, column-major, ld m) in place; tau[j] and the
+// diagonal of R (alpha[j]) into shared memory.
+__device__ void hm_qr(double *M, int m, int k, double *tau, double *alpha, double *red)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = 0; j < k; j++) {
+        double *v = M + (int64_t)j * m;
+        double l2 = 0.0;
+        for (int i = j + threadIdx.x; i < m; i += HM_BT) l2 += v[i] * v[i];
+        const double nrm = sqrt(hm_block_sum(l2, red));
+        if (nrm == 0.0) {
+            if (threadIdx.x == 0) { tau[j] = 0.0; alpha[j] = 0.0; }
+            __syncthreads();
+            continue;
+        }
+        const double a0 = v[j];
+        const double al = a0 > 0 ? -nrm : nrm;
+        __syncthreads();
+        if (threadIdx.x == 0) { v[j] = a0 - al; alpha[j] = al; }
+        __syncthreads();
+        double vl = 0.0;
+        for (int i = j + threadIdx.x; i < m; i += HM_BT) vl += v[i] * v[i];
+        const double tj = 2.0 / hm_block_sum(vl, red);
+        if (threadIdx.x == 0) tau[j] = tj;
+        // the remaining columns, one warp per column
+        for (int c = j + 1 + w; c < k; c += HM_BT / 32) {
+            double *mc = M + (int64_t)c * m;
+            double s = 0.0;
+            for (int i = j + lane; i < m; i += 32) s += v[i] * mc[i];
+            s = warp_sum(s) * tj;
+            for (int i = j + lane; i < m; i += 32) mc[i] -= s * v[i];
+        }
+        __syncthreads();
+    }
+}
+
+// X (m x r, column-major, ld m) = Q [Y; 0] with Q = H_0 ... H_{k-1} from hm_qr;
+// column c of Y is ycol(c)[0..k).
+template <class YF>
+__device__ void hm_apply_q(const double *M, int m, int k, const double *tau, double *X, int r, YF ycol)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int c = w; c < r; c += HM_BT / 32) {
+        double *xc = X + (int64_t)c * m;
+        for (int i = lane; i < m; i += 32) xc[i] = (i < k) ? ycol(c, i) : 0.0;
+        __syncwarp();
+        for (int j = k - 1; j >= 0; j--) {
+            if (tau[j] == 0.0) continue;
+            const double *v = M + (int64_t)j * m;
+            double s = 0.0;
+            for (int i = j + lane; i < m; i += 32) s += v[i] * xc[i];
+            s = warp_sum(s) * tau[j];
+            for (int i = j + lane; i < m; i += 32) xc[i] -= s * v[i];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(HM_BT) hm_aca_kernel(const AcaLeaf *__restrict__ leaves, AcaGeom g, double eps,
+                                                       double *__restrict__ scratch, char *__restrict__ flags,
+                                                       int *__restrict__ rank_out)
+{
+    extern __shared__ __align__(16) double hm_sm[];
+    double *U = hm_sm;                          // k x k, column-major (G, then U)
+    double *W = U + HM_KMAX * HM_KMAX;          // k x k
+    double *tauA = W + HM_KMAX * HM_KMAX, *tauB = tauA + HM_KMAX, *alA = tauB + HM_KMAX, *alB = alA + HM_KMAX;
+    double *Sv = alB + HM_KMAX, *aq = Sv + HM_KMAX, *bq = aq + HM_KMAX, *cache = bq + HM_KMAX;
+    double *red = cache + HM_KMAX;              // 64 doubles: reductions
+    __shared__ int redi[HM_BT / 32];
+    __shared__ int ord[HM_KMAX];
+    __shared__ int s_i, s_k, s_done;
+    __shared__ double s_norm2;
+
+    const AcaLeaf L = leaves[blockIdx.x];
+    const int m = L.nr, n = L.nc;
+    double *A = scratch + L.soff, *B = A + (int64_t)m * HM_KMAX;
+    double *XA = B + (int64_t)n * HM_KMAX, *XB = XA + (int64_t)m * HM_KMAX;
+    char *rused = flags + L.foff, *cused = rused + m;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    auto ent = [&](int ii, int jj) { return aca_entry(g, g.perm[L.r0 + ii], g.perm[L.c0 + jj]); };
+
+    // ---- partial-pivot ACA ----
+    if (tid == 0) { s_i = 0; s_k = 0; s_done = 0; s_norm2 = 0.0; }
+    int zero_rows = 0;
+    int result = 0;
+    __syncthreads();
+    const int kcap = min(m, n);
+    while (true) {
+        const int k = s_k, is = s_i;
+        if (k >= kcap) { result = k; break; }
+        if (k >= HM_KMAX) { result = -1; break; }
+        if (tid == 0) rused[is] = 1;
+        for (int q = tid; q < k; q += HM_BT) cache[q] = A[(int64_t)q * m + is];
+        __syncthreads();
+        double *row = B + (int64_t)k * n;
+        double bv = 0.0;
+        int bj = -1;
+        for (int j = tid; j < n; j += HM_BT) {
+            double v = ent(is, j);
+            for (int q = 0; q < k; q++) v -= cache[q] * B[(int64_t)q * n + j];
+            row[j] = v;
+            if (!cused[j] && fabs(v) > bv) { bv = fabs(v); bj = j; }
+        }
+        double best;
+        int js;
+        hm_block_argmax(bv, bj, red, redi, best, js);
+        if (js < 0 || best <= 1e-300) {
+            // zero residual row: try another unused row
+            if (++zero_rows > 3) { result = k; break; }
+            __syncthreads();
+            if (tid == 0) {
+                int nxt = -1;
+                for (int i = 0; i < m; i++)
+                    if (!rused[i]) { nxt = i; break; }
+                s_i = nxt;
+            }
+            __syncthreads();
+            if (s_i < 0) { result = k; break; }
+            continue;
+        }
+        const double piv = row[js];
+        __syncthreads();
+        if (tid == 0) cused[js] = 1;
+        for (int q = tid; q < k; q += HM_BT) cache[q] = B[(int64_t)q * n + js];
+        __syncthreads();
+        for (int j = tid; j < n; j += HM_BT) row[j] /= piv;
+        double *col = A + (int64_t)k * m;
+        double bc = -1.0;
+        int bi = -1;
+        for (int i = tid; i < m; i += HM_BT) {
+            double v = ent(i, js);
+            for (int q = 0; q < k; q++) v -= cache[q] * A[(int64_t)q * m + i];
+            col[i] = v;
+        }
+        __syncthreads();
+        double la = 0.0, lb = 0.0;
+        for (int i = tid; i < m; i += HM_BT) {
+            la += col[i] * col[i];
+            if (!rused[i] && fabs(col[i]) > bc) { bc = fabs(col[i]); bi = i; }
+        }
+        for (int j = tid; j < n; j += HM_BT) lb += row[j] * row[j];
+        const double an = hm_block_sum(la, red);
+        const double bn = hm_block_sum(lb, red);
+        // a_q.a_k and b_q.b_k, one warp per q
+        for (int q = w; q < k; q += HM_BT / 32) {
+            double sa = 0.0, sb = 0.0;
+            for (int i = lane; i < m; i += 32) sa += A[(int64_t)q * m + i] * col[i];
+            for (int j = lane; j < n; j += 32) sb += B[(int64_t)q * n + j] * row[j];
+            sa = warp_sum(sa);
+            sb = warp_sum(sb);
+            if (lane == 0) { aq[q] = sa; bq[q] = sb; }
+        }
+        double nb;
+        int ni;
+        hm_block_argmax(bc, bi, red + 8, redi, nb, ni);   // next pivot row (after aq/bq: the sync inside orders them)
+        if (tid == 0) {
+            double cross = 0.0;
+            for (int q = 0; q < k; q++) cross += aq[q] * bq[q];
+            s_norm2 += 2.0 * cross + an * bn;
+            s_k = k + 1;
+            s_done = (sqrt(an * bn) <= eps * sqrt(fabs(s_norm2))) ? 1 : (ni < 0 ? 1 : 0);
+            s_i = ni;
+        }
+        __syncthreads();
+        if (s_done) { result = s_k; break; }
+    }
+    __syncthreads();
+    int k = result;
+    if (k <= 0) {
+        if (tid == 0) rank_out[blockIdx.x] = k;
+        return;
+    }
+    if (k >= min(m, n)) {
+        // no recompression: the ACA factors as they are
+        for (int64_t q = tid; q < (int64_t)m * k; q += HM_BT) XA[q] = A[q];
+        for (int64_t q = tid; q < (int64_t)n * k; q += HM_BT) XB[q] = B[q];
+        if (tid == 0) rank_out[blockIdx.x] = k;
+        return;
+    }
+    // ---- recompression ----
+    hm_qr(A, m, k, tauA, alA, red);
+    hm_qr(B, n, k, tauB, alB, red);
+    // G = R_A R_B^T into U (column-major), W = identity
+    for (int e = tid; e < k * k; e += HM_BT) {
+        const int r = e % k, c = e / k;
+        double sg = 0.0;
+        for (int q = max(r, c); q < k; q++) {
+            const double ra = (q == r) ? alA[r] : A[(int64_t)q * m + r];
+            const double rb = (q == c) ? alB[c] : B[(int64_t)q * n + c];
+            sg += ra * rb;
+        }
+        U[c * k + r] = sg;
+        W[c * k + r] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    // one-sided Jacobi: sweeps of k' - 1 rounds (k' = k rounded up to even;
+    // the extra column, if any, is a bye), k'/2 disjoint pairs per round
+    const int kp = (k + 1) & ~1;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0.0;
+        for (int rd = 0; rd < kp - 1; rd++) {
+            for (int pr = w; pr < kp / 2; pr += HM_BT / 32) {
+                // round-robin pairing: position 0 fixed, the others rotate
+                int a = (pr == 0) ? 0 : 1 + (pr - 1 + rd) % (kp - 1);
+                int b = 1 + (kp - 2 - pr + rd) % (kp - 1);
+                int p = min(a, b), q = max(a, b);
+                if (q >= k || p == q) continue;
+                double sa = 0.0, sb = 0.0, sg = 0.0;
+                for (int i = lane; i < k; i += 32) {
+                    const double up = U[p * k + i], uq = U[q * k + i];
+                    sa += up * up;
+                    sb += uq * uq;
+                    sg += up * uq;
+                }
+                sa = warp_sum(sa);
+                sb = warp_sum(sb);
+                sg = warp_sum(sg);
+                if (fabs(sg) <= 1e-300) continue;
+                off = fmax(off, fabs(sg) / sqrt(sa * sb));
+                const double zeta = (sb - sa) / (2.0 * sg);
+                const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                for (int i = lane; i < k; i += 32) {
+                    const double up = U[p * k + i], uq = U[q * k + i];
+                    U[p * k + i] = cs * up - sn * uq;
+                    U[q * k + i] = sn * up + cs * uq;
+                    const double wp = W[p * k + i], wq = W[q * k + i];
+                    W[p * k + i] = cs * wp - sn * wq;
+                    W[q * k + i] = sn * wp + cs * wq;
+                }
+            }
+            __syncthreads();
+        }
+        // largest off-diagonal measure of the sweep over the warps
+        off = fmax(off, __shfl_xor_sync(0xffffffffu, off, 16));
+        __syncthreads();
+        if (lane == 0) red[w] = off;
+        __syncthreads();
+        double mo = 0.0;
+        for (int q = 0; q < HM_BT / 32; q++) mo = fmax(mo, red[q]);
+        __syncthreads();
+        if (mo < 1e-15) break;
+    }
+    // singular values (column norms), normalised U, order by decreasing value
+    for (int j = w; j < k; j += HM_BT / 32) {
+        double sn = 0.0;
+        for (int i = lane; i < k; i += 32) sn += U[j * k + i] * U[j * k + i];
+        sn = sqrt(warp_sum(sn));
+        if (lane == 0) Sv[j] = sn;
+        __syncwarp();
+        if (sn > 0)
+            for (int i = lane; i < k; i += 32) U[j * k + i] /= sn;
+    }
+    __syncthreads();
+    for (int j = tid; j < k; j += HM_BT) {
+        int pos = 0;
+        for (int q = 0; q < k; q++) pos += (Sv[q] > Sv[j]) || (Sv[q] == Sv[j] && q < j);
+        ord[pos] = j;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int r = 0;
+        for (int i = 0; i < k; i++) {
+            r = i + 1;
+            if (Sv[ord[i]] <= eps * Sv[ord[0]]) break;
+        }
+        s_k = r;
+    }
+    __syncthreads();
+    const int r = s_k;
+    hm_apply_q(A, m, k, tauA, XA, r, [&](int c, int i) { return U[ord[c] * k + i] * Sv[ord[c]]; });
+    hm_apply_q(B, n, k, tauB, XB, r, [&](int c, int i) { return W[ord[c] * k + i]; });
+    if (tid == 0) rank_out[blockIdx.x] = r;
+}
+
+// Factors of rank r > 0 from the scratch X regions into the stored layout
+// (A'^T rank x lda and B'^T rank x ld, rank-major, padding left as it is):
+// dst offsets relative to the start of the batch's segment.
+struct AcaPlace {
+    int64_t foff, goff;   // A'^T and B'^T offsets in the segment
+    int lda, ld, rank;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) hm_aca_place_kernel(const AcaLeaf *__restrict__ leaves,
+                                                           const AcaPlace *__restrict__ place,
+                                                           const double *__restrict__ scratch, T *__restrict__ dst)
+{
+    const AcaLeaf L = leaves[blockIdx.x];
+    const AcaPlace P = place[blockIdx.x];
+    if (P.rank <= 0) return;
+    const double *XA = scratch + L.soff + (int64_t)(L.nr + L.nc) * HM_KMAX;
+    const double *XB = XA + (int64_t)L.nr * HM_KMAX;
+    for (int64_t e = threadIdx.x; e < (int64_t)P.rank * L.nr; e += blockDim.x) {
+        const int q = (int)(e / L.nr), i = (int)(e % L.nr);
+        dst[P.foff + (int64_t)q * P.lda + i] = (T)XA[(int64_t)q * L.nr + i];
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)P.rank * L.nc; e += blockDim.x) {
+        const int q = (int)(e / L.nc), j = (int)(e % L.nc);
+        dst[P.goff + (int64_t)q * P.ld + j] = (T)XB[(int64_t)q * L.nc + j];
+    }
+}
+
 // y(pos) = sum of the slots of row pos (fixed order), stored at the
 // original element index in the K.V result arrays (partials with one chunk).
 __global__ void hm_gather_kernel(int64_t Ntot, int ncomp, const int *__restrict__ inst_of,
