@@ -86,6 +86,7 @@ def load():
         "dfn_mlp_infer": (i32, [ctypes.POINTER(ctypes.c_float), i64, ctypes.POINTER(ctypes.c_float),
                                 ctypes.POINTER(ctypes.c_float)]),
         "dfn_set_graphs": (i32, [P, i32]),
+        "dfn_set_cg_form": (i32, [P, i32]),
         "dfn_autotune": (i32, [P, ctypes.c_void_p]),
         "dfn_kernel_batch": (i32, [P, dp, dp, dp]),
         "dfn_velocity": (i32, [P, dp]),
@@ -138,8 +139,10 @@ def autotune(lib, h, storage, pressure):
     if pressure == "cg":
         ms["pressure_cg_cta"] = t.ms[2]
         ms["pressure_cg_cluster"] = t.ms[3]
+        ms["pressure_cg_cta_smem"] = t.ms[5]
     else:
         ms["pressure_warp"] = t.ms[2]
         ms["pressure_thread"] = t.ms[3]
     return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
-            "cg_cluster": bool(t.cg_cluster), "cg_cluster_ctas": int(t.cg_cluster_ctas), "ms": ms}
+            "cg_form": ("cta", "cluster", "cta_smem")[t.cg_cluster], "cg_cluster_ctas": int(t.cg_cluster_ctas),
+            "ms": ms}

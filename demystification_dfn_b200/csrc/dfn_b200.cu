@@ -119,8 +119,10 @@ struct dfn_handle {
     int tc_variant = 0;                   // 0 persistent, 1 unit per CTA deepest ring, 2 unit per CTA 2-stage ring
     int sms = 148;                        // streaming multiprocessors of the device
     int pcl = 0, pcl_n = 0, pcl_max = 0;  // cluster CG: CTAs per cluster, largest range, clusters at once
-    int pcl_mode = -1;                    // -1: clusters when they all fit at once, 0: never, 1: always (autotuner)
+    int pcl_mode = -1;                    // -1: clusters when they all fit at once, 0: one CTA on global memory,
+                                          // 1: clusters, 2: one CTA with shared-memory vectors (autotuner)
     bool pcl_lean = false;                // x in global memory, M p recomputed (long ranges)
+    bool pcl_ok = false;                  // the shared-memory CG forms can be launched
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -333,7 +335,7 @@ static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl,
     cfg = cudaLaunchConfig_t{};
     cfg.gridDim = dim3(gx, gy);
     cfg.blockDim = dim3(PCL_THREADS);
-    cfg.dynamicSmemBytes = pcl_smem_bytes(n, lean);
+    cfg.dynamicSmemBytes = cl == 1 ? (size_t)PCL_SMEM_CAP : pcl_smem_bytes(n, lean);
     cfg.stream = stream;
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cl;
@@ -346,13 +348,14 @@ static void pcl_config(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int cl,
 static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys, double dt_explicit, int ninst)
 {
     const bool clusters = h->pcl > 0 && (h->pcl_mode == 1 || (h->pcl_mode < 0 && nsys * ninst <= h->pcl_max));
-    if (h->pressure == DFN_PRESSURE_CG && clusters) {
-        // few systems: one cluster of CTAs per system, vectors in shared memory
+    const int cl = h->pcl_mode == 2 ? 1 : (clusters ? h->pcl : 0);
+    if (h->pressure == DFN_PRESSURE_CG && cl > 0) {
+        // one cluster of cl CTAs per system, vectors in shared memory
         cudaLaunchConfig_t cfg;
         cudaLaunchAttribute at[1];
-        pcl_config(cfg, at, h->pcl, h->pcl_n, h->pcl_lean, (unsigned)(nsys * h->pcl), (unsigned)ninst, h->stream);
+        pcl_config(cfg, at, cl, h->pcl_n, h->pcl_lean, (unsigned)(nsys * cl), (unsigned)ninst, h->stream);
         CK(cudaLaunchKernelEx(&cfg, pressure_cg_cluster_kernel, h->pg, (const Inst *)h->inst, h->ctl, mask, kind,
-                              sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, h->pcl_lean ? 1 : 0));
+                              sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, h->pcl_lean ? 1 : 0, h->pcoef));
     } else if (h->pressure != DFN_PRESSURE_TRIDIAG) {
         dim3 grid((unsigned)nsys, (unsigned)ninst);
         pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
@@ -1338,6 +1341,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     // 16 roomy, 16 lean, 8 lean whose ranges fit in shared memory, taking
     // the first shape the device can schedule; systems under 2048 elements
     // keep the one-CTA solver
+    bool attrs_ok = false;
     if (h->pressure == DFN_PRESSURE_CG) {
         int64_t nmax = 0;
         for (int i = 0; i < count; i++) nmax = std::max<int64_t>(nmax, h->hinst[i].N);
@@ -1353,12 +1357,12 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
         // the attributes are per function, shared by every handle: set to
         // the largest values any handle may use
-        const bool attrs =
+        attrs_ok =
             cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
                 cudaSuccess &&
             cudaFuncSetAttribute(pressure_cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  PCL_SMEM_CAP) == cudaSuccess;
-        for (size_t q = 0; attrs && q < cand.size(); q++) {
+        for (size_t q = 0; attrs_ok && q < cand.size(); q++) {
             const Shape &sh = cand[q];
             const int n = (int)((nmax + sh.cl - 1) / sh.cl);
             int nc = 0;
@@ -1372,6 +1376,14 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
                 h->pcl_max = nc;
                 break;
             }
+        }
+        if (attrs_ok) {
+            // one CTA per system with shared-memory vectors (autotuner's choice)
+            int nc = 0;
+            cudaLaunchConfig_t cfg;
+            cudaLaunchAttribute at[1];
+            pcl_config(cfg, at, 1, 0, false, 1, 1, h->stream);
+            h->pcl_ok = cudaOccupancyMaxActiveClusters(&nc, pressure_cg_cluster_kernel, &cfg) == cudaSuccess && nc > 0;
         }
         cudaGetLastError();   // an unsupported shape leaves the one-CTA solver in place
     }
@@ -1451,18 +1463,29 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         r.gemv_impl = best;
     }
     r.tri_thread = h->tri_thread ? 1 : 0;
-    if (h->pressure == DFN_PRESSURE_CG && h->pcl > 0) {
-        for (int v = 0; v < 2; v++) {
+    if (h->pressure == DFN_PRESSURE_CG && h->pcl_ok) {
+        // one CTA on global memory -> ms[2], clusters -> ms[3] (when this
+        // handle has a cluster form), one CTA on shared memory -> ms[5]
+        double msv[3] = {0.0, 0.0, 0.0};
+        for (int v = 0; v < 3; v++) {
+            if (v == 1 && h->pcl == 0) continue;
             h->pcl_mode = v;
-            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, r.ms[2 + v]));
+            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, msv[v]));
         }
-        h->pcl_mode = r.ms[3] < r.ms[2] ? 1 : 0;
+        int best = 0;
+        for (int v = 1; v < 3; v++)
+            if (msv[v] > 0.0 && msv[v] < msv[best]) best = v;
+        h->pcl_mode = best;
+        r.ms[2] = msv[0];
+        r.ms[3] = msv[1];
+        r.ms[5] = msv[2];
     }
     r.cg_cluster_ctas = h->pressure == DFN_PRESSURE_CG ? h->pcl : 0;
-    r.cg_cluster = (h->pressure == DFN_PRESSURE_CG && h->pcl > 0 &&
-                    (h->pcl_mode == 1 || (h->pcl_mode < 0 && 5 * h->B <= h->pcl_max)))
-                       ? 1
-                       : 0;
+    r.cg_cluster = 0;
+    if (h->pressure == DFN_PRESSURE_CG) {
+        if (h->pcl_mode == 2) r.cg_cluster = 2;
+        else if (h->pcl > 0 && (h->pcl_mode == 1 || (h->pcl_mode < 0 && 5 * h->B <= h->pcl_max))) r.cg_cluster = 1;
+    }
     if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {
         for (int v = 0; v < 2; v++) {
             h->tri_thread = v == 1;
@@ -1484,6 +1507,21 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)
     CK(cudaSetDevice(h->dev));
     CK(cudaStreamSynchronize(h->stream));
     h->use_graphs = enable != 0;
+    drop_graph(h);
+    return DFN_OK;
+}
+
+int32_t dfn_set_cg_form(dfn_handle *h, int32_t form)
+{
+    if (!h) return DFN_ERR_ARG;
+    if (form < -1 || form > 2 || h->pressure != DFN_PRESSURE_CG || (form >= 1 && !h->pcl_ok) ||
+        (form == 1 && h->pcl == 0)) {
+        g_err = "CG form not available on this handle (CG pressure; 1 needs systems of 2048 elements or more)";
+        return DFN_ERR_ARG;
+    }
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->pcl_mode = form;
     drop_graph(h);
     return DFN_OK;
 }

@@ -1137,9 +1137,14 @@ __device__ int cg_solve_cluster(const PressParams &p, double dt, int64_t k0, int
 // with exact = 0. Instance i is split into ranges of ceil(N_i / CL)
 // elements (dynamic shared memory sized for the largest instance); lean:
 // x of system s in work + 24 eoff_i + 4 N_i s (the one-CTA solver's x).
+// With clusters of one CTA (launched with PCL_SMEM_CAP bytes) the layout is
+// chosen per system (roomy, lean, or, when even the lean layout does not
+// fit, the one-CTA solver on global memory: cg_system with the work vectors
+// and cached coefficients of pressure_cg_batch_kernel).
 __global__ void __launch_bounds__(PCL_THREADS, 1)
     pressure_cg_cluster_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl, int mask, int kind, int sys0,
-                               double dt_explicit, double *Ptemp, double *Pdot, double *work, int lean)
+                               double dt_explicit, double *Ptemp, double *Pdot, double *work, int lean,
+                               double *coef)
 {
     extern __shared__ __align__(16) double pcl_sm[];
     __shared__ double red[66];
@@ -1153,12 +1158,22 @@ __global__ void __launch_bounds__(PCL_THREADS, 1)
     const int sys = sys0 + (int)(blockIdx.x / ncl);
     const int64_t N = I.N;
     const int n = (int)((N + ncl - 1) / ncl);
-    const int64_t k0 = (int64_t)rank * n;
-    const int nk = (int)max((int64_t)0, min((int64_t)n, N - k0));
-    const PclVec v = pcl_vec(pcl_sm, n, lean != 0, work + 24 * I.eoff + (int64_t)sys * 4 * N + k0);
     StepCtl *c = ctl + i;
     if (threadIdx.x == 0) iters = 0;
     __syncthreads();
+    if (ncl == 1) {
+        if (pcl_smem_bytes(n, true) > (size_t)PCL_SMEM_CAP) {
+            double *x = work + 24 * I.eoff + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
+            cg_system(p, c, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
+                      Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, 0,
+                      coef + 18 * I.eoff + (int64_t)sys * 3 * N);
+            return;
+        }
+        lean = pcl_smem_bytes(n, false) > (size_t)PCL_SMEM_CAP ? 1 : 0;
+    }
+    const int64_t k0 = (int64_t)rank * n;
+    const int nk = (int)max((int64_t)0, min((int64_t)n, N - k0));
+    const PclVec v = pcl_vec(pcl_sm, n, lean != 0, work + 24 * I.eoff + (int64_t)sys * 4 * N + k0);
     double dt = sys_dt(c, kind, sys, dt_explicit);
     int ier = cg_solve_cluster(p, dt, k0, nk, n, v, red, &iters);
     int guard = 0;

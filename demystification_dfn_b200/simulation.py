@@ -97,6 +97,13 @@ class Simulation:
         pressure solve) on this handle's data and keep the fastest."""
         return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
 
+    def set_cg_form(self, form):
+        """CG pressure solves by "cta" (one CTA per system, global memory),
+        "cluster" (a thread-block cluster per system, shared memory),
+        "cta_smem" (one CTA per system, shared memory) or "default"."""
+        code = {"default": -1, "cta": 0, "cluster": 1, "cta_smem": 2}[form]
+        _lib.check(self.lib.dfn_set_cg_form(self.h, code), self.lib)
+
     def set_graphs(self, enable: bool):
         """Replay the solve loop's rounds as a CUDA graph (default) or launch
         every kernel on its own; results are identical."""

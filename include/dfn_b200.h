@@ -202,16 +202,18 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * unit per CTA with the deepest shared-memory ring (gemv_impl 1, ms[1]) or
  * with a 2-stage ring (two CTAs per SM; gemv_impl 2, ms[4], timed when it
  * differs from the deepest ring); all give identical results.
- * CG pressure (DFN_PRESSURE_CG) with systems of 2048 elements or more: the
- * stage systems of the batch solved by one CTA each (ms[2]) or by a cluster
- * of CTAs each (ms[3]); cg_cluster = 1 when the cluster form is kept,
- * cg_cluster_ctas = CTAs per cluster of this handle's cluster form (2 to
- * 16; 0 when it has none). The two differ in the order of the dot-product
- * sums (equal to rounding).
+ * CG pressure (DFN_PRESSURE_CG): the stage systems of the batch solved by one
+ * CTA each on global memory (ms[2]), by a cluster of CTAs each with the
+ * vectors in shared memory (ms[3]; handles with systems of 2048 elements or
+ * more) or by one CTA each with the vectors in shared memory (ms[5]; larger
+ * systems of the batch on global memory); cg_cluster = 0, 1 or 2 names the
+ * form kept, cg_cluster_ctas = CTAs per cluster of this handle's cluster
+ * form (2 to 16; 0 when it has none). The forms differ in the order of the
+ * dot-product sums (equal to rounding).
  * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
  * the short segments use threads once a launch has at least 16384 of them,
  * and the CG uses clusters when all of a launch's clusters fit on the GPU at
- * once. ms[5] is reserved (0). No counterpart in the reference. */
+ * once. No counterpart in the reference. */
 typedef struct dfn_tuning {
     int32_t gemv_impl;
     int32_t tri_thread;
@@ -229,6 +231,15 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
  * one by one so that each K.V launch is timed. No counterpart in the
  * reference (a host loop of subroutine calls). */
 int32_t dfn_set_graphs(dfn_handle *h, int32_t enable);
+/* Form of the CG pressure solves (DFN_PRESSURE_CG handles): -1 the default
+ * rule (clusters when a launch's clusters all fit on the GPU at once, else
+ * one CTA per system on global memory), 0 one CTA per system on global
+ * memory, 1 one thread-block cluster per system with shared-memory vectors
+ * (systems of 2048 elements or more), 2 one CTA per system with shared-memory
+ * vectors (systems too large for them on global memory). The forms agree to
+ * the solver tolerance. dfn_autotune sets the fastest. No counterpart in the
+ * reference. */
+int32_t dfn_set_cg_form(dfn_handle *h, int32_t form);
 /* A batch of independent networks in one handle (no counterpart in the
  * reference, which runs one network per process). All networks share the
  * fracture mode and the options; each keeps its own state, step size,

@@ -139,17 +139,20 @@ def test_autotune_keeps_results():
 
 def test_autotune_cg_cluster_choice_equal_to_rounding():
     """Networks of 2048 elements or more: the autotuner times the stage
-    pressure systems solved by one CTA each and by a cluster of CTAs each;
-    both forms stop at max|r| < tol_solver, so runs with either agree to the
-    solver tolerance (here after 6 steps: slip rate to 1e-6 relative)."""
+    pressure systems solved by one CTA each on global memory, by a cluster of
+    CTAs each and by one CTA each on shared memory; all stop at
+    max|r| < tol_solver, so runs with any of them agree to the solver
+    tolerance (here after 6 steps: slip rate to 1e-6 relative)."""
     ps = [networks.fault_network(n_faults=150, box=3000.0, seed=s, tol=1e-8) for s in (31, 32)]
     out = []
     for tune in (False, True):
         with Ensemble(ps, pressure="cg") as ens:
             if tune:
                 t = ens.autotune()
-                assert t["ms"]["pressure_cg_cta"] > 0 and t["ms"]["pressure_cg_cluster"] > 0
-                assert t["cg_cluster"] == (t["ms"]["pressure_cg_cluster"] < t["ms"]["pressure_cg_cta"])
+                ms = t["ms"]
+                assert ms["pressure_cg_cta"] > 0 and ms["pressure_cg_cluster"] > 0 and ms["pressure_cg_cta_smem"] > 0
+                best = min(("cta", "cluster", "cta_smem"), key=lambda f: ms["pressure_cg_" + f])
+                assert t["cg_form"] == best
             reps = ens.solve(n_steps=6)
             assert all(r["status"] == 0 for r in reps)
             out.append([ens.state(i) for i in range(len(ps))])
@@ -157,3 +160,26 @@ def test_autotune_cg_cluster_choice_equal_to_rounding():
         N = len(a["P"])
         assert abs(a["time"] - b["time"]) <= 1e-9 * a["time"]
         assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-6 * np.abs(a["Y"][:N]).max()
+
+
+def test_cg_forms_agree_on_an_uneven_batch():
+    """A batch of four ensemble networks of uneven size (some fit the shared
+    memory of one CTA, some do not and use the global-memory solver in the
+    same launch): every CG form gives the same run to the solver tolerance."""
+    ps = [networks.ensemble_member(s) for s in (3, 5, 9, 12)]
+    sizes = None
+    out = {}
+    for form in ("default", "cta", "cta_smem"):
+        with Ensemble(ps, pressure="cg") as ens:
+            sizes = ens.n_elements
+            ens.set_cg_form(form)
+            reps = ens.solve(n_steps=6)
+            assert all(r["status"] == 0 for r in reps)
+            out[form] = [ens.state(i) for i in range(len(ps))]
+    assert min(sizes) < 5700 < max(sizes)
+    for form in ("cta", "cta_smem"):
+        for a, b in zip(out["default"], out[form]):
+            N = len(a["P"])
+            assert abs(a["time"] - b["time"]) <= 1e-9 * a["time"]
+            assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-6 * np.abs(a["Y"][:N]).max()
+            assert np.abs(a["P"] - b["P"]).max() <= 1e-6 * np.abs(a["P"]).max()

@@ -95,15 +95,19 @@ def _cluster_case(case):
 
 @pytest.mark.parametrize("case", ["single4000", "net300", "net500"])
 @pytest.mark.parametrize("dt", [10.0, 3600.0, 86400.0])
-def test_pressure_cg_cluster_matches_oracle(case, dt):
-    """The cluster CG (vectors in shared memory, reductions across the CTAs
-    of a cluster) stops at the same criterion max|r| < tol_solver as the
-    reference CG: both are within 1e3 * tol_solver Pa of each other and of
-    the exact implicit step, or both report non-convergence."""
+@pytest.mark.parametrize("form", ["cluster", "cta_smem", "cta"])
+def test_pressure_cg_cluster_matches_oracle(case, dt, form):
+    """Each form of the CG (a cluster of CTAs with the vectors in shared
+    memory and reductions across the cluster; one CTA with the vectors in
+    shared memory, the lean layout for N = 5 748, the global-memory solver
+    for N = 10 215; one CTA on global memory) stops at the same criterion
+    max|r| < tol_solver as the reference CG: all are within 1e3 * tol_solver
+    Pa of it and of the exact implicit step, or all report non-convergence."""
     p = _cluster_case(case)
     o = Oracle(p)
     with Simulation(p, pressure="cg") as s:
         assert s.N >= 2048
+        s.set_cg_form(form)
         gP, gd, gi = s.compute_P(dt)
         oP, od, oi = o.compute_P(dt)
         assert gi == oi
