@@ -12,9 +12,10 @@
     python -m demystification_dfn_b200.profile_case tc_round [cg|tridiag]
         the same batch, six solve rounds launched one by one (launch list of
         a round: GEMM, pressure, friction, step control).
-    python -m demystification_dfn_b200.profile_case hmatrix_kv
-        the 4000-fault network (N = 81 750) as an H-matrix (leaf 64, eta 2,
-        ACA 1e-6, FP32 factors): three K.V launches (three kernels each).
+    python -m demystification_dfn_b200.profile_case hmatrix_kv [n_faults box_m]
+        the 4000-fault network in 20 km x 20 km (N = 81 750; or n_faults in a
+        box_m square) as an H-matrix (leaf 64, eta 2, ACA 1e-6, FP32
+        factors): three K.V launches (several kernels each).
     python -m demystification_dfn_b200.profile_case hmatrix_autotune
         the same network with CG pressure: the autotuner's timing of the
         stage pressure systems by one CTA each and by a cluster of CTAs each
@@ -76,7 +77,9 @@ def main(argv):
     elif case == "hmatrix_kv":
         from .simulation import Simulation
 
-        p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
+        nf = int(argv[1]) if len(argv) > 1 else 4000
+        box = float(argv[2]) if len(argv) > 2 else 20000.0
+        p = networks.fault_network(n_faults=nf, box=box, seed=0, kernel="hmatrix", tol=1e-6)
         e = Simulation(p, storage="fp32", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
         rng = np.random.default_rng(0)
         for _ in range(3):
