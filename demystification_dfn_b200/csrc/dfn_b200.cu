@@ -123,6 +123,10 @@ struct dfn_handle {
                                           // 1: clusters, 2: one CTA with shared-memory vectors (autotuner)
     bool pcl_lean = false;                // x in global memory, M p recomputed (long ranges)
     bool pcl_ok = false;                  // the shared-memory CG forms can be launched
+    int64_t ncross = 0;                   // fault crossings over the batch
+    int64_t *xptr = nullptr;              // [Ntot + 1] crossing rows of the pressure system
+    XCon *xcon = nullptr;
+    int64_t *xrows = nullptr, *xrows_ptr = nullptr;
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -358,9 +362,13 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
                               sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, h->pcl_lean ? 1 : 0, h->pcoef));
     } else if (h->pressure != DFN_PRESSURE_TRIDIAG) {
         dim3 grid((unsigned)nsys, (unsigned)ninst);
-        pressure_cg_batch_kernel<<<grid, 1024, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit,
-                                                               h->Ptemp, h->Pdot_s, h->pwork,
-                                                               h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0, h->pcoef);
+        const int exact = h->pressure == DFN_PRESSURE_CG_EXACT ? 1 : 0;
+        if (h->ncross > 0)
+            pressure_cg_batch_kernel<true><<<grid, 1024, 0, h->stream>>>(
+                h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, exact, h->pcoef);
+        else
+            pressure_cg_batch_kernel<false><<<grid, 1024, 0, h->stream>>>(
+                h->pg, h->inst, h->ctl, mask, kind, sys0, dt_explicit, h->Ptemp, h->Pdot_s, h->pwork, exact, h->pcoef);
     } else {
         const int64_t nshort = (ninst == h->B) ? h->nshort : h->nshort0;
         const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
@@ -641,6 +649,81 @@ struct LrSegment {
     int64_t start, len;   // values of the low-rank region
     DevBuf buf;
 };
+
+// find_fault_crossing (src/initialisation.f90:279-344) for every network
+// of the batch: node pairs of two faults closer than 0.01 times the smaller
+// of the two faults' smallest element length. Each crossing couples the (up
+// to) two elements around the node on one fault with those on the other;
+// the pressure rows store, in crossing order, each coupling's partner
+// elements and harmonic-mean permeabilities (XCon). Returns the crossings.
+static int64_t build_crossings(const dfn_problem *probs, int count, const std::vector<Inst> &hinst,
+                               std::vector<int64_t> &xptr, std::vector<XCon> &xcon)
+{
+    int64_t Ntot = 0;
+    for (int i = 0; i < count; i++) Ntot += hinst[i].N;
+    std::vector<std::vector<XCon>> rows((size_t)Ntot);
+    int64_t ncross = 0;
+    auto harm = [](double k1, double k2) { return (k1 + k2 > 0.0) ? 2.0 * k1 * k2 / (k1 + k2) : 0.0; };
+    for (int i = 0; i < count; i++) {
+        const dfn_problem &p = probs[i];
+        const int64_t F = p.nb_fault, e0 = hinst[i].eoff;
+        const double *nd = p.node, *perm = p.permeability;
+        std::vector<int64_t> first((size_t)F), nel((size_t)F);
+        std::vector<double> minds((size_t)F);
+        int64_t cnt = 0;
+        for (int64_t f = 0; f < F; f++) {
+            first[f] = cnt;
+            nel[f] = p.fault_nb_element[f];
+            double m = INFINITY;
+            for (int64_t e = cnt; e < cnt + nel[f]; e++) {
+                const double dx = nd[2 * e + 2] - nd[2 * e], dy = nd[2 * e + 3] - nd[2 * e + 1];
+                m = std::min(m, std::sqrt(dx * dx + dy * dy));
+            }
+            minds[f] = m;
+            cnt += nel[f] + 1;
+        }
+        for (int64_t f1 = 0; f1 < F; f1++)
+            for (int64_t f2 = f1 + 1; f2 < F; f2++) {
+                const double thr = 0.01 * std::min(minds[f1], minds[f2]);
+                for (int64_t a = 0; a <= nel[f1]; a++) {
+                    const double *p1 = nd + 2 * (first[f1] + a);
+                    for (int64_t b = 0; b <= nel[f2]; b++) {
+                        const double *p2 = nd + 2 * (first[f2] + b);
+                        const double d = std::sqrt((p1[0] - p2[0]) * (p1[0] - p2[0]) + (p1[1] - p2[1]) * (p1[1] - p2[1]));
+                        if (!(d < thr)) continue;
+                        ncross++;
+                        const int64_t e1[2] = {a >= 1 ? first[f1] + a - 1 : -1, a < nel[f1] ? first[f1] + a : -1};
+                        const int64_t e2[2] = {b >= 1 ? first[f2] + b - 1 : -1, b < nel[f2] ? first[f2] + b : -1};
+                        for (int side = 0; side < 2; side++)
+                            for (int j = 0; j < 2; j++) {
+                                const int64_t row = side == 0 ? e1[j] : e2[j];
+                                if (row < 0) continue;
+                                const int64_t *o = side == 0 ? e2 : e1;
+                                XCon x;
+                                x.a = o[0] >= 0 ? o[0] : row;
+                                x.b = o[1] >= 0 ? o[1] : row;
+                                // harmonic means with the first fault's element first
+                                if (side == 0) {
+                                    x.kl = o[0] >= 0 ? harm(perm[row], perm[o[0]]) : 0.0;
+                                    x.kr = o[1] >= 0 ? harm(perm[row], perm[o[1]]) : 0.0;
+                                } else {
+                                    x.kl = o[0] >= 0 ? harm(perm[o[0]], perm[row]) : 0.0;
+                                    x.kr = o[1] >= 0 ? harm(perm[o[1]], perm[row]) : 0.0;
+                                }
+                                rows[(size_t)(e0 + row)].push_back(x);
+                            }
+                    }
+                }
+            }
+    }
+    xptr.assign((size_t)Ntot + 1, 0);
+    xcon.clear();
+    for (int64_t k = 0; k < Ntot; k++) {
+        xcon.insert(xcon.end(), rows[(size_t)k].begin(), rows[(size_t)k].end());
+        xptr[(size_t)k + 1] = (int64_t)xcon.size();
+    }
+    return ncross;
+}
 
 static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_options &opt)
 {
@@ -928,7 +1011,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
@@ -1335,6 +1418,43 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     PressGlobal &pg = h->pg;
     pg.P = h->P; pg.permx = h->permx; pg.ds = h->ds; pg.src_fault = h->src_fault; pg.src_elem = h->src_elem;
     pg.src_Q = h->src_Q; pg.src_tb = h->src_tb; pg.src_te = h->src_te;
+    pg.xptr = nullptr;
+    pg.xcon = nullptr;
+    pg.xrows = nullptr;
+    pg.xrows_ptr = nullptr;
+    {
+        std::vector<int64_t> xp;
+        std::vector<XCon> xc;
+        h->ncross = build_crossings(probs, count, h->hinst, xp, xc);
+        if (h->ncross > 0) {
+            if (h->pressure == DFN_PRESSURE_TRIDIAG) {
+                g_err = "the network has fault crossings, which couple pressure rows outside the three diagonals: "
+                        "use a CG pressure solver";
+                dfn_destroy(h);
+                return DFN_ERR_ARG;
+            }
+            CKC(cudaMalloc((void **)&h->xptr, sizeof(int64_t) * xp.size()));
+            CKC(cudaMemcpy(h->xptr, xp.data(), sizeof(int64_t) * xp.size(), cudaMemcpyHostToDevice));
+            CKC(cudaMalloc((void **)&h->xcon, sizeof(XCon) * std::max<size_t>(xc.size(), 1)));
+            if (!xc.empty()) CKC(cudaMemcpy(h->xcon, xc.data(), sizeof(XCon) * xc.size(), cudaMemcpyHostToDevice));
+            // per network, its rows that have crossings (network-local indices)
+            std::vector<int64_t> rows, rptr(1, 0);
+            for (int i = 0; i < count; i++) {
+                const Inst &I = h->hinst[i];
+                for (int64_t k = 0; k < I.N; k++)
+                    if (xp[(size_t)(I.eoff + k) + 1] > xp[(size_t)(I.eoff + k)]) rows.push_back(k);
+                rptr.push_back((int64_t)rows.size());
+            }
+            CKC(cudaMalloc((void **)&h->xrows, sizeof(int64_t) * std::max<size_t>(rows.size(), 1)));
+            if (!rows.empty()) CKC(cudaMemcpy(h->xrows, rows.data(), sizeof(int64_t) * rows.size(), cudaMemcpyHostToDevice));
+            CKC(cudaMalloc((void **)&h->xrows_ptr, sizeof(int64_t) * rptr.size()));
+            CKC(cudaMemcpy(h->xrows_ptr, rptr.data(), sizeof(int64_t) * rptr.size(), cudaMemcpyHostToDevice));
+            pg.xptr = h->xptr;
+            pg.xcon = h->xcon;
+            pg.xrows = h->xrows;
+            pg.xrows_ptr = h->xrows_ptr;
+        }
+    }
 
     // cluster CG (CG mode): the fewest CTAs per cluster (2 to 16) whose
     // ranges hold at most PCL_NTARGET elements, else the first of 8 roomy,
@@ -1342,7 +1462,9 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     // the first shape the device can schedule; systems under 2048 elements
     // keep the one-CTA solver
     bool attrs_ok = false;
-    if (h->pressure == DFN_PRESSURE_CG) {
+    // (networks with fault crossings keep the one-CTA solver: their rows
+    // couple elements of other faults, anywhere in the system)
+    if (h->pressure == DFN_PRESSURE_CG && h->ncross == 0) {
         int64_t nmax = 0;
         for (int i = 0; i < count; i++) nmax = std::max<int64_t>(nmax, h->hinst[i].N);
         struct Shape { int cl; bool lean; };
@@ -1510,6 +1632,8 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)
     drop_graph(h);
     return DFN_OK;
 }
+
+int64_t dfn_crossing_count(const dfn_handle *h) { return h ? h->ncross : -1; }
 
 int32_t dfn_set_cg_form(dfn_handle *h, int32_t form)
 {

@@ -561,6 +561,23 @@ struct PressParams {
     const int64_t *src_elem;    // 0-based global element index
     const double *src_Q, *src_tb, *src_te;
     const double *ctl_time;     // &ctl->time
+    // fault crossings (null when the network has none): contributions of
+    // row k are xcon[xptr[k] .. xptr[k+1]); xrows lists the nxrows rows
+    // that have any
+    const int64_t *xptr;
+    const struct XCon *xcon;
+    const int64_t *xrows;
+    int64_t nxrows;
+};
+
+// One fault-crossing contribution to a row of the pressure system: partner
+// elements a and b (instance-local; the row itself where the partner is
+// absent) and the harmonic means kl, kr of the permeabilities (0 where
+// absent). Built on the host as find_fault_crossing
+// (src/initialisation.f90:279-344) finds the crossings.
+struct XCon {
+    int64_t a, b;
+    double kl, kr;
 };
 
 // kx*dt/(porosity*dyn_viscosity*(fluid_comp+rock_comp)*ds**2)
@@ -587,6 +604,36 @@ __device__ __forceinline__ void prow(const PressParams &p, int64_t k, double dt,
         A2 = add_(1.0, pcoef(p, add_(p.permx[k], p.permx[k + 1]), dt, p.ds[k]));
         A3 = -pcoef(p, p.permx[k + 1], dt, p.ds[k + 1]);
     }
+}
+
+// Fault-crossing coupling of row k (src/fluid_diffusion.f90:213-295,
+// 338-405, with the element length of the row itself in every coefficient
+// and every term divided by the diagonal): the diagonal gains
+// kl dt/(c ds_k^2) + kr dt/(c ds_k^2) per contribution, the product gains
+// (-cl v_a + (cl + cr) v_k - cr v_b) / diag_k, both in contribution order
+// after the row's own stencil.
+__device__ __forceinline__ bool prow_x(const PressParams &p, int64_t k)
+{
+    return p.xptr != nullptr && p.xptr[k + 1] > p.xptr[k];
+}
+__device__ __forceinline__ double pdiag_x(const PressParams &p, int64_t k, double dt, double A2)
+{
+    for (int64_t c = p.xptr[k]; c < p.xptr[k + 1]; c++) {
+        const XCon x = p.xcon[c];
+        A2 = add_(add_(A2, pcoef(p, x.kl, dt, p.ds[k])), pcoef(p, x.kr, dt, p.ds[k]));
+    }
+    return A2;
+}
+__device__ __forceinline__ double pterms_x(const PressParams &p, int64_t k, double dt, double dg, const double *v,
+                                           double m)
+{
+    for (int64_t c = p.xptr[k]; c < p.xptr[k + 1]; c++) {
+        const XCon x = p.xcon[c];
+        const double cl = pcoef(p, x.kl, dt, p.ds[k]), cr = pcoef(p, x.kr, dt, p.ds[k]);
+        const double t = add_(add_(mul_(-cl, v[x.a]), mul_(add_(cl, cr), v[k])), mul_(-cr, v[x.b]));
+        m = add_(m, __ddiv_rn(t, dg));
+    }
+    return m;
 }
 
 // Source contribution (before division by diag) at element k for step dt:
@@ -706,6 +753,21 @@ __device__ __forceinline__ double pmatvec_row(const PressParams &p, int64_t k, d
     return __ddiv_rn(m, A2);
 }
 
+// Row k of a row with fault-crossing contributions, from scratch: its own
+// stencil over the diagonal that includes the crossings, then the crossing
+// terms (the reference's order).
+__device__ __forceinline__ double pmatvec_row_x(const PressParams &p, int64_t k, double dt, const double *v)
+{
+    double A1, A2, A3;
+    prow(p, k, dt, A1, A2, A3);
+    const double dg = pdiag_x(p, k, dt, A2);
+    double m;
+    if (k == 0) m = add_(mul_(A2, v[0]), mul_(A3, v[1]));
+    else if (k == p.N - 1) m = add_(mul_(A1, v[k - 1]), mul_(A2, v[k]));
+    else m = add_(add_(mul_(A1, v[k - 1]), mul_(A2, v[k])), mul_(A3, v[k + 1]));
+    return pterms_x(p, k, dt, dg, v, __ddiv_rn(m, dg));
+}
+
 // The same row with the coefficients of prow taken from a cache (identical
 // operands and order, so identical results).
 __device__ __forceinline__ double pmatvec_row_c(int64_t k, int64_t N, double A1, double A2, double A3, const double *v)
@@ -771,6 +833,10 @@ __device__ __forceinline__ double seq_dot(const double *a, const double *b, int6
 // during a solve, are computed once into cf, and the residual's sum of
 // squares and max-norm share one reduction (red: 66 doubles); the iterates
 // are the same as without.
+// XC: the network has fault crossings (rows with crossing terms are
+// recomputed after the plain stencil pass; instantiated only for such
+// handles).
+template <bool XC>
 __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, double *pv, double *Mp, double *red,
                         long long *iters, int exact, double *cf = nullptr)
 {
@@ -794,6 +860,25 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
         lmax = fmax(lmax, fabs(rk));
         lrr += rk * rk;
     }
+    if constexpr (XC) {
+        // rows with fault crossings, from scratch, by the thread that owns
+        // them; then the reductions over the corrected residual
+        for (int64_t q = 0; q < p.nxrows; q++) {
+            const int64_t k = p.xrows[q];
+            if (k % nt != tid) continue;
+            double A1, A2, A3;
+            prow(p, k, dt, A1, A2, A3);
+            const double rk = add_(pb1(p, k, dt, pdiag_x(p, k, dt, A2)), -pmatvec_row_x(p, k, dt, p.P));
+            r[k] = rk;
+            pv[k] = rk;
+        }
+        lmax = 0.0;
+        lrr = 0.0;
+        for (int64_t k = tid; k < N; k += nt) {
+            lmax = fmax(lmax, fabs(r[k]));
+            lrr += r[k] * r[k];
+        }
+    }
     double errmax = block_max(lmax, red) / p.tol;
     long long it = 0;
     // rr carried between iterations: sum(rk**2) of iteration i+1 equals
@@ -809,6 +894,16 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
                                           : pmatvec_row_s(k, N, c1[k], c3[k], pv));
             Mp[k] = m;
             lpap += pv[k] * m;
+        }
+        if constexpr (XC) {
+            // rows with fault crossings, from scratch, by their owner thread
+            for (int64_t q = 0; q < p.nxrows; q++) {
+                const int64_t k = p.xrows[q];
+                if (k % nt != tid) continue;
+                const double m = pmatvec_row_x(p, k, dt, pv);
+                lpap += pv[k] * (m - Mp[k]);
+                Mp[k] = m;
+            }
         }
         const double pap = exact ? seq_dot(pv, Mp, N, red) : block_sum(lpap, red);
         const double alpha = rr / pap;
@@ -844,20 +939,21 @@ __device__ int cg_solve(const PressParams &p, double dt, double *x, double *r, d
 
 // One system of the reference CG for one instance (whole CTA), shared by
 // the batched solver and the allocation-free entry point.
+template <bool XC = false>
 __device__ void cg_system(const PressParams &p, StepCtl *ctl, int kind, int sys, double dt_explicit, double *Pt,
                           double *Pd, double *x, double *r, double *pv, double *Mp, double *red, long long *iters,
                           int exact, double *cf = nullptr)
 {
     const int64_t N = p.N;
     double dt = sys_dt(ctl, kind, sys, dt_explicit);
-    int ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact, cf);
+    int ier = cg_solve<XC>(p, dt, x, r, pv, Mp, red, iters, exact, cf);
     if (kind == 0) {
         // probe: src/solver.f90:81-92, halve t_try until the solve converges
         int guard = 0;
         while (ier == 1 && guard < 1100) {
             dt = dt / 2.0;
             guard++;
-            ier = cg_solve(p, dt, x, r, pv, Mp, red, iters, exact, cf);
+            ier = cg_solve<XC>(p, dt, x, r, pv, Mp, red, iters, exact, cf);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -921,6 +1017,9 @@ struct PressGlobal {
     const double *P, *permx, *ds;
     const int64_t *src_fault, *src_elem;   // src_elem: 0-based within the instance
     const double *src_Q, *src_tb, *src_te;
+    const int64_t *xptr;                   // [Ntot + 1] crossing rows (null: no crossings)
+    const XCon *xcon;
+    const int64_t *xrows, *xrows_ptr;      // rows with crossings of instance i: xrows[xrows_ptr[i] ..)
 };
 
 __device__ __forceinline__ PressParams press_params(const PressGlobal &g, const Inst &I, int i, const StepCtl *ctl)
@@ -931,11 +1030,16 @@ __device__ __forceinline__ PressParams press_params(const PressGlobal &g, const 
     p.nsrc = I.nsrc; p.src_fault = g.src_fault + I.soff; p.src_elem = g.src_elem + I.soff;
     p.src_Q = g.src_Q + I.soff; p.src_tb = g.src_tb + I.soff; p.src_te = g.src_te + I.soff;
     p.ctl_time = &ctl[i].time;
+    p.xptr = g.xptr ? g.xptr + I.eoff : nullptr;
+    p.xcon = g.xcon;
+    p.xrows = g.xptr ? g.xrows + g.xrows_ptr[i] : nullptr;
+    p.nxrows = g.xptr ? g.xrows_ptr[i + 1] - g.xrows_ptr[i] : 0;
     return p;
 }
 
 // Batched CG: CTA (system s, instance i). Work of instance i: 24*eoff, then
 // 4*N_i per system; outputs Ptemp/Pdot at 6*eoff + sys*N_i.
+template <bool XC>
 __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
                                                                  int mask, int kind, int sys0, double dt_explicit,
                                                                  double *Ptemp, double *Pdot, double *work, int exact,
@@ -952,9 +1056,9 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
     double *x = work + 24 * I.eoff + (int64_t)sys * 4 * N, *r = x + N, *pv = r + N, *Mp = pv + N;
     if (threadIdx.x == 0) iters = 0;
     __syncthreads();
-    cg_system(p, ctl + i, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
-              Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact,
-              coef + 18 * I.eoff + (int64_t)sys * 3 * N);
+    cg_system<XC>(p, ctl + i, kind, sys, dt_explicit, Ptemp + 6 * I.eoff + (int64_t)sys * N,
+                  Pdot + 6 * I.eoff + (int64_t)sys * N, x, r, pv, Mp, red, &iters, exact,
+                  coef + 18 * I.eoff + (int64_t)sys * 3 * N);
 }
 
 // ---------------------------------------------------------------------------

@@ -92,6 +92,45 @@ def single_fault(n_el=4000, length=40e3, mode="modeII", a=0.007, b=0.005, Dc=4e-
     return p
 
 
+def crossing_pair(n_el=100, length=1000.0, angle_deg=60.0, mode="modeII", shift=0.0, P1=1e6, q_kgs=0.0,
+                  permeability=1e-13, tol=1e-8, **kw):
+    """Two straight faults of n_el elements (n_el even) crossing at their
+    middle nodes (a fault crossing in the sense of find_fault_crossing,
+    src/initialisation.f90:279-344): fault 1 along x, fault 2 at angle_deg,
+    moved by ``shift`` metres along y (shift 0: the middle nodes coincide).
+    Fault 1 starts at pore pressure P1, fault 2 at 0."""
+    if n_el % 2:
+        raise ValueError("n_el must be even (the faults cross at their middle nodes)")
+    p = single_fault(n_el=n_el, length=length, mode=mode, q_kgs=q_kgs, permeability=permeability, tol=tol,
+                     name="crossing_pair", **kw)
+    base = p.faults[0]
+    q = DemystiFicatioN(2)
+    q.hyperparameter = p.hyperparameter
+    q.hyperparameter.nb_fault = 2
+    q.material_loading = p.material_loading
+    th = np.deg2rad(angle_deg)
+    s = np.linspace(-length / 2, length / 2, n_el + 1)
+    for i, f in enumerate(q.faults):
+        f.nb_element = n_el
+        for name in ("a", "b", "Dc", "f0", "V0", "sigmaN", "V", "theta", "permeability"):
+            getattr(f, name)[:] = getattr(base, name)
+        f.P[:] = P1 if i == 0 else 0.0
+        if i == 0:
+            f.node[0, :] = s
+            f.node[1, :] = 0.0
+        else:
+            f.node[0, :] = s * np.cos(th)
+            f.node[1, :] = s * np.sin(th) + shift
+    if q_kgs:
+        f0 = q.faults[0]
+        f0.nb_source = 1
+        f0.Q[:] = base.Q
+        f0.t_injection_beg[:] = base.t_injection_beg
+        f0.t_injection_end[:] = base.t_injection_end
+        f0.index_injection[:] = base.index_injection
+    return q
+
+
 def _seg_dist(p1, p2, q1, q2):
     """Minimum distance between segment p1-p2 and segments q1-q2 (arrays)."""
     def pt_seg(p, a, b):

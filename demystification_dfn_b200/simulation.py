@@ -97,6 +97,11 @@ class Simulation:
         pressure solve) on this handle's data and keep the fastest."""
         return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
 
+    @property
+    def crossing_count(self):
+        """Fault crossings that couple the pressure of the networks."""
+        return int(self.lib.dfn_crossing_count(self.h))
+
     def set_cg_form(self, form):
         """CG pressure solves by "cta" (one CTA per system, global memory),
         "cluster" (a thread-block cluster per system, shared memory),

@@ -57,9 +57,18 @@ enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_B
  * dot products (systems of 2048 elements or more, when a launch has few of
  * them, are solved by a cluster of 2 to 16 CTAs holding the vectors in shared
  * memory: a tree of another shape, so such a network's results can differ
- * in rounding between a batch and a handle of its own); DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
+ * in rounding between a batch and a handle of its own; networks with fault
+ * crossings always use one CTA per system); DFN_PRESSURE_CG_EXACT sums them sequentially as the reference
  * does, reproducing its rounding and iteration counts bit for bit (slower
- * for large N); DFN_PRESSURE_TRIDIAG solves the same implicit step exactly. */
+ * for large N); DFN_PRESSURE_TRIDIAG solves the same implicit step exactly
+ * (networks without fault crossings: dfn_create rejects the others).
+ * Fault crossings (node pairs of two faults closer than 0.01 times the
+ * smaller of their smallest element lengths, as find_fault_crossing,
+ * src/initialisation.f90:279-344) couple the pressure of the elements around
+ * the crossing node (src/fluid_diffusion.f90:213-295, 338-405), with every
+ * coefficient using its own row's element length and every term divided by
+ * the diagonal (the reference uses ds(1) and a stale ds(k-1), and divides
+ * one row by the element index). */
 enum { DFN_PRESSURE_CG = 0, DFN_PRESSURE_TRIDIAG = 1, DFN_PRESSURE_CG_EXACT = 2 };
 
 /*
@@ -252,6 +261,8 @@ int32_t dfn_batch_size(const dfn_handle *h);
 int32_t dfn_destroy(dfn_handle *h);
 int32_t dfn_set_stream(dfn_handle *h, void *cuda_stream);
 int64_t dfn_nb_element(const dfn_handle *h);
+/* Fault crossings found over the batch (see the pressure solver notes). */
+int64_t dfn_crossing_count(const dfn_handle *h);
 /* Bytes of stored kernel matrices (K.V algorithmic bytes per evaluation). */
 int64_t dfn_kernel_bytes(const dfn_handle *h);
 

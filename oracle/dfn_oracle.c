@@ -54,6 +54,11 @@ typedef struct orc {
     /* counters */
     int64_t cg_iters, rhs_evals, attempts, rejected, halvings, stage_noconv;
     int last_status;
+    /* fault crossings: per element row, xptr[k]..xptr[k+1] contributions
+     * (partner elements xa, xb; harmonic permeabilities xkl, xkr) */
+    int64_t ncross, nxc;
+    int64_t *xptr, *xa, *xb;
+    double *xkl, *xkr;
 } orc;
 
 static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
@@ -96,6 +101,93 @@ static void orc_ini_value(orc *o)
     for (int64_t k = 1; k < N; k++)
         o->permx[k] = 2.0 * o->perm[k - 1] * o->perm[k] / (o->perm[k - 1] + o->perm[k]);
 }
+
+/* find_fault_crossing (src/initialisation.f90:279-344): node pairs of two
+ * faults closer than 0.01 * the smaller of the two faults' smallest element
+ * length. Each crossing couples the (up to) two elements around the node on
+ * one fault with those on the other (src/fluid_diffusion.f90:213-295,
+ * 338-405), here with the corrections of that model: every coefficient uses
+ * the element length of its own row (the reference uses ds(1) in the
+ * diagonal and a stale ds(k-1) in the product), every row divides by the
+ * diagonal (one reference row divides by the element index), and elements
+ * outside the fault (fake elements, or none before the first fault) are not
+ * coupled. Contributions of a row are kept in crossing order, each crossing
+ * updating its rows in the order element1(node-1), element1(node),
+ * element2(node-1), element2(node). */
+static double orc_harm(double k1, double k2) { return (k1 + k2 > 0.0) ? 2.0 * k1 * k2 / (k1 + k2) : 0.0; }
+
+static void orc_find_crossings(orc *o)
+{
+    int64_t N = o->N, F = o->F;
+    double *minds = (double *)xcalloc(F, 8);
+    for (int64_t f = 0; f < F; f++) {
+        double m = INFINITY;
+        for (int64_t e = 0; e < o->fault_n[f]; e++) m = fmin(m, o->ds[o->fault_first[f] + e]);
+        minds[f] = m;
+    }
+    /* pass 1: crossings; pass 2: contributions per row */
+    int64_t cap = 0, n = 0;
+    int64_t *cr = NULL;   /* (f1, f2, a, b) with a, b 0-based local nodes */
+    for (int64_t f1 = 0; f1 < F; f1++)
+        for (int64_t f2 = f1 + 1; f2 < F; f2++) {
+            double thr = 0.01 * fmin(minds[f1], minds[f2]);
+            for (int64_t a = 0; a <= o->fault_n[f1]; a++) {
+                const double *p1 = o->node + 2 * (o->fault_first[f1] + a);
+                for (int64_t b = 0; b <= o->fault_n[f2]; b++) {
+                    const double *p2 = o->node + 2 * (o->fault_first[f2] + b);
+                    double d = sqrt((p1[0] - p2[0]) * (p1[0] - p2[0]) + (p1[1] - p2[1]) * (p1[1] - p2[1]));
+                    if (!(d < thr)) continue;
+                    if (n == cap) { cap = cap ? 2 * cap : 16; cr = (int64_t *)realloc(cr, sizeof(int64_t) * 4 * cap); }
+                    cr[4 * n] = f1; cr[4 * n + 1] = f2; cr[4 * n + 2] = a; cr[4 * n + 3] = b;
+                    n++;
+                }
+            }
+        }
+    o->ncross = n;
+    /* rows and partners per crossing: element left (a-1) and right (a) of
+     * the node, -1 where outside the fault */
+    int64_t *rows = (int64_t *)xcalloc(4 * n, 8), *pa = (int64_t *)xcalloc(4 * n, 8), *pb = (int64_t *)xcalloc(4 * n, 8);
+    double *kl = (double *)xcalloc(4 * n, 8), *kr = (double *)xcalloc(4 * n, 8);
+    int64_t m = 0;
+    for (int64_t c = 0; c < n; c++) {
+        int64_t f1 = cr[4 * c], f2 = cr[4 * c + 1], a = cr[4 * c + 2], b = cr[4 * c + 3];
+        int64_t e1[2] = {a >= 1 ? o->fault_first[f1] + a - 1 : -1, a < o->fault_n[f1] ? o->fault_first[f1] + a : -1};
+        int64_t e2[2] = {b >= 1 ? o->fault_first[f2] + b - 1 : -1, b < o->fault_n[f2] ? o->fault_first[f2] + b : -1};
+        for (int side = 0; side < 2; side++)
+            for (int j = 0; j < 2; j++) {
+                int64_t row = side == 0 ? e1[j] : e2[j];
+                if (row < 0) continue;
+                const int64_t *other = side == 0 ? e2 : e1;
+                rows[m] = row;
+                pa[m] = other[0] >= 0 ? other[0] : row;
+                pb[m] = other[1] >= 0 ? other[1] : row;
+                /* harmonic means with the fault-1 element first */
+                if (side == 0) {
+                    kl[m] = other[0] >= 0 ? orc_harm(o->perm[row], o->perm[other[0]]) : 0.0;
+                    kr[m] = other[1] >= 0 ? orc_harm(o->perm[row], o->perm[other[1]]) : 0.0;
+                } else {
+                    kl[m] = other[0] >= 0 ? orc_harm(o->perm[other[0]], o->perm[row]) : 0.0;
+                    kr[m] = other[1] >= 0 ? orc_harm(o->perm[other[1]], o->perm[row]) : 0.0;
+                }
+                m++;
+            }
+    }
+    /* CSR by row, crossing order kept within a row */
+    o->nxc = m;
+    o->xptr = (int64_t *)xcalloc(N + 1, 8);
+    for (int64_t q = 0; q < m; q++) o->xptr[rows[q] + 1]++;
+    for (int64_t k = 0; k < N; k++) o->xptr[k + 1] += o->xptr[k];
+    o->xa = (int64_t *)xcalloc(m, 8); o->xb = (int64_t *)xcalloc(m, 8);
+    o->xkl = (double *)xcalloc(m, 8); o->xkr = (double *)xcalloc(m, 8);
+    int64_t *fill = (int64_t *)xcalloc(N, 8);
+    for (int64_t q = 0; q < m; q++) {
+        int64_t r = rows[q], at = o->xptr[r] + fill[r]++;
+        o->xa[at] = pa[q]; o->xb[at] = pb[q]; o->xkl[at] = kl[q]; o->xkr[at] = kr[q];
+    }
+    free(fill); free(rows); free(pa); free(pb); free(kl); free(kr); free(cr); free(minds);
+}
+
+int64_t orc_crossings(const orc *o) { return o->ncross; }
 
 orc *orc_create(const dfn_problem *p)
 {
@@ -149,6 +241,7 @@ orc *orc_create(const dfn_problem *p)
     o->Pdot = (double *)xcalloc(N, 8);
     o->SigmaT_dot = (double *)xcalloc(N, 8); o->SigmaN_dot = (double *)xcalloc(N, 8);
     orc_ini_value(o);
+    orc_find_crossings(o);
     /* solve() entry: src/solver.f90:50-56 */
     o->time = p->time0; o->t_try = 100.0; o->it_count = 0;
     o->kernel_impl = 0;
@@ -162,7 +255,7 @@ void orc_destroy(orc *o)
     void *ptrs[] = {o->fault_n, o->fault_first, o->node, o->elem, o->ds, o->tan, o->nrm, o->a, o->b,
                     o->Dc, o->f0, o->V0, o->nload, o->sload, o->perm, o->permx, o->fake, o->src_fault,
                     o->src_index, o->src_Q, o->src_tb, o->src_te, o->Y, o->P, o->Pdot, o->SigmaT_dot,
-                    o->SigmaN_dot, o->KT, o->KN};
+                    o->SigmaN_dot, o->KT, o->KN, o->xptr, o->xa, o->xb, o->xkl, o->xkr};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     orc_hmat_free((struct orc_hmat *)o->hmat);
     free(o);
@@ -357,8 +450,8 @@ void orc_kernel(orc *o, const double *slip, double *sT, double *sN)
 }
 
 /* ---------------------------------------------------------------------- */
-/* Pore pressure: src/fluid_diffusion.f90. No fault crossings (the crossing
- * terms of :213-295 apply only to coincident nodes).                       */
+/* Pore pressure: src/fluid_diffusion.f90, with the fault-crossing coupling
+ * of orc_find_crossings.                                                   */
 static inline double orc_coef(const orc *o, double kx, double dt, double dsv)
 {
     /* kx*dt/(porosity*dyn_viscosity*(fluid_comp+rock_comp)*ds**2) */
@@ -375,6 +468,10 @@ static void orc_diag(const orc *o, double dt, double *diag)
     for (int64_t k = 1; k < N - 1; k++)
         diag[k] = 1.0 + (px[k] + px[k + 1]) * dt /
                             (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k] * ds[k]));
+    /* crossing terms (src/fluid_diffusion.f90:338-405, own-row ds) */
+    for (int64_t k = 0; k < N; k++)
+        for (int64_t q = o->xptr[k]; q < o->xptr[k + 1]; q++)
+            diag[k] = diag[k] + orc_coef(o, o->xkl[q], dt, ds[k]) + orc_coef(o, o->xkr[q], dt, ds[k]);
 }
 
 /* compute_MatrixVector: src/fluid_diffusion.f90:163-204 */
@@ -396,6 +493,13 @@ static void orc_matvec(const orc *o, const double *v, double dt, const double *d
         A3 = -px[k + 1] * dt / (o->porosity * o->dyn_visc * (o->fluid_comp + o->rock_comp) * (ds[k + 1] * ds[k + 1]));
         out[k] = (A1 * v[k - 1] + A2 * v[k] + A3 * v[k + 1]) / diag[k];
     }
+    /* crossing terms (src/fluid_diffusion.f90:213-295, own-row ds, / diag) */
+    for (int64_t k = 0; k < N; k++)
+        for (int64_t q = o->xptr[k]; q < o->xptr[k + 1]; q++) {
+            double cl = orc_coef(o, o->xkl[q], dt, ds[k]), cr = orc_coef(o, o->xkr[q], dt, ds[k]);
+            double X1 = -cl, X2 = cl + cr, X3 = -cr;
+            out[k] = out[k] + (X1 * v[o->xa[q]] + X2 * v[k] + X3 * v[o->xb[q]]) / diag[k];
+        }
 }
 
 /* Right-hand side b1 with the injection sources (src/fluid_diffusion.f90:44-64).
@@ -491,6 +595,8 @@ static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, 
 /* Exact solve of the same implicit step with the unscaled tridiagonal
  * system (Thomas algorithm); used by tests to check both CG and the GPU
  * tridiagonal solver. Not a reference routine. */
+/* Exact tridiagonal solve of the same implicit step (networks without
+ * fault crossings: a crossing couples rows outside the three diagonals). */
 void orc_pressure_exact(const orc *o, double dt, double *P_temp)
 {
     int64_t N = o->N;

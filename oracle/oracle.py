@@ -46,6 +46,7 @@ def load():
         "orc_kernel": (None, [V, dp, dp, dp]),
         "orc_compute_P": (cint, [V, dbl, dp, dp]),
         "orc_pressure_exact": (None, [V, dbl, dp]),
+        "orc_crossings": (i64, [V]),
         "orc_rhs": (cint, [V, dbl, dp, dp]),
         "orc_rkqs": (cint, [V, dp, dp, i64, dp, dbl, dbl, dp, dp, dp]),
         "orc_solve_step": (cint, [V]),
@@ -142,6 +143,10 @@ class Oracle:
         Pt, Pd = np.zeros(self.N), np.zeros(self.N)
         ier = self.lib.orc_compute_P(self.o, float(dt), ptr(Pt), ptr(Pd))
         return Pt, Pd, ier
+
+    def crossings(self):
+        """Fault crossings found as find_fault_crossing does."""
+        return int(self.lib.orc_crossings(self.o))
 
     def pressure_exact(self, dt):
         Pt = np.zeros(self.N)

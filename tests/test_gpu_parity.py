@@ -171,6 +171,54 @@ def test_pressure_cg_nonconvergence_sets_ier():
         assert ier2 in (0, 1)
 
 
+@pytest.mark.parametrize("case", ["pair", "shipped"])
+@pytest.mark.parametrize("dt", [60.0, 3600.0, 86400.0])
+def test_pressure_with_fault_crossings_matches_oracle(case, dt):
+    """Fault-crossing coupling: the same crossings as the oracle, and the
+    reference-order CG (cg_exact) bitwise the oracle's; the tree-reduced CG
+    within the solver tolerance."""
+    import refconfigs
+
+    p = networks.crossing_pair(n_el=100) if case == "pair" else refconfigs.problem("network")
+    o = Oracle(p)
+    oP, od, oi = o.compute_P(dt)
+    with Simulation(p, pressure="cg_exact") as s:
+        assert s.crossing_count == o.crossings() > 0
+        gP, gd, gi = s.compute_P(dt)
+        assert gi == oi
+        if oi == 0:
+            assert np.array_equal(gP, oP) and np.array_equal(gd, od)
+    with Simulation(p, pressure="cg") as s:
+        gP, gd, gi = s.compute_P(dt)
+        assert gi == oi
+        if oi == 0:
+            assert np.abs(gP - oP).max() < 1e3 * p.hyperparameter.tol_solver
+
+
+def test_tridiagonal_pressure_rejects_fault_crossings():
+    from demystification_dfn_b200 import _lib
+
+    with pytest.raises(_lib.DfnError):
+        Simulation(networks.crossing_pair(n_el=100), pressure="tridiag")
+
+
+def test_batch_with_fault_crossings_equals_separate_runs():
+    """Networks with crossings in one batch follow their own runs bit for bit."""
+    from demystification_dfn_b200.ensemble import Ensemble
+
+    ps = [networks.crossing_pair(n_el=100, angle_deg=a, q_kgs=20.0, tol=1e-6) for a in (45.0, 70.0)]
+    with Ensemble(ps, pressure="cg") as ens:
+        assert ens.crossing_count == 2
+        reps = ens.solve(n_steps=8)
+        assert all(r["status"] == 0 for r in reps)
+        for i, p in enumerate(ps):
+            with Simulation(p, pressure="cg") as s:
+                s.solve_steps(8)
+                a, b = ens.state(i), s.state()
+                assert a["time"] == b["time"]
+                assert np.array_equal(a["Y"], b["Y"]) and np.array_equal(a["P"], b["P"])
+
+
 @pytest.mark.parametrize("dt", [0.5, 300.0, 86400.0])
 def test_pressure_tridiag_is_exact(dt):
     p = net(seed=6, n=5, mode="modeII", q_kgs=20.0)

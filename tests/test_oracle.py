@@ -171,3 +171,33 @@ def test_solve_loop_policies():
     assert np.isclose(s["time"], log.sum(), rtol=1e-12)
     assert log.max() <= 86400.0
     assert o.counters()["rhs_evals"] >= 6 * 12
+
+
+def test_fault_crossing_couples_the_pressure():
+    """find_fault_crossing restated: two faults sharing a node cross once;
+    fluid at 1 MPa on fault 1 reaches the elements of fault 2 around the
+    crossing in one implicit step (and only near it), while the same faults
+    1 m apart stay decoupled (fault 2 keeps exactly 0)."""
+    n = 100
+    p = networks.crossing_pair(n_el=n, shift=0.0)
+    o = Oracle(p)
+    assert o.crossings() == 1
+    Pt, _, ier = o.compute_P(3600.0)
+    assert ier == 0
+    f2 = Pt[n + 1:]
+    near, far = f2[n // 2 - 1:n // 2 + 1], np.concatenate([f2[:5], f2[-5:]])
+    assert near.min() > 1e5 and np.abs(far).max() < 1e-3 * near.min()
+    assert Pt[n // 2 - 1:n // 2 + 1].max() < 1e6        # fault 1 loses fluid at the crossing
+    o2 = Oracle(networks.crossing_pair(n_el=n, shift=1.0))
+    assert o2.crossings() == 0
+    Pt2, _, _ = o2.compute_P(3600.0)
+    assert np.all(Pt2[n + 1:] == 0.0)
+
+
+def test_shipped_network_has_fault_crossings():
+    """The reference's shipped 10-fault network shares nodes between faults
+    (13 crossings by the reference's criterion)."""
+    import refconfigs
+
+    o = Oracle(refconfigs.problem("network"))
+    assert o.crossings() == 13
