@@ -17,6 +17,8 @@
 #include "tc_gemm.cuh"
 
 #include <algorithm>
+#include <unordered_map>
+#include <array>
 #include <deque>
 #include <cstdio>
 #include <cstring>
@@ -682,39 +684,70 @@ static int64_t build_crossings(const dfn_problem *probs, int count, const std::v
             minds[f] = m;
             cnt += nel[f] + 1;
         }
-        for (int64_t f1 = 0; f1 < F; f1++)
-            for (int64_t f2 = f1 + 1; f2 < F; f2++) {
-                const double thr = 0.01 * std::min(minds[f1], minds[f2]);
+        // candidate node pairs from a hashed grid whose cells are as large as
+        // the largest pair threshold (a pair within its threshold lies in the
+        // same or a neighbouring cell); crossings then in the reference's
+        // loop order (fault 1, fault 2, node of fault 1, node of fault 2)
+        double maxthr = 0.0;
+        for (int64_t f = 0; f < F; f++) maxthr = std::max(maxthr, 0.01 * minds[f]);
+        std::vector<std::array<int64_t, 4>> found;   // f1, f2, a, b (local 0-based nodes)
+        if (maxthr > 0.0 && F > 1) {
+            std::unordered_map<uint64_t, std::vector<std::pair<int64_t, int64_t>>> grid;   // cell -> (fault, node)
+            auto cell = [&](double x, double y, int64_t dx, int64_t dy) {
+                const int64_t cx = (int64_t)std::floor(x / maxthr) + dx, cy = (int64_t)std::floor(y / maxthr) + dy;
+                return ((uint64_t)cx * 0x9E3779B97F4A7C15ull) ^ (uint64_t)cy;
+            };
+            for (int64_t f = 0; f < F; f++)
+                for (int64_t a = 0; a <= nel[f]; a++) {
+                    const double *q = nd + 2 * (first[f] + a);
+                    grid[cell(q[0], q[1], 0, 0)].push_back({f, a});
+                }
+            for (int64_t f1 = 0; f1 < F; f1++)
                 for (int64_t a = 0; a <= nel[f1]; a++) {
                     const double *p1 = nd + 2 * (first[f1] + a);
-                    for (int64_t b = 0; b <= nel[f2]; b++) {
-                        const double *p2 = nd + 2 * (first[f2] + b);
-                        const double d = std::sqrt((p1[0] - p2[0]) * (p1[0] - p2[0]) + (p1[1] - p2[1]) * (p1[1] - p2[1]));
-                        if (!(d < thr)) continue;
-                        ncross++;
-                        const int64_t e1[2] = {a >= 1 ? first[f1] + a - 1 : -1, a < nel[f1] ? first[f1] + a : -1};
-                        const int64_t e2[2] = {b >= 1 ? first[f2] + b - 1 : -1, b < nel[f2] ? first[f2] + b : -1};
-                        for (int side = 0; side < 2; side++)
-                            for (int j = 0; j < 2; j++) {
-                                const int64_t row = side == 0 ? e1[j] : e2[j];
-                                if (row < 0) continue;
-                                const int64_t *o = side == 0 ? e2 : e1;
-                                XCon x;
-                                x.a = o[0] >= 0 ? o[0] : row;
-                                x.b = o[1] >= 0 ? o[1] : row;
-                                // harmonic means with the first fault's element first
-                                if (side == 0) {
-                                    x.kl = o[0] >= 0 ? harm(perm[row], perm[o[0]]) : 0.0;
-                                    x.kr = o[1] >= 0 ? harm(perm[row], perm[o[1]]) : 0.0;
-                                } else {
-                                    x.kl = o[0] >= 0 ? harm(perm[o[0]], perm[row]) : 0.0;
-                                    x.kr = o[1] >= 0 ? harm(perm[o[1]], perm[row]) : 0.0;
-                                }
-                                rows[(size_t)(e0 + row)].push_back(x);
+                    for (int64_t dx = -1; dx <= 1; dx++)
+                        for (int64_t dy = -1; dy <= 1; dy++) {
+                            auto it = grid.find(cell(p1[0], p1[1], dx, dy));
+                            if (it == grid.end()) continue;
+                            for (const auto &fb : it->second) {
+                                const int64_t f2 = fb.first, b = fb.second;
+                                if (f2 <= f1) continue;
+                                const double *p2 = nd + 2 * (first[f2] + b);
+                                // the same criterion as the reference's double loop
+                                const double thr = 0.01 * std::min(minds[f1], minds[f2]);
+                                const double d = std::sqrt((p1[0] - p2[0]) * (p1[0] - p2[0]) +
+                                                           (p1[1] - p2[1]) * (p1[1] - p2[1]));
+                                if (d < thr) found.push_back({f1, f2, a, b});
                             }
-                    }
+                        }
                 }
-            }
+            std::sort(found.begin(), found.end());
+            found.erase(std::unique(found.begin(), found.end()), found.end());
+        }
+        for (const auto &c : found) {
+            const int64_t f1 = c[0], f2 = c[1], a = c[2], b = c[3];
+            ncross++;
+            const int64_t e1[2] = {a >= 1 ? first[f1] + a - 1 : -1, a < nel[f1] ? first[f1] + a : -1};
+            const int64_t e2[2] = {b >= 1 ? first[f2] + b - 1 : -1, b < nel[f2] ? first[f2] + b : -1};
+            for (int side = 0; side < 2; side++)
+                for (int j = 0; j < 2; j++) {
+                    const int64_t row = side == 0 ? e1[j] : e2[j];
+                    if (row < 0) continue;
+                    const int64_t *o = side == 0 ? e2 : e1;
+                    XCon x;
+                    x.a = o[0] >= 0 ? o[0] : row;
+                    x.b = o[1] >= 0 ? o[1] : row;
+                    // harmonic means with the first fault's element first
+                    if (side == 0) {
+                        x.kl = o[0] >= 0 ? harm(perm[row], perm[o[0]]) : 0.0;
+                        x.kr = o[1] >= 0 ? harm(perm[row], perm[o[1]]) : 0.0;
+                    } else {
+                        x.kl = o[0] >= 0 ? harm(perm[o[0]], perm[row]) : 0.0;
+                        x.kr = o[1] >= 0 ? harm(perm[o[1]], perm[row]) : 0.0;
+                    }
+                    rows[(size_t)(e0 + row)].push_back(x);
+                }
+        }
     }
     xptr.assign((size_t)Ntot + 1, 0);
     xcon.clear();
