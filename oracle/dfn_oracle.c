@@ -128,9 +128,24 @@ static void orc_find_crossings(orc *o)
     /* pass 1: crossings; pass 2: contributions per row */
     int64_t cap = 0, n = 0;
     int64_t *cr = NULL;   /* (f1, f2, a, b) with a, b 0-based local nodes */
+    /* bounding boxes of the faults' nodes: pairs farther apart than the
+     * threshold are skipped (the loop order is the reference's) */
+    double *bb = (double *)xcalloc(4 * F, 8);
+    for (int64_t f = 0; f < F; f++) {
+        bb[4 * f] = bb[4 * f + 2] = INFINITY;
+        bb[4 * f + 1] = bb[4 * f + 3] = -INFINITY;
+        for (int64_t a = 0; a <= o->fault_n[f]; a++) {
+            const double *q = o->node + 2 * (o->fault_first[f] + a);
+            bb[4 * f] = fmin(bb[4 * f], q[0]); bb[4 * f + 1] = fmax(bb[4 * f + 1], q[0]);
+            bb[4 * f + 2] = fmin(bb[4 * f + 2], q[1]); bb[4 * f + 3] = fmax(bb[4 * f + 3], q[1]);
+        }
+    }
     for (int64_t f1 = 0; f1 < F; f1++)
         for (int64_t f2 = f1 + 1; f2 < F; f2++) {
             double thr = 0.01 * fmin(minds[f1], minds[f2]);
+            if (bb[4 * f1] > bb[4 * f2 + 1] + thr || bb[4 * f2] > bb[4 * f1 + 1] + thr ||
+                bb[4 * f1 + 2] > bb[4 * f2 + 3] + thr || bb[4 * f2 + 2] > bb[4 * f1 + 3] + thr)
+                continue;
             for (int64_t a = 0; a <= o->fault_n[f1]; a++) {
                 const double *p1 = o->node + 2 * (o->fault_first[f1] + a);
                 for (int64_t b = 0; b <= o->fault_n[f2]; b++) {
@@ -184,7 +199,7 @@ static void orc_find_crossings(orc *o)
         int64_t r = rows[q], at = o->xptr[r] + fill[r]++;
         o->xa[at] = pa[q]; o->xb[at] = pb[q]; o->xkl[at] = kl[q]; o->xkr[at] = kr[q];
     }
-    free(fill); free(rows); free(pa); free(pb); free(kl); free(kr); free(cr); free(minds);
+    free(fill); free(rows); free(pa); free(pb); free(kl); free(kr); free(cr); free(minds); free(bb);
 }
 
 int64_t orc_crossings(const orc *o) { return o->ncross; }
