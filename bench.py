@@ -606,14 +606,18 @@ def main():
     outs = [torch.empty(N, dtype=torch.float64).pin_memory().numpy() for _ in range(5)]
     e2e_steps = max(10, args.steps // 2)
     tcur, ttry = st["time"], st["t_try"]
+    v0_dc = np.asarray(sim.arrays.V0) / np.asarray(sim.arrays.Dc)
+    psi = Yh[N:2 * N]
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         r = sim.step_host(Yh, Ph, tcur, ttry, outs)
         # next step's input is this step's result, read back on the host
+        # (psi = ln(theta V0 / Dc), in place)
         Yh[:N] = outs[0]
-        Yh[N:2 * N] = np.log(outs[1] * sim.arrays.V0 / sim.arrays.Dc)
+        np.multiply(outs[1], v0_dc, out=psi)
+        np.log(psi, out=psi)
         Yh[2 * N:] = outs[4]
         Ph[:] = outs[2]
         tcur, ttry = r.time, r.t_try
