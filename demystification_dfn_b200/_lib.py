@@ -88,6 +88,7 @@ def load():
         "dfn_set_graphs": (i32, [P, i32]),
         "dfn_set_cg_form": (i32, [P, i32]),
         "dfn_crossing_count": (i64, [P]),
+        "dfn_set_tri_shape": (i32, [P, i32]),
         "dfn_autotune": (i32, [P, ctypes.c_void_p]),
         "dfn_kernel_batch": (i32, [P, dp, dp, dp]),
         "dfn_velocity": (i32, [P, dp]),
@@ -144,6 +145,7 @@ def autotune(lib, h, storage, pressure):
     else:
         ms["pressure_warp"] = t.ms[2]
         ms["pressure_thread"] = t.ms[3]
-    return {"gemv_impl": names[t.gemv_impl], "short_segments": "thread" if t.tri_thread else "warp",
+        ms["pressure_tile"] = t.ms[5]
+    return {"gemv_impl": names[t.gemv_impl], "short_segments": ("warp", "thread", "tile")[t.tri_thread],
             "cg_form": ("cta", "cluster", "cta_smem")[t.cg_cluster], "cg_cluster_ctas": int(t.cg_cluster_ctas),
             "ms": ms}

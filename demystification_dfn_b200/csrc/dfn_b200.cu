@@ -97,7 +97,9 @@ struct dfn_handle {
     int64_t nlong = 0, nlong0 = 0;
     int *short_seg = nullptr;             // the others
     int64_t nshort = 0, nshort0 = 0;
-    bool tri_thread = false;              // short segments: one thread (true) or one warp each
+    int tri_shape = 0;                    // short segments: 0 a warp each, 1 a thread each, 2 tiles
+    int2 *tri_tiles = nullptr;            // tiles of consecutive short segments (first in short_seg, count)
+    int64_t ntri_tiles = 0, ntri_tiles0 = 0;
     int64_t nsrc_tot = 0, part_tot = 0;
     // geometry and parameters (concatenated)
     double *node = nullptr, *elem = nullptr, *ds = nullptr, *tan = nullptr, *nrm = nullptr, *permx = nullptr;
@@ -374,7 +376,18 @@ static int launch_pressure(dfn_handle *h, int mask, int kind, int sys0, int nsys
     } else {
         const int64_t nshort = (ninst == h->B) ? h->nshort : h->nshort0;
         const int64_t nlong = (ninst == h->B) ? h->nlong : h->nlong0;
-        if (nshort > 0 && h->tri_thread) {
+        if (nshort > 0 && h->tri_shape == 2) {
+            const int64_t nt = (ninst == h->B) ? h->ntri_tiles : h->ntri_tiles0;
+            dim3 grid((unsigned)nt, (unsigned)nsys);
+            pressure_tridiag_tile_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0,
+                                                                      dt_explicit, h->seg_start, h->seg_inst,
+                                                                      h->short_seg, h->tri_tiles, h->Ptemp,
+                                                                      h->Pdot_s);
+            if (nlong > 0) {
+                h->launches++;
+                CKL();
+            }
+        } else if (nshort > 0 && h->tri_shape == 1) {
             dim3 grid((unsigned)((nshort + 127) / 128), (unsigned)nsys);
             pressure_tridiag_thread_kernel<<<grid, 128, 0, h->stream>>>(h->pg, h->inst, h->ctl, mask, kind, sys0,
                                                                         dt_explicit, h->seg_start, h->seg_inst,
@@ -1044,7 +1057,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
@@ -1353,7 +1366,27 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         // default launch shape of the short segments (dfn_autotune measures
         // instead): warps while the segments fill few waves of warps, threads
         // once there are tens of thousands
-        h->tri_thread = h->nshort >= 16384;
+        h->tri_shape = h->nshort >= 16384 ? 2 : 0;
+        // tiles: runs of consecutive short segments of one network, at most
+        // TRI_TILE elements and 128 segments each; network 0's first
+        std::vector<int2> tl;
+        for (size_t q = 0; q < sh.size();) {
+            size_t r = q + 1;
+            int64_t ne = seg[sh[q] + 1] - seg[sh[q]];
+            while (r < sh.size() && r - q < 128 && sh[r] == sh[r - 1] + 1 && sinst[sh[r]] == sinst[sh[q]] &&
+                   ne + (seg[sh[r] + 1] - seg[sh[r]]) <= TRI_TILE) {
+                ne += seg[sh[r] + 1] - seg[sh[r]];
+                r++;
+            }
+            tl.push_back(make_int2((int)q, (int)(r - q)));
+            if (sinst[sh[q]] == 0) h->ntri_tiles0 = (int64_t)tl.size();
+            q = r;
+        }
+        h->ntri_tiles = (int64_t)tl.size();
+        if (!tl.empty()) {
+            DALLOC(h->tri_tiles, tl.size());
+            HCOPY(h->tri_tiles, tl.data(), tl.size());
+        }
         if (h->nlong) {
             DALLOC(h->long_seg, lg.size());
             HCOPY(h->long_seg, lg.data(), lg.size());
@@ -1617,7 +1650,7 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         r.ms[4] = msv[2];
         r.gemv_impl = best;
     }
-    r.tri_thread = h->tri_thread ? 1 : 0;
+    r.tri_thread = h->tri_shape;
     if (h->pressure == DFN_PRESSURE_CG && h->pcl_ok) {
         // one CTA on global memory -> ms[2], clusters -> ms[3] (when this
         // handle has a cluster form), one CTA on shared memory -> ms[5]
@@ -1642,12 +1675,20 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         else if (h->pcl > 0 && (h->pcl_mode == 1 || (h->pcl_mode < 0 && 5 * h->B <= h->pcl_max))) r.cg_cluster = 1;
     }
     if (h->pressure == DFN_PRESSURE_TRIDIAG && h->nshort > 0) {
-        for (int v = 0; v < 2; v++) {
-            h->tri_thread = v == 1;
-            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, r.ms[2 + v]));
+        // warps -> ms[2], threads -> ms[3], tiles -> ms[5]
+        double msv[3];
+        for (int v = 0; v < 3; v++) {
+            h->tri_shape = v;
+            TRY(time_it([&]() { return launch_pressure(h, M_ALL, 2, 1, 5, 100.0, h->B); }, 3, msv[v]));
         }
-        h->tri_thread = r.ms[3] < r.ms[2];
-        r.tri_thread = h->tri_thread ? 1 : 0;
+        int best = 0;
+        for (int v = 1; v < 3; v++)
+            if (msv[v] < msv[best]) best = v;
+        h->tri_shape = best;
+        r.ms[2] = msv[0];
+        r.ms[3] = msv[1];
+        r.ms[5] = msv[2];
+        r.tri_thread = best;
     }
     h->prof = prof;
     drop_graph(h);
@@ -1667,6 +1708,20 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)
 }
 
 int64_t dfn_crossing_count(const dfn_handle *h) { return h ? h->ncross : -1; }
+
+int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape)
+{
+    if (!h) return DFN_ERR_ARG;
+    if (shape < 0 || shape > 2 || h->pressure != DFN_PRESSURE_TRIDIAG) {
+        g_err = "short-segment shape is 0, 1 or 2 on a tridiagonal-pressure handle";
+        return DFN_ERR_ARG;
+    }
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->tri_shape = shape;
+    drop_graph(h);
+    return DFN_OK;
+}
 
 int32_t dfn_set_cg_form(dfn_handle *h, int32_t form)
 {

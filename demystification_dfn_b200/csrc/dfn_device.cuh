@@ -1575,6 +1575,82 @@ __global__ void __launch_bounds__(128) pressure_tridiag_thread_kernel(PressGloba
     if (bad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
+// Short segments in tiles: one 128-thread CTA per tile of consecutive
+// short segments (at most TRI_TILE elements and 128 segments: tiles[b] =
+// (first entry in seg_list, count)), grid (tiles, systems). P, ds and the
+// face permeabilities of the tile are staged into shared memory with
+// coalesced loads, each thread solves one segment with the recurrence of
+// pressure_tridiag_thread_kernel (the same operations: identical results)
+// from shared memory, and the results leave with coalesced stores.
+#define TRI_TILE 1024
+
+__global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
+                                                                    int mask, int kind, int sys0,
+                                                                    double dt_explicit, const int64_t *seg_start,
+                                                                    const int *seg_inst, const int *seg_list,
+                                                                    const int2 *tiles, double *Ptemp, double *Pdot)
+{
+    __shared__ double sP[TRI_TILE], sds[TRI_TILE + 2], spx[TRI_TILE + 1], sc[TRI_TILE], sd[TRI_TILE];
+    const int2 t = tiles[blockIdx.x];
+    const int sg0 = seg_list[t.x];
+    const int i = seg_inst[sg0];
+    if (!takes_part(ctl, i, mask)) return;   // one instance per tile
+    const Inst I = inst[i];
+    const PressParams p = press_params(g, I, i, ctl);
+    const int sys = sys0 + blockIdx.y;
+    const int64_t N = I.N;
+    const double dt = sys_dt(ctl + i, kind, sys, dt_explicit);
+    const int64_t e0 = seg_start[sg0] - I.eoff, e1 = seg_start[seg_list[t.x + t.y - 1] + 1] - I.eoff;
+    const int n = (int)(e1 - e0);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) sP[j] = p.P[e0 + j];
+    for (int j = threadIdx.x; j < n + 2; j += blockDim.x) {
+        const int64_t k = e0 - 1 + j;
+        sds[j] = (k >= 0 && k < N) ? p.ds[k] : 1.0;   // outside the network: never read by prow
+    }
+    for (int j = threadIdx.x; j <= n; j += blockDim.x) spx[j] = p.permx[e0 + j];
+    __syncthreads();
+    PressParams q = p;   // the same parameters, arrays in shared memory
+    q.P = sP - e0;
+    q.ds = sds - (e0 - 1);
+    q.permx = spx - e0;
+    bool bad = false;
+    if ((int)threadIdx.x < t.y) {
+        const int sg = seg_list[t.x + threadIdx.x];
+        const int64_t k0 = seg_start[sg] - I.eoff, k1 = seg_start[sg + 1] - I.eoff;
+        double cprev = 0.0, dprev = 0.0;
+        for (int64_t k = k0; k < k1; k++) {
+            double A1, A2, A3;
+            prow(q, k, dt, A1, A2, A3);
+            if (k == k0) A1 = 0.0;
+            if (k == k1 - 1) A3 = 0.0;
+            const double rhs = add_(q.P[k], psource(q, k, dt));
+            const double rden = 1.0 / (A2 - A1 * cprev);
+            const double c = A3 * rden;
+            const double d = (rhs - A1 * dprev) * rden;
+            sc[k - e0] = c;
+            sd[k - e0] = d;
+            cprev = c;
+            dprev = d;
+        }
+        const double rdt = (dt < 1e-9) ? 0.0 : 1.0 / dt;
+        double xn = 0.0;
+        for (int64_t k = k1 - 1; k >= k0; k--) {
+            const double xk = sd[k - e0] - sc[k - e0] * xn;
+            xn = xk;
+            sc[k - e0] = xk;                       // P_temp
+            sd[k - e0] = (xk - q.P[k]) * rdt;      // P_dot
+            if (!isfinite(xk)) bad = true;
+        }
+    }
+    __syncthreads();
+    double *Pt = Ptemp + 6 * I.eoff + (int64_t)sys * N, *Pd = Pdot + 6 * I.eoff + (int64_t)sys * N;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        Pt[e0 + j] = sc[j];
+        Pd[e0 + j] = sd[j];
+    }
+    if (bad) atomicCAS(&ctl[i].status, 0, 4);
+}
+
 // Short segments, one warp each: grid (ceil(segments / 8), systems),
 // blockDim 256; seg_list holds the launch's short segments.
 __global__ void __launch_bounds__(256) pressure_tridiag_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,

@@ -66,6 +66,10 @@ class Ensemble:
         """Fault crossings that couple the pressure of the networks."""
         return int(self.lib.dfn_crossing_count(self.h))
 
+    def set_tri_shape(self, shape):
+        """Short tridiagonal segments by "warp", "thread" or "tile"."""
+        _lib.check(self.lib.dfn_set_tri_shape(self.h, {"warp": 0, "thread": 1, "tile": 2}[shape]), self.lib)
+
     def set_cg_form(self, form):
         """CG pressure solves by "cta" (one CTA per system, global memory),
         "cluster" (a thread-block cluster per system, shared memory),

@@ -202,9 +202,12 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
 /* Autotuner: times the interchangeable launch shapes on the handle's own
  * data and keeps the fastest. K.V: TMA bulk copies or 128-bit loads
  * (gemv_impl 0/1, bitwise identical results); tridiagonal pressure: short
- * segments (<= 64 elements) solved by one thread each (sequential Thomas) or
- * one warp each (scans), equal to rounding. ms[] = milliseconds per launch of
- * K.V TMA, K.V LDG, pressure by warps, pressure by threads (0 = not timed).
+ * segments (<= 64 elements) solved by one warp each (scans; tri_thread 0,
+ * ms[2]), one thread each (sequential Thomas; 1, ms[3]) or one thread each
+ * in tiles staged through shared memory (the same recurrence, identical to
+ * the threads; 2, ms[5]), the warps equal to the others to rounding.
+ * ms[0] and ms[1] = milliseconds per launch of K.V TMA and LDG (0 = not
+ * timed).
  * For DFN_STORE_BF16X2_TC handles the K.V choices are instead the
  * tensor-core GEMM as a persistent kernel (one CTA per SM walking the work
  * units, epilogue overlapped with the next unit; gemv_impl 0, ms[0]), one
@@ -220,7 +223,7 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * form (2 to 16; 0 when it has none). The forms differ in the order of the
  * dot-product sums (equal to rounding).
  * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
- * the short segments use threads once a launch has at least 16384 of them,
+ * the short segments use tiles once a launch has at least 16384 of them,
  * and the CG uses clusters when all of a launch's clusters fit on the GPU at
  * once. No counterpart in the reference. */
 typedef struct dfn_tuning {
@@ -249,6 +252,11 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable);
  * the solver tolerance. dfn_autotune sets the fastest. No counterpart in the
  * reference. */
 int32_t dfn_set_cg_form(dfn_handle *h, int32_t form);
+/* Launch shape of the short tridiagonal segments (DFN_PRESSURE_TRIDIAG
+ * handles): 0 one warp per segment (scans), 1 one thread per segment, 2 one
+ * thread per segment in tiles staged through shared memory (identical to 1).
+ * dfn_autotune sets the fastest. No counterpart in the reference. */
+int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape);
 /* A batch of independent networks in one handle (no counterpart in the
  * reference, which runs one network per process). All networks share the
  * fracture mode and the options; each keeps its own state, step size,

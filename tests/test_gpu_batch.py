@@ -183,3 +183,25 @@ def test_cg_forms_agree_on_an_uneven_batch():
             assert abs(a["time"] - b["time"]) <= 1e-9 * a["time"]
             assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-6 * np.abs(a["Y"][:N]).max()
             assert np.abs(a["P"] - b["P"]).max() <= 1e-6 * np.abs(a["P"]).max()
+
+
+@pytest.mark.parametrize("mode", ["modeII", "modeIII"])
+def test_tridiagonal_tiles_equal_threads_bitwise(mode):
+    """Short segments solved in shared-memory tiles give the bits of the
+    thread-per-segment solve (the same recurrence); the warp scans agree to
+    rounding. A batch of ensemble networks: many short segments, tiles
+    across fault and fake elements."""
+    ps = [networks.ensemble_member(s, n_faults=60, mode=mode) for s in (2, 4, 6)]
+    out = {}
+    for shape in ("thread", "tile", "warp"):
+        with Ensemble(ps, pressure="tridiag") as ens:
+            ens.set_tri_shape(shape)
+            reps = ens.solve(n_steps=10)
+            assert all(r["status"] == 0 for r in reps)
+            out[shape] = [ens.state(i) for i in range(len(ps))]
+    for a, b in zip(out["thread"], out["tile"]):
+        assert a["time"] == b["time"]
+        assert np.array_equal(a["Y"], b["Y"]) and np.array_equal(a["P"], b["P"])
+    for a, b in zip(out["thread"], out["warp"]):
+        N = len(a["P"])
+        assert np.abs(a["Y"][:N] - b["Y"][:N]).max() <= 1e-6 * np.abs(a["Y"][:N]).max()
