@@ -131,6 +131,7 @@ struct dfn_handle {
     int64_t *xptr = nullptr;              // [Ntot + 1] crossing rows of the pressure system
     XCon *xcon = nullptr;
     int64_t *xrows = nullptr, *xrows_ptr = nullptr;
+    double *tcoef = nullptr;              // tridiagonal row factors (3 per element; tridiagonal handles)
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
     StepCtl *ctl = nullptr;
@@ -1057,7 +1058,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
@@ -1488,6 +1489,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     pg.xcon = nullptr;
     pg.xrows = nullptr;
     pg.xrows_ptr = nullptr;
+    pg.tcoef = nullptr;
     {
         std::vector<int64_t> xp;
         std::vector<XCon> xc;
@@ -1520,6 +1522,13 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
             pg.xrows = h->xrows;
             pg.xrows_ptr = h->xrows_ptr;
         }
+    }
+    if (h->pressure == DFN_PRESSURE_TRIDIAG) {
+        CKC(cudaMalloc((void **)&h->tcoef, sizeof(double) * 3 * (size_t)h->Ntot));
+        tri_coef_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(pg, h->inst, h->inst_of, h->Ntot, h->tcoef);
+        h->launches++;
+        CKC(cudaGetLastError());
+        pg.tcoef = h->tcoef;
     }
 
     // cluster CG (CG mode): the fewest CTAs per cluster (2 to 16) whose

@@ -568,6 +568,9 @@ struct PressParams {
     const struct XCon *xcon;
     const int64_t *xrows;
     int64_t nxrows;
+    // tridiagonal solver: per element the dt-free factors (u, v, w) of its
+    // row, A1 = -dt u, A2 = 1 + dt v, A3 = -dt w (tridiagonal handles only)
+    const double *tcoef;
 };
 
 // One fault-crossing contribution to a row of the pressure system: partner
@@ -604,6 +607,18 @@ __device__ __forceinline__ void prow(const PressParams &p, int64_t k, double dt,
         A2 = add_(1.0, pcoef(p, add_(p.permx[k], p.permx[k + 1]), dt, p.ds[k]));
         A3 = -pcoef(p, p.permx[k + 1], dt, p.ds[k + 1]);
     }
+}
+
+// Row coefficients for the tridiagonal solver (tridiagonal handles, which
+// always carry p.tcoef): from the precomputed dt-free factors, one
+// multiplication each instead of a division; equal to prow up to rounding.
+__device__ __forceinline__ void prow_tri(const PressParams &p, int64_t k, double dt, double &A1, double &A2,
+                                         double &A3)
+{
+    const double *t = p.tcoef + 3 * k;
+    A1 = -(dt * t[0]);
+    A2 = 1.0 + dt * t[1];
+    A3 = -(dt * t[2]);
 }
 
 // Fault-crossing coupling of row k (src/fluid_diffusion.f90:213-295,
@@ -1020,6 +1035,7 @@ struct PressGlobal {
     const int64_t *xptr;                   // [Ntot + 1] crossing rows (null: no crossings)
     const XCon *xcon;
     const int64_t *xrows, *xrows_ptr;      // rows with crossings of instance i: xrows[xrows_ptr[i] ..)
+    const double *tcoef;                   // [3 Ntot] tridiagonal row factors (null: computed by prow)
 };
 
 __device__ __forceinline__ PressParams press_params(const PressGlobal &g, const Inst &I, int i, const StepCtl *ctl)
@@ -1034,6 +1050,7 @@ __device__ __forceinline__ PressParams press_params(const PressGlobal &g, const 
     p.xcon = g.xcon;
     p.xrows = g.xptr ? g.xrows + g.xrows_ptr[i] : nullptr;
     p.nxrows = g.xptr ? g.xrows_ptr[i + 1] - g.xrows_ptr[i] : 0;
+    p.tcoef = g.tcoef ? g.tcoef + 3 * I.eoff : nullptr;
     return p;
 }
 
@@ -1484,7 +1501,7 @@ __device__ __forceinline__ void tri_segment(const PressParams &p, double dt, int
     tri_rows<MAXM, false>(nr, [&](int j) {
         const int64_t k = k0 + r0 + j;
         double A1, A2, A3;
-        prow(p, k, dt, A1, A2, A3);
+        prow_tri(p, k, dt, A1, A2, A3);
         if (k == k0) A1 = 0.0;
         if (k == k1 - 1) A3 = 0.0;
         at(0, j) = A1; at(1, j) = A2; at(2, j) = A3;
@@ -1551,7 +1568,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_thread_kernel(PressGloba
 #pragma unroll 4
     for (int64_t k = k0; k < k1; k++) {
         double A1, A2, A3;
-        prow(p, k, dt, A1, A2, A3);
+        prow_tri(p, k, dt, A1, A2, A3);
         if (k == k0) A1 = 0.0;
         if (k == k1 - 1) A3 = 0.0;
         const double rhs = add_(p.P[k], psource(p, k, dt));
@@ -1575,13 +1592,46 @@ __global__ void __launch_bounds__(128) pressure_tridiag_thread_kernel(PressGloba
     if (bad) atomicCAS(&ctl[i].status, 0, 4);
 }
 
+// dt-free row factors of the tridiagonal solver (prow's coefficients divided
+// by dt): u = kx_k / (c ds_{k-1}^2), v = (kx_k + kx_{k+1}) / (c ds_k^2),
+// w = kx_{k+1} / (c ds_{k+1}^2), c = porosity dyn_viscosity (fluid_comp +
+// rock_comp), with prow's first and last rows.
+__global__ void tri_coef_kernel(PressGlobal g, const Inst *inst, const int *inst_of, int64_t Ntot, double *tcoef)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= Ntot) return;
+    const int i = inst_of[e];
+    const Inst I = inst[i];
+    const int64_t N = I.N, k = e - I.eoff;
+    const double *px = g.permx + I.eoff + i, *ds = g.ds + I.eoff;
+    const double c = I.porosity * I.dyn_visc * I.comp;
+    double u, v, w;
+    if (k == 0) {
+        u = 0.0;
+        v = px[1] / (c * (ds[0] * ds[0]));
+        w = v;
+    } else if (k == N - 1) {
+        u = px[N - 1] / (c * (ds[N - 1] * ds[N - 1]));
+        v = u;
+        w = 0.0;
+    } else {
+        u = px[k] / (c * (ds[k - 1] * ds[k - 1]));
+        v = (px[k] + px[k + 1]) / (c * (ds[k] * ds[k]));
+        w = px[k + 1] / (c * (ds[k + 1] * ds[k + 1]));
+    }
+    tcoef[3 * e] = u;
+    tcoef[3 * e + 1] = v;
+    tcoef[3 * e + 2] = w;
+}
+
 // Short segments in tiles: one 128-thread CTA per tile of consecutive
 // short segments (at most TRI_TILE elements and 128 segments: tiles[b] =
 // (first entry in seg_list, count)), grid (tiles, systems). P, ds and the
 // face permeabilities of the tile are staged into shared memory with
-// coalesced loads, each thread solves one segment with the recurrence of
-// pressure_tridiag_thread_kernel (the same operations: identical results)
-// from shared memory, and the results leave with coalesced stores.
+// coalesced loads (P and the precomputed row factors), each thread solves
+// one segment with the recurrence of pressure_tridiag_thread_kernel (the
+// same operations: identical results) from shared memory, and the results
+// leave with coalesced stores.
 #define TRI_TILE 1024
 
 __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
@@ -1590,7 +1640,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal 
                                                                     const int *seg_inst, const int *seg_list,
                                                                     const int2 *tiles, double *Ptemp, double *Pdot)
 {
-    __shared__ double sP[TRI_TILE], sds[TRI_TILE + 2], spx[TRI_TILE + 1], sc[TRI_TILE], sd[TRI_TILE];
+    __shared__ double sP[TRI_TILE], st[3 * TRI_TILE], sc[TRI_TILE], sd[TRI_TILE];
     const int2 t = tiles[blockIdx.x];
     const int sg0 = seg_list[t.x];
     const int i = seg_inst[sg0];
@@ -1603,16 +1653,11 @@ __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal 
     const int64_t e0 = seg_start[sg0] - I.eoff, e1 = seg_start[seg_list[t.x + t.y - 1] + 1] - I.eoff;
     const int n = (int)(e1 - e0);
     for (int j = threadIdx.x; j < n; j += blockDim.x) sP[j] = p.P[e0 + j];
-    for (int j = threadIdx.x; j < n + 2; j += blockDim.x) {
-        const int64_t k = e0 - 1 + j;
-        sds[j] = (k >= 0 && k < N) ? p.ds[k] : 1.0;   // outside the network: never read by prow
-    }
-    for (int j = threadIdx.x; j <= n; j += blockDim.x) spx[j] = p.permx[e0 + j];
+    for (int j = threadIdx.x; j < 3 * n; j += blockDim.x) st[j] = p.tcoef[3 * e0 + j];
     __syncthreads();
-    PressParams q = p;   // the same parameters, arrays in shared memory
+    PressParams q = p;   // the same parameters, P and the row factors in shared memory
     q.P = sP - e0;
-    q.ds = sds - (e0 - 1);
-    q.permx = spx - e0;
+    q.tcoef = st - 3 * e0;
     bool bad = false;
     if ((int)threadIdx.x < t.y) {
         const int sg = seg_list[t.x + threadIdx.x];
@@ -1620,7 +1665,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal 
         double cprev = 0.0, dprev = 0.0;
         for (int64_t k = k0; k < k1; k++) {
             double A1, A2, A3;
-            prow(q, k, dt, A1, A2, A3);
+            prow_tri(q, k, dt, A1, A2, A3);
             if (k == k0) A1 = 0.0;
             if (k == k1 - 1) A3 = 0.0;
             const double rhs = add_(q.P[k], psource(q, k, dt));
@@ -1632,7 +1677,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal 
             cprev = c;
             dprev = d;
         }
-        const double rdt = (dt < 1e-9) ? 0.0 : 1.0 / dt;
+            const double rdt = (dt < 1e-9) ? 0.0 : 1.0 / dt;
         double xn = 0.0;
         for (int64_t k = k1 - 1; k >= k0; k--) {
             const double xk = sd[k - e0] - sc[k - e0] * xn;
