@@ -438,11 +438,13 @@ static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t 
 {
     FricParams f = fric_params(h, nelem);
     f.off_explicit = off_explicit;
-    const unsigned grid = (unsigned)((nelem + 255) / 256);
+    // 128-thread blocks without the learned guess: five per SM at its
+    // register count (two of 256 threads); 256 with it (the network image in
+    // shared memory is staged once per block)
     if (h->form == DFN_FORM_NEWTON && h->guess == DFN_GUESS_MLP)
-        friction_kernel<true><<<grid, 256, sizeof(MlpTC), h->stream>>>(f, stage, sys, mask);
+        friction_kernel<true><<<(unsigned)((nelem + 255) / 256), 256, sizeof(MlpTC), h->stream>>>(f, stage, sys, mask);
     else
-        friction_kernel<false><<<grid, 256, 0, h->stream>>>(f, stage, sys, mask);
+        friction_kernel<false><<<(unsigned)((nelem + 127) / 128), 128, 0, h->stream>>>(f, stage, sys, mask);
     h->launches++;
     CKL();
     return DFN_OK;

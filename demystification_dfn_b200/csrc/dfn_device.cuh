@@ -1918,7 +1918,8 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
 // (LEARNED: three CTAs of 256 threads per SM, so that the rarely taken
 // inference path spills rather than cost the element path its occupancy.)
 template <bool LEARNED>
-__global__ void __launch_bounds__(256, LEARNED ? 3 : 1) friction_kernel(FricParams f, int stage, int sys, int mask)
+__global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction_kernel(FricParams f, int stage, int sys,
+                                                                                   int mask)
 {
     extern __shared__ __align__(16) unsigned char fric_smem[];
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
