@@ -193,14 +193,21 @@ def leg_single_fault(args, local, stream):
     return out
 
 
+def hmatrix_network():
+    """4000 seeded faults in 20 km x 20 km (~82k elements), tectonic shear
+    loading of 1e-9 m/s (mu v / L per fault)."""
+    from demystification_dfn_b200 import networks
+
+    return networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6, v_load=1e-9)
+
+
 def leg_hmatrix(args, local, stream):
     """4000 seeded faults in 20 km x 20 km (~82k elements), H-matrix with
     leaf 64, eta 2, ACA 1e-6, FP32 factors, FP64 sums."""
-    from demystification_dfn_b200 import networks
     from demystification_dfn_b200.simulation import Simulation
 
     hbm, _ = peaks()
-    p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
+    p = hmatrix_network()
     t0 = time.perf_counter()
     s = Simulation(p, storage="fp32", pressure=args.pressure, device=local, gemv=args.gemv, hmat_leaf=64,
                    hmat_eta=2.0, hmat_eps=1e-6)
@@ -216,7 +223,8 @@ def leg_hmatrix(args, local, stream):
     kavg = kms / max(kn, 1)
     gbs = s.kernel_bytes / (kavg / 1e3) / 1e9
     dense_equiv = 2 * s.N * s.N * 4
-    out = {"workload": "4000 faults 20x20 km, H-matrix leaf 64 eta 2 ACA 1e-6, FP32 factors", "n_elements": s.N,
+    out = {"workload": "4000 faults 20x20 km, shear loading 1e-9 m/s, H-matrix leaf 64 eta 2 ACA 1e-6, FP32 factors",
+           "n_elements": s.N,
            "build_s": build_s, "stats": st, "steps_per_s": n / (ms / 1e3), "kv_avg_ms": kavg,
            "kv_bytes": s.kernel_bytes, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
            "compression_vs_dense_fp32": s.kernel_bytes / dense_equiv, "simulated_s": rep["time"]}
@@ -484,6 +492,43 @@ def leg_ensemble_span(args, local, stream, storage="fp32", wall_limit=240.0):
     return out
 
 
+def leg_hmatrix_span(args, local, stream, wall_limit=300.0):
+    """The H-matrix network (config of leg_hmatrix) toward its 100-year span:
+    chunks of 500 accepted steps until 100 simulated years or the wall-time
+    limit; reports the simulated time reached and the largest slip rate at
+    the chunk ends (seismic phases: V > 1e-3 m/s). Not in the default legs."""
+    from demystification_dfn_b200.networks import YEAR
+    from demystification_dfn_b200.simulation import Simulation
+
+    from demystification_dfn_b200 import _lib
+    from demystification_dfn_b200.layout import DfnReport
+
+    s = Simulation(hmatrix_network(), storage="fp32", pressure=args.pressure, device=local, gemv=args.gemv,
+                   hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
+    s.set_stream(stream.cuda_stream)
+    s.autotune()
+    span = 100.0 * YEAR
+    reps = (DfnReport * 1)()
+    t0 = time.perf_counter()
+    vmax, t_seismic = 0.0, None
+    while True:
+        _lib.check(s.lib.dfn_solve_batch(s.h, 500, float(span), reps), s.lib)
+        rep = reps[0].as_dict()
+        v = float(np.abs(s.velocity()).max())
+        if v > vmax:
+            vmax = v
+        if t_seismic is None and v > 1e-3:
+            t_seismic = rep["time"]
+        if rep["status"] != 0 or rep["time"] >= span * (1 - 1e-12) or time.perf_counter() - t0 > wall_limit:
+            break
+    wall = time.perf_counter() - t0
+    out = {"span_years": 100.0, "reached_years": rep["time"] / YEAR, "accepted_steps": int(rep["it_count"]),
+           "wall_s": wall, "steps_per_s": rep["it_count"] / wall, "max_V_seen": vmax,
+           "first_seismic_time_years": None if t_seismic is None else t_seismic / YEAR, "status": int(rep["status"])}
+    s.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -535,7 +580,8 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--legs", default="precision,ensemble,single_fault,hmatrix,tensor_core,span,learned,cpu",
                     help="comma list of the extra legs to run (ensemble_span, the 64 networks over 1 "
-                         "simulated year, is available but not in the default list)")
+                         "simulated year, and hmatrix_span, the H-matrix network toward 100 years, are "
+                         "available but not in the default list)")
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -724,6 +770,8 @@ def main():
         extras["span"] = leg_span(args, local, stream)
     if rank == 0 and "ensemble_span" in legs:
         extras["ensemble_span"] = leg_ensemble_span(args, local, stream)
+    if rank == 0 and "hmatrix_span" in legs:
+        extras["hmatrix_span"] = leg_hmatrix_span(args, local, stream)
     if rank == 0 and "learned" in legs:
         extras["learned_newton"] = leg_learned(args, local, stream)
 

@@ -155,8 +155,11 @@ def _seg_dist(p1, p2, q1, q2):
 def fault_network(n_faults=800, box=7000.0, seed=0, length_range=(50.0, 500.0), strike_deg=(30.0, 10.0),
                   ds=10.0, a=0.010, b=0.015, noise=0.10, Dc=1e-3, f0=0.6, V0=1e-6, sigmaN=-50e6, V_init=1e-12,
                   dP=10e6, permeability=1e-13, mode="modeII", tol=1e-8, max_it=10, min_gap=None,
-                  q_kgs=None, name=None, kernel="direct"):
-    """Seeded random fault network (see module docstring)."""
+                  q_kgs=None, name=None, kernel="direct", v_load=0.0):
+    """Seeded random fault network (see module docstring). ``v_load`` (m/s)
+    adds tectonic shear loading: each fault's shear_loading_dot is
+    mu * v_load / L_f (its own length as the stiffness scale of the
+    equivalent slip rate), e.g. 0.06-0.6 Pa/s for 1e-9 m/s on 50-500 m faults."""
     rng = np.random.default_rng(seed)
     gap = ds if min_gap is None else min_gap
     lo, hi = np.log(length_range[0]), np.log(length_range[1])
@@ -207,6 +210,8 @@ def fault_network(n_faults=800, box=7000.0, seed=0, length_range=(50.0, 500.0), 
         f.theta[:] = np.log(V0 / f.V)
         f.P[:] = 0.0
         f.permeability[:] = permeability
+        if v_load:
+            f.shear_loading_dot[:] = p.material_loading.mu * v_load / L
         if i == stepped:
             # pressure step on the first half of the chosen fault; it diffuses
             # along the fault so that dP/dt drives the friction law
