@@ -228,7 +228,22 @@ def leg_hmatrix(args, local, stream):
            "build_s": build_s, "stats": st, "steps_per_s": n / (ms / 1e3), "kv_avg_ms": kavg,
            "kv_bytes": s.kernel_bytes, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
            "compression_vs_dense_fp32": s.kernel_bytes / dense_equiv, "simulated_s": rep["time"]}
+    st32 = s.state()
     s.close()
+    # the same 13 steps with FP64 factors (the FP64 H-matrix reference run)
+    s = Simulation(p, storage="fp64", pressure=args.pressure, device=local, gemv=args.gemv, hmat_leaf=64,
+                   hmat_eta=2.0, hmat_eps=1e-6)
+    s.set_stream(stream.cuda_stream)
+    s.solve_steps(3 + n)
+    st64 = s.state()
+    s.close()
+    N = len(st64["P"])
+    V32, V64 = st32["Y"][:N], st64["Y"][:N]
+    out["fp32_vs_fp64_factors"] = {
+        "rel_err_V": float(np.abs(V32 - V64).max() / np.abs(V64).max()),
+        "rel_err_psi": float(np.abs(st32["Y"][N:2 * N] - st64["Y"][N:2 * N]).max() / np.abs(st64["Y"][N:2 * N]).max()),
+        "rel_err_time": abs(st32["time"] - st64["time"]) / st64["time"],
+        "compared_after": "13 accepted steps from the same start"}
     return out
 
 
