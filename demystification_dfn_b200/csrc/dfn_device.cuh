@@ -627,10 +627,6 @@ __device__ __forceinline__ void prow_tri(const PressParams &p, int64_t k, double
 // kl dt/(c ds_k^2) + kr dt/(c ds_k^2) per contribution, the product gains
 // (-cl v_a + (cl + cr) v_k - cr v_b) / diag_k, both in contribution order
 // after the row's own stencil.
-__device__ __forceinline__ bool prow_x(const PressParams &p, int64_t k)
-{
-    return p.xptr != nullptr && p.xptr[k + 1] > p.xptr[k];
-}
 __device__ __forceinline__ double pdiag_x(const PressParams &p, int64_t k, double dt, double A2)
 {
     for (int64_t c = p.xptr[k]; c < p.xptr[k + 1]; c++) {
