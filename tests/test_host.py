@@ -101,3 +101,23 @@ def test_create_rejects_bad_problem(lib):
     h = ctypes.c_void_p()
     assert lib.dfn_create(ctypes.byref(c), None, ctypes.byref(h)) == 5
     assert b"nb_element" in lib.dfn_last_error()
+
+
+def test_tectonic_loading_and_crossing_pair_builders():
+    """Network builders: v_load sets each fault's shear stressing rate to
+    mu * v_load / L_f; crossing_pair shares exactly one node between its two
+    faults (shift 0) and none when shifted."""
+    import numpy as np
+
+    p = networks.fault_network(n_faults=12, box=1500.0, seed=3, v_load=1e-9)
+    mu = p.material_loading.mu
+    for f in p.faults:
+        L = float(np.hypot(*(f.node[:, -1] - f.node[:, 0])))
+        assert np.allclose(f.shear_loading_dot, mu * 1e-9 / L, rtol=1e-9)
+    q = networks.fault_network(n_faults=12, box=1500.0, seed=3)
+    assert all(np.all(f.shear_loading_dot == 0.0) for f in q.faults)
+    for shift, shared in ((0.0, 1), (1.0, 0)):
+        c = networks.crossing_pair(n_el=20, shift=shift)
+        a, b = c.faults[0].node.T, c.faults[1].node.T
+        d = np.sqrt(((a[:, None, :] - b[None, :, :]) ** 2).sum(-1))
+        assert int((d < 1e-9).sum()) == shared
