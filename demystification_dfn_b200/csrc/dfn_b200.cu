@@ -79,6 +79,10 @@ struct dfn_handle {
     // handle's stream (captured on cap_stream: capture needs a stream other
     // than the legacy default one a caller may have set)
     cudaStream_t cap_stream = nullptr;
+    // H-matrix K.V: the low-rank leaves run on side_stream beside the dense
+    // rows (fork after the permutation, join before the row sums)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int64_t graph_kernels = 0;
     bool use_graphs = true;
@@ -208,30 +212,37 @@ static const size_t kTmaSmem = TMA_STAGES * GEMV_CHUNK_BYTES + 2 * TMA_STAGES * 
 static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, bool only0)
 {
     const int64_t n1 = only0 ? h->hn1_0 : h->hn1, n2 = only0 ? h->hn2_0 : h->hn2;
+    const int64_t n3 = only0 ? h->hn3_0 : h->hn3, n4 = only0 ? h->hn4_0 : h->hn4;
     const int64_t ne = only0 ? h->hinst[0].N : h->Ntot;
     hm_permute_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->inst_of, h->inst, h->ctl, mask, h->hperm,
                                                                  Vbase, vmul, h->hxp);
     h->launches++;
     CKL();
-    if (n1 > 0) {
+    // the low-rank leaves (latency-bound) on the side stream, issued first,
+    // beside the dense rows (bandwidth-bound) on the handle's stream
+    const bool fork = (n1 > 0 || n4 > 0) && n3 > 0 && h->side_stream;
+    cudaStream_t ls = fork ? h->side_stream : h->stream;
+    if (fork) {
+        CK(cudaEventRecord(h->ev_fork, h->stream));
+        CK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    }
+    if (n4 > 0) {
         if (h->store == 0)
-            hm_lowrank_kernel<double><<<(unsigned)n1, 256, 0, h->stream>>>(
-                h->ht1, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hz);
+            hm_lowrank_fused_kernel<double><<<(unsigned)n4, 256, 0, ls>>>(
+                h->hl4, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
         else
-            hm_lowrank_kernel<float><<<(unsigned)n1, 256, 0, h->stream>>>(
-                h->ht1, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hz);
+            hm_lowrank_fused_kernel<float><<<(unsigned)n4, 256, 0, ls>>>(
+                h->hl4, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
         h->launches++;
         CKL();
     }
-    const int64_t n3 = only0 ? h->hn3_0 : h->hn3;
-    const int64_t n4 = only0 ? h->hn4_0 : h->hn4;
-    if (n4 > 0) {
+    if (n1 > 0) {
         if (h->store == 0)
-            hm_lowrank_fused_kernel<double><<<(unsigned)n4, 256, 0, h->stream>>>(
-                h->hl4, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+            hm_lowrank_kernel<double><<<(unsigned)n1, 256, 0, ls>>>(
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hz);
         else
-            hm_lowrank_fused_kernel<float><<<(unsigned)n4, 256, 0, h->stream>>>(
-                h->hl4, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+            hm_lowrank_kernel<float><<<(unsigned)n1, 256, 0, ls>>>(
+                h->ht1, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hz);
         h->launches++;
         CKL();
     }
@@ -244,6 +255,10 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
                                                                         (const float *)h->hvals, h->hxp, h->hout);
         h->launches++;
         CKL();
+    }
+    if (fork) {
+        CK(cudaEventRecord(h->ev_join, h->side_stream));
+        CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
     if (n2 > 0) {
         if (h->store == 0)
@@ -555,7 +570,7 @@ static int build_graph(dfn_handle *h)
     h->graph_kernels = h->launches - l0;
     h->launches = l0;
     if (st == DFN_OK && e2 == cudaSuccess && g) {
-        e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+        e = cudaGraphInstantiate(&h->graph_exec, g, cudaGraphInstantiateFlagUseNodePriority);
         if (e != cudaSuccess) {
             h->graph_exec = nullptr;
             st = DFN_ERR_CUDA;
@@ -1074,6 +1089,9 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    if (h->side_stream) cudaStreamDestroy(h->side_stream);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return DFN_OK;
@@ -1401,6 +1419,13 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     }
 
     if (h->hmat) {
+        // side stream of the low-rank leaves, at the highest priority so that
+        // their CTAs are placed first and the dense rows fill around them
+        int lo_pri = 0, hi_pri = 0;
+        CKC(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+        CKC(cudaStreamCreateWithPriority(&h->side_stream, cudaStreamNonBlocking, hi_pri));
+        CKC(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
         const int st = build_hmatrix(h, probs, opt);
         if (st != DFN_OK) {
             dfn_destroy(h);
