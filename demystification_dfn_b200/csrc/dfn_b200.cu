@@ -83,6 +83,7 @@ struct dfn_handle {
     // rows (fork after the permutation, join before the row sums)
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_pfork = nullptr, ev_pjoin = nullptr;   // pressure solves beside a K.V
     cudaGraphExec_t graph_exec = nullptr;
     int64_t graph_kernels = 0;
     bool use_graphs = true;
@@ -473,6 +474,31 @@ static ElemParams elem_params(dfn_handle *h)
 }
 
 
+// Pressure solves on at most half the SMs (the CG on a few thread-block
+// clusters) run on the side stream beside the K.V that follows them: they
+// depend only on the stage times, not on the stage state. The stage kernel
+// that reads them waits for the join.
+static bool pressure_beside(dfn_handle *h, int nsys, int ninst)
+{
+    if (!h->side_stream || h->pressure != DFN_PRESSURE_CG || h->pcl <= 0 || h->pcl_mode == 0 || h->pcl_mode == 2)
+        return false;
+    if (h->pcl_mode < 0 && (int64_t)nsys * ninst > h->pcl_max) return false;
+    return (int64_t)nsys * ninst * h->pcl <= h->sms / 2;
+}
+
+static int launch_pressure_side(dfn_handle *h, int mask, int kind, int sys0, int nsys, int ninst)
+{
+    CK(cudaEventRecord(h->ev_pfork, h->stream));
+    CK(cudaStreamWaitEvent(h->side_stream, h->ev_pfork, 0));
+    cudaStream_t main = h->stream;
+    h->stream = h->side_stream;
+    const int st = launch_pressure(h, mask, kind, sys0, nsys, 0.0, ninst);
+    h->stream = main;
+    TRY(st);
+    CK(cudaEventRecord(h->ev_pjoin, h->side_stream));
+    return DFN_OK;
+}
+
 // One RK attempt (stages 2..6 and the error test) of every network in `mask`.
 static int run_attempt(dfn_handle *h, int mask)
 {
@@ -482,12 +508,13 @@ static int run_attempt(dfn_handle *h, int mask)
     CKL();
     // the Newton formulation interpolates the stage pressure in time and
     // needs only the full-step system (c = 1)
-    if (h->form == DFN_FORM_NEWTON)
-        TRY(launch_pressure(h, mask, 1, 4, 1, 0.0, h->B));
-    else
-        TRY(launch_pressure(h, mask, 1, 1, 5, 0.0, h->B));
+    const int sys0 = h->form == DFN_FORM_NEWTON ? 4 : 1, nsys = h->form == DFN_FORM_NEWTON ? 1 : 5;
+    const bool beside = pressure_beside(h, nsys, h->B);
+    if (beside) TRY(launch_pressure_side(h, mask, 1, sys0, nsys, h->B));
+    else TRY(launch_pressure(h, mask, 1, sys0, nsys, 0.0, h->B));
     for (int s = 2; s <= 6; s++) {
         TRY(launch_gemv(h, mask, h->ytmp, 3, false));
+        if (s == 2 && beside) CK(cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
         TRY(launch_friction(h, s, s - 1, mask, h->Ntot));
     }
     decide_kernel<<<blocks_of(h->B, 128), 128, 0, h->stream>>>(h->ctl, h->B, mask);
@@ -505,8 +532,11 @@ static int run_round(dfn_handle *h)
     CKL();
     // CG probe at t_try (halving on non-convergence); its solution is the
     // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
-    TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
+    const bool beside = pressure_beside(h, 1, h->B);
+    if (beside) TRY(launch_pressure_side(h, M_NEW, 0, 0, 1, h->B));
+    else TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
     TRY(launch_gemv(h, M_NEW, h->Y, 3, false));
+    if (beside) CK(cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
     TRY(launch_friction(h, 1, 0, M_NEW, h->Ntot));
     set_h_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B);
     h->launches++;
@@ -1092,6 +1122,8 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->side_stream) cudaStreamDestroy(h->side_stream);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_pfork) cudaEventDestroy(h->ev_pfork);
+    if (h->ev_pjoin) cudaEventDestroy(h->ev_pjoin);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return DFN_OK;
@@ -1418,14 +1450,19 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
     }
 
-    if (h->hmat) {
-        // side stream of the low-rank leaves, at the highest priority so that
-        // their CTAs are placed first and the dense rows fill around them
+    {
+        // side stream at the highest priority (its CTAs are placed first):
+        // the H-matrix's low-rank leaves beside its dense rows, and pressure
+        // solves on a few thread-block clusters beside a K.V
         int lo_pri = 0, hi_pri = 0;
         CKC(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
         CKC(cudaStreamCreateWithPriority(&h->side_stream, cudaStreamNonBlocking, hi_pri));
         CKC(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&h->ev_pfork, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&h->ev_pjoin, cudaEventDisableTiming));
+    }
+    if (h->hmat) {
         const int st = build_hmatrix(h, probs, opt);
         if (st != DFN_OK) {
             dfn_destroy(h);
