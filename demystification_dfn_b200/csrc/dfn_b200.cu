@@ -84,6 +84,7 @@ struct dfn_handle {
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_pfork = nullptr, ev_pjoin = nullptr;   // pressure solves beside a K.V
+    cudaStream_t side_lo = nullptr;       // lowest priority: tiled pressure filling around the tensor-core GEMM
     cudaGraphExec_t graph_exec = nullptr;
     int64_t graph_kernels = 0;
     bool use_graphs = true;
@@ -474,28 +475,34 @@ static ElemParams elem_params(dfn_handle *h)
 }
 
 
-// Pressure solves on at most half the SMs (the CG on a few thread-block
-// clusters) run on the side stream beside the K.V that follows them: they
-// depend only on the stage times, not on the stage state. The stage kernel
-// that reads them waits for the join.
-static bool pressure_beside(dfn_handle *h, int nsys, int ninst)
+// Pressure solves beside the K.V that follows them (they depend only on the
+// stage times, not on the stage state); the stage kernel that reads them
+// waits for the join. Returns the stream: the high-priority one for the CG on
+// a few thread-block clusters (at most half the SMs: placed first, the K.V
+// streams on the others), the lowest-priority one for the tiled tridiagonal
+// solve of a tensor-core batch (one tile CTA fits beside each persistent GEMM
+// CTA; issued after the GEMM, so that the GEMM's CTAs are placed first and the
+// tiles fill around them), or none (in line). The fork event is recorded
+// before the K.V in both cases.
+static cudaStream_t pressure_beside(dfn_handle *h, int nsys, int ninst)
 {
-    if (!h->side_stream || h->pressure != DFN_PRESSURE_CG || h->pcl <= 0 || h->pcl_mode == 0 || h->pcl_mode == 2)
-        return false;
-    if (h->pcl_mode < 0 && (int64_t)nsys * ninst > h->pcl_max) return false;
-    return (int64_t)nsys * ninst * h->pcl <= h->sms / 2;
+    if (!h->side_stream) return nullptr;
+    if (h->pressure == DFN_PRESSURE_TRIDIAG)
+        return (h->tc && h->tc_variant == 0 && h->tri_shape == 2 && h->nlong == 0) ? h->side_lo : nullptr;
+    if (h->pressure != DFN_PRESSURE_CG || h->pcl <= 0 || h->pcl_mode == 0 || h->pcl_mode == 2) return nullptr;
+    if (h->pcl_mode < 0 && (int64_t)nsys * ninst > h->pcl_max) return nullptr;
+    return ((int64_t)nsys * ninst * h->pcl <= h->sms / 2) ? h->side_stream : nullptr;
 }
 
-static int launch_pressure_side(dfn_handle *h, int mask, int kind, int sys0, int nsys, int ninst)
+static int launch_pressure_side(dfn_handle *h, cudaStream_t side, int mask, int kind, int sys0, int nsys, int ninst)
 {
-    CK(cudaEventRecord(h->ev_pfork, h->stream));
-    CK(cudaStreamWaitEvent(h->side_stream, h->ev_pfork, 0));
+    CK(cudaStreamWaitEvent(side, h->ev_pfork, 0));
     cudaStream_t main = h->stream;
-    h->stream = h->side_stream;
+    h->stream = side;
     const int st = launch_pressure(h, mask, kind, sys0, nsys, 0.0, ninst);
     h->stream = main;
     TRY(st);
-    CK(cudaEventRecord(h->ev_pjoin, h->side_stream));
+    CK(cudaEventRecord(h->ev_pjoin, side));
     return DFN_OK;
 }
 
@@ -509,11 +516,14 @@ static int run_attempt(dfn_handle *h, int mask)
     // the Newton formulation interpolates the stage pressure in time and
     // needs only the full-step system (c = 1)
     const int sys0 = h->form == DFN_FORM_NEWTON ? 4 : 1, nsys = h->form == DFN_FORM_NEWTON ? 1 : 5;
-    const bool beside = pressure_beside(h, nsys, h->B);
-    if (beside) TRY(launch_pressure_side(h, mask, 1, sys0, nsys, h->B));
-    else TRY(launch_pressure(h, mask, 1, sys0, nsys, 0.0, h->B));
+    cudaStream_t side = pressure_beside(h, nsys, h->B);
+    const bool beside = side != nullptr, after = side == h->side_lo;
+    if (beside) CK(cudaEventRecord(h->ev_pfork, h->stream));
+    if (beside && !after) TRY(launch_pressure_side(h, side, mask, 1, sys0, nsys, h->B));
+    else if (!beside) TRY(launch_pressure(h, mask, 1, sys0, nsys, 0.0, h->B));
     for (int s = 2; s <= 6; s++) {
         TRY(launch_gemv(h, mask, h->ytmp, 3, false));
+        if (s == 2 && after) TRY(launch_pressure_side(h, side, mask, 1, sys0, nsys, h->B));
         if (s == 2 && beside) CK(cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
         TRY(launch_friction(h, s, s - 1, mask, h->Ntot));
     }
@@ -532,10 +542,13 @@ static int run_round(dfn_handle *h)
     CKL();
     // CG probe at t_try (halving on non-convergence); its solution is the
     // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
-    const bool beside = pressure_beside(h, 1, h->B);
-    if (beside) TRY(launch_pressure_side(h, M_NEW, 0, 0, 1, h->B));
-    else TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
+    cudaStream_t side = pressure_beside(h, 1, h->B);
+    const bool beside = side != nullptr, after = side == h->side_lo;
+    if (beside) CK(cudaEventRecord(h->ev_pfork, h->stream));
+    if (beside && !after) TRY(launch_pressure_side(h, side, M_NEW, 0, 0, 1, h->B));
+    else if (!beside) TRY(launch_pressure(h, M_NEW, 0, 0, 1, 0.0, h->B));
     TRY(launch_gemv(h, M_NEW, h->Y, 3, false));
+    if (after) TRY(launch_pressure_side(h, side, M_NEW, 0, 0, 1, h->B));
     if (beside) CK(cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
     TRY(launch_friction(h, 1, 0, M_NEW, h->Ntot));
     set_h_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B);
@@ -1120,6 +1133,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->side_stream) cudaStreamDestroy(h->side_stream);
+    if (h->side_lo) cudaStreamDestroy(h->side_lo);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->ev_pfork) cudaEventDestroy(h->ev_pfork);
@@ -1457,6 +1471,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         int lo_pri = 0, hi_pri = 0;
         CKC(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
         CKC(cudaStreamCreateWithPriority(&h->side_stream, cudaStreamNonBlocking, hi_pri));
+        CKC(cudaStreamCreateWithPriority(&h->side_lo, cudaStreamNonBlocking, lo_pri));
         CKC(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&h->ev_pfork, cudaEventDisableTiming));

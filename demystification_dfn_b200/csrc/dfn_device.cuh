@@ -1628,7 +1628,7 @@ __global__ void tri_coef_kernel(PressGlobal g, const Inst *inst, const int *inst
 // one segment with the recurrence of pressure_tridiag_thread_kernel (the
 // same operations: identical results) from shared memory, and the results
 // leave with coalesced stores.
-#define TRI_TILE 1024
+#define TRI_TILE 512   // 24 KB of shared memory: one tile CTA fits beside a persistent GEMM CTA
 
 __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal g, const Inst *inst, StepCtl *ctl,
                                                                     int mask, int kind, int sys0,
