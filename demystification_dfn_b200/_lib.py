@@ -87,6 +87,7 @@ def load():
                                 ctypes.POINTER(ctypes.c_float)]),
         "dfn_set_graphs": (i32, [P, i32]),
         "dfn_set_cg_form": (i32, [P, i32]),
+        "dfn_set_hmat_small_leaves": (i32, [P, i32]),
         "dfn_crossing_count": (i64, [P]),
         "dfn_set_tri_shape": (i32, [P, i32]),
         "dfn_autotune": (i32, [P, ctypes.c_void_p]),

@@ -155,6 +155,10 @@ struct dfn_handle {
     HTask *ht3 = nullptr;
     int64_t hn4 = 0, hn4_0 = 0;                        // low-rank leaves done whole
     int *hl4 = nullptr;
+    int64_t hn5 = 0, hn5_0 = 0;                        // small low-rank leaves done whole, one warp each
+    int *hl5 = nullptr;                                // their blocks (one CTA each when small_form = 1)
+    HLeafW *hlw = nullptr;                             // their descriptors (one warp each)
+    int small_form = 0;                                // small leaves: 0 one warp each, 1 one CTA each
     void *hvals = nullptr;
     int *hperm = nullptr;
     int64_t *hrowptr = nullptr, *hslots = nullptr;
@@ -215,6 +219,7 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
 {
     const int64_t n1 = only0 ? h->hn1_0 : h->hn1, n2 = only0 ? h->hn2_0 : h->hn2;
     const int64_t n3 = only0 ? h->hn3_0 : h->hn3, n4 = only0 ? h->hn4_0 : h->hn4;
+    const int64_t n5 = only0 ? h->hn5_0 : h->hn5;
     const int64_t ne = only0 ? h->hinst[0].N : h->Ntot;
     hm_permute_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->inst_of, h->inst, h->ctl, mask, h->hperm,
                                                                  Vbase, vmul, h->hxp);
@@ -222,11 +227,31 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
     CKL();
     // the low-rank leaves (latency-bound) on the side stream, issued first,
     // beside the dense rows (bandwidth-bound) on the handle's stream
-    const bool fork = (n1 > 0 || n4 > 0) && n3 > 0 && h->side_stream;
+    const bool fork = (n1 > 0 || n4 > 0 || n5 > 0) && n3 > 0 && h->side_stream;
     cudaStream_t ls = fork ? h->side_stream : h->stream;
     if (fork) {
         CK(cudaEventRecord(h->ev_fork, h->stream));
         CK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    }
+    if (n5 > 0 && h->small_form == 1) {
+        if (h->store == 0)
+            hm_lowrank_fused_kernel<double><<<(unsigned)n5, 256, 0, ls>>>(
+                h->hl5, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+        else
+            hm_lowrank_fused_kernel<float><<<(unsigned)n5, 256, 0, ls>>>(
+                h->hl5, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        h->launches++;
+        CKL();
+    } else if (n5 > 0) {
+        const unsigned g = (unsigned)((n5 + 3) / 4);
+        if (h->store == 0)
+            hm_lowrank_warp_kernel<double><<<g, 128, 0, ls>>>(h->hlw, n5, h->ctl, mask, (const double *)h->hvals,
+                                                              h->hxp, h->hout);
+        else
+            hm_lowrank_warp_kernel<float><<<g, 128, 0, ls>>>(h->hlw, n5, h->ctl, mask, (const float *)h->hvals,
+                                                             h->hxp, h->hout);
+        h->launches++;
+        CKL();
     }
     if (n4 > 0) {
         if (h->store == 0)
@@ -849,6 +874,8 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     std::vector<HBlk> blks;
     std::vector<HTask> t1, t2, t3;
     std::vector<int> l4;
+    std::vector<int> l5;     // small whole low-rank leaves (one warp each), and their descriptors
+    std::vector<HLeafW> lw;
     int64_t dense_off = 0;   // values of the dense region (first in the device array)
     int64_t lr_off = 0;      // values of the low-rank region (after it)
     const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
@@ -990,7 +1017,14 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 if (H.dense) {
                     for (int r = 0; r < L.nr; r += HM_ROWS) t3.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
                 } else if (L.nc <= HM_COLS) {
-                    l4.push_back(bi);   // whole leaf in one CTA
+                    // whole leaf: one warp when small, else one CTA
+                    if ((int64_t)H.rank * (hb.lda + hb.ld) * (int64_t)vsz <= HM_WARP_LEAF_BYTES &&
+                        hb.ld / VW <= 32 * HM_WARP_XV) {
+                        l5.push_back(bi);
+                        lw.push_back(HLeafW{hb.foff, e0 + L.c0, slot, i, H.rank, hb.lda, hb.ld, L.nr, bi});
+                    } else {
+                        l4.push_back(bi);
+                    }
                 } else {
                     for (int j = 0; j < hb.ntask1; j++)
                         t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
@@ -1005,6 +1039,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
             h->hn2_0 = (int64_t)t2.size();
             h->hn3_0 = (int64_t)t3.size();
             h->hn4_0 = (int64_t)l4.size();
+            h->hn5_0 = (int64_t)l5.size();
         }
     }
     // tasks must list network 0 first for the operator entry points; they
@@ -1018,6 +1053,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     h->hn2 = (int64_t)t2.size();
     h->hn3 = (int64_t)t3.size();
     h->hn4 = (int64_t)l4.size();
+    h->hn5 = (int64_t)l5.size();
     h->hblocks = (int64_t)blks.size();
     h->kv_bytes = (h->hdense_vals + h->hlr_vals) * (int64_t)vsz;   // stored entries, padding excluded
     // device values: [dense leaves | low-rank factors]
@@ -1039,6 +1075,11 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     if (!t2.empty()) CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hl4, std::max<size_t>(l4.size(), 1) * sizeof(int)));
     if (!l4.empty()) CK(cudaMemcpy(h->hl4, l4.data(), l4.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&h->hl5, std::max<size_t>(l5.size(), 1) * sizeof(int)));
+    if (!l5.empty()) CK(cudaMemcpy(h->hl5, l5.data(), l5.size() * sizeof(int), cudaMemcpyHostToDevice));
+    for (HLeafW &w : lw) w.aoff += dense_off;   // low-rank values follow the dense region
+    CK(cudaMalloc((void **)&h->hlw, std::max<size_t>(lw.size(), 1) * sizeof(HLeafW)));
+    if (!lw.empty()) CK(cudaMemcpy(h->hlw, lw.data(), lw.size() * sizeof(HLeafW), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->ht3, std::max<size_t>(t3.size(), 1) * sizeof(HTask)));
     if (!t3.empty()) CK(cudaMemcpy(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
@@ -1118,7 +1159,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,
@@ -1822,6 +1863,18 @@ int32_t dfn_set_cg_form(dfn_handle *h, int32_t form)
     CK(cudaSetDevice(h->dev));
     CK(cudaStreamSynchronize(h->stream));
     h->pcl_mode = form;
+    drop_graph(h);
+    return DFN_OK;
+}
+
+int32_t dfn_set_hmat_small_leaves(dfn_handle *h, int32_t form)
+{
+    if (!h) return DFN_ERR_ARG;
+    if (!h->hmat) { g_err = "handle uses the dense kernel"; return DFN_ERR_UNSUPPORTED; }
+    if (form < 0 || form > 1) { g_err = "form must be 0 (one warp per leaf) or 1 (one CTA per leaf)"; return DFN_ERR_ARG; }
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->small_form = form;
     drop_graph(h);
     return DFN_OK;
 }

@@ -194,6 +194,96 @@ __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__rest
     }
 }
 
+// Small low-rank leaves, one warp each (four per 128-thread CTA), from a
+// compact descriptor list (one load per leaf before its factors): z = B^T xp
+// with lanes in groups of the B^T row's vector count (several rank rows per
+// pass when the rows are short; the lane's x vectors held in registers),
+// then y = A z with a 16-byte vector of A rows per lane (rows summed over
+// the rank in order, as in hm_lowrank_fused_kernel), written to the leaf's
+// output slots. Leaves qualify when their factors take at most
+// HM_WARP_LEAF_BYTES and their B^T rows at most 32 * HM_WARP_XV vectors.
+// These leaves are a few KB each and latency-bound: a SM holds the loads of
+// dozens of them in flight, against 8 with one CTA per leaf.
+constexpr int HM_WARP_LEAF_BYTES = 32 * 1024;
+constexpr int HM_WARP_XV = 2;
+
+struct HLeafW {
+    int64_t aoff;     // A^T offset (values); B^T follows at aoff + rank * lda
+    int64_t xoff;     // first column of the leaf in xp
+    int64_t outoff;   // first output slot of the leaf's rows
+    int inst, rank, lda, ld, nr, blk;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+                                                                  const StepCtl *__restrict__ ctl, int mask,
+                                                                  const T *__restrict__ vals,
+                                                                  const double *__restrict__ xp,
+                                                                  double *__restrict__ out)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    __shared__ double zs[4][hmat::kMaxRank];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t k = (int64_t)blockIdx.x * 4 + warp;
+    if (k >= n) return;   // warp-uniform; the kernel has no block barrier
+    const HLeafW d = leaves[k];
+    if (!takes_part(ctl, d.inst, mask)) return;
+    const int rank = d.rank, nv = d.ld / W;
+    int g = 1;
+    while (g < nv && g < 32) g <<= 1;
+    const int sub = lane / g, v0 = lane % g, rp = 32 / g;
+    double xv[HM_WARP_XV][W];
+#pragma unroll
+    for (int m = 0; m < HM_WARP_XV; m++) {
+        const int v = v0 + m * g;
+#pragma unroll
+        for (int c = 0; c < W; c++) xv[m][c] = (v < nv) ? __ldg(xp + d.xoff + v * W + c) : 0.0;
+    }
+    const T *A = vals + d.aoff;
+    const VT *Bt = reinterpret_cast<const VT *>(A + (int64_t)rank * d.lda);
+    double *z = zs[warp];
+#pragma unroll 4
+    for (int q0 = 0; q0 < rank; q0 += rp) {
+        const int q = q0 + sub;
+        double acc = 0.0;
+        if (q < rank) {
+#pragma unroll
+            for (int m = 0; m < HM_WARP_XV; m++) {
+                const int v = v0 + m * g;
+                if (v < nv) {
+                    double f[W];
+                    HVec<T>::unpack(Bt[(int64_t)q * nv + v], f);
+#pragma unroll
+                    for (int c = 0; c < W; c++) acc = fma(f[c], xv[m][c], acc);
+                }
+            }
+        }
+        for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (v0 == 0 && q < rank) z[q] = acc;
+    }
+    __syncwarp();
+    const int nav = (d.nr + W - 1) / W;   // vectors of an A row (padding rows are zero)
+    const int avl = d.lda / W;
+    const VT *Av = reinterpret_cast<const VT *>(A);
+    for (int rv = lane; rv < nav; rv += 32) {
+        double acc[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) acc[c] = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < rank; q++) {
+            double a[W];
+            HVec<T>::unpack(Av[(int64_t)q * avl + rv], a);
+            const double zq = z[q];
+#pragma unroll
+            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < W; c++)
+            if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
+    }
+}
+
 // Rows of low-rank leaves: one thread per row, sum over the rank of
 // A^T[q][row] z[q] (coalesced across the threads for each q).
 template <typename T>

@@ -20,6 +20,10 @@
         the same network with CG pressure: the autotuner's timing of the
         stage pressure systems by one CTA each and by a cluster of CTAs each
         (one JSON line).
+    python -m demystification_dfn_b200.profile_case hmatrix_round
+        the same network with shear loading (1e-9 m/s) and CG pressure: four
+        solve steps launched one by one (launch list of a step: the H-matrix
+        K.V kernels, the pressure solves, the stage kernel, step control).
     python -m demystification_dfn_b200.profile_case ensemble_round
         eight 120-fault networks (FP32 storage, tridiagonal pressure), forty
         solve rounds launched one by one.
@@ -92,6 +96,13 @@ def main(argv):
         p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6)
         e = Simulation(p, storage="fp32", pressure="cg", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
         print(json.dumps(e.autotune()))
+    elif case == "hmatrix_round":
+        from .simulation import Simulation
+
+        p = networks.fault_network(n_faults=4000, box=20000.0, seed=0, kernel="hmatrix", tol=1e-6, v_load=1e-9)
+        e = Simulation(p, storage="fp32", pressure="cg", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
+        e.set_graphs(False)
+        e.solve_steps(4)
     elif case == "ensemble_round":
         e = Ensemble([networks.ensemble_member(s, n_faults=120) for s in range(64, 72)], storage="fp32",
                      pressure="tridiag")

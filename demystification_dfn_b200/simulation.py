@@ -106,6 +106,11 @@ class Simulation:
         """Short tridiagonal segments by "warp", "thread" or "tile"."""
         _lib.check(self.lib.dfn_set_tri_shape(self.h, {"warp": 0, "thread": 1, "tile": 2}[shape]), self.lib)
 
+    def set_hmat_small_leaves(self, form):
+        """H-matrix handles: whole low-rank leaves of at most 32 KiB by one
+        "warp" each (the default) or one "cta" each."""
+        _lib.check(self.lib.dfn_set_hmat_small_leaves(self.h, {"warp": 0, "cta": 1}[form]), self.lib)
+
     def set_cg_form(self, form):
         """CG pressure solves by "cta" (one CTA per system, global memory),
         "cluster" (a thread-block cluster per system, shared memory),

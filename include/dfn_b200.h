@@ -252,6 +252,13 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable);
  * the solver tolerance. dfn_autotune sets the fastest. No counterpart in the
  * reference. */
 int32_t dfn_set_cg_form(dfn_handle *h, int32_t form);
+/* H-matrix handles: the whole low-rank leaves of at most 32 KiB of factors
+ * by one warp each, four per CTA (form 0, the default: the loads of many
+ * leaves in flight per SM), or by one CTA each (form 1, like the larger
+ * leaves). The forms sum each leaf in another order (agreement to
+ * rounding). No counterpart in the reference (ZGEMV per leaf,
+ * src/hmatrix/calculation_hmat.f90:3-165). */
+int32_t dfn_set_hmat_small_leaves(dfn_handle *h, int32_t form);
 /* Launch shape of the short tridiagonal segments (DFN_PRESSURE_TRIDIAG
  * handles): 0 one warp per segment (scans), 1 one thread per segment, 2 one
  * thread per segment in tiles staged through shared memory (identical to 1).

@@ -48,6 +48,26 @@ def test_hmat_kv_against_dense_oracle(mode, storage):
             assert rel(gN, dN) < tol and rel(hN, dN) < tol
 
 
+@pytest.mark.parametrize("storage", ["fp64", "fp32"])
+def test_hmat_small_leaves_by_warp_or_cta(storage):
+    """Whole low-rank leaves of a few KB by one warp each (default) or by one
+    CTA each: the same products summed in another order, so K.V agrees to
+    rounding, and the warp form repeats bit for bit."""
+    p = hnet("modeII", seed=4, n=60, box=2000.0)
+    kw = dict(storage=storage, pressure="tridiag", hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6)
+    with Simulation(p, **kw) as s:
+        assert s.hmat_stats()["lowrank_leaves"] > 400
+        v = np.random.default_rng(3).normal(size=s.N) * 1e-9
+        warp = s.kernel(v)
+        assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), warp))
+        s.set_hmat_small_leaves("cta")
+        cta = s.kernel(v)
+        for a, b in zip(warp, cta):
+            assert rel(a, b) < 1e-12
+        s.set_hmat_small_leaves("warp")
+        assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), warp))
+
+
 def test_hmat_reference_defaults_on_shipped_bp6():
     """The reference's own BP6 input uses static_kernel = hmatrix with its
     defaults (nleaf 100, eta 3, eps 1e-8)."""
