@@ -225,9 +225,10 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
                                                                  Vbase, vmul, h->hxp);
     h->launches++;
     CKL();
-    // the low-rank leaves (latency-bound) on the side stream, issued first,
-    // beside the dense rows (bandwidth-bound) on the handle's stream
-    const bool fork = (n1 > 0 || n4 > 0 || n5 > 0) && n3 > 0 && h->side_stream;
+    // the low-rank leaves (latency-bound; the rows of the wide ones after
+    // their z partials) on the side stream, issued first, beside the dense
+    // rows (bandwidth-bound) on the handle's stream
+    const bool fork = (n1 > 0 || n2 > 0 || n4 > 0 || n5 > 0) && n3 > 0 && h->side_stream;
     cudaStream_t ls = fork ? h->side_stream : h->stream;
     if (fork) {
         CK(cudaEventRecord(h->ev_fork, h->stream));
@@ -273,6 +274,16 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         h->launches++;
         CKL();
     }
+    if (n2 > 0) {
+        if (h->store == 0)
+            hm_rows_kernel<double><<<(unsigned)n2, 256, 0, ls>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                        (const double *)h->hvals, h->hz, h->hout);
+        else
+            hm_rows_kernel<float><<<(unsigned)n2, 256, 0, ls>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
+                                                                       (const float *)h->hvals, h->hz, h->hout);
+        h->launches++;
+        CKL();
+    }
     if (n3 > 0) {
         if (h->store == 0)
             hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
@@ -286,16 +297,6 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
     if (fork) {
         CK(cudaEventRecord(h->ev_join, h->side_stream));
         CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
-    }
-    if (n2 > 0) {
-        if (h->store == 0)
-            hm_rows_kernel<double><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
-                                                                        (const double *)h->hvals, h->hz, h->hout);
-        else
-            hm_rows_kernel<float><<<(unsigned)n2, 256, 0, h->stream>>>(h->ht2, h->hblk, h->inst, h->ctl, mask,
-                                                                       (const float *)h->hvals, h->hz, h->hout);
-        h->launches++;
-        CKL();
     }
     hm_gather_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->ncomp, h->inst_of, h->inst, h->ctl, mask,
                                                                 h->hperm, h->hrowptr, h->hslots, h->hout, h->partT,
