@@ -948,7 +948,10 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 const int64_t seg0 = lr_off;
                 for (size_t t = 0; t < al.size(); t++) {
                     HostLeaf &H = host[lr[q0 + t]];
-                    const int rk = ranks[t] > hmat::kMaxRank ? -1 : ranks[t];
+                    // dense where the ACA did not converge, or where its factors
+                    // would not be smaller than the block
+                    int rk = ranks[t] > hmat::kMaxRank ? -1 : ranks[t];
+                    if (rk > 0 && (int64_t)(al[t].nr + al[t].nc) * rk >= (int64_t)al[t].nr * al[t].nc) rk = -1;
                     pl[t] = AcaPlace{0, 0, 0, 0, 0};
                     if (rk < 0) continue;   // did not converge: stored dense
                     H.dense = 0;

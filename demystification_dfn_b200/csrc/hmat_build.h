@@ -33,7 +33,7 @@ namespace hmat {
 // Largest rank stored as a low-rank leaf (the reference stops beyond 20,
 // src/hmatrix/H_matrix_construction.f90:59; 2D point clouds at eps 1e-6
 // and eta 2 need more, and a block that would exceed it is stored dense).
-constexpr int kMaxRank = 64;
+constexpr int kMaxRank = 128;
 
 struct Cluster {
     int first, last;   // inclusive, positions in cluster order

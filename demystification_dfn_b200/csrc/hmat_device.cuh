@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(256) hm_fill_dense_kernel(const HTask *__restr
 //     residual column into A, ||S_k||_F^2 updated by 2 sum_q (a_q.a_k)(b_q.b_k)
 //     + |a_k|^2 |b_k|^2, stop at |a_k||b_k| <= eps ||S_k||_F, next pivot row
 //     = the largest unused |a_k(i)|; -1 beyond HM_KMAX terms (stored dense);
-//   recompression (when 0 < k < min(m, n)): Householder QR of A and B in
+//   recompression (when 0 < k < min(m, n) and k <= HM_KSVD; blocks of more
+//     terms keep their ACA factors): Householder QR of A and B in
 //     place (reflectors below the diagonal, R above it, R's diagonal and the
 //     reflector scales in shared memory), one-sided Jacobi SVD of
 //     R_A R_B^T (k x k, shared memory; rotations of a sweep in parallel
@@ -370,17 +371,22 @@ __global__ void __launch_bounds__(256) hm_fill_dense_kernel(const HTask *__restr
 // Results: rank[b] (-1 dense, 0 zero block) and the factors A' (m x r) and
 // B' (n x r), column-major by rank, in the leaf's X regions of the scratch.
 // Sums are block reductions in a fixed order (deterministic).
-#define HM_KMAX 64
+#define HM_KMAX 128   // ACA terms at most
+#define HM_KSVD 64    // recompression up to this rank (its k x k matrices in shared memory)
 #define HM_BT 128
 
 struct AcaLeaf {
     int r0, c0, nr, nc;
-    int64_t soff;     // scratch doubles: A (nr x 64), B (nc x 64), XA (nr x 64), XB (nc x 64)
+    int64_t soff;     // scratch doubles: A, B, XA, XB (nr, nc, nr, nc x HM_KMAX)
     int64_t foff;     // char flags: nr row flags, nc column flags
 };
 
-// Dynamic shared memory of hm_aca_kernel: G/U and W (64 x 64 each) + small arrays.
-constexpr size_t hm_aca_smem_bytes() { return (size_t)(2 * HM_KMAX * HM_KMAX + 8 * HM_KMAX + 64) * sizeof(double); }
+// Dynamic shared memory of hm_aca_kernel: G/U and W (HM_KSVD^2 each), five
+// HM_KSVD arrays, three HM_KMAX arrays and 64 doubles of reductions.
+constexpr size_t hm_aca_smem_bytes()
+{
+    return (size_t)(2 * HM_KSVD * HM_KSVD + 5 * HM_KSVD + 3 * HM_KMAX + 64) * sizeof(double);
+}
 
 __device__ __forceinline__ double hm_block_sum(double v, double *red)
 {
@@ -497,12 +503,12 @@ __global__ void __launch_bounds__(HM_BT) hm_aca_kernel(const AcaLeaf *__restrict
 {
     extern __shared__ __align__(16) double hm_sm[];
     double *U = hm_sm;                          // k x k, column-major (G, then U)
-    double *W = U + HM_KMAX * HM_KMAX;          // k x k
-    double *tauA = W + HM_KMAX * HM_KMAX, *tauB = tauA + HM_KMAX, *alA = tauB + HM_KMAX, *alB = alA + HM_KMAX;
-    double *Sv = alB + HM_KMAX, *aq = Sv + HM_KMAX, *bq = aq + HM_KMAX, *cache = bq + HM_KMAX;
+    double *W = U + HM_KSVD * HM_KSVD;          // k x k
+    double *tauA = W + HM_KSVD * HM_KSVD, *tauB = tauA + HM_KSVD, *alA = tauB + HM_KSVD, *alB = alA + HM_KSVD;
+    double *Sv = alB + HM_KSVD, *aq = Sv + HM_KSVD, *bq = aq + HM_KMAX, *cache = bq + HM_KMAX;
     double *red = cache + HM_KMAX;              // 64 doubles: reductions
     __shared__ int redi[HM_BT / 32];
-    __shared__ int ord[HM_KMAX];
+    __shared__ int ord[HM_KSVD];
     __shared__ int s_i, s_k, s_done;
     __shared__ double s_norm2;
 
@@ -605,7 +611,7 @@ __global__ void __launch_bounds__(HM_BT) hm_aca_kernel(const AcaLeaf *__restrict
         if (tid == 0) rank_out[blockIdx.x] = k;
         return;
     }
-    if (k >= min(m, n)) {
+    if (k >= min(m, n) || k > HM_KSVD) {
         // no recompression: the ACA factors as they are
         for (int64_t q = tid; q < (int64_t)m * k; q += HM_BT) XA[q] = A[q];
         for (int64_t q = tid; q < (int64_t)n * k; q += HM_BT) XB[q] = B[q];
