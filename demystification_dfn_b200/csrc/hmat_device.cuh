@@ -39,7 +39,7 @@ struct HTask { int blk, start, count, chunk; };
 
 constexpr int HM_COLS = 1024;  // columns per step-1 task
 constexpr int HM_ROWS = 64;    // rows per step-2 task of a dense leaf
-constexpr int HM_LROWS = 256;  // rows per step-2 task of a low-rank leaf
+constexpr int HM_LROWS = 1024; // rows per step-2 task of a low-rank leaf (a 16-byte vector per thread)
 constexpr int HM_XPAD = 8;     // zero doubles after xp (padded columns read them)
 
 template <typename T> struct HVec;
@@ -67,8 +67,9 @@ __global__ void hm_permute_kernel(int64_t Ntot, const int *__restrict__ inst_of,
     xp[e] = Vbase[(int64_t)vmul * I.eoff + perm[e]];
 }
 
-// z partial of one column chunk: warp w takes rank rows q = w, w+8, ...;
-// lanes stream the row's columns in 16-byte vectors.
+// z partial of one column chunk: the chunk's x staged once in shared memory;
+// warp w takes rank rows q = w, w+8, ... two at a time (independent sums, so
+// their loads overlap); lanes stream a row's columns in 16-byte vectors.
 template <typename T>
 __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
                                                          const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
@@ -77,25 +78,41 @@ __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict
 {
     using VT = typename HVec<T>::V;
     constexpr int W = HVec<T>::W;
+    __shared__ __align__(16) double xs[HM_COLS + HM_XPAD];
     const HTask t = tasks[blockIdx.x];
     const HBlk b = blks[t.blk];
-    if (!takes_part(ctl, b.inst, mask)) return;
+    if (!takes_part(ctl, b.inst, mask)) return;   // CTA-uniform: before the barrier
     const Inst &I = inst[b.inst];
     const double *x = xp + I.eoff + b.c0 + t.start;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nv = (t.count + W - 1) / W;    // vectors of the chunk (padding columns are zero)
-    for (int q = w; q < b.rank; q += 8) {
-        const VT *row = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld + t.start);
-        double s = 0.0;
+    for (int j = threadIdx.x; j < nv * W; j += blockDim.x) xs[j] = x[j];
+    __syncthreads();
+    for (int q = w; q < b.rank; q += 16) {
+        const bool two = q + 8 < b.rank;
+        const VT *row0 = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld + t.start);
+        const VT *row1 = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)(two ? q + 8 : q) * b.ld + t.start);
+        double s0 = 0.0, s1 = 0.0;
         for (int v = lane; v < nv; v += 32) {
-            double f[W];
-            HVec<T>::unpack(row[v], f);
+            double f0[W], f1[W];
+            HVec<T>::unpack(row0[v], f0);
+            HVec<T>::unpack(row1[v], f1);
 #pragma unroll
-            for (int j = 0; j < W; j++) s = fma(f[j], x[v * W + j], s);
+            for (int j = 0; j < W; j++) {
+                const double xv = xs[v * W + j];
+                s0 = fma(f0[j], xv, s0);
+                s1 = fma(f1[j], xv, s1);
+            }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) zpart[b.zoff + (int64_t)t.chunk * b.rank + q] = s;
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        }
+        if (lane == 0) {
+            zpart[b.zoff + (int64_t)t.chunk * b.rank + q] = s0;
+            if (two) zpart[b.zoff + (int64_t)t.chunk * b.rank + q + 8] = s1;
+        }
     }
 }
 
@@ -152,9 +169,11 @@ __global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__
     }
 }
 
-// Low-rank leaves of at most HM_COLS columns, whole: z = B^T xp into shared
-// memory (warp per rank row), then the rows y = A z (thread per row); one
-// CTA per leaf, no partial sums in global memory.
+// Low-rank leaves of at most HM_COLS columns, whole: x staged in shared
+// memory, z = B^T xp into shared memory (warp per rank row, two rows at a
+// time), then the rows y = A z (a 16-byte vector of A rows per thread, each
+// row summed over the rank in order); one CTA per leaf, no partial sums in
+// global memory.
 template <typename T>
 __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__restrict__ leaves,
                                                                const HBlk *__restrict__ blks,
@@ -166,31 +185,59 @@ __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__rest
     using VT = typename HVec<T>::V;
     constexpr int W = HVec<T>::W;
     __shared__ double z[hmat::kMaxRank];
+    __shared__ __align__(16) double xs[HM_COLS + HM_XPAD];
     const HBlk b = blks[leaves[blockIdx.x]];
-    if (!takes_part(ctl, b.inst, mask)) return;
+    if (!takes_part(ctl, b.inst, mask)) return;   // CTA-uniform: before the barriers
     const Inst &I = inst[b.inst];
     const double *x = xp + I.eoff + b.c0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nv = (b.nc + W - 1) / W;
-    for (int q = w; q < b.rank; q += 8) {
-        const VT *row = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld);
-        double s = 0.0;
+    for (int j = threadIdx.x; j < nv * W; j += blockDim.x) xs[j] = x[j];
+    __syncthreads();
+    for (int q = w; q < b.rank; q += 16) {
+        const bool two = q + 8 < b.rank;
+        const VT *row0 = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)q * b.ld);
+        const VT *row1 = reinterpret_cast<const VT *>(vals + b.goff + (int64_t)(two ? q + 8 : q) * b.ld);
+        double s0 = 0.0, s1 = 0.0;
         for (int v = lane; v < nv; v += 32) {
-            double f[W];
-            HVec<T>::unpack(row[v], f);
+            double f0[W], f1[W];
+            HVec<T>::unpack(row0[v], f0);
+            HVec<T>::unpack(row1[v], f1);
 #pragma unroll
-            for (int j = 0; j < W; j++) s = fma(f[j], x[v * W + j], s);
+            for (int j = 0; j < W; j++) {
+                const double xv = xs[v * W + j];
+                s0 = fma(f0[j], xv, s0);
+                s1 = fma(f1[j], xv, s1);
+            }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) z[q] = s;
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        }
+        if (lane == 0) {
+            z[q] = s0;
+            if (two) z[q + 8] = s1;
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < b.nr; i += blockDim.x) {
-        const T *a = vals + b.foff + i;
-        double s = 0.0;
-        for (int q = 0; q < b.rank; q++) s = fma((double)a[(int64_t)q * b.lda], z[q], s);
-        out[b.outoff + i] = s;
+    const int nav = (b.nr + W - 1) / W, avl = b.lda / W;
+    const VT *Av = reinterpret_cast<const VT *>(vals + b.foff);
+    for (int iv = threadIdx.x; iv < nav; iv += blockDim.x) {
+        double acc[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) acc[c] = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < b.rank; q++) {
+            double a[W];
+            HVec<T>::unpack(Av[(int64_t)q * avl + iv], a);
+            const double zq = z[q];
+#pragma unroll
+            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < W; c++)
+            if (iv * W + c < b.nr) out[b.outoff + iv * W + c] = acc[c];
     }
 }
 
@@ -284,14 +331,17 @@ __global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *_
     }
 }
 
-// Rows of low-rank leaves: one thread per row, sum over the rank of
-// A^T[q][row] z[q] (coalesced across the threads for each q).
+// Rows of low-rank leaves: a 16-byte vector of A rows per thread (rows of a
+// task start at a multiple of HM_LROWS), each row the sum over the rank of
+// A^T[q][row] z[q] in order.
 template <typename T>
 __global__ void __launch_bounds__(256) hm_rows_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                       int mask, const T *__restrict__ vals,
                                                       const double *__restrict__ zpart, double *__restrict__ out)
 {
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
     __shared__ double z[hmat::kMaxRank];
     const HTask t = tasks[blockIdx.x];
     const HBlk b = blks[t.blk];
@@ -303,12 +353,23 @@ __global__ void __launch_bounds__(256) hm_rows_kernel(const HTask *__restrict__ 
         z[threadIdx.x] = s;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < t.count; i += blockDim.x) {
-        const int row = t.start + i;
-        const T *a = vals + b.foff + row;
-        double s = 0.0;
-        for (int q = 0; q < r; q++) s = fma((double)a[(int64_t)q * b.lda], z[q], s);
-        out[b.outoff + row] = s;
+    const int nav = (t.count + W - 1) / W, avl = b.lda / W, v0 = t.start / W;
+    const VT *Av = reinterpret_cast<const VT *>(vals + b.foff);
+    for (int iv = threadIdx.x; iv < nav; iv += blockDim.x) {
+        double acc[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) acc[c] = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < r; q++) {
+            double a[W];
+            HVec<T>::unpack(Av[(int64_t)q * avl + v0 + iv], a);
+            const double zq = z[q];
+#pragma unroll
+            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < W; c++)
+            if (iv * W + c < t.count) out[b.outoff + t.start + iv * W + c] = acc[c];
     }
 }
 
