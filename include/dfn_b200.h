@@ -113,7 +113,12 @@ typedef struct dfn_options {
                                  tensor-core storage: 0 persistent GEMM, 1 / 2 one unit
                                  per CTA with the deepest / a 2-stage ring */
     /* H-matrix parameters for static_kernel = hmatrix (0 = the reference's
-     * defaults nleaf=100, eta=3, eps_ACA=1e-8, src/variables.f90:122-124) */
+     * defaults nleaf=100, eta=3, eps_ACA=1e-8, src/variables.f90:122-124).
+     * Admissible blocks get a partial-pivot ACA of at most 128 terms to
+     * eps_ACA (recompressed when at most 64); a block whose ACA does not
+     * converge within 128 terms, or whose factors would not be smaller than
+     * the block, is stored dense (the reference truncates at rank 20,
+     * src/hmatrix/H_matrix_construction.f90:59). */
     int32_t hmat_leaf;
     /* DFN_FORM_V integrates V as the reference does; DFN_FORM_NEWTON
      * integrates slip and psi and solves the friction law for V by Newton

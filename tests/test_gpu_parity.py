@@ -401,7 +401,8 @@ def test_event_onset_matches_oracle(mode):
     """A velocity-weakening fault (a = 0.010 < b = 0.015) loaded by a 200 kg/s
     injection reaches seismic slip rates within ~70 steps: the first accepted
     step with max V > 1e-3 m/s comes at the same step and, in simulated time,
-    within 1e-6 of the simulated span (the north-star event-onset target)."""
+    within 1e-6 of the simulated span (the event-onset tolerance of the
+    seismic-cycle runs)."""
     p = networks.single_fault(n_el=200, length=2000.0, a=0.010, b=0.015, Dc=1e-3, q_kgs=200.0, tol=1e-6,
                               mode=mode)
     o = Oracle(p, threads=4)
