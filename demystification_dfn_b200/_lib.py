@@ -17,6 +17,7 @@ STATUS = {
     0: "ok", 1: "pressure CG did not converge", 2: "stepsize underflow in rkqs",
     3: "normal traction became extensional", 4: "non-finite value", 5: "invalid argument",
     6: "CUDA error", 7: "unsupported", 8: "too many rejected attempts", 9: "device allocation failed",
+    10: "a bounded device wait expired",
 }
 
 EXPORTS = [
@@ -86,6 +87,7 @@ def load():
         "dfn_mlp_infer": (i32, [ctypes.POINTER(ctypes.c_float), i64, ctypes.POINTER(ctypes.c_float),
                                 ctypes.POINTER(ctypes.c_float)]),
         "dfn_set_graphs": (i32, [P, i32]),
+        "dfn_set_wait_limit": (i32, [P, i32]),
         "dfn_set_cg_form": (i32, [P, i32]),
         "dfn_set_hmat_small_leaves": (i32, [P, i32]),
         "dfn_crossing_count": (i64, [P]),

@@ -17,12 +17,12 @@
 #include "tc_gemm.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <unordered_map>
 #include <array>
 #include <deque>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -120,6 +120,7 @@ struct dfn_handle {
     double *Ptemp = nullptr, *Pdot_s = nullptr, *pwork = nullptr, *vin = nullptr, *vout = nullptr, *snap = nullptr;
     double *pcoef = nullptr;              // CG row coefficients [6][3N] per network
     int *err_flag = nullptr;
+    int wait_polls = MBAR_POLLS;          // polls of the TMA K.V pipeline's bounded waits
     void *K = nullptr;
     size_t K_bytes = 0;
     int64_t kv_bytes = 0;         // algorithmic bytes of one K.V over the batch
@@ -187,7 +188,7 @@ static const int kProfMax = 16384;
 typedef void (*gemv_fn)(const int4 *, const Inst *, const StepCtl *, int, const uint4 *, const double *, int,
                         double *, double *);
 typedef void (*gemv_tma_fn)(const int4 *, const Inst *, const StepCtl *, int, const uint4 *, const double *, int,
-                            double *, double *, int *);
+                            double *, double *, int, int *);
 
 static gemv_fn pick_gemv(int mode, int store)
 {
@@ -365,7 +366,7 @@ static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, b
     } else if (h->gemv_impl == 0) {
         gemv_tma_fn fn = pick_gemv_tma(h->mode, h->store);
         fn<<<(unsigned)ntiles, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(
-            h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul, h->partT, h->partN, h->err_flag);
+            h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul, h->partT, h->partN, h->wait_polls, h->err_flag);
     } else {
         gemv_fn fn = pick_gemv(h->mode, h->store);
         fn<<<(unsigned)ntiles, GEMV_WARPS * 32, 0, h->stream>>>(h->tiles, h->inst, h->ctl, mask, K, Vbase, vmul,
@@ -598,8 +599,11 @@ static int sync_ctl(dfn_handle *h)
     int flag = 0;
     CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
-        g_err = "bounded wait expired in the TMA K.V pipeline";
-        return DFN_ERR_CUDA;
+        // reported once: the flag is cleared so that the handle can be
+        // reused after the caller has restored its state
+        CK(cudaMemset(h->err_flag, 0, sizeof(int)));
+        g_err = "a bounded wait of a K.V pipeline expired (its partial sums are incomplete)";
+        return DFN_ERR_TIMEOUT;
     }
     return DFN_OK;
 }
@@ -1142,6 +1146,7 @@ const char *dfn_status_string(int32_t s)
     case DFN_ERR_UNSUPPORTED: return "unsupported feature";
     case DFN_ERR_ATTEMPTS: return "too many rejected attempts in one step";
     case DFN_ERR_NOMEM: return "device allocation failed";
+    case DFN_ERR_TIMEOUT: return "a bounded device wait expired";
     default: return "unknown status";
     }
 }
@@ -1188,6 +1193,13 @@ int32_t dfn_destroy(dfn_handle *h)
     return DFN_OK;
 }
 
+static bool all_finite(const double *x, int64_t n)
+{
+    for (int64_t i = 0; i < n; i++)
+        if (!std::isfinite(x[i])) return false;
+    return true;
+}
+
 static int check_problem(const dfn_problem *p)
 {
     const int64_t N = p->nb_element, F = p->nb_fault;
@@ -1209,6 +1221,14 @@ static int check_problem(const dfn_problem *p)
             return DFN_ERR_ARG;
         }
     }
+    // the initial state must be finite (the reference would carry a NaN
+    // into every right-hand side and reject every attempt)
+    const double *st[4] = {p->V, p->theta, p->sigmaN, p->P};
+    for (int j = 0; j < 4; j++)
+        if (!all_finite(st[j], N)) {
+            g_err = "non-finite value in the initial state (V, theta, sigmaN or P)";
+            return DFN_ERR_NONFINITE;
+        }
     return DFN_OK;
 }
 
@@ -1840,6 +1860,14 @@ int32_t dfn_set_graphs(dfn_handle *h, int32_t enable)
     return DFN_OK;
 }
 
+int32_t dfn_set_wait_limit(dfn_handle *h, int32_t polls)
+{
+    if (!h) return DFN_ERR_ARG;
+    h->wait_polls = polls < 0 ? MBAR_POLLS : polls;
+    drop_graph(h);   // a captured graph holds the old limit in its kernel parameters
+    return DFN_OK;
+}
+
 int64_t dfn_crossing_count(const dfn_handle *h) { return h ? h->ncross : -1; }
 
 int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape)
@@ -1944,7 +1972,11 @@ int32_t dfn_kernel_batch(dfn_handle *h, const double *slip, double *sT, double *
     if (st != DFN_OK) return st;
     int flag = 0;
     CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) { g_err = "a K.V kernel gave up waiting on its pipeline"; return DFN_ERR_CUDA; }
+    if (flag) {
+        CK(cudaMemset(h->err_flag, 0, sizeof(int)));
+        g_err = "a bounded wait of a K.V pipeline expired (its partial sums are incomplete)";
+        return DFN_ERR_TIMEOUT;
+    }
     return DFN_OK;
 }
 
@@ -2102,6 +2134,10 @@ int32_t dfn_set_state(dfn_handle *h, const double *Y, const double *P, double ti
     if (!h) return DFN_ERR_ARG;
     TRY(single_only(h));
     const int64_t N = h->hinst[0].N;
+    if ((Y && !all_finite(Y, 3 * N)) || (P && !all_finite(P, N)) || !std::isfinite(time) || !std::isfinite(t_try)) {
+        g_err = "dfn_set_state: non-finite value in the state";
+        return DFN_ERR_NONFINITE;
+    }
     CK(cudaSetDevice(h->dev));
     if (Y) CK(cudaMemcpyAsync(h->Y, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
     if (P) CK(cudaMemcpyAsync(h->P, P, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
@@ -2138,6 +2174,10 @@ int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, dou
     if (!h || !Y_in || !P_in) return DFN_ERR_ARG;
     TRY(single_only(h));
     const int64_t N = h->hinst[0].N;
+    if (!all_finite(Y_in, 3 * N) || !all_finite(P_in, N) || !std::isfinite(time_in) || !std::isfinite(t_try_in)) {
+        g_err = "dfn_step_host: non-finite value in the state";
+        return DFN_ERR_NONFINITE;
+    }
     CK(cudaSetDevice(h->dev));
     TRY(sync_ctl(h));
     CK(cudaMemcpyAsync(h->Y, Y_in, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
@@ -2164,31 +2204,20 @@ static const int64_t kNoAllocCtlDoubles = 32;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocCtlDoubles + 4 * (int64_t)DFN_NOALLOC_MAX_ELEMENTS];
 static_assert(sizeof(StepCtl) <= kNoAllocCtlDoubles * sizeof(double), "controller does not fit the scratch header");
 
-static const int kNoAllocMaxDevices = 128;
-static double *g_noalloc_addr[kNoAllocMaxDevices];  // device address per device ordinal, set once
-static std::mutex g_noalloc_mu;
-
-// Device address of the scratch array on the current device, looked up
-// once per device with that device current.
+// Device address of the scratch array in the context current on the
+// calling thread. Looked up on every call (cheap next to the call's own
+// stream synchronisation): the address belongs to the context that loaded
+// the module, so a cached value would go stale after cudaDeviceReset or
+// under another context of the same device.
 static int noalloc_scratch(double **out)
 {
-    int dev = -1;
-    CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) {
-        g_err = "device ordinal out of range for the allocation-free scratch table";
-        return DFN_ERR_ARG;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        set_err("cudaGetSymbolAddress(g_noalloc_scratch)", e, __FILE__, __LINE__);
+        return DFN_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            set_err("cudaGetSymbolAddress(g_noalloc_scratch)", e, __FILE__, __LINE__);
-            return DFN_ERR_CUDA;
-        }
-        g_noalloc_addr[dev] = static_cast<double *>(p);
-    }
-    *out = g_noalloc_addr[dev];
+    *out = static_cast<double *>(p);
     return DFN_OK;
 }
 
@@ -2241,7 +2270,11 @@ int32_t dfn_compute_P_noalloc(int64_t N, double dt, double time, const double *d
     StepCtl c;
     CK(cudaMemcpyAsync(&c, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    *ier = (c.status == 1) ? 1 : 0;
+    // ier = 1 for the CG cap (outputs untouched) and for a non-finite
+    // solution (outputs written, as the reference's maxval test after the
+    // update, src/fluid_diffusion.f90:146-148); the latter also returns
+    // DFN_ERR_NONFINITE
+    *ier = (c.status == 1 || c.status == 4) ? 1 : 0;
     if (c.status != 0 && c.status != 1) return c.status;
     return DFN_OK;
 }

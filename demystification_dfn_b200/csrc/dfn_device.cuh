@@ -46,7 +46,7 @@ struct StepCtl {
     double t_end;     // stop when time >= t_end (t_end > 0)
     int step_attempts, max_attempts;
     int pfail_mask;   // bit s: pressure system s of this attempt hit the CG cap
-    int pad2;
+    int commit_bad;   // committed state of this step: bit 0 sigmaN > 0, bit 1 non-finite
     long long stage_noconv;  // stage pressure solves that hit the CG cap
     long long newton_solves, newton_iters, newton_fail;  // Newton formulation counters
 };
@@ -429,11 +429,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded wait: returns false if the phase did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Bounded wait: returns false if the phase did not complete within `limit`
+// polls (0: give up at once).
+constexpr int MBAR_POLLS = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit = MBAR_POLLS)
 {
     uint32_t ok = 0;
-    for (int it = 0; it < (1 << 22); it++) {
+    for (int it = 0; it < limit; it++) {
         asm volatile("{\n\t.reg .pred p;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"
@@ -461,7 +463,7 @@ template <int MODE, int STORE>
 __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
     gemv_tma_kernel(const int4 *__restrict__ tiles, const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                     int mask, const uint4 *__restrict__ Kbase, const double *__restrict__ Vbase, int vmul,
-                    double *__restrict__ partT, double *__restrict__ partN, int *err_flag)
+                    double *__restrict__ partT, double *__restrict__ partN, int wait_polls, int *err_flag)
 {
     constexpr int BPC = KFmt<MODE, STORE>::BPC;
     constexpr int CPV = 16 / BPC;
@@ -499,7 +501,10 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
             int i = 0;
             for (; i < nrows; i++) {
                 int s = i % TMA_STAGES;
-                if (i >= TMA_STAGES && !mbar_wait(&empty[s], ((i / TMA_STAGES) - 1) & 1)) { bad_s = 1; break; }
+                if (i >= TMA_STAGES && !mbar_wait(&empty[s], ((i / TMA_STAGES) - 1) & 1, wait_polls)) {
+                    bad_s = 1;
+                    break;
+                }
                 mbar_expect_tx(&full[s], GEMV_CHUNK_BYTES);
                 tma_bulk_g2s(stage + s * (GEMV_CHUNK_BYTES / 16), K + (r0 + i) * row_bytes + c * GEMV_CHUNK_BYTES,
                              GEMV_CHUNK_BYTES, &full[s]);
@@ -517,7 +522,7 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
             }
         for (int i = warp; i < nrows; i += TMA_CONSUMERS) {
             int s = i % TMA_STAGES;
-            if (!mbar_wait(&full[s], (i / TMA_STAGES) & 1)) { bad_s = 1; break; }
+            if (!mbar_wait(&full[s], (i / TMA_STAGES) & 1, wait_polls)) { bad_s = 1; break; }
             const uint4 *sp = stage + s * (GEMV_CHUNK_BYTES / 16) + lane;
             uint4 q[GEMV_LPL];
 #pragma unroll
@@ -537,8 +542,9 @@ __global__ void __launch_bounds__((TMA_CONSUMERS + 1) * 32)
     }
     __syncthreads();
     if (bad_s && threadIdx.x == 0) {
-        // error path: wait (bounded) for the copies still in flight before
-        // the CTA's shared memory is released, then report
+        // error path: wait (bounded, with the full limit whatever wait_polls
+        // is) for the copies still in flight before the CTA's shared memory
+        // is released, then report
         int issued = issued_s;
         for (int i = (issued > TMA_STAGES ? issued - TMA_STAGES : 0); i < issued; i++)
             mbar_wait(&full[i % TMA_STAGES], (i / TMA_STAGES) & 1);
@@ -2163,6 +2169,7 @@ __global__ void step_begin_kernel(StepCtl *ctl, const Inst *inst, int B, const d
     c.accepted = 0;
     c.probe_ier = 0;
     c.step_attempts = 0;
+    c.commit_bad = 0;
     c.x = 0.0;
     if (c.t_try > 10.0) {
         const Inst &I = inst[i];
@@ -2185,6 +2192,10 @@ __global__ void set_h_kernel(StepCtl *ctl, int B)
 
 // Accepted attempts: Y = yout, and the pressure commit compute_P(t_did),
 // which equals the stage-5 solve of the accepted attempt (dt = 0 + 1.0*h).
+// The whole state is committed before the stop rules look at it, as the
+// reference commits Y, P and time before check_errors (src/solver.f90:
+// 170-197): an extensional or non-finite component only raises a flag here,
+// which finish_kernel turns into the status after the time update.
 __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, double *P, double *Pdot,
                               const double *Ptemp, const double *Pdot_s)
 {
@@ -2197,13 +2208,15 @@ __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, doub
     const int64_t N = I.N, k = e - I.eoff;
     double *yi = y + 3 * I.eoff;
     const double *yo = yout + 3 * I.eoff;
+    int bad = 0;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const double v = yo[j * N + k];
         yi[j * N + k] = v;
-        if (j == 2 && v > 0.0) atomicCAS(&ep.ctl[i].status, 0, 3);
-        if (!isfinite(v)) atomicCAS(&ep.ctl[i].status, 0, 4);
+        if (j == 2 && v > 0.0) bad |= 1;
+        if (!isfinite(v)) bad |= 2;
     }
+    if (bad) atomicOr(&ep.ctl[i].commit_bad, bad);
     if (!(c.pfail_mask & (1 << 4))) {
         P[e] = Ptemp[6 * I.eoff + 4 * N + k];
         Pdot[e] = Pdot_s[6 * I.eoff + 4 * N + k];
@@ -2211,7 +2224,9 @@ __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, doub
 }
 
 // End of one pass of solve() per instance (src/solver.f90:117-196): time,
-// t_try with the 1-day cap, and the instance's next phase.
+// t_try with the 1-day cap, the stop rules on the committed state
+// (check_errors, src/solver.f90:412-418; non-finite values too) and the
+// instance's next phase.
 __global__ void finish_kernel(StepCtl *ctl, int B, double t_cap)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2224,6 +2239,11 @@ __global__ void finish_kernel(StepCtl *ctl, int B, double t_cap)
     if (tn > t_cap) tn = t_cap;
     c.t_try = tn;
     c.steps_done += 1;
+    if (c.commit_bad) {
+        c.status = (c.commit_bad & 1) ? 3 : 4;
+        c.phase = PH_DONE;
+        return;
+    }
     bool done = (c.steps_done >= c.target_steps) || (c.t_end > 0.0 && c.time >= c.t_end * (1.0 - 1e-14));
     c.phase = done ? PH_DONE : PH_NEW;
 }

@@ -1,8 +1,9 @@
 """The learned initial guess of the friction Newton solve.
 
-A small FP32 MLP (6 -> 64 -> 64 -> 1, SiLU) predicts the correction that
-radiation damping makes to the analytic guess w0 = tau/(sigma_eff a) of the
-friction-law root w = asinh(V C/(2 V0)). It is trained on solves that the
+A small FP32 MLP (7 -> 64 -> 64 -> 1, SiLU) predicts the correction from the
+bounded analytic start wa (the friction-only root w0 = tau/(sigma_eff a) or
+the radiation-only root, whichever is nearer zero) to the friction-law root
+w = asinh(V C/(2 V0)). It is trained on solves that the
 Newton formulation records while it runs, by the library's own GPU forward
 and backward kernels (dfn_mlp_train); the Newton solve stays the judge: a
 guess only sets the starting point, convergence is tested on the FP64

@@ -123,6 +123,12 @@ class Simulation:
         every kernel on its own; results are identical."""
         _lib.check(self.lib.dfn_set_graphs(self.h, 1 if enable else 0), self.lib)
 
+    def set_wait_limit(self, polls):
+        """Polls of the bounded waits of the TMA K.V pipeline before a kernel
+        gives up (None: the default); the next call then raises DfnError
+        with status 10 (DFN_ERR_TIMEOUT)."""
+        _lib.check(self.lib.dfn_set_wait_limit(self.h, -1 if polls is None else int(polls)), self.lib)
+
     @property
     def kernel_bytes(self):
         return int(self.lib.dfn_kernel_bytes(self.h))

@@ -42,7 +42,8 @@ typedef enum dfn_status {
     DFN_ERR_CUDA = 6,        /* a CUDA runtime call failed */
     DFN_ERR_UNSUPPORTED = 7, /* feature not available in this build */
     DFN_ERR_ATTEMPTS = 8,    /* more rejected RK attempts in one step than the device budget */
-    DFN_ERR_NOMEM = 9        /* device allocation failed */
+    DFN_ERR_NOMEM = 9,       /* device allocation failed */
+    DFN_ERR_TIMEOUT = 10     /* a bounded wait inside a kernel expired (the kernel stopped early) */
 } dfn_status;
 
 enum { DFN_MODE_II = 2, DFN_MODE_III = 3 };                    /* hyperparameter/fracture_mode */
@@ -248,6 +249,15 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
  * one by one so that each K.V launch is timed. No counterpart in the
  * reference (a host loop of subroutine calls). */
 int32_t dfn_set_graphs(dfn_handle *h, int32_t enable);
+/* Polls of the bounded waits in the TMA K.V pipeline (gemv_impl 0 of the
+ * dense storages) before a kernel gives up: it then stops streaming, waits
+ * with the full limit for its own copies in flight, raises an error flag
+ * and returns; the next call that reads the step controllers returns
+ * DFN_ERR_TIMEOUT once (the partial sums of that K.V are incomplete, so the
+ * state must be restored, e.g. with dfn_set_state). polls < 0 restores the
+ * default (2^22 polls, far beyond any copy's latency); 0 gives up at the
+ * first wait, which tests the error path. No counterpart in the reference. */
+int32_t dfn_set_wait_limit(dfn_handle *h, int32_t polls);
 /* Form of the CG pressure solves (DFN_PRESSURE_CG handles): -1 the default
  * rule (clusters when a launch's clusters all fit on the GPU at once, else
  * one CTA per system on global memory), 0 one CTA per system on global
@@ -354,30 +364,36 @@ int32_t dfn_kernel_device(dfn_handle *h, const double *d_slip, double *d_stressT
 /* ---- allocation-free pressure step ------------------------------------ */
 /* No counterpart in the reference: an extra entry point of this library.
  *
- * The same implicit pressure step as dfn_compute_P (the reference's CG, with
- * its 200-iteration cap), for callers that must not allocate device memory:
- * host programs that give all device memory to their own pool allocator at
- * start-up (so a cudaMalloc would fail or fight the pool), and time-stepping
- * loops that cannot afford the device-wide synchronisation cudaMalloc and
- * cudaFree may cause. It needs no handle and allocates nothing; the caller
- * passes every input and output as device pointers.
+ * The implicit pressure step of dfn_compute_P (the reference's CG, with its
+ * 200-iteration cap) for networks WITHOUT fault crossings, for callers that
+ * must not allocate device memory: host programs that give all device
+ * memory to their own pool allocator at start-up (so a cudaMalloc would fail
+ * or fight the pool), and time-stepping loops that cannot afford the
+ * device-wide synchronisation cudaMalloc and cudaFree may cause. It needs no
+ * handle and allocates nothing; the caller passes every input and output as
+ * device pointers. It takes no crossing arrays, so for a network with fault
+ * crossings it solves the uncoupled chain; use dfn_compute_P there.
  *
  * Its CG work vectors live in one fixed device array inside this library,
  * sized for DFN_NOALLOC_MAX_ELEMENTS elements (about 2 MiB); every GPU that
  * loads the library holds that array until the process exits. Larger
- * problems are rejected with DFN_ERR_ARG. Work runs on the calling thread's
- * current device and on `stream` (NULL = legacy default stream); the call
- * returns after the step has finished. The first call on a device looks up
- * the array's device address once for that device; make that first call
- * before any stream capture. All calls share the one array, so calls that
+ * problems are rejected with DFN_ERR_ARG. Work runs in the calling thread's
+ * current context and on `stream` (NULL = legacy default stream); every
+ * call looks up the array's address in that context, copies the solver's
+ * status to host memory and synchronises `stream`, so it must not be issued
+ * while `stream` (or a stream the legacy default stream waits on) is being
+ * captured into a CUDA graph. All calls share the one array, so calls that
  * overlap on the GPU (other threads or streams) race; serialise them.
  *
  * Inputs: d_P (committed pressure), d_permeability_x (N+1 face values as
  * built by the reference, src/initialisation.f90:252-269), d_ds (element
  * lengths), the fluid constants, tol_solver, and the sources (fault id
  * 1-based, element index 0-based into the concatenated element arrays).
- * Outputs: d_P_temp, d_P_dot; *ier = 1 when CG hits its iteration cap, in
- * which case the outputs are left untouched, as in the reference. */
+ * Outputs: d_P_temp, d_P_dot. *ier = 1 when CG hits its iteration cap (the
+ * outputs are left untouched and the call returns DFN_OK, as the
+ * reference's compute_P returns early) and when the solution is not finite
+ * (the outputs are written, as in the reference, src/fluid_diffusion.f90:
+ * 146-148, and the call returns DFN_ERR_NONFINITE). */
 #define DFN_NOALLOC_MAX_ELEMENTS 65536
 int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const double *d_P,
                               const double *d_permeability_x, const double *d_ds, double porosity,

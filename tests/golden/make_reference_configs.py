@@ -5,7 +5,8 @@ of the reference checkout (the only input files it ships; it ships no outputs)
 with the package's HDF5 reader and stores every dataset as a flat array, so
 that tests can rebuild the exact problems on machines without the reference.
 
-Usage: python tests/golden/make_reference_configs.py /root/reference
+Usage: python tests/golden/make_reference_configs.py REFERENCE_ROOT
+(or with DFN_REFERENCE_ROOT set in the environment).
 """
 import os
 import sys
@@ -40,4 +41,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DFN_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("usage: make_reference_configs.py REFERENCE_ROOT (or set DFN_REFERENCE_ROOT)")
+    main(root)

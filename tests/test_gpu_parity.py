@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from oracle import Oracle
-from demystification_dfn_b200 import networks
+from demystification_dfn_b200 import build_arrays, networks
 from demystification_dfn_b200.simulation import Simulation
 
 pytestmark = pytest.mark.gpu
@@ -335,6 +335,87 @@ def test_snapshot_and_step_host():
         assert np.allclose(snap["theta"], a.Dc / a.V0 * np.exp(st["Y"][N:2 * N]), rtol=1e-14)
         assert np.array_equal(snap["tractionNel"], st["Y"][2 * N:])
         assert snap["time"] == st["time"]
+
+
+def test_snapshot_matches_oracle():
+    """save_data's fields after 7 accepted steps (src/solver.f90:211-222):
+    V, theta = Dc/V0 exp(psi), P, tractionTel (the shear stress rate of the
+    last right-hand side: stage 6 of the accepted attempt) and tractionNel
+    (sigmaN), against the oracle's state and its last stress rates."""
+    p = net(seed=10, n=4, tol=1e-6)
+    o = Oracle(p)
+    o.use_dense()
+    with Simulation(p, pressure="cg_exact") as s:
+        s.solve_steps(7)
+        snap = s.snapshot()
+    st, _ = o.solve_steps(7)
+    assert st == 0
+    r = o.state()
+    sT, sN, _ = o.last_stress()
+    N = len(r["P"])
+    a = build_arrays(p)
+    assert abs(snap["time"] - r["time"]) <= 1e-8 * r["time"]
+    assert rel(snap["V"], r["Y"][:N]) < 1e-8
+    assert rel(snap["theta"], a.Dc / a.V0 * np.exp(r["Y"][N:2 * N])) < 1e-8
+    assert rel(snap["P"], r["P"]) < 1e-8
+    assert rel(snap["tractionTel"], sT) < 1e-8
+    assert rel(snap["tractionNel"], r["Y"][2 * N:]) < 1e-8
+    assert np.array_equal(snap["permeability"], a.permeability)
+
+
+def test_benchmark_network_rhs_and_steps_match_oracle():
+    """The benchmarked workload itself: the seeded 800-fault network (N =
+    16 013, mode II, dense FP64 kernel, 10 MPa pore-pressure step, tol 1e-8).
+    One right-hand side at the initial state against the oracle's
+    matrix-free directII (src/kernel_calculation/directModeII.f90:33-103) at
+    1e-9, then 5 accepted solve() steps (src/solver.f90:59-198) with the
+    bitwise reference CG against the oracle's: slip rate, log-state, normal
+    traction, pressure and time within 1e-8."""
+    import bench
+
+    p = bench.make_problem(0)
+    o = Oracle(p, threads=os.cpu_count() or 1)
+    with Simulation(p, pressure="cg_exact") as s:
+        N = s.N
+        assert N == 16013
+        Y = s.arrays.Y0()
+        for x in (1.0, 100.0):
+            g = s.friction_law(x, Y)
+            r = o.friction_law(x, Y)
+            for j in range(3):
+                assert rel(g[j * N:(j + 1) * N], r[j * N:(j + 1) * N]) < 1e-9, (x, j)
+        rep = s.solve_steps(5)
+        g = s.state()
+    st, _ = o.solve_steps(5)
+    r = o.state()
+    assert st == 0 and rep["status"] == 0 and g["it_count"] == r["it_count"] == 5
+    assert abs(g["time"] - r["time"]) <= 1e-8 * r["time"]
+    for j in range(3):
+        assert rel(g["Y"][j * N:(j + 1) * N], r["Y"][j * N:(j + 1) * N]) < 1e-8, j
+    assert rel(g["P"], r["P"]) < 1e-8
+
+
+@pytest.mark.parametrize("pressure", ["cg_exact", "tridiag"])
+def test_single_fault_config_mode2_run_matches_oracle(pressure):
+    """The single-fault configuration in plane strain (mode II): one 40 km
+    fault of 4000 x 10 m elements, a = 0.007, b = 0.005, 50 kg/s injection at
+    the centre, tol 1e-8; 40 accepted steps against the oracle (matrix-free
+    directII, reference CG) within 1e-8. The tridiagonal solve is the exact
+    solution of the same implicit step, so its pressure agrees with the CG's
+    to the CG tolerance, far below the state tolerance."""
+    p = networks.single_fault(mode="modeII")
+    o = Oracle(p, threads=os.cpu_count() or 1)
+    with Simulation(p, pressure=pressure) as s:
+        rep = s.solve_steps(40)
+        g = s.state()
+    st, _ = o.solve_steps(40)
+    r = o.state()
+    N = len(r["P"])
+    assert N == 4000 and st == 0 and rep["status"] == 0
+    assert abs(g["time"] - r["time"]) <= 1e-8 * r["time"]
+    for j in range(3):
+        assert rel(g["Y"][j * N:(j + 1) * N], r["Y"][j * N:(j + 1) * N]) < 1e-8, j
+    assert rel(g["P"], r["P"]) < 1e-8
 
 
 def test_fp32_storage_run_close_to_fp64():

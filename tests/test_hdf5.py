@@ -8,7 +8,10 @@ from demystification_dfn_b200 import build_arrays
 from demystification_dfn_b200.hdf5 import read_config
 import refconfigs
 
-REF = "/root/reference/problems"
+# the reference checkout's problems/ folder, when the environment names a
+# checkout (DFN_REFERENCE_ROOT); the golden fixture covers the other tests
+_ROOT = os.environ.get("DFN_REFERENCE_ROOT", "")
+REF = os.path.join(_ROOT, "problems") if _ROOT else ""
 
 
 def test_golden_bp6_problem():
@@ -33,7 +36,7 @@ def test_golden_network_problem():
     assert a.fracture_mode == 2
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference checkout not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="DFN_REFERENCE_ROOT does not name a reference checkout")
 def test_reader_matches_golden_on_shipped_files():
     for tag, rel in (("bp6", "BP6QD_A_4000"), ("network", "network_rate_strengthening")):
         p = read_config(os.path.join(REF, rel, "config"))

@@ -103,6 +103,21 @@ def test_create_rejects_bad_problem(lib):
     assert b"nb_element" in lib.dfn_last_error()
 
 
+def test_create_rejects_nonfinite_state(lib):
+    """A NaN or Inf in the initial state is refused before any device work
+    (DFN_ERR_NONFINITE), with or without a GPU."""
+    import numpy as np
+    from demystification_dfn_b200.layout import to_c
+
+    for field, bad in (("V", np.nan), ("sigmaN", np.inf), ("P", -np.inf)):
+        p = networks.small_network(seed=0, n_faults=2)
+        getattr(p.faults[1], field)[3] = bad
+        c = to_c(build_arrays(p))
+        h = ctypes.c_void_p()
+        assert lib.dfn_create(ctypes.byref(c), None, ctypes.byref(h)) == 4
+        assert b"non-finite" in lib.dfn_last_error()
+
+
 def test_tectonic_loading_and_crossing_pair_builders():
     """Network builders: v_load sets each fault's shear stressing rate to
     mu * v_load / L_f; crossing_pair shares exactly one node between its two
