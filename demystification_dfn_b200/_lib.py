@@ -88,6 +88,8 @@ def load():
                                 ctypes.POINTER(ctypes.c_float)]),
         "dfn_set_graphs": (i32, [P, i32]),
         "dfn_set_wait_limit": (i32, [P, i32]),
+        "dfn_get_slip": (i32, [P, i32, dp]),
+        "dfn_set_slip": (i32, [P, i32, dp]),
         "dfn_set_cg_form": (i32, [P, i32]),
         "dfn_set_hmat_small_leaves": (i32, [P, i32]),
         "dfn_crossing_count": (i64, [P]),

@@ -119,6 +119,10 @@ struct dfn_handle {
     double *kbuf = nullptr, *SigT = nullptr, *SigN = nullptr, *partT = nullptr, *partN = nullptr;
     double *Ptemp = nullptr, *Pdot_s = nullptr, *pwork = nullptr, *vin = nullptr, *vout = nullptr, *snap = nullptr;
     double *pcoef = nullptr;              // CG row coefficients [6][3N] per network
+    // slip of the V formulation, integrated by the same Cash-Karp stages
+    // outside the error norm: committed, the attempt's 5th-order value, and
+    // the partial stage sum C1 V1 + C3 V3 + C4 V4
+    double *slip = nullptr, *slip_out = nullptr, *slip_acc = nullptr;
     int *err_flag = nullptr;
     int wait_polls = MBAR_POLLS;          // polls of the TMA K.V pipeline's bounded waits
     void *K = nullptr;
@@ -169,6 +173,7 @@ struct dfn_handle {
     // Newton formulation and the learned guess
     int form = 0, guess = 0, newton_maxit = 50;
     double newton_tol = 1e-13;
+    double max_step = 86400.0;            // cap on t_try after an accepted step (the reference's one day)
     double *tau0 = nullptr, *wlast = nullptr, *vnow = nullptr;
     MlpTC *mlp = nullptr;                 // tensor-core image of the learned guess
     float *rec_x = nullptr, *rec_t = nullptr;
@@ -474,6 +479,7 @@ static FricParams fric_params(dfn_handle *h, int64_t nelem)
     f.yout = h->yout; f.ctl = h->ctl;
     f.form = h->form; f.guess = h->guess; f.maxit = h->newton_maxit; f.tol = h->newton_tol; f.off_explicit = 0.0;
     f.tau0 = h->tau0; f.wlast = h->wlast; f.vnow = h->vnow; f.mlp = h->mlp;
+    f.slip = h->slip; f.slip_out = h->slip_out; f.slip_acc = h->slip_acc;
     f.rec_x = h->rec_x; f.rec_t = h->rec_t; f.rec_n = h->rec_n; f.rec_cap = h->rec_cap;
     return f;
 }
@@ -582,11 +588,12 @@ static int run_round(dfn_handle *h)
     h->launches++;
     CKL();
     TRY(run_attempt(h, M_ACTIVE));
-    commit_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(elem_params(h), h->Y, h->yout, h->P, h->Pdot,
-                                                                  h->Ptemp, h->Pdot_s);
+    commit_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(
+        elem_params(h), h->Y, h->yout, h->P, h->Pdot, h->Ptemp, h->Pdot_s,
+        h->form == DFN_FORM_NEWTON ? nullptr : h->slip, h->slip_out);
     h->launches++;
     CKL();
-    finish_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B, 86400.0);
+    finish_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B, h->max_step);
     h->launches++;
     CKL();
     return DFN_OK;
@@ -1167,7 +1174,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
+    void *ptrs[] = {h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
@@ -1299,6 +1306,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     h->guess = (opt.newton_guess >= 0 && opt.newton_guess <= 3) ? opt.newton_guess : 0;
     h->newton_maxit = opt.newton_maxit > 0 ? opt.newton_maxit : 50;
     h->newton_tol = opt.newton_tol > 0 ? opt.newton_tol : 1e-13;
+    h->max_step = opt.max_step > 0 ? opt.max_step : 86400.0;
     const int bpc = bytes_per_col(h->mode, h->store);
     const int64_t CW = GEMV_CHUNK_BYTES / bpc;
     // static_kernel selects the dense kernel ("direct") or the H-matrix
@@ -1396,6 +1404,8 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     if (h->pressure != DFN_PRESSURE_TRIDIAG) DALLOC(h->pcoef, 18 * Nt);
     DALLOC(h->vin, 3 * h->hinst[0].N); DALLOC(h->vout, 3 * h->hinst[0].N); DALLOC(h->snap, 5 * Nt);
     DALLOC(h->err_flag, 1); DALLOC(h->ctl, count);
+    DALLOC(h->slip, Nt); DALLOC(h->slip_out, Nt); DALLOC(h->slip_acc, Nt);
+    CKC(cudaMemset(h->slip, 0, sizeof(double) * Nt));
     DALLOC(h->src_fault, soff); DALLOC(h->src_elem, soff); DALLOC(h->src_Q, soff); DALLOC(h->src_tb, soff);
     DALLOC(h->src_te, soff);
     CKC(cudaMemset(h->err_flag, 0, sizeof(int)));
@@ -2112,6 +2122,32 @@ int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, d
     if (time) *time = h->h_ctl[i].time;
     if (t_try) *t_try = h->h_ctl[i].t_try;
     if (it_count) *it_count = h->h_ctl[i].it_count;
+    return DFN_OK;
+}
+
+int32_t dfn_get_slip(dfn_handle *h, int32_t i, double *slip)
+{
+    if (!h || !slip || i < 0 || i >= h->B) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    const Inst &I = h->hinst[i];
+    const double *src = (h->form == DFN_FORM_NEWTON) ? h->Y + 3 * I.eoff : h->slip + I.eoff;
+    CK(cudaMemcpyAsync(slip, src, sizeof(double) * I.N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DFN_OK;
+}
+
+int32_t dfn_set_slip(dfn_handle *h, int32_t i, const double *slip)
+{
+    if (!h || !slip || i < 0 || i >= h->B) return DFN_ERR_ARG;
+    const Inst &I = h->hinst[i];
+    if (!all_finite(slip, I.N)) {
+        g_err = "dfn_set_slip: non-finite slip";
+        return DFN_ERR_NONFINITE;
+    }
+    CK(cudaSetDevice(h->dev));
+    double *dst = (h->form == DFN_FORM_NEWTON) ? h->Y + 3 * I.eoff : h->slip + I.eoff;
+    CK(cudaMemcpyAsync(dst, slip, sizeof(double) * I.N, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return DFN_OK;
 }
 

@@ -1784,6 +1784,9 @@ struct FricParams {
     double *wlast;                // [Ntot] last solution, warm start
     double *vnow;                 // [Ntot] V of this evaluation
     const MlpTC *mlp;             // tensor-core image of the learned guess (global)
+    // V formulation: slip as a passive component (dslip/dt = V)
+    const double *slip;           // [Ntot] committed
+    double *slip_out, *slip_acc;  // [Ntot] the attempt's 5th-order slip, partial stage sum
     float *rec_x, *rec_t;         // recorded solves
     unsigned long long *rec_n;
     long long rec_cap;
@@ -1963,9 +1966,10 @@ __global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction
             // stage pressure must be smooth in the stage time. It is linear
             // between the committed P (c = 0) and the implicit-Euler P over
             // the whole step (system 4, c = 1), which is what is committed.
+            // (stage 1 takes P itself: the full-step system of this attempt
+            // is not solved yet)
             const double p0 = f.Pc[I.eoff + k];
-            const double c = (stage == 1) ? 0.0 : ck_a(stage);
-            Pt = add_(p0, mul_(c, f.Ptemp[6 * I.eoff + 4 * N + k] - p0));
+            Pt = (stage == 1) ? p0 : add_(p0, mul_(ck_a(stage), f.Ptemp[6 * I.eoff + 4 * N + k] - p0));
         }
         if (f.form == 1) {
             const double off = (stage == 0) ? f.off_explicit
@@ -2018,7 +2022,17 @@ __global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction
             const double h = ctl->h;
 #pragma unroll
             for (int j = 0; j < 3; j++) yt[j * N + k] = ck_combine(stage + 1, h, yi[j * N + k], kb, S, j * N + k);
-        } else if (stage == 6) {
+        }
+        if (f.form == 0 && stage >= 3) {
+            // slip of the V formulation: k_s(slip) = V of the stage input,
+            // 5th-order combination in the reference's operand order
+            // (src/ode_solver/ode_bs.f90:223), outside the error norm
+            if (stage == 3) f.slip_acc[e] = add_(mul_(CK_C1, yi[k]), mul_(CK_C3, V));
+            else if (stage == 4) f.slip_acc[e] = add_(f.slip_acc[e], mul_(CK_C4, V));
+            else if (stage == 6)
+                f.slip_out[e] = add_(f.slip[e], mul_(ctl->h, add_(f.slip_acc[e], mul_(CK_C6, V))));
+        }
+        if (stage == 6) {
             const double h = ctl->h;
             const double *ysc = f.yscal + 3 * I.eoff;
             double *yo = f.yout + 3 * I.eoff;
@@ -2197,7 +2211,7 @@ __global__ void set_h_kernel(StepCtl *ctl, int B)
 // 170-197): an extensional or non-finite component only raises a flag here,
 // which finish_kernel turns into the status after the time update.
 __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, double *P, double *Pdot,
-                              const double *Ptemp, const double *Pdot_s)
+                              const double *Ptemp, const double *Pdot_s, double *slip, const double *slip_out)
 {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= ep.Ntot) return;
@@ -2217,6 +2231,7 @@ __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, doub
         if (!isfinite(v)) bad |= 2;
     }
     if (bad) atomicOr(&ep.ctl[i].commit_bad, bad);
+    if (slip) slip[e] = slip_out[e];
     if (!(c.pfail_mask & (1 << 4))) {
         P[e] = Ptemp[6 * I.eoff + 4 * N + k];
         Pdot[e] = Pdot_s[6 * I.eoff + 4 * N + k];

@@ -19,7 +19,7 @@ from .simulation import make_options
 class Ensemble:
     def __init__(self, problems, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
                  hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0,
-                 newton_tol=0.0):
+                 newton_tol=0.0, max_step=0.0):
         self.lib = _lib.load()
         self.arrays = [p if isinstance(p, ProblemArrays) else build_arrays(p) for p in problems]
         if not self.arrays:
@@ -28,7 +28,7 @@ class Ensemble:
         self._storage = storage
         self._pressure = pressure
         opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
-                           formulation, guess, newton_maxit, newton_tol)
+                           formulation, guess, newton_maxit, newton_tol, max_step)
         self._cs = [to_c(a) for a in self.arrays]
         arr = (DfnProblem * self.B)(*self._cs)
         self._arr = arr
@@ -125,6 +125,12 @@ class Ensemble:
         _lib.check(self.lib.dfn_get_state_instance(self.h, int(i), ptr(Y), ptr(P), ctypes.byref(t),
                                                    ctypes.byref(tt), ctypes.byref(it)), self.lib)
         return {"Y": Y, "P": P, "time": t.value, "t_try": tt.value, "it_count": it.value}
+
+    def slip(self, i):
+        """Slip (m) of network i (see Simulation.slip)."""
+        out = np.empty(self.arrays[i].N)
+        _lib.check(self.lib.dfn_get_slip(self.h, int(i), ptr(out)), self.lib)
+        return out
 
     def report(self, i):
         rep = DfnReport()

@@ -189,7 +189,7 @@ class DfnOptions(ctypes.Structure):
                 ("gemv_impl", ctypes.c_int32), ("hmat_leaf", ctypes.c_int32), ("formulation", ctypes.c_int32),
                 ("hmat_eta", ctypes.c_double), ("hmat_eps", ctypes.c_double),
                 ("newton_guess", ctypes.c_int32), ("newton_maxit", ctypes.c_int32),
-                ("newton_tol", ctypes.c_double)]
+                ("newton_tol", ctypes.c_double), ("max_step", ctypes.c_double)]
 
 
 class DfnReport(ctypes.Structure):

@@ -33,9 +33,11 @@ GUESS = {"analytic": 0, "mlp": 1, "warm": 2, "quasistatic": 3}
 
 
 def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64, hmat_leaf=0,
-                 hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0, newton_tol=0.0):
+                 hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0, newton_tol=0.0,
+                 max_step=0.0):
     """dfn_options; the H-matrix parameters default (0) to the reference's
-    nleaf=100, eta=3, eps_ACA=1e-8 (src/variables.f90:122-124)."""
+    nleaf=100, eta=3, eps_ACA=1e-8 (src/variables.f90:122-124); max_step 0
+    is the reference's one-day cap on the trial step."""
     opt = DfnOptions()
     lib.dfn_default_options(ctypes.byref(opt))
     opt.formulation = FORMULATION[formulation]
@@ -50,18 +52,19 @@ def make_options(lib, storage="fp64", pressure="cg", device=0, gemv="tma", max_a
     opt.hmat_leaf = int(hmat_leaf)
     opt.hmat_eta = float(hmat_eta)
     opt.hmat_eps = float(hmat_eps)
+    opt.max_step = float(max_step)
     return opt
 
 
 class Simulation:
     def __init__(self, problem, storage="fp64", pressure="cg", device=0, gemv="tma", max_attempts=64,
                  hmat_leaf=0, hmat_eta=0.0, hmat_eps=0.0, formulation="v", guess="analytic", newton_maxit=0,
-                 newton_tol=0.0):
+                 newton_tol=0.0, max_step=0.0):
         self.lib = _lib.load()
         self.arrays = problem if isinstance(problem, ProblemArrays) else build_arrays(problem)
         self.N = self.arrays.N
         opt = make_options(self.lib, storage, pressure, device, gemv, max_attempts, hmat_leaf, hmat_eta, hmat_eps,
-                           formulation, guess, newton_maxit, newton_tol)
+                           formulation, guess, newton_maxit, newton_tol, max_step)
         self.formulation = formulation
         self._storage = storage
         self._pressure = pressure
@@ -231,6 +234,17 @@ class Simulation:
         rep = DfnReport()
         _lib.check(self.lib.dfn_get_report(self.h, 0, ctypes.byref(rep)), self.lib)
         return rep.as_dict()
+
+    def slip(self):
+        """Slip (m): the integral of V in the V formulation (a passive
+        component of the RK stages), the state in the Newton formulation."""
+        out = np.empty(self.N)
+        _lib.check(self.lib.dfn_get_slip(self.h, 0, ptr(out)), self.lib)
+        return out
+
+    def set_slip(self, slip):
+        slip = np.ascontiguousarray(slip, dtype=np.float64)
+        _lib.check(self.lib.dfn_set_slip(self.h, 0, ptr(slip)), self.lib)
 
     def velocity(self):
         V = np.empty(self.N)

@@ -130,6 +130,8 @@ typedef struct dfn_options {
     int32_t newton_guess;     /* DFN_GUESS_* initial guess of the Newton solve */
     int32_t newton_maxit;     /* Newton iteration cap (0 = 50) */
     double newton_tol;        /* |residual| <= tol * (|tau| + sigma_eff*a*|w|) (0 = 1e-13) */
+    double max_step;          /* cap on the next trial step after each accepted step, s
+                                 (0 = the reference's one day, src/solver.f90:117-120) */
 } dfn_options;
 
 /* Newton formulation (options.formulation = DFN_FORM_NEWTON). The state is
@@ -342,6 +344,16 @@ int32_t dfn_step_host(dfn_handle *h, const double *Y_in, const double *P_in, dou
 int32_t dfn_solve_batch(dfn_handle *h, int64_t n_steps, double t_end, dfn_report *reps);
 int32_t dfn_get_state_instance(dfn_handle *h, int32_t i, double *Y, double *P, double *time, double *t_try,
                                int64_t *it_count);
+/* Slip of network i (m). The reference allocates slip
+ * (src/configuration.f90:190) but never updates it; here, in the V
+ * formulation, it is the integral of V carried by the same Cash-Karp stages
+ * as a passive component outside the error norm, slip + h (C1 V1 + C3 V3 +
+ * C4 V4 + C6 V6) with V_s the slip rate of stage s (src/ode_solver/
+ * ode_bs.f90:223), zero at dfn_create and committed with the state; in the
+ * Newton formulation it is the first block of the state. dfn_set_slip
+ * overwrites it (e.g. after dfn_set_state). */
+int32_t dfn_get_slip(dfn_handle *h, int32_t i, double *slip);
+int32_t dfn_set_slip(dfn_handle *h, int32_t i, const double *slip);
 /* Counters and status of network i since the handle was created. */
 int32_t dfn_get_report(dfn_handle *h, int32_t i, dfn_report *rep);
 

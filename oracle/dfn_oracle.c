@@ -59,6 +59,17 @@ typedef struct orc {
     int64_t ncross, nxc;
     int64_t *xptr, *xa, *xb;
     double *xkl, *xkr;
+    /* slip: integrated as a passive component (dslip/dt = V) of the V
+     * formulation, outside the error norm; the reference allocates it
+     * (src/configuration.f90:190) but never updates it */
+    double *slip;
+    /* Newton slip formulation (the library's DFN_FORM_NEWTON): form 1 means
+     * Y = [slip | psi | sigmaN0] and V solved from the friction law */
+    int form, nguess, nmaxit;
+    double ntol, time0;
+    double max_step; /* cap on t_try after a step (the reference's one day) */
+    double *tau0;
+    int64_t newton_solves, newton_iters, newton_fail;
 } orc;
 
 static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
@@ -255,6 +266,11 @@ orc *orc_create(const dfn_problem *p)
 #undef CP
     o->Pdot = (double *)xcalloc(N, 8);
     o->SigmaT_dot = (double *)xcalloc(N, 8); o->SigmaN_dot = (double *)xcalloc(N, 8);
+    o->slip = (double *)xcalloc(N, 8);
+    o->tau0 = (double *)xcalloc(N, 8);
+    o->time0 = p->time0;
+    o->nmaxit = 50; o->ntol = 1e-13;
+    o->max_step = 24 * 60 * 60;
     orc_ini_value(o);
     orc_find_crossings(o);
     /* solve() entry: src/solver.f90:50-56 */
@@ -270,13 +286,15 @@ void orc_destroy(orc *o)
     void *ptrs[] = {o->fault_n, o->fault_first, o->node, o->elem, o->ds, o->tan, o->nrm, o->a, o->b,
                     o->Dc, o->f0, o->V0, o->nload, o->sload, o->perm, o->permx, o->fake, o->src_fault,
                     o->src_index, o->src_Q, o->src_tb, o->src_te, o->Y, o->P, o->Pdot, o->SigmaT_dot,
-                    o->SigmaN_dot, o->KT, o->KN, o->xptr, o->xa, o->xb, o->xkl, o->xkr};
+                    o->SigmaN_dot, o->KT, o->KN, o->xptr, o->xa, o->xb, o->xkl, o->xkr, o->slip, o->tau0};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     orc_hmat_free((struct orc_hmat *)o->hmat);
     free(o);
 }
 
 void orc_set_threads(orc *o, int n) { o->nthreads = n < 1 ? 1 : n; }
+/* cap on t_try after each step (src/solver.f90:117-120 uses one day) */
+void orc_set_max_step(orc *o, double s) { o->max_step = s > 0.0 ? s : 24 * 60 * 60; }
 void orc_set_kernel_impl(orc *o, int impl) { o->kernel_impl = impl; }
 int64_t orc_n(const orc *o) { return o->N; }
 
@@ -716,9 +734,21 @@ static void orc_rkck_cb(orc_derivs_fn derivs, void *ctx, const double *y, const 
 }
 
 /* rkqs: src/ode_solver/ode_bs.f90:125-174. Returns 0 or DFN_ERR_UNDERFLOW.
- * counters (attempts, rejected) may be NULL. */
+ * counters (attempts, rejected) may be NULL. The error norm runs over the
+ * first nerr components (the others are integrated passively). */
+static int orc_rkqs_nerr(orc_derivs_fn derivs, void *ctx, int64_t *counters, double *y, const double *dydx,
+                         int64_t n, int64_t nerr, double *x, double htry, double eps, const double *yscal,
+                         double *hdid, double *hnext);
+
 int orc_rkqs_cb(orc_derivs_fn derivs, void *ctx, int64_t *counters, double *y, const double *dydx, int64_t n,
                 double *x, double htry, double eps, const double *yscal, double *hdid, double *hnext)
+{
+    return orc_rkqs_nerr(derivs, ctx, counters, y, dydx, n, n, x, htry, eps, yscal, hdid, hnext);
+}
+
+static int orc_rkqs_nerr(orc_derivs_fn derivs, void *ctx, int64_t *counters, double *y, const double *dydx,
+                         int64_t n, int64_t nerr, double *x, double htry, double eps, const double *yscal,
+                         double *hdid, double *hnext)
 {
     const double SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25;
     const double ERRCON = (double)1.89e-4f; /* default-real literal in the reference */
@@ -728,7 +758,7 @@ int orc_rkqs_cb(orc_derivs_fn derivs, void *ctx, int64_t *counters, double *y, c
         if (counters) counters[0]++;
         orc_rkck_cb(derivs, ctx, y, dydx, n, *x, h, ytemp, yerr);
         errmax = 0.0;
-        for (int64_t i = 0; i < n; i++) errmax = fmax(errmax, fabs(yerr[i] / yscal[i]));
+        for (int64_t i = 0; i < nerr; i++) errmax = fmax(errmax, fabs(yerr[i] / yscal[i]));
         errmax = errmax / eps;
         if (errmax <= 1.0) break;
         if (counters) counters[1]++;
@@ -756,11 +786,26 @@ int orc_rkqs(orc *o, double *y, const double *dydx, int64_t n, double *x, double
     return st;
 }
 
+/* derivs of the V formulation with slip appended: [V psi sigma slip]' =
+ * [friction RHS, V] (slip is passive: nothing reads it back). */
+static void orc_rhs_slip_cb(double x, int64_t n, const double *y, double *dydx, void *ctx)
+{
+    orc *o = (orc *)ctx;
+    int64_t N = o->N;
+    (void)n;
+    orc_rhs(o, x, y, dydx);
+    for (int64_t k = 0; k < N; k++) dydx[3 * N + k] = y[k];
+}
+
+static int orc_newton_solve_step(orc *o);
+
 /* ---------------------------------------------------------------------- */
 /* One pass of the solve() loop: src/solver.f90:59-198 (printing and file
- * output excluded). Returns 0, or a dfn_status code. */
+ * output excluded). Returns 0, or a dfn_status code. Slip rides along as a
+ * fourth block outside the error norm. */
 int orc_solve_step(orc *o)
 {
+    if (o->form == 1) return orc_newton_solve_step(o);
     int64_t N = o->N, n = 3 * N;
     o->it_count++;
     if (o->t_try > 10.0) {
@@ -776,16 +821,25 @@ int orc_solve_step(orc *o)
         ier = orc_compute_P(o, o->t_try, Pt, o->Pdot);
         if (++guard > 2000) { free(Pt); return DFN_ERR_NOCONV; }
     }
-    double *Ydot = (double *)malloc(8 * n), *yscal = (double *)malloc(8 * n);
+    double *y4 = (double *)malloc(8 * 4 * N), *Ydot = (double *)malloc(8 * 4 * N), *yscal = (double *)malloc(8 * n);
+    memcpy(y4, o->Y, 8 * n);
+    memcpy(y4 + n, o->slip, 8 * N);
     double time_temp = 0.0;
-    orc_rhs(o, o->t_try, o->Y, Ydot);
+    orc_rhs_slip_cb(o->t_try, 4 * N, y4, Ydot, o);
     for (int64_t i = 0; i < n; i++) yscal[i] = fabs(o->Y[i]) + fabs(Ydot[i] * o->t_try) + o->tol;
     double t_did = 0, t_next = 0;
-    int st = orc_rkqs(o, o->Y, Ydot, n, &time_temp, o->t_try, o->tol, yscal, &t_did, &t_next);
+    int64_t c[2] = {0, 0};
+    int st = orc_rkqs_nerr(orc_rhs_slip_cb, o, c, y4, Ydot, 4 * N, n, &time_temp, o->t_try, o->tol, yscal, &t_did,
+                           &t_next);
+    o->attempts += c[0];
+    o->rejected += c[1];
     free(Ydot); free(yscal);
-    if (st) { free(Pt); return st; }
+    if (st) { free(Pt); free(y4); return st; }
+    memcpy(o->Y, y4, 8 * n);
+    memcpy(o->slip, y4 + n, 8 * N);
+    free(y4);
     o->t_try = t_next;
-    if (o->t_try > 24 * 60 * 60) o->t_try = 24 * 60 * 60;
+    if (o->t_try > o->max_step) o->t_try = o->max_step;
     ier = orc_compute_P(o, t_did, o->P, o->Pdot);
     free(Pt);
     o->time = o->time + t_did;
@@ -805,6 +859,245 @@ int orc_solve_steps(orc *o, int64_t nsteps, double *hdid_log)
         if (st) { o->last_status = st; return st; }
     }
     return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Newton slip formulation: the library's DFN_FORM_NEWTON restated. It has
+ * no counterpart in the reference, which integrates V; the friction law it
+ * solves is the reference's (src/friction/RateStateAgingModeII.f90:54-68,
+ * whose time derivative is the reference's dV/dt):
+ *   state Y = [slip | psi | sigmaN0]   (slip 0 and tau0 set at entry)
+ *   tau   = tau0 + prefactor K_T.slip + shear_loading_dot (t - time0)
+ *   sigma = sigmaN0 + prefactor K_N.slip + normal_loading_dot (t - time0)
+ *           (mode III: no K_N term)
+ *   g(w)  = tau - eta V(w) - s a w = 0,  s = -(sigma + P),
+ *           V(w) = (2 V0/C) sinh w,  C = exp((f0 + b psi)/a),  eta = mu/(2 cs)
+ * Newton on w from the bounded start (the friction-only root w0 = tau/(s a)
+ * or the radiation-only root wr, eta V(wr) = tau, whichever is nearer
+ * zero; guess 3 takes w0), steps limited to |dw| <= 10, converged when
+ * |g| <= tol (|tau| + s a |w|); s <= 0: V = tau/eta. dslip/dt = V,
+ * dpsi/dt = the aging law, dsigmaN0/dt = 0. The stage pressure is linear
+ * in the stage time between the committed P (c = 0) and the implicit-Euler
+ * pressure over the whole step (c = 1), which is what is committed. */
+static const double ORC_LN2 = 0.6931471805599453;
+
+static double orc_w_radiation(double tau, double eta, double lnA)
+{
+    double at = fabs(tau);
+    if (at == 0.0) return 0.0;
+    double lz = log(at / eta) - lnA;
+    double wr = (lz > 20.0) ? lz + ORC_LN2 : asinh(exp(lz));
+    return copysign(wr, tau);
+}
+
+static void orc_eta_v(double w, double lnA, double eta, double *ev, double *edv)
+{
+    double aw = fabs(w);
+    double e = exp(lnA + aw - ORC_LN2);
+    double q = exp(-2.0 * aw);
+    *ev = eta * copysign(e * (1.0 - q), w);
+    *edv = eta * e * (1.0 + q);
+}
+
+static double orc_v_of_w(double w, double lnA)
+{
+    double aw = fabs(w);
+    return copysign(exp(lnA + aw - ORC_LN2) * (1.0 - exp(-2.0 * aw)), w);
+}
+
+static double orc_newton_w(double tau, double s, double a, double lnA, double eta, double w, double tol, int maxit,
+                           int *iters, int *ok)
+{
+    *iters = 0;
+    *ok = 0;
+    for (int it = 0; it <= maxit; it++) {
+        double ev, edv;
+        orc_eta_v(w, lnA, eta, &ev, &edv);
+        double g = tau - ev - s * a * w;
+        if (fabs(g) <= tol * (fabs(tau) + s * a * fabs(w) + 1e-300)) { *ok = 1; break; }
+        if (it == maxit) break;
+        double dw = g / (edv + s * a);
+        dw = fmax(fmin(dw, 10.0), -10.0);
+        w += dw;
+        (*iters)++;
+    }
+    return w;
+}
+
+/* Switches the formulation (0: V, the reference's; 1: Newton). Newton:
+ * tau0 such that the current V satisfies the friction law at slip 0 with
+ * the committed P, then slip = 0. guess 0 bounded start, 3 friction-only
+ * start; maxit 0 = 50, tol 0 = 1e-13. */
+int orc_set_formulation(orc *o, int form, int guess, int maxit, double tol)
+{
+    if (form != 0 && form != 1) return DFN_ERR_ARG;
+    if (guess != 0 && guess != 3) return DFN_ERR_UNSUPPORTED;
+    o->form = form;
+    o->nguess = guess;
+    o->nmaxit = maxit > 0 ? maxit : 50;
+    o->ntol = tol > 0.0 ? tol : 1e-13;
+    if (form == 0) return 0;
+    int64_t N = o->N;
+    double eta = o->mu / (2.0 * o->cs);
+    for (int64_t k = 0; k < N; k++) {
+        double V = o->Y[k], psi = o->Y[N + k], sig = o->Y[2 * N + k];
+        double t0 = 0.0;
+        if (!o->fake[k]) {
+            double C = exp((o->f0[k] + o->b[k] * psi) / o->a[k]);
+            double w = asinh(V * C / (2.0 * o->V0[k]));
+            t0 = eta * V - (sig + o->P[k]) * o->a[k] * w;
+        }
+        o->tau0[k] = t0;
+        o->Y[k] = 0.0;
+    }
+    o->time0 = o->time;
+    return 0;
+}
+
+/* Right-hand side of the Newton formulation at offset `off` from the step
+ * start with the stage pressure Pt; V of the evaluation into Vout (may be
+ * NULL). */
+static void orc_newton_rhs(orc *o, double off, const double *Pt, const double *Y, double *Yd, double *Vout)
+{
+    int64_t N = o->N;
+    orc_kernel(o, Y, o->SigmaT_dot, o->SigmaN_dot);
+    o->rhs_evals++;
+    double eta = o->mu / (2.0 * o->cs);
+    double tt = (o->time - o->time0) + off;
+    const double *psi = Y + N, *sig0 = Y + 2 * N;
+    for (int64_t k = 0; k < N; k++) {
+        Yd[2 * N + k] = 0.0;
+        if (o->fake[k]) { Yd[k] = 0.0; Yd[N + k] = 0.0; if (Vout) Vout[k] = 0.0; continue; }
+        double tau = o->tau0[k] + o->SigmaT_dot[k] + o->sload[k] * tt;
+        double sig = ((o->mode == DFN_MODE_II) ? sig0[k] + o->SigmaN_dot[k] : sig0[k]) + o->nload[k] * tt;
+        double s = -(sig + Pt[k]);
+        double a = o->a[k], V;
+        if (s > 0.0) {
+            double lnA = log(2.0 * o->V0[k]) - (o->f0[k] + o->b[k] * psi[k]) / a;
+            double w0 = tau / (s * a);
+            double wr = orc_w_radiation(tau, eta, lnA);
+            double w = (o->nguess != 3 && fabs(wr) < fabs(w0)) ? wr : w0;
+            int it, ok;
+            w = orc_newton_w(tau, s, a, lnA, eta, w, o->ntol, o->nmaxit, &it, &ok);
+            o->newton_solves++;
+            o->newton_iters += it;
+            if (!ok) o->newton_fail++;
+            V = orc_v_of_w(w, lnA);
+        } else {
+            V = tau / eta;
+        }
+        if (Vout) Vout[k] = V;
+        Yd[k] = V;
+        Yd[N + k] = o->V0[k] / o->Dc[k] * exp(-psi[k]) - fabs(V) / o->Dc[k];
+    }
+}
+
+/* One pass of solve() in the Newton formulation: the V formulation's loop
+ * (probe with halving, scaling right-hand side, rkqs, 1-day cap, pressure
+ * commit, time, stop rules), with the stage pressures above. */
+static int orc_newton_solve_step(orc *o)
+{
+    static const double A[7] = {0.0, 0.0, 0.2, 0.3, 0.6, 1.0, 0.875};
+    const double SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25;
+    const double ERRCON = (double)1.89e-4f;
+    int64_t N = o->N, n = 3 * N;
+    o->it_count++;
+    if (o->t_try > 10.0) {
+        for (int64_t s = 0; s < o->nsrc; s++)
+            if (o->time < o->src_tb[s] && o->time + o->t_try > o->src_tb[s]) o->t_try = 10.0;
+    }
+    double *w = (double *)malloc(8 * (13 * n + 3 * N));
+    double *k1 = w, *k2 = w + n, *k3 = w + 2 * n, *k4 = w + 3 * n, *k5 = w + 4 * n, *k6 = w + 5 * n;
+    double *yt = w + 6 * n, *yout = w + 7 * n, *yscal = w + 8 * n, *yerr = w + 9 * n;
+    double *Pfull = w + 13 * n, *Pdf = Pfull + N, *Pst = Pdf + N;
+    double **ks[7] = {NULL, NULL, &k2, &k3, &k4, &k5, &k6};
+    /* the probe: src/solver.f90:81-92 (its solution is not used here) */
+    int ier = orc_compute_P(o, o->t_try, Pst, Pdf);
+    int guard = 0;
+    while (ier == 1) {
+        o->t_try = o->t_try / 2.0;
+        o->halvings++;
+        ier = orc_compute_P(o, o->t_try, Pst, Pdf);
+        if (++guard > 2000) { free(w); return DFN_ERR_NOCONV; }
+    }
+    orc_newton_rhs(o, 0.0, o->P, o->Y, k1, NULL);
+    for (int64_t i = 0; i < n; i++) yscal[i] = fabs(o->Y[i]) + fabs(k1[i] * o->t_try) + o->tol;
+    double h = o->t_try, errmax, hnext;
+    int ier_full;
+    for (;;) {
+        o->attempts++;
+        ier_full = orc_compute_P_mode(o, 0.0 + A[5] * h, Pfull, Pdf, 1);
+        const double *y = o->Y;
+        for (int st = 2; st <= 6; st++) {
+            for (int64_t i = 0; i < n; i++) {
+                switch (st) {
+                case 2: yt[i] = y[i] + 0.2 * h * k1[i]; break;
+                case 3: yt[i] = y[i] + h * (B31 * k1[i] + B32 * k2[i]); break;
+                case 4: yt[i] = y[i] + h * (B41 * k1[i] + B42 * k2[i] + B43 * k3[i]); break;
+                case 5: yt[i] = y[i] + h * (B51 * k1[i] + B52 * k2[i] + B53 * k3[i] + B54 * k4[i]); break;
+                default:
+                    yt[i] = y[i] + h * (B61 * k1[i] + B62 * k2[i] + B63 * k3[i] + B64 * k4[i] + B65 * k5[i]);
+                }
+            }
+            for (int64_t k = 0; k < N; k++) Pst[k] = o->P[k] + A[st] * (Pfull[k] - o->P[k]);
+            orc_newton_rhs(o, 0.0 + A[st] * h, Pst, yt, *ks[st], NULL);
+        }
+        for (int64_t i = 0; i < n; i++) yout[i] = y[i] + h * (C1 * k1[i] + C3 * k3[i] + C4 * k4[i] + C6 * k6[i]);
+        for (int64_t i = 0; i < n; i++)
+            yerr[i] = h * (DC1 * k1[i] + DC3 * k3[i] + DC4 * k4[i] + DC5 * k5[i] + DC6 * k6[i]);
+        errmax = 0.0;
+        for (int64_t i = 0; i < n; i++) errmax = fmax(errmax, fabs(yerr[i] / yscal[i]));
+        errmax = errmax / o->tol;
+        if (errmax <= 1.0) break;
+        o->rejected++;
+        double htemp = SAFETY * h * pow(errmax, PSHRNK);
+        h = copysign(fmax(fabs(htemp), 0.1 * fabs(h)), h);
+        if (0.0 + h == 0.0) { free(w); return DFN_ERR_UNDERFLOW; }
+    }
+    hnext = (errmax > ERRCON) ? SAFETY * h * pow(errmax, PGROW) : 5.0 * h;
+    memcpy(o->Y, yout, 8 * n);
+    o->t_try = hnext;
+    if (o->t_try > o->max_step) o->t_try = o->max_step;
+    /* the commit compute_P(t_did) is the full-step solve of the accepted
+     * attempt; a capped solve keeps P, as the reference's early return */
+    if (ier_full == 0) {
+        memcpy(o->Pdot, Pdf, 8 * N);
+        memcpy(o->P, Pfull, 8 * N);
+    }
+    o->time = o->time + h;
+    free(w);
+    for (int64_t k = 0; k < N; k++)
+        if (o->Y[2 * N + k] > 0) return DFN_ERR_EXTENSIONAL;
+    for (int64_t i = 0; i < n; i++)
+        if (!isfinite(o->Y[i])) return DFN_ERR_NONFINITE;
+    return 0;
+}
+
+/* Slip rate at the current state (Newton: the friction law solved with the
+ * committed P; V formulation: the state itself). */
+void orc_velocity(orc *o, double *V)
+{
+    int64_t N = o->N;
+    if (o->form != 1) { memcpy(V, o->Y, 8 * N); return; }
+    double *Yd = (double *)malloc(8 * 3 * N);
+    int64_t c[4] = {o->rhs_evals, o->newton_solves, o->newton_iters, o->newton_fail};
+    orc_newton_rhs(o, 0.0, o->P, o->Y, Yd, V);
+    o->rhs_evals = c[0]; o->newton_solves = c[1]; o->newton_iters = c[2]; o->newton_fail = c[3];
+    free(Yd);
+}
+
+/* Slip (V formulation: the passive integral of V; Newton: the state). */
+void orc_get_slip(const orc *o, double *slip)
+{
+    memcpy(slip, o->form == 1 ? o->Y : o->slip, 8 * o->N);
+}
+void orc_set_slip(orc *o, const double *slip)
+{
+    memcpy(o->form == 1 ? o->Y : o->slip, slip, 8 * o->N);
+}
+void orc_newton_counters(const orc *o, int64_t *c)
+{
+    c[0] = o->newton_solves; c[1] = o->newton_iters; c[2] = o->newton_fail;
 }
 
 /* ---------------------------------------------------------------------- */

@@ -60,6 +60,12 @@ def load():
         "orc_hmat_build": (cint, [V, cint, dbl, dbl]),
         "orc_hmat_perm": (None, [V, ctypes.POINTER(ctypes.c_int)]),
         "orc_hmat_stats": (None, [V, ctypes.POINTER(i64)]),
+        "orc_set_formulation": (cint, [V, cint, cint, cint, dbl]),
+        "orc_set_max_step": (None, [V, dbl]),
+        "orc_velocity": (None, [V, dp]),
+        "orc_get_slip": (None, [V, dp]),
+        "orc_set_slip": (None, [V, dp]),
+        "orc_newton_counters": (None, [V, ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -94,6 +100,39 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+    def set_formulation(self, form, guess="analytic", maxit=0, tol=0.0):
+        """"v" (the reference's ODE) or "newton" (the library's Newton slip
+        formulation restated: state [slip, psi, sigmaN0], V from the friction
+        law); guess "analytic" (bounded start) or "quasistatic"."""
+        st = self.lib.orc_set_formulation(self.o, {"v": 0, "newton": 1}[form],
+                                          {"analytic": 0, "quasistatic": 3}[guess], int(maxit), float(tol))
+        if st:
+            raise ValueError(f"oracle formulation status {st}")
+
+    def set_max_step(self, seconds):
+        """Cap on the trial step after each step (0: the reference's one day)."""
+        self.lib.orc_set_max_step(self.o, float(seconds))
+
+    def velocity(self):
+        V = np.empty(self.N)
+        self.lib.orc_velocity(self.o, ptr(V))
+        return V
+
+    def slip(self):
+        """Slip: the passive integral of V (V formulation) or the state (Newton)."""
+        s = np.empty(self.N)
+        self.lib.orc_get_slip(self.o, ptr(s))
+        return s
+
+    def set_slip(self, slip):
+        slip = np.ascontiguousarray(slip, dtype=np.float64)
+        self.lib.orc_set_slip(self.o, ptr(slip))
+
+    def newton_counters(self):
+        c = (ctypes.c_int64 * 3)()
+        self.lib.orc_newton_counters(self.o, c)
+        return dict(zip(["solves", "iters", "fail"], list(c)))
 
     def set_threads(self, n):
         self.lib.orc_set_threads(self.o, int(n))

@@ -379,11 +379,16 @@ def test_benchmark_network_rhs_and_steps_match_oracle():
         N = s.N
         assert N == 16013
         Y = s.arrays.Y0()
+        # the network starts at steady state, where dpsi/dt = V0/Dc e^-psi -
+        # V/Dc is rounding noise: it is measured against the size of its
+        # terms, V/Dc
+        psi_scale = np.abs(Y[:N] / s.arrays.Dc).max()
         for x in (1.0, 100.0):
             g = s.friction_law(x, Y)
             r = o.friction_law(x, Y)
-            for j in range(3):
-                assert rel(g[j * N:(j + 1) * N], r[j * N:(j + 1) * N]) < 1e-9, (x, j)
+            assert rel(g[:N], r[:N]) < 1e-9, x
+            assert np.abs(g[N:2 * N] - r[N:2 * N]).max() < 1e-9 * psi_scale, x
+            assert rel(g[2 * N:], r[2 * N:]) < 1e-9, x
         rep = s.solve_steps(5)
         g = s.state()
     st, _ = o.solve_steps(5)

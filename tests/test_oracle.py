@@ -8,7 +8,7 @@ import pytest
 
 from oracle import Oracle, load
 from demystification_dfn_b200 import networks
-from demystification_dfn_b200.layout import ptr
+from demystification_dfn_b200.layout import build_arrays, ptr
 
 
 def straight(n=64, mode="modeIII", **kw):
@@ -201,3 +201,57 @@ def test_shipped_network_has_fault_crossings():
 
     o = Oracle(refconfigs.problem("network"))
     assert o.crossings() == 13
+
+
+def _run_capped(p, form, hmax, T):
+    """The oracle in one formulation with every step capped at hmax (the
+    first one too), to simulated time T."""
+    o = Oracle(p)
+    o.use_dense()
+    o.set_formulation(form)
+    o.set_max_step(hmax)
+    s = o.state()
+    o.set_state(s["Y"], s["P"], s["time"], hmax, 0)
+    st, _ = o.solve_steps(int(round(T / hmax)))
+    assert st == 0 and abs(o.state()["time"] - T) <= 1e-9 * T
+    return o
+
+
+def test_newton_restatement_agrees_with_the_v_formulation_without_pressure():
+    """Without pore-pressure forcing the two formulations integrate the same
+    ODE (the reference's dV/dt is the time derivative of the friction law the
+    Newton formulation solves). With the same steps (a tolerance every
+    attempt meets, steps capped at 10 s) slip rate and slip agree to 1e-9;
+    the Newton formulation's first V is the initial V (a root of the friction
+    law at slip 0, to the Newton tolerance)."""
+    p = networks.small_network(seed=31, n_faults=4, tol=1e-3, dP=0.0)
+    real = ~build_arrays(p).fake_mask
+    o = Oracle(p)
+    o.set_formulation("newton")
+    V0 = build_arrays(p).Y0()[:o.N]
+    # the Newton residual test (1e-13 of the stress) resolves w to about
+    # 1e-13 w, so V = (2 V0/C) sinh w to about 1e-11
+    assert np.abs(o.velocity() - V0)[real].max() <= 1e-10 * np.abs(V0).max()
+    a, b = _run_capped(p, "v", 10.0, 600.0), _run_capped(p, "newton", 10.0, 600.0)
+    for x, y in ((b.velocity(), a.velocity()), (b.slip(), a.slip())):
+        assert np.abs(x - y)[real].max() <= 1e-9 * np.abs(y).max()
+    assert b.newton_counters()["fail"] == 0
+
+
+def test_formulation_gap_under_pressure_is_first_order_in_the_step():
+    """With a 10 MPa pore-pressure step diffusing along one fault the two
+    formulations differ at O(h): the reference's V formulation takes the
+    pressure of each stage as an implicit-Euler step from the committed P
+    and its secant rate, the Newton formulation interpolates P linearly over
+    the step. Halving the step cap halves their gap in slip rate and slip
+    (both converge to the same solution)."""
+    p = networks.small_network(seed=9, n_faults=4, tol=1e-3)
+    real = ~build_arrays(p).fake_mask
+    gaps = []
+    for hmax in (20.0, 10.0, 5.0):
+        a, b = _run_capped(p, "v", hmax, 400.0), _run_capped(p, "newton", hmax, 400.0)
+        Va, Vb = a.velocity(), b.velocity()
+        gaps.append(np.abs(Vb - Va)[real].max() / np.abs(Va).max())
+    assert gaps[0] > 0.02
+    for g1, g2 in zip(gaps, gaps[1:]):
+        assert 1.8 <= g1 / g2 <= 2.2, gaps
