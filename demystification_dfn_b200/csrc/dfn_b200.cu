@@ -15,6 +15,7 @@
 #include "hmat_device.cuh"
 #include "newton.cuh"
 #include "tc_gemm.cuh"
+#include "kv_shared64.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -65,8 +66,9 @@ unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 int bytes_per_col(int mode, int store)
 {
-    if (mode == DFN_MODE_II) return store == DFN_STORE_FP64 ? 16 : 8;
-    return store == DFN_STORE_FP64 ? 8 : 4;
+    const bool f64 = store == DFN_STORE_FP64 || store == DFN_STORE_FP64_SHARED;
+    if (mode == DFN_MODE_II) return f64 ? 16 : 8;
+    return f64 ? 8 : 4;
 }
 
 }  // namespace
@@ -145,6 +147,11 @@ struct dfn_handle {
     double *tcoef = nullptr;              // tridiagonal row factors (3 per element; tridiagonal handles)
     int64_t tc_kpad = 0, tc_mpad = 0, tc_mrows = 0;
     __nv_bfloat16 *tc_A = nullptr, *tc_B = nullptr;   // [hi | lo] each, swizzled tiles
+    // shared-geometry batch in FP64 (DFN_STORE_FP64_SHARED): one K, splits of
+    // the columns, packed V of all members per stage
+    bool s64 = false;
+    int s64_split = 1, s64_kps = 0, s64_nkc = 0, s64_rp = S64_MEM;
+    double *s64_vt = nullptr;
     StepCtl *ctl = nullptr;
     StepCtl *h_ctl = nullptr;     // pinned mirror, B entries
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -356,6 +363,27 @@ static int launch_tc(dfn_handle *h, const double *Vbase, int vmul)
     return DFN_OK;
 }
 
+// Shared-geometry K.V in FP64: V of every member packed per column, then one
+// GEMM over (row tile, member tile, column split).
+static int launch_s64(dfn_handle *h, const double *Vbase, int vmul)
+{
+    const Inst &I = h->hinst[0];
+    const int64_t nv = I.Np * h->s64_rp;
+    s64_pack_v_kernel<<<blocks_of(nv, 256), 256, 0, h->stream>>>(Vbase, vmul, h->inst, I.N, h->B, h->s64_rp, I.Np,
+                                                                 h->s64_vt);
+    h->launches++;
+    CKL();
+    dim3 grid((unsigned)((I.N + S64_ROWS - 1) / S64_ROWS), (unsigned)(h->s64_rp / S64_MEM), (unsigned)h->s64_split);
+    const double *K = static_cast<const double *>(h->K);
+    if (h->mode == DFN_MODE_II)
+        s64_gemm_kernel<2><<<grid, S64_THREADS, s64_smem_bytes(2), h->stream>>>(
+            K, h->s64_vt, h->inst, I.N, I.Np, h->B, h->s64_rp, h->s64_kps, h->s64_nkc, h->partT, h->partN);
+    else
+        s64_gemm_kernel<3><<<grid, S64_THREADS, s64_smem_bytes(3), h->stream>>>(
+            K, h->s64_vt, h->inst, I.N, I.Np, h->B, h->s64_rp, h->s64_kps, h->s64_nkc, h->partT, h->partN);
+    return DFN_OK;
+}
+
 // K.V of all networks (only0 = false) or of network 0 (only0 = true);
 // V of network i is Vbase[vmul*eoff_i + l].
 static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, bool only0)
@@ -368,6 +396,8 @@ static int launch_gemv(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         TRY(launch_hmat(h, mask, Vbase, vmul, only0));
     } else if (h->tc) {
         TRY(launch_tc(h, Vbase, vmul));
+    } else if (h->s64) {
+        TRY(launch_s64(h, Vbase, vmul));
     } else if (h->gemv_impl == 0) {
         gemv_tma_fn fn = pick_gemv_tma(h->mode, h->store);
         fn<<<(unsigned)ntiles, (TMA_CONSUMERS + 1) * 32, kTmaSmem, h->stream>>>(
@@ -1174,7 +1204,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
+    void *ptrs[] = {h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
@@ -1277,7 +1307,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     *out = nullptr;
     dfn_options opt;
     if (opt_in) opt = *opt_in; else dfn_default_options(&opt);
-    if (opt.kernel_storage < 0 || opt.kernel_storage > 3) { g_err = "bad kernel_storage"; return DFN_ERR_ARG; }
+    if (opt.kernel_storage < 0 || opt.kernel_storage > 4) { g_err = "bad kernel_storage"; return DFN_ERR_ARG; }
     if (opt.pressure_solver < 0 || opt.pressure_solver > 2) { g_err = "bad pressure_solver"; return DFN_ERR_ARG; }
     for (int i = 0; i < count; i++) {
         TRY(check_problem(&probs[i]));
@@ -1318,18 +1348,19 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
             dfn_destroy(h);
             return DFN_ERR_ARG;
         }
-    if (h->hmat && h->store == DFN_STORE_BF16X2) {
+    if (h->hmat && (h->store == DFN_STORE_BF16X2 || h->store == DFN_STORE_FP64_SHARED)) {
         g_err = "the H-matrix path stores FP64 or FP32 factors";
         dfn_destroy(h);
         return DFN_ERR_UNSUPPORTED;
     }
     h->ncomp = (h->mode == DFN_MODE_II) ? 2 : 1;
     h->tc = h->store == DFN_STORE_BF16X2_TC;
-    if (h->tc) {
+    h->s64 = h->store == DFN_STORE_FP64_SHARED;
+    if (h->tc || h->s64) {
         const dfn_problem &p0 = probs[0];
         std::string why;
         if (h->hmat) why = "the H-matrix path has its own storage";
-        if (count > 256) why = "at most 256 networks share one tensor-core kernel matrix";
+        if (count > 256) why = "at most 256 networks share one kernel matrix";
         for (int i = 1; i < count && why.empty(); i++) {
             const dfn_problem &q = probs[i];
             if (q.nb_element != p0.nb_element || q.nb_fault != p0.nb_fault || q.fracture_mode != p0.fracture_mode ||
@@ -1342,6 +1373,24 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
             dfn_destroy(h);
             return DFN_ERR_ARG;
         }
+        const int64_t N0 = p0.nb_element;
+        if (h->s64) {
+            // column splits: the fewest that fill whole waves (three CTAs per SM)
+            h->s64_rp = ((count + S64_MEM - 1) / S64_MEM) * S64_MEM;
+            h->s64_nkc = (int)((N0 + S64_COLS - 1) / S64_COLS);
+            const int64_t tiles = ((N0 + S64_ROWS - 1) / S64_ROWS) * (h->s64_rp / S64_MEM);
+            const int64_t slots = (int64_t)h->sms * 3;
+            double best = -1.0;
+            for (int sp = 1; sp <= 16 && sp <= h->s64_nkc; sp++) {
+                const int64_t units = tiles * sp;
+                const double eff = (double)units / (double)(((units + slots - 1) / slots) * slots);
+                if (eff > best + 0.02) { best = eff; h->s64_split = sp; }
+            }
+            h->s64_kps = (h->s64_nkc + h->s64_split - 1) / h->s64_split;
+        }
+    }
+    if (h->tc) {
+        const dfn_problem &p0 = probs[0];
         const int64_t N0 = p0.nb_element;
         h->tc_mrows = h->ncomp * N0;
         h->tc_nmt = (int)((h->tc_mrows + TC_BM - 1) / TC_BM);
@@ -1367,10 +1416,11 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         const dfn_problem &p = probs[i];
         Inst &I = h->hinst[i];
         I.N = p.nb_element;
-        I.Np = (h->hmat || h->tc) ? I.N : ((I.N + CW - 1) / CW) * CW;
+        I.Np = (h->hmat || h->tc) ? I.N : (h->s64 ? ((I.N + S64_COLS - 1) / S64_COLS) * S64_COLS
+                                                 : ((I.N + CW - 1) / CW) * CW);
         I.eoff = eoff;
-        I.nchunk = h->hmat ? 1 : (h->tc ? h->tc_split : I.Np / CW);
-        I.kvec = kvec;
+        I.nchunk = h->hmat ? 1 : (h->tc ? h->tc_split : (h->s64 ? h->s64_split : I.Np / CW));
+        I.kvec = h->s64 ? 0 : kvec;   // a shared-geometry batch has one matrix
         I.poff = poff;
         I.soff = soff;
         I.nsrc = p.nb_source;
@@ -1381,10 +1431,11 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         I.tol = p.tol_solver;
         I.t0 = p.time0;
         eoff += I.N;
-        if (!h->hmat && !h->tc) kvec += I.N * I.Np * bpc / 16;
+        if (!h->hmat && !h->tc && !h->s64) kvec += I.N * I.Np * bpc / 16;
+        if (h->s64 && i == 0) kvec = I.N * I.Np * bpc / 16;
         poff += I.nchunk * I.N;
         soff += I.nsrc;
-        if (!h->hmat && !h->tc) h->kv_bytes += I.N * I.N * bpc;
+        if (!h->hmat && !h->tc && (!h->s64 || i == 0)) h->kv_bytes += I.N * I.N * bpc;
     }
     const int64_t Nt = eoff;
     h->Ntot = Nt;
@@ -1595,7 +1646,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         }
         h->tc_variant = opt.gemv_impl;
     }
-    // dense kernel matrices, one per network
+    // dense kernel matrices, one per network (one for a shared-geometry batch)
     h->K_bytes = (size_t)std::max<int64_t>(kvec, 1) * 16;
     if (!h->hmat && !h->tc) {
         cudaError_t e = cudaMalloc(&h->K, h->K_bytes);
@@ -1605,8 +1656,23 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
             return DFN_ERR_NOMEM;
         }
     }
+    if (h->s64) {
+        const Inst &I = h->hinst[0];
+        dim3 grid((unsigned)I.N, (unsigned)((I.Np + 255) / 256));
+        if (h->mode == 2)
+            assemble_kernel<2, 0><<<grid, 256, 0, h->stream>>>(I.N, I.Np, h->node, h->elem, h->tan, h->nrm, h->K);
+        else
+            assemble_kernel<3, 0><<<grid, 256, 0, h->stream>>>(I.N, I.Np, h->node, h->elem, h->tan, h->nrm, h->K);
+        h->launches++;
+        CKC(cudaGetLastError());
+        DALLOC(h->s64_vt, I.Np * h->s64_rp);
+        CKC(cudaFuncSetAttribute(s64_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)s64_smem_bytes(2)));
+        CKC(cudaFuncSetAttribute(s64_gemm_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)s64_smem_bytes(3)));
+    }
     std::vector<int4> tiles;
-    for (int i = 0; i < count && !h->hmat && !h->tc; i++) {
+    for (int i = 0; i < count && !h->hmat && !h->tc && !h->s64; i++) {
         const Inst &I = h->hinst[i];
         const int64_t e0 = I.eoff;
         void *Ki = static_cast<unsigned char *>(h->K) + I.kvec * 16;
@@ -1785,7 +1851,7 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         return DFN_OK;
     };
     r.gemv_impl = h->gemv_impl;
-    if (!h->hmat && !h->tc) {
+    if (!h->hmat && !h->tc && !h->s64) {
         const int keep = h->gemv_impl;
         for (int impl = 0; impl < 2; impl++) {
             h->gemv_impl = impl;

@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from .layout import DfnOptions, DfnReport, ProblemArrays, build_arrays, ptr, to_c
 
-STORAGE = {"fp64": 0, "fp32": 1, "bf16x2": 2, "bf16x2_tc": 3}
+STORAGE = {"fp64": 0, "fp32": 1, "bf16x2": 2, "bf16x2_tc": 3, "fp64_shared": 4}
 PRESSURE = {"cg": 0, "tridiag": 1, "cg_exact": 2}
 GEMV = {"tma": 0, "ldg": 1, "tc_persistent": 0, "tc_ring_deep": 1, "tc_ring_2stage": 2}
 

@@ -52,8 +52,13 @@ enum { DFN_KERNEL_DIRECT = 0, DFN_KERNEL_HMATRIX = 1 };        /* hyperparameter
  * one geometry (same nb_element, nodes, fracture mode and elastic constants;
  * up to 256 networks), K is stored once as BF16 hi + lo matrices and the
  * K.V of all networks of a stage is one tcgen05 tensor-core GEMM (BF16
- * products, FP32 accumulation). No counterpart in the reference. */
-enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_BF16X2_TC = 3 };
+ * products, FP32 accumulation). DFN_STORE_FP64_SHARED: the same shared K
+ * in FP64 and an FP64 GEMM on the CUDA cores (K streamed once per stage for
+ * all networks, products and sums in FP64), the counterpart that isolates
+ * the tensor-core arithmetic from the sharing. No counterpart in the
+ * reference. */
+enum { DFN_STORE_FP64 = 0, DFN_STORE_FP32 = 1, DFN_STORE_BF16X2 = 2, DFN_STORE_BF16X2_TC = 3,
+       DFN_STORE_FP64_SHARED = 4 };
 /* Pressure solver: DFN_PRESSURE_CG is the reference's CG with tree-reduced
  * dot products (systems of 2048 elements or more, when a launch has few of
  * them, are solved by a cluster of 2 to 16 CTAs holding the vectors in shared
