@@ -234,6 +234,7 @@ def leg_hmatrix(args, local, stream):
     build_s = time.perf_counter() - t0
     s.set_stream(stream.cuda_stream)
     st = s.hmat_stats()
+    tune = s.autotune()
     s.solve_steps(3)
     s.profile_kv(True)
     n = 10
@@ -245,7 +246,7 @@ def leg_hmatrix(args, local, stream):
     dense_equiv = 2 * s.N * s.N * 4
     out = {"workload": "4000 faults 20x20 km, shear loading 1e-9 m/s, H-matrix leaf 64 eta 2 ACA 1e-6, FP32 factors",
            "n_elements": s.N,
-           "build_s": build_s, "stats": st, "steps_per_s": n / (ms / 1e3), "kv_avg_ms": kavg,
+           "build_s": build_s, "stats": st, "autotune": tune, "steps_per_s": n / (ms / 1e3), "kv_avg_ms": kavg,
            "kv_bytes": s.kernel_bytes, "kv_GBps": gbs, "kv_frac_of_measured_hbm": gbs / hbm,
            "compression_vs_dense_fp32": s.kernel_bytes / dense_equiv, "simulated_s": rep["time"]}
     st32 = s.state()
@@ -313,17 +314,23 @@ def leg_learned(args, local, stream):
                        "to t = %.0e s" % t_end,
            "train_samples": int(len(t)), "train_loss_first_last": [float(loss[0]), float(loss[1])],
            "train_s": time.perf_counter() - t0, "networks": len(test_nets)}
-    runs = (("newton_fp64_analytic", "newton", "analytic", "fp64"),
-            ("newton_fp32_quasistatic", "newton", "quasistatic", "fp32"),
-            ("newton_fp32_analytic", "newton", "analytic", "fp32"),
-            ("newton_fp32_mlp", "newton", "mlp", "fp32"),
-            ("v_fp64", "v", "analytic", "fp64"))
+    runs = (("newton_fp64_analytic", "newton", "analytic", "fp64", None),
+            ("newton_fp32_quasistatic", "newton", "quasistatic", "fp32", None),
+            ("newton_fp32_analytic", "newton", "analytic", "fp32", None),
+            ("newton_fp32_mlp", "newton", "mlp", "fp32", None),
+            ("newton_fp32_mlp_ungated", "newton", "mlp", "fp32", 0.0),
+            ("newton_fp32_mlp_gate1e-2", "newton", "mlp", "fp32", 1e-2),
+            ("newton_fp32_mlp_gate1e-3", "newton", "mlp", "fp32", 1e-3),
+            ("newton_fp32_mlp_never", "newton", "mlp", "fp32", 1e300),
+            ("v_fp64", "v", "analytic", "fp64", None))
     ref = None
-    for name, form, guess, store in runs:
+    for name, form, guess, store, gate in runs:
         e = Ensemble(test_nets, storage=store, pressure="tridiag", device=local, formulation=form, guess=guess)
         e.set_stream(stream.cuda_stream)
         if guess == "mlp":
             e.set_mlp(w)
+            if gate is not None:
+                e.set_mlp_gate(gate)
         out["elements"] = int(sum(e.n_elements))
         reps, ms = _timed(stream, lambda: e.solve(n_steps=max_steps, t_end=t_end, check=False))
         steps = sum(r["it_count"] for r in reps)
@@ -331,6 +338,7 @@ def leg_learned(args, local, stream):
                "newton_solves": int(sum(r["newton_solves"] for r in reps)),
                "newton_iterations": int(sum(r["newton_iters"] for r in reps)),
                "newton_fail": int(sum(r["newton_fail"] for r in reps)),
+               "mlp_warps": int(sum(r["mlp_warps"] for r in reps)),
                "reached_t_end": sum(1 for r in reps if abs(r["time"] - t_end) <= 1e-9 * t_end),
                "status_counts": {str(s): sum(1 for r in reps if r["status"] == s)
                                  for s in sorted({r["status"] for r in reps})}}
@@ -374,6 +382,7 @@ def leg_learned(args, local, stream):
         b = out["newton_fp32_" + base]
         if b["newton_iterations"]:
             out["newton_iterations_per_solve_saved_vs_" + base] = 1.0 - per(m) / per(b)
+    out["time_to_t_end_newton_fp32_analytic_over_mlp"] = out["newton_fp32_analytic"]["ms_to_t_end"] / m["ms_to_t_end"]
     out["time_to_t_end_v_fp64_over_newton_fp32_mlp"] = out["v_fp64"]["ms_to_t_end"] / m["ms_to_t_end"]
     out["time_to_t_end_newton_fp64_over_newton_fp32_mlp"] = (out["newton_fp64_analytic"]["ms_to_t_end"]
                                                               / m["ms_to_t_end"])
@@ -400,7 +409,8 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
     variants = (("v_fp64", "v", "fp64", "analytic"), ("v_fp32", "v", "fp32", "analytic"),
                 ("v_bf16x2", "v", "bf16x2", "analytic"), ("newton_fp64", "newton", "fp64", "analytic"),
                 ("newton_fp32", "newton", "fp32", "analytic"), ("newton_fp32_mlp", "newton", "fp32", "mlp"),
-                ("newton_bf16x2_mlp", "newton", "bf16x2", "mlp"))
+                ("newton_bf16x2_mlp", "newton", "bf16x2", "mlp"), ("newton_hmat_fp32", "newton", "fp32", "analytic"))
+    hmembers = networks.ensemble(64, kernel="hmatrix")
     # the learned guess: solves recorded on held-out networks, trained on the GPU
     held = [networks.ensemble_member(s) for s in range(64, 72)]
     rec = Ensemble(held, storage="fp32", pressure="tridiag", device=local, formulation="newton")
@@ -417,13 +427,18 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
                        "loss_first_last": [float(loss[0]), float(loss[1])]}}
     slips_ref = {}
     for name, form, store, guess in variants:
-        e = Ensemble(members, storage=store, pressure="tridiag", device=local, formulation=form, guess=guess)
+        hm = "hmat" in name
+        t0 = time.perf_counter()
+        e = Ensemble(hmembers if hm else members, storage=store, pressure="tridiag", device=local,
+                     formulation=form, guess=guess, **(dict(hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-7) if hm else {}))
+        create_s = time.perf_counter() - t0
         e.set_stream(stream.cuda_stream)
         if guess == "mlp":
             e.set_mlp(weights)
         tune = e.autotune()
         reps, ms_end = _timed(stream, lambda: e.solve(t_end=t_end, check=False))
         res = {"elements": int(sum(e.n_elements)), "kv_bytes": e.kernel_bytes, "ms_to_t_end": ms_end,
+               "create_s": create_s,
                "steps_to_t_end": int(sum(r["it_count"] for r in reps)),
                "reached_t_end": sum(1 for r in reps if abs(r["time"] - t_end) <= 1e-9 * t_end),
                "status_counts": {str(c): sum(1 for r in reps if r["status"] == c)
@@ -449,8 +464,13 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
         e.profile_kv(False)
         kavg = kms / max(kn, 1)
         live = sum(1 for r in reps2 if r["status"] == 0)
+        # the K.V of all 64 networks back to back (launches inside the loop
+        # skip the networks that sit out a round, so their mean understates
+        # a full launch)
+        kfull = e.time_kernel(10)
         res.update({"network_steps_per_s": len(members) * n_steps / (ms / 1e3), "networks_ok": live,
-                    "kv_avg_ms": kavg, "kv_frac_of_measured_hbm": e.kernel_bytes / (kavg / 1e3) / 1e9 / hbm,
+                    "kv_avg_ms_in_loop": kavg, "kv_ms_all_networks": kfull,
+                    "kv_frac_of_measured_hbm": e.kernel_bytes / (kfull / 1e3) / 1e9 / hbm,
                     "kv_impl": tune["gemv_impl"],
                     "newton_iterations_per_solve": (sum(r["newton_iters"] for r in reps) /
                                                     max(sum(r["newton_solves"] for r in reps), 1))})
@@ -669,10 +689,15 @@ def run_case(argv):
     python bench.py --case tc_round [cg|tridiag]
         the same batch, six solve rounds launched one by one (launch list of
         a round: GEMM, pressure, friction, step control).
-    python bench.py --case hmatrix_kv [n_faults box_m]
+    python bench.py --case hmatrix_kv [n_faults box_m [tuned]]
         the 4000-fault network in 20 km x 20 km (N = 81 750; or n_faults in a
         box_m square) as an H-matrix (leaf 64, eta 2, ACA 1e-6, FP32
-        factors): three K.V launches (several kernels each).
+        factors): three K.V launches (several kernels each); "tuned" runs the
+        autotuner first, "grids D W" sets the CTAs of the dense-row and
+        small-leaf kernels (dfn_set_hmat_grids).
+    python bench.py --case s64_kv [R]
+        R realisations (default 64) of the 800-fault network sharing one FP64
+        kernel matrix: three K.V launches of the FP64 GEMM (4.1 GB per launch).
     python bench.py --case hmatrix_autotune
         the same network with CG pressure: the autotuner's timing of the
         stage pressure systems by one CTA each and by a cluster of CTAs each
@@ -734,9 +759,25 @@ def run_case(argv):
         box = float(argv[2]) if len(argv) > 2 else 20000.0
         p = networks.fault_network(n_faults=nf, box=box, seed=0, kernel="hmatrix", tol=1e-6)
         e = Simulation(p, storage="fp32", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-6)
+        if len(argv) > 3 and argv[3] == "tuned":
+            import json
+
+            print(json.dumps(e.autotune()))
+        elif len(argv) > 5 and argv[3] == "grids":
+            e.set_hmat_grids(int(argv[4]), int(argv[5]))
         rng = np.random.default_rng(0)
         for _ in range(3):
             e.kernel(rng.normal(size=e.N))
+    elif case == "s64_kv":
+        # R realisations of the 800-fault network, FP64 shared kernel matrix:
+        # three K.V launches of the FP64 GEMM (4.1 GB of K per launch)
+        R = int(argv[1]) if len(argv) > 1 else 64
+        base = networks.fault_network(n_faults=800, seed=0)
+        e = Ensemble(networks.shared_geometry_ensemble(R, base=base, seed=0), storage="fp64_shared")
+        rng = np.random.default_rng(0)
+        N = e.n_elements[0]
+        for _ in range(3):
+            e.kernel([rng.normal(size=N) for _ in range(R)])
     elif case == "hmatrix_autotune":
         import json
 

@@ -75,6 +75,7 @@ def load():
         "dfn_profile_kv_read": (i32, [P, dp, ctypes.POINTER(i64)]),
         "dfn_get_report": (i32, [P, i32, ctypes.POINTER(DfnReport)]),
         "dfn_set_mlp": (i32, [P, ctypes.POINTER(ctypes.c_float)]),
+        "dfn_set_mlp_gate": (i32, [P, dbl]),
         "dfn_record": (i32, [P, i64]),
         "dfn_record_read": (i32, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64,
                                   ctypes.POINTER(i64)]),
@@ -94,6 +95,7 @@ def load():
         "dfn_set_hmat_small_leaves": (i32, [P, i32]),
         "dfn_crossing_count": (i64, [P]),
         "dfn_set_tri_shape": (i32, [P, i32]),
+        "dfn_set_hmat_grids": (i32, [P, i64, i64]),
         "dfn_autotune": (i32, [P, ctypes.c_void_p]),
         "dfn_kernel_batch": (i32, [P, dp, dp, dp]),
         "dfn_velocity": (i32, [P, dp]),
@@ -129,17 +131,23 @@ def check(status, lib=None):
 
 class DfnTuning(ctypes.Structure):
     _fields_ = [("gemv_impl", ctypes.c_int32), ("tri_thread", ctypes.c_int32), ("ms", ctypes.c_double * 6),
-                ("cg_cluster", ctypes.c_int32), ("cg_cluster_ctas", ctypes.c_int32)]
+                ("cg_cluster", ctypes.c_int32), ("cg_cluster_ctas", ctypes.c_int32),
+                ("hm_dense_grid", ctypes.c_int64), ("hm_warp_grid", ctypes.c_int64)]
 
 
-def autotune(lib, h, storage, pressure):
+def autotune(lib, h, storage, pressure, hmat=False):
     """dfn_autotune on handle h; names the K.V shapes of the handle's storage
     and the pressure shapes of its solver."""
     t = DfnTuning()
     check(lib.dfn_autotune(h, ctypes.byref(t)), lib)
+    extra = {}
     if storage == "bf16x2_tc":
         names = ("tc_persistent", "tc_ring_deep", "tc_ring_2stage")
         ms = {"kv_tc_persistent": t.ms[0], "kv_tc_ring_deep": t.ms[1], "kv_tc_ring_2stage": t.ms[4]}
+    elif hmat:
+        names = ("tma", "ldg")
+        ms = {"kv_hmat_best": t.ms[0], "kv_hmat_one_cta_per_task": t.ms[1]}
+        extra = {"hm_dense_grid": int(t.hm_dense_grid), "hm_warp_grid": int(t.hm_warp_grid)}
     else:
         names = ("tma", "ldg")
         ms = {"kv_tma": t.ms[0], "kv_ldg": t.ms[1]}
@@ -153,4 +161,4 @@ def autotune(lib, h, storage, pressure):
         ms["pressure_tile"] = t.ms[5]
     return {"gemv_impl": names[t.gemv_impl], "short_segments": ("warp", "thread", "tile")[t.tri_thread],
             "cg_form": ("cta", "cluster", "cta_smem")[t.cg_cluster], "cg_cluster_ctas": int(t.cg_cluster_ctas),
-            "ms": ms}
+            "ms": ms, **extra}

@@ -171,6 +171,8 @@ struct dfn_handle {
     int *hl5 = nullptr;                                // their blocks (one CTA each when small_form = 1)
     HLeafW *hlw = nullptr;                             // their descriptors (one warp each)
     int small_form = 0;                                // small leaves: 0 one warp each, 1 one CTA each
+    int64_t hm_dense_grid = 0, hm_warp_grid = 0;       // CTAs of the dense-row and small-leaf kernels (0: one
+                                                       // per task / per four leaves; else a persistent grid)
     void *hvals = nullptr;
     int *hperm = nullptr;
     int64_t *hrowptr = nullptr, *hslots = nullptr;
@@ -183,6 +185,7 @@ struct dfn_handle {
     double max_step = 86400.0;            // cap on t_try after an accepted step (the reference's one day)
     double *tau0 = nullptr, *wlast = nullptr, *vnow = nullptr;
     MlpTC *mlp = nullptr;                 // tensor-core image of the learned guess
+    double mlp_gate = 1e-1;               // relative residual of the analytic start that calls for it
     float *rec_x = nullptr, *rec_t = nullptr;
     unsigned long long *rec_n = nullptr;
     long long rec_cap = 0;
@@ -257,7 +260,8 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         h->launches++;
         CKL();
     } else if (n5 > 0) {
-        const unsigned g = (unsigned)((n5 + 3) / 4);
+        const int64_t gfull = (n5 + 3) / 4;
+        const unsigned g = (unsigned)((h->hm_warp_grid > 0 && h->hm_warp_grid < gfull) ? h->hm_warp_grid : gfull);
         if (h->store == 0)
             hm_lowrank_warp_kernel<double><<<g, 128, 0, ls>>>(h->hlw, n5, h->ctl, mask, (const double *)h->hvals,
                                                               h->hxp, h->hout);
@@ -298,12 +302,13 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         CKL();
     }
     if (n3 > 0) {
+        const unsigned g3 = (unsigned)((h->hm_dense_grid > 0 && h->hm_dense_grid < n3) ? h->hm_dense_grid : n3);
         if (h->store == 0)
-            hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
-                                                                         (const double *)h->hvals, h->hxp, h->hout);
+            hm_dense_kernel<double><<<g3, 256, 0, h->stream>>>(h->ht3, n3, h->hblk, h->inst, h->ctl, mask,
+                                                               (const double *)h->hvals, h->hxp, h->hout);
         else
-            hm_dense_kernel<float><<<(unsigned)n3, 256, 0, h->stream>>>(h->ht3, h->hblk, h->inst, h->ctl, mask,
-                                                                        (const float *)h->hvals, h->hxp, h->hout);
+            hm_dense_kernel<float><<<g3, 256, 0, h->stream>>>(h->ht3, n3, h->hblk, h->inst, h->ctl, mask,
+                                                              (const float *)h->hvals, h->hxp, h->hout);
         h->launches++;
         CKL();
     }
@@ -508,7 +513,7 @@ static FricParams fric_params(dfn_handle *h, int64_t nelem)
     f.Ptemp = h->Ptemp; f.Pdot = h->Pdot_s; f.Pc = h->P; f.y = h->Y; f.ytmp = h->ytmp; f.kbuf = h->kbuf; f.yscal = h->yscal;
     f.yout = h->yout; f.ctl = h->ctl;
     f.form = h->form; f.guess = h->guess; f.maxit = h->newton_maxit; f.tol = h->newton_tol; f.off_explicit = 0.0;
-    f.tau0 = h->tau0; f.wlast = h->wlast; f.vnow = h->vnow; f.mlp = h->mlp;
+    f.tau0 = h->tau0; f.wlast = h->wlast; f.vnow = h->vnow; f.mlp = h->mlp; f.mlp_gate = h->mlp_gate;
     f.slip = h->slip; f.slip_out = h->slip_out; f.slip_acc = h->slip_acc;
     f.rec_x = h->rec_x; f.rec_t = h->rec_t; f.rec_n = h->rec_n; f.rec_cap = h->rec_cap;
     return f;
@@ -518,11 +523,9 @@ static int launch_friction(dfn_handle *h, int stage, int sys, int mask, int64_t 
 {
     FricParams f = fric_params(h, nelem);
     f.off_explicit = off_explicit;
-    // 128-thread blocks without the learned guess: five per SM at its
-    // register count (two of 256 threads); 256 with it (the network image in
-    // shared memory is staged once per block)
+    // 128-thread blocks: five per SM at the register count (two of 256)
     if (h->form == DFN_FORM_NEWTON && h->guess == DFN_GUESS_MLP)
-        friction_kernel<true><<<(unsigned)((nelem + 255) / 256), 256, sizeof(MlpTC), h->stream>>>(f, stage, sys, mask);
+        friction_kernel<true><<<(unsigned)((nelem + 127) / 128), 128, 0, h->stream>>>(f, stage, sys, mask);
     else
         friction_kernel<false><<<(unsigned)((nelem + 127) / 128), 128, 0, h->stream>>>(f, stage, sys, mask);
     h->launches++;
@@ -754,6 +757,7 @@ static void fill_report(const StepCtl &c, dfn_report *r)
     r->cg_iterations = c.cg_iters; r->probe_halvings = c.halvings; r->time = c.time; r->t_try = c.t_try;
     r->last_hdid = c.hdid; r->status = c.status; r->pad = 0; r->stage_cg_failures = c.stage_noconv;
     r->newton_solves = c.newton_solves; r->newton_iters = c.newton_iters; r->newton_fail = c.newton_fail;
+    r->mlp_warps = c.mlp_warps;
 }
 
 // ---------------------------------------------------------------------------
@@ -1861,6 +1865,27 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         r.gemv_impl = h->gemv_impl;
         (void)keep;
     }
+    if (h->hmat) {
+        // grids of the dense-row and small-leaf kernels: one CTA per task
+        // (0) or persistent grids of 4 or 8 CTAs per SM; identical results
+        const int64_t opts[3] = {0, 4 * (int64_t)h->sms, 8 * (int64_t)h->sms};
+        double best = 1e300;
+        int64_t bd = 0, bw = 0;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                h->hm_dense_grid = opts[a];
+                h->hm_warp_grid = 2 * opts[b];
+                double ms = 0.0;
+                TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, ms));
+                if (ms < best) { best = ms; bd = opts[a]; bw = 2 * opts[b]; }
+                if (a == 0 && b == 0) r.ms[1] = ms;
+            }
+        h->hm_dense_grid = bd;
+        h->hm_warp_grid = bw;
+        r.ms[0] = best;
+        r.hm_dense_grid = bd;
+        r.hm_warp_grid = bw;
+    }
     if (h->tc) {
         // persistent -> ms[0], unit per CTA with the deepest ring -> ms[1],
         // unit per CTA with a 2-stage ring -> ms[4] (when that is another shape)
@@ -1945,6 +1970,18 @@ int32_t dfn_set_wait_limit(dfn_handle *h, int32_t polls)
 }
 
 int64_t dfn_crossing_count(const dfn_handle *h) { return h ? h->ncross : -1; }
+
+int32_t dfn_set_hmat_grids(dfn_handle *h, int64_t dense_ctas, int64_t warp_ctas)
+{
+    if (!h || dense_ctas < 0 || warp_ctas < 0) return DFN_ERR_ARG;
+    if (!h->hmat) return DFN_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->hm_dense_grid = dense_ctas;
+    h->hm_warp_grid = warp_ctas;
+    drop_graph(h);
+    return DFN_OK;
+}
 
 int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape)
 {
@@ -2399,6 +2436,16 @@ int32_t dfn_set_mlp(dfn_handle *h, const float *weights)
         set_err("dfn_set_mlp", e, __FILE__, __LINE__);
         return DFN_ERR_CUDA;
     }
+    return DFN_OK;
+}
+
+int32_t dfn_set_mlp_gate(dfn_handle *h, double rel)
+{
+    if (!h || !(rel >= 0.0)) return DFN_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->mlp_gate = rel;
+    drop_graph(h);   // a captured graph holds the old gate in its kernel parameters
     return DFN_OK;
 }
 

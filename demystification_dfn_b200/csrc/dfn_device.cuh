@@ -49,6 +49,7 @@ struct StepCtl {
     int commit_bad;   // committed state of this step: bit 0 sigmaN > 0, bit 1 non-finite
     long long stage_noconv;  // stage pressure solves that hit the CG cap
     long long newton_solves, newton_iters, newton_fail;  // Newton formulation counters
+    long long mlp_warps;     // warps that evaluated the learned guess
 };
 
 // Cash-Karp tableau, src/ode_solver/ode_bs.f90:200-210.
@@ -1784,6 +1785,7 @@ struct FricParams {
     double *wlast;                // [Ntot] last solution, warm start
     double *vnow;                 // [Ntot] V of this evaluation
     const MlpTC *mlp;             // tensor-core image of the learned guess (global)
+    double mlp_gate;              // relative residual of the analytic start above which it is evaluated
     // V formulation: slip as a passive component (dslip/dt = V)
     const double *slip;           // [Ntot] committed
     double *slip_out, *slip_acc;  // [Ntot] the attempt's 5th-order slip, partial stage sum
@@ -1801,7 +1803,8 @@ struct NPre {
     double tau, s, lnA, wa, ga;
     int kind;          // 0 fake element, 1 no frictional strength, 2 solve
     bool wa_ok;        // the analytic start meets the tolerance
-    bool need;         // the network is evaluated for this element
+    bool need;         // the analytic start misses the tolerance (the learned guess may help)
+    bool big;          // ... by more than the gate: calls for the network in this warp
     float x[MLP_IN];
 };
 
@@ -1814,6 +1817,7 @@ __device__ __forceinline__ void newton_pre(const FricParams &f, int64_t e, int m
     q.s = -(sig + Pt);
     q.wa_ok = true;
     q.need = false;
+    q.big = false;
     q.kind = f.fake[e] ? 0 : (q.s > 0.0 ? 2 : 1);
     if (q.kind != 2) return;
     const double s = q.s, tau = q.tau;
@@ -1835,14 +1839,20 @@ __device__ __forceinline__ void newton_pre(const FricParams &f, int64_t e, int m
         q.ga = fabs(tau - eva - s * a * q.wa);
         q.wa_ok = q.ga <= f.tol * (fabs(tau) + s * a * fabs(q.wa) + 1e-300);
         if (!q.wa_ok) mlp_features(q.wa, w0, wr, psi, s, Pt, a, b, q.x);
+        // the network is worth its cost only in warps where Newton from the
+        // analytic start would take several iterations (a relative residual
+        // above the gate); the warp then offers the guess to every element
+        // whose start misses the tolerance, since its slowest lane sets the
+        // warp's iteration count
         q.need = (f.guess == 1) && !q.wa_ok;
+        q.big = q.need && q.ga > f.mlp_gate * (fabs(tau) + s * a * fabs(q.wa) + 1e-300);
     }
 }
 
 // Second half: the solve from the chosen start, the slip rate and the
 // derivatives [dslip, dpsi, dsigma0]; ym is the network's output.
 __device__ __forceinline__ void newton_post(const FricParams &f, int64_t e, double eta, double psi, const NPre &q,
-                                            float ym, double &dV, double &dpsi, double &dsig, int &iters, int &ok)
+                                            float ym, bool have_ym, double &dV, double &dpsi, double &dsig, int &iters, int &ok)
 {
     iters = 0;
     ok = 1;
@@ -1859,7 +1869,7 @@ __device__ __forceinline__ void newton_post(const FricParams &f, int64_t e, doub
         V = q.tau / eta;
     } else {
         double w = q.wa;
-        if (q.need) {
+        if (q.need && have_ym) {
             // the learned guess is judged by the FP64 residual: Newton
             // starts from whichever of the two guesses fits better
             const double wm = q.wa + 10.0 * (double)ym;
@@ -1920,13 +1930,9 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
 // LEARNED: Newton formulation with the learned guess (a separate
 // instantiation keeps the tensor-core inference's registers out of the
 // other variants).
-// (LEARNED: three CTAs of 256 threads per SM, so that the rarely taken
-// inference path spills rather than cost the element path its occupancy.)
 template <bool LEARNED>
-__global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction_kernel(FricParams f, int stage, int sys,
-                                                                                   int mask)
+__global__ void __launch_bounds__(128, 5) friction_kernel(FricParams f, int stage, int sys, int mask)
 {
-    extern __shared__ __align__(16) unsigned char fric_smem[];
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int myi = -1;
     int nit = 0, nsolve = 0, nfail = 0;
@@ -1941,6 +1947,7 @@ __global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction
     NPre q;
     q.kind = 0;
     q.need = false;
+    q.big = false;
 #pragma unroll
     for (int i = 0; i < MLP_IN; i++) q.x[i] = 0.0f;
     if (myi >= 0) {
@@ -1978,17 +1985,17 @@ __global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction
             newton_pre(f, e, f.mode, I.mu_2cs, tt, psi, sig, T, Nn, Pt, q);
         }
     }
-    // the learned guess: the network's image goes to shared memory only in
-    // blocks where some element needs it, and runs only in those warps
+    // the learned guess: evaluated only by warps that hold an element whose
+    // analytic start misses the tolerance by more than the gate; the
+    // network's FP16 image is read from global memory (11 KB, L1-resident
+    // after the first warp), so warps need no block barrier
     float ym = 0.0f;
+    bool have_ym = false;
     if constexpr (LEARNED) {
-        MlpTC &S = *reinterpret_cast<MlpTC *>(fric_smem);
-        if (__syncthreads_or(q.need)) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(f.mlp);
-            uint4 *dst = reinterpret_cast<uint4 *>(fric_smem);
-            for (int p = threadIdx.x; p < (int)(sizeof(MlpTC) / 16); p += blockDim.x) dst[p] = src[p];
-            __syncthreads();
-            if (__any_sync(0xffffffffu, q.need)) ym = mlp_warp_tc(S, q.x);
+        if (__any_sync(0xffffffffu, q.big)) {
+            ym = mlp_warp_tc_call(f.mlp, q.x[0], q.x[1], q.x[2], q.x[3], q.x[4], q.x[5], q.x[6]);
+            have_ym = true;
+            if ((threadIdx.x & 31) == 0 && myi >= 0) atomicAdd((unsigned long long *)&f.ctl[myi].mlp_warps, 1ull);
         }
     }
     // phase 2: derivatives and the Cash-Karp stage arithmetic
@@ -2001,7 +2008,7 @@ __global__ void __launch_bounds__(LEARNED ? 256 : 128, LEARNED ? 3 : 5) friction
         double dV, dpsi, dsig;
         if (f.form == 1) {
             int ok = 1;
-            newton_post(f, e, I.mu_2cs, psi, q, ym, dV, dpsi, dsig, nit, ok);
+            newton_post(f, e, I.mu_2cs, psi, q, ym, have_ym, dV, dpsi, dsig, nit, ok);
             nsolve = f.fake[e] ? 0 : 1;
             nfail = ok ? 0 : 1;
         } else {

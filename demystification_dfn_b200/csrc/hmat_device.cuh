@@ -116,18 +116,15 @@ __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict
     }
 }
 
-// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
-// xp; four rows per half-warp in flight (their loads issued together).
 template <typename T>
-__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
-                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
-                                                       int mask, const T *__restrict__ vals,
-                                                       const double *__restrict__ xp, double *__restrict__ out)
+__device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restrict__ blks,
+                                              const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl, int mask,
+                                              const T *__restrict__ vals, const double *__restrict__ xp,
+                                              double *__restrict__ out)
 {
     using VT = typename HVec<T>::V;
     constexpr int W = HVec<T>::W;
     constexpr int U = 4;
-    const HTask t = tasks[blockIdx.x];
     const HBlk b = blks[t.blk];
     if (!takes_part(ctl, b.inst, mask)) return;
     const Inst &I = inst[b.inst];
@@ -167,6 +164,22 @@ __global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__
             if (hl == 0 && i0 + u < t.count) out[b.outoff + t.start + i0 + u] = s[u];
         }
     }
+}
+
+// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
+// xp; four rows per half-warp in flight (their loads issued together). CTA
+// c takes tasks c, c + gridDim.x, ... (a grid of one CTA per task, or a
+// persistent grid: the leaves are a few KB each, so a CTA per task spends
+// much of its life starting up; the rows' arithmetic is the same either way).
+template <typename T>
+__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
+                                                       const HBlk *__restrict__ blks,
+                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
+                                                       int mask, const T *__restrict__ vals,
+                                                       const double *__restrict__ xp, double *__restrict__ out)
+{
+    for (int64_t tk = blockIdx.x; tk < ntasks; tk += gridDim.x)
+        hm_dense_task<T>(tasks[tk], blks, inst, ctl, mask, vals, xp, out);
 }
 
 // Low-rank leaves of at most HM_COLS columns, whole: x staged in shared
@@ -262,20 +275,13 @@ struct HLeafW {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
-                                                                  const StepCtl *__restrict__ ctl, int mask,
-                                                                  const T *__restrict__ vals,
-                                                                  const double *__restrict__ xp,
-                                                                  double *__restrict__ out)
+__device__ __forceinline__ void hm_lowrank_warp_leaf(const HLeafW &d, const T *__restrict__ vals,
+                                                     const double *__restrict__ xp, double *__restrict__ out,
+                                                     double *z)
 {
     using VT = typename HVec<T>::V;
     constexpr int W = HVec<T>::W;
-    __shared__ double zs[4][hmat::kMaxRank];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t k = (int64_t)blockIdx.x * 4 + warp;
-    if (k >= n) return;   // warp-uniform; the kernel has no block barrier
-    const HLeafW d = leaves[k];
-    if (!takes_part(ctl, d.inst, mask)) return;
+    const int lane = threadIdx.x & 31;
     const int rank = d.rank, nv = d.ld / W;
     int g = 1;
     while (g < nv && g < 32) g <<= 1;
@@ -289,7 +295,6 @@ __global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *_
     }
     const T *A = vals + d.aoff;
     const VT *Bt = reinterpret_cast<const VT *>(A + (int64_t)rank * d.lda);
-    double *z = zs[warp];
 #pragma unroll 4
     for (int q0 = 0; q0 < rank; q0 += rp) {
         const int q = q0 + sub;
@@ -328,6 +333,25 @@ __global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *_
 #pragma unroll
         for (int c = 0; c < W; c++)
             if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
+    }
+    __syncwarp();   // z is rewritten by the warp's next leaf
+}
+
+// Warp w of CTA c takes leaves 4c + w, 4c + w + 4 gridDim.x, ... (one leaf
+// per warp with a grid covering the list, or a persistent grid).
+template <typename T>
+__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+                                                                  const StepCtl *__restrict__ ctl, int mask,
+                                                                  const T *__restrict__ vals,
+                                                                  const double *__restrict__ xp,
+                                                                  double *__restrict__ out)
+{
+    __shared__ double zs[4][hmat::kMaxRank];
+    const int warp = threadIdx.x >> 5;
+    for (int64_t k = (int64_t)blockIdx.x * 4 + warp; k < n; k += (int64_t)gridDim.x * 4) {
+        const HLeafW d = leaves[k];
+        if (!takes_part(ctl, d.inst, mask)) continue;   // warp-uniform; the kernel has no block barrier
+        hm_lowrank_warp_leaf<T>(d, vals, xp, out, zs[warp]);
     }
 }
 

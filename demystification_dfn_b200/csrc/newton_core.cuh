@@ -113,7 +113,7 @@ __device__ __forceinline__ uint32_t pack_h2(float lo, float hi)
 }
 
 // All 32 lanes call it (converged); returns the output for this lane's row.
-__device__ __forceinline__ float mlp_warp_tc(const MlpTC &S, const float x[MLP_IN])
+__device__ __forceinline__ float mlp_warp_tc_body(const MlpTC &S, const float x[MLP_IN])
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -201,6 +201,21 @@ __device__ __forceinline__ float mlp_warp_tc(const MlpTC &S, const float x[MLP_I
         }
     }
     return r + S.b3;
+}
+
+__device__ __forceinline__ float mlp_warp_tc(const MlpTC &S, const float x[MLP_IN])
+{
+    return mlp_warp_tc_body(S, x);
+}
+
+// The same inference as a called function, for the stage kernel: its
+// registers are then allocated apart from the element path's (which every
+// element takes, while the inference runs in a few warps).
+__device__ __noinline__ float mlp_warp_tc_call(const MlpTC *S, float x0, float x1, float x2, float x3, float x4,
+                                               float x5, float x6)
+{
+    const float x[MLP_IN] = {x0, x1, x2, x3, x4, x5, x6};
+    return mlp_warp_tc_body(*S, x);
 }
 
 // eta*V(w) and eta*dV/dw without overflow: V = (2V0/C) sinh(w) with

@@ -59,7 +59,7 @@ class Ensemble:
     def autotune(self):
         """Time the interchangeable launch shapes (K.V copy path, short-segment
         pressure solve) on this handle's data and keep the fastest."""
-        return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
+        return _lib.autotune(self.lib, self.h, self._storage, self._pressure, hmat=self.arrays[0].static_kernel == 1)
 
     @property
     def crossing_count(self):
@@ -140,6 +140,11 @@ class Ensemble:
     def set_mlp(self, weights):
         w = np.ascontiguousarray(weights, dtype=np.float32)
         _lib.check(self.lib.dfn_set_mlp(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.lib)
+
+    def set_mlp_gate(self, rel):
+        """Evaluate the learned guess only where the analytic start's
+        relative residual exceeds rel (dfn_set_mlp_gate)."""
+        _lib.check(self.lib.dfn_set_mlp_gate(self.h, float(rel)), self.lib)
 
     def record(self, capacity):
         _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)

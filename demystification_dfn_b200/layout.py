@@ -198,7 +198,7 @@ class DfnReport(ctypes.Structure):
                 ("probe_halvings", ctypes.c_int64), ("time", ctypes.c_double), ("t_try", ctypes.c_double),
                 ("last_hdid", ctypes.c_double), ("status", ctypes.c_int32), ("pad", ctypes.c_int32),
                 ("stage_cg_failures", ctypes.c_int64), ("newton_solves", ctypes.c_int64),
-                ("newton_iters", ctypes.c_int64), ("newton_fail", ctypes.c_int64)]
+                ("newton_iters", ctypes.c_int64), ("newton_fail", ctypes.c_int64), ("mlp_warps", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}

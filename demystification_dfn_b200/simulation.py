@@ -98,7 +98,7 @@ class Simulation:
     def autotune(self):
         """Time the interchangeable launch shapes (K.V copy path, short-segment
         pressure solve) on this handle's data and keep the fastest."""
-        return _lib.autotune(self.lib, self.h, self._storage, self._pressure)
+        return _lib.autotune(self.lib, self.h, self._storage, self._pressure, hmat=self.arrays.static_kernel == 1)
 
     @property
     def crossing_count(self):
@@ -113,6 +113,11 @@ class Simulation:
         """H-matrix handles: whole low-rank leaves of at most 32 KiB by one
         "warp" each (the default) or one "cta" each."""
         _lib.check(self.lib.dfn_set_hmat_small_leaves(self.h, {"warp": 0, "cta": 1}[form]), self.lib)
+
+    def set_hmat_grids(self, dense_ctas=0, warp_ctas=0):
+        """H-matrix handles: CTAs of the dense-row and small-leaf kernels
+        (0: one per task; n: a persistent grid of n CTAs). Identical results."""
+        _lib.check(self.lib.dfn_set_hmat_grids(self.h, int(dense_ctas), int(warp_ctas)), self.lib)
 
     def set_cg_form(self, form):
         """CG pressure solves by "cta" (one CTA per system, global memory),
@@ -217,6 +222,11 @@ class Simulation:
     def set_mlp(self, weights):
         w = np.ascontiguousarray(weights, dtype=np.float32)
         _lib.check(self.lib.dfn_set_mlp(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self.lib)
+
+    def set_mlp_gate(self, rel):
+        """Evaluate the learned guess only where the analytic start's
+        relative residual exceeds rel (dfn_set_mlp_gate)."""
+        _lib.check(self.lib.dfn_set_mlp_gate(self.h, float(rel)), self.lib)
 
     def record(self, capacity):
         _lib.check(self.lib.dfn_record(self.h, int(capacity)), self.lib)

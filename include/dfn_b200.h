@@ -195,6 +195,7 @@ typedef struct dfn_report {
     int64_t newton_solves;     /* element Newton solves (Newton formulation) */
     int64_t newton_iters;      /* Newton iterations summed over the solves */
     int64_t newton_fail;       /* solves that hit the iteration cap */
+    int64_t mlp_warps;         /* warps (32 elements) that evaluated the learned guess */
 } dfn_report;
 
 typedef struct dfn_handle dfn_handle;
@@ -235,6 +236,9 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * form kept, cg_cluster_ctas = CTAs per cluster of this handle's cluster
  * form (2 to 16; 0 when it has none). The forms differ in the order of the
  * dot-product sums (equal to rounding).
+ * H-matrix handles: the K.V with the dense-row and small-leaf kernels on one
+ * CTA per task or on persistent grids of 4 or 8 CTAs per SM (identical
+ * results); ms[0] the fastest combination, ms[1] one CTA per task.
  * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
  * the short segments use tiles once a launch has at least 16384 of them,
  * and the CG uses clusters when all of a launch's clusters fit on the GPU at
@@ -245,6 +249,8 @@ typedef struct dfn_tuning {
     double ms[6];
     int32_t cg_cluster;
     int32_t cg_cluster_ctas;
+    int64_t hm_dense_grid;    /* H-matrix handles: CTAs of the dense-row kernel kept (0: one per task) */
+    int64_t hm_warp_grid;     /* and of the small-leaf kernel (0: one per four leaves) */
 } dfn_tuning;
 int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t);
 
@@ -286,6 +292,12 @@ int32_t dfn_set_hmat_small_leaves(dfn_handle *h, int32_t form);
  * thread per segment in tiles staged through shared memory (identical to 1).
  * dfn_autotune sets the fastest. No counterpart in the reference. */
 int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape);
+/* H-matrix handles: CTAs of the dense-row kernel and of the small-leaf
+ * kernel (one warp per leaf); 0 = one CTA per task (per four leaves), n > 0
+ * = a grid of n CTAs looping over the tasks (leaves). Same arithmetic per
+ * row, identical results. dfn_autotune sets the fastest. No counterpart in
+ * the reference. */
+int32_t dfn_set_hmat_grids(dfn_handle *h, int64_t dense_ctas, int64_t warp_ctas);
 /* A batch of independent networks in one handle (no counterpart in the
  * reference, which runs one network per process). All networks share the
  * fracture mode and the options; each keeps its own state, step size,
@@ -423,6 +435,13 @@ int32_t dfn_compute_P_noalloc(int64_t nb_element, double dt, double time, const 
 /* Sets the MLP weights (DFN_MLP_PARAMS floats, host memory) used by
  * DFN_GUESS_MLP. */
 int32_t dfn_set_mlp(dfn_handle *h, const float *weights);
+/* The gate of the learned guess: a warp evaluates the network only when one
+ * of its elements' analytic start leaves a residual above rel * (|tau| +
+ * sigma_eff a |w|) (default 1e-1: Newton from such a start takes four or
+ * more iterations; closer starts converge in a few, which an FP16 network's
+ * guess cannot beat); the warp then offers the guess to every element whose
+ * start misses the tolerance. 0 evaluates it wherever a start misses. */
+int32_t dfn_set_mlp_gate(dfn_handle *h, double rel);
 /* Records converged Newton solves: for every solve, the 6 MLP inputs and the
  * training target (w* - wa)/10, FP32, in a device buffer of `capacity`
  * samples (capacity 0 stops recording). dfn_record_read copies up to `max`

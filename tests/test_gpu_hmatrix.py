@@ -68,6 +68,32 @@ def test_hmat_small_leaves_by_warp_or_cta(storage):
         assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), warp))
 
 
+@pytest.mark.parametrize("storage", ["fp64", "fp32"])
+def test_hmat_persistent_grids_are_bitwise(storage):
+    """The dense-row and small-leaf kernels on persistent grids (a few CTAs
+    looping over the tasks) do each row's arithmetic as with one CTA per
+    task: K.V and a few solve steps are bitwise identical, and the
+    autotuner's pick keeps them so."""
+    p = hnet("modeII", seed=4, n=60, box=2000.0)
+    kw = dict(storage=storage, pressure="tridiag", hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6)
+    with Simulation(p, **kw) as s:
+        v = np.random.default_rng(5).normal(size=s.N) * 1e-9
+        base = s.kernel(v)
+        for dense, warp in ((148, 296), (1, 1), (37, 5)):
+            s.set_hmat_grids(dense, warp)
+            assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base)), (dense, warp)
+        s.set_hmat_grids(0, 0)
+        s.solve_steps(6)
+        ref = s.state()
+    with Simulation(p, **kw) as s:
+        tune = s.autotune()
+        assert "hm_dense_grid" in tune
+        assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base))
+        s.solve_steps(6)
+        g = s.state()
+    assert np.array_equal(g["Y"], ref["Y"]) and g["time"] == ref["time"]
+
+
 def test_hmat_reference_defaults_on_shipped_bp6():
     """The reference's own BP6 input uses static_kernel = hmatrix with its
     defaults (nleaf 100, eta 3, eps 1e-8)."""
