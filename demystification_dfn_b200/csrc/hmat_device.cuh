@@ -271,6 +271,7 @@ struct HLeafW {
     int64_t aoff;     // A^T offset (values); B^T follows at aoff + rank * lda
     int64_t xoff;     // first column of the leaf in xp
     int64_t outoff;   // first output slot of the leaf's rows
+    int64_t zoff;     // its z in the partial-sum array (row-tile form)
     int inst, rank, lda, ld, nr, blk;
 };
 
@@ -353,6 +354,133 @@ __global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *_
         if (!takes_part(ctl, d.inst, mask)) continue;   // warp-uniform; the kernel has no block barrier
         hm_lowrank_warp_leaf<T>(d, vals, xp, out, zs[warp]);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Row-tile form of the K.V (no per-leaf output slots, no gather):
+//   Z. z_b = B_b^T xp of every low-rank leaf: the small ones one warp each
+//      (hm_z_warp_kernel), the others in column chunks (hm_lowrank_kernel),
+//      partial sums per chunk;
+//   R. one CTA per row tile, a leaf cluster of the cluster tree (at most
+//      nleaf rows) of one network and component: every block whose row
+//      cluster contains the tile adds its rows' part, F xp for a dense leaf
+//      and A z for a low-rank one, in block order, and the tile's rows go
+//      straight to the K.V partial sums in element order.
+// The block partition is built from pairs of clusters, so a leaf cluster
+// lies inside the row cluster of every block it meets: the tiles split each
+// block's rows, and every stored value is read once per K.V.
+struct HTile {
+    int inst, comp, p0, nr;   // network, component, first position (cluster order), rows
+    int64_t b0, b1;           // its blocks: tile_blk[b0 .. b1), in block order
+};
+
+// z of the small low-rank leaves, one warp each (CTA c: leaves 4c + w,
+// 4c + w + 4 gridDim.x, ...): lanes in groups of the B^T row's vector
+// count, several rank rows per pass, as hm_lowrank_warp_kernel's first half.
+template <typename T>
+__global__ void __launch_bounds__(128, 8) hm_z_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+                                                            const StepCtl *__restrict__ ctl, int mask,
+                                                            const T *__restrict__ vals, const double *__restrict__ xp,
+                                                            double *__restrict__ zpart)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t k = (int64_t)blockIdx.x * 4 + warp; k < n; k += (int64_t)gridDim.x * 4) {
+        const HLeafW d = leaves[k];
+        if (!takes_part(ctl, d.inst, mask)) continue;   // warp-uniform; no block barrier
+        const int rank = d.rank, nv = d.ld / W;
+        int g = 1;
+        while (g < nv && g < 32) g <<= 1;
+        const int sub = lane / g, v0 = lane % g, rp = 32 / g;
+        double xv[HM_WARP_XV][W];
+#pragma unroll
+        for (int m = 0; m < HM_WARP_XV; m++) {
+            const int v = v0 + m * g;
+#pragma unroll
+            for (int c = 0; c < W; c++) xv[m][c] = (v < nv) ? __ldg(xp + d.xoff + v * W + c) : 0.0;
+        }
+        const VT *Bt = reinterpret_cast<const VT *>(vals + d.aoff + (int64_t)rank * d.lda);
+#pragma unroll 4
+        for (int q0 = 0; q0 < rank; q0 += rp) {
+            const int q = q0 + sub;
+            double acc = 0.0;
+            if (q < rank) {
+#pragma unroll
+                for (int m = 0; m < HM_WARP_XV; m++) {
+                    const int v = v0 + m * g;
+                    if (v < nv) {
+                        double f[W];
+                        HVec<T>::unpack(Bt[(int64_t)q * nv + v], f);
+#pragma unroll
+                        for (int c = 0; c < W; c++) acc = fma(f[c], xv[m][c], acc);
+                    }
+                }
+            }
+            for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (v0 == 0 && q < rank) zpart[d.zoff + q] = acc;
+        }
+    }
+}
+
+// Rows of one tile: warp w takes tile rows 8w .. 8w+7, four lanes per row
+// (lane group g takes F vectors v = g, g+4, ... of a dense row, rank terms
+// q = g, g+4, ... of a low-rank one); the four partials are summed by two
+// shuffles in fixed order and added to the row's sum block after block.
+template <typename T>
+__global__ void __launch_bounds__(256) hm_tile_rows_kernel(const HTile *__restrict__ tiles,
+                                                           const int *__restrict__ tile_blk,
+                                                           const HBlk *__restrict__ blks,
+                                                           const Inst *__restrict__ inst,
+                                                           const StepCtl *__restrict__ ctl, int mask,
+                                                           const T *__restrict__ vals,
+                                                           const double *__restrict__ xp,
+                                                           const double *__restrict__ zpart,
+                                                           const int *__restrict__ perm, double *__restrict__ partT,
+                                                           double *__restrict__ partN)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    const HTile tl = tiles[blockIdx.x];
+    if (!takes_part(ctl, tl.inst, mask)) return;
+    const Inst &I = inst[tl.inst];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int row = warp * 8 + (lane >> 2), g = lane & 3;
+    if (warp * 8 >= tl.nr) return;   // warp-uniform: whole warps past the tile's rows
+    const bool active = row < tl.nr;
+    const double *x0 = xp + I.eoff;
+    double acc = 0.0;
+    for (int64_t k = tl.b0; k < tl.b1; k++) {
+        const HBlk b = blks[tile_blk[k]];
+        const int lr = tl.p0 - b.r0 + row;   // row within the block
+        double s = 0.0;
+        if (active) {
+            if (b.dense) {
+                const VT *F = reinterpret_cast<const VT *>(vals + b.foff + (int64_t)lr * b.ld);
+                const double *x = x0 + b.c0;
+                const int nv = (b.nc + W - 1) / W;
+                for (int v = g; v < nv; v += 4) {
+                    double f[W];
+                    HVec<T>::unpack(F[v], f);
+#pragma unroll
+                    for (int c = 0; c < W; c++) s = fma(f[c], x[v * W + c], s);
+                }
+            } else {
+                const T *At = vals + b.foff + lr;
+                const double *zp = zpart + b.zoff;
+                const int r = b.rank;
+                for (int q = g; q < r; q += 4) {
+                    double z = zp[q];
+                    for (int j = 1; j < b.ntask1; j++) z += zp[(int64_t)j * r + q];
+                    s = fma((double)At[(int64_t)q * b.lda], z, s);
+                }
+            }
+        }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        acc += s;
+    }
+    if (active && g == 0) (tl.comp == 0 ? partT : partN)[I.poff + perm[I.eoff + tl.p0 + row]] = acc;
 }
 
 // Rows of low-rank leaves: a 16-byte vector of A rows per thread (rows of a
