@@ -125,6 +125,9 @@ struct dfn_handle {
     // outside the error norm: committed, the attempt's 5th-order value, and
     // the partial stage sum C1 V1 + C3 V3 + C4 V4
     double *slip = nullptr, *slip_out = nullptr, *slip_acc = nullptr;
+    // permeability evolution (permeability_coupling = 1): k*, kmin, Snk
+    bool pcoup = false;
+    double *kstar = nullptr, *kmin = nullptr, *Snk = nullptr;
     int *err_flag = nullptr;
     int wait_polls = MBAR_POLLS;          // polls of the TMA K.V pipeline's bounded waits
     void *K = nullptr;
@@ -644,6 +647,25 @@ static int run_attempt(dfn_handle *h, int mask)
     return DFN_OK;
 }
 
+// Permeability coupling: the permeability and face values of the networks
+// in `mask` from their committed sigmaN and P (accepted_only: those whose
+// attempt of this round was accepted), then the tridiagonal row factors.
+static int perm_refresh(dfn_handle *h, int mask, int accepted_only)
+{
+    perm_update_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(elem_params(h), mask, accepted_only, h->Y,
+                                                                        h->P, h->kstar, h->kmin, h->Snk, h->perm,
+                                                                        h->permx);
+    h->launches++;
+    CKL();
+    if (h->tcoef) {
+        tri_coef_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(h->pg, h->inst, h->inst_of, h->Ntot,
+                                                                        h->tcoef);
+        h->launches++;
+        CKL();
+    }
+    return DFN_OK;
+}
+
 // One round of the solve() loop for every network of the batch.
 static int run_round(dfn_handle *h)
 {
@@ -651,6 +673,8 @@ static int run_round(dfn_handle *h)
     step_begin_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->inst, h->B, h->src_tb);
     h->launches++;
     CKL();
+    // coupled permeability of a new step: from sigmaN and P committed
+    if (h->pcoup) TRY(perm_refresh(h, M_NEW, 0));
     // CG probe at t_try (halving on non-convergence); its solution is the
     // pressure of the scaling RHS evaluated at dt = t_try (src/solver.f90:81-101).
     cudaStream_t side = pressure_beside(h, 1, h->B);
@@ -668,9 +692,20 @@ static int run_round(dfn_handle *h)
     TRY(run_attempt(h, M_ACTIVE));
     commit_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(
         elem_params(h), h->Y, h->yout, h->P, h->Pdot, h->Ptemp, h->Pdot_s,
-        h->form == DFN_FORM_NEWTON ? nullptr : h->slip, h->slip_out);
+        h->form == DFN_FORM_NEWTON ? nullptr : h->slip, h->slip_out, h->pcoup ? 0 : 1);
     h->launches++;
     CKL();
+    if (h->pcoup) {
+        // the reference's commit compute_P(t_did) sees the new sigmaN and the
+        // old P (src/solver.f90:174 after rkqs): its own solve, not the
+        // stage-5 one, then P committed where it converged
+        TRY(perm_refresh(h, M_ACTIVE, 1));
+        TRY(launch_pressure(h, M_ACTIVE, 3, 5, 1, 0.0, h->B));
+        commit_p_kernel<<<blocks_of(h->Ntot, 256), 256, 0, h->stream>>>(elem_params(h), h->P, h->Pdot, h->Ptemp,
+                                                                        h->Pdot_s);
+        h->launches++;
+        CKL();
+    }
     finish_kernel<<<bb, 128, 0, h->stream>>>(h->ctl, h->B, h->max_step);
     h->launches++;
     CKL();
@@ -1297,7 +1332,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->htile, h->htb, h->ht1z, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
+    void *ptrs[] = {h->kstar, h->kmin, h->Snk, h->htile, h->htb, h->ht1z, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
@@ -1350,6 +1385,18 @@ static int check_problem(const dfn_problem *p)
             g_err = "source fault/index out of range";
             return DFN_ERR_ARG;
         }
+    }
+    if (p->permeability_coupling != 0 && p->permeability_coupling != 1) {
+        g_err = "permeability_coupling must be 0 or 1";
+        return DFN_ERR_ARG;
+    }
+    if (p->permeability_coupling == 1) {
+        if (!p->kmin || !p->Snk) { g_err = "permeability_coupling = 1 needs kmin and Snk"; return DFN_ERR_ARG; }
+        for (int64_t k = 0; k < N; k++)
+            if (!(p->Snk[k] != 0.0) || !std::isfinite(p->Snk[k]) || !std::isfinite(p->kmin[k])) {
+                g_err = "permeability coupling: Snk must be finite and nonzero, kmin finite";
+                return DFN_ERR_ARG;
+            }
     }
     // the initial state must be finite (the reference would carry a NaN
     // into every right-hand side and reject every attempt)
@@ -1405,6 +1452,14 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     for (int i = 0; i < count; i++) {
         TRY(check_problem(&probs[i]));
         if (probs[i].fracture_mode != probs[0].fracture_mode) { g_err = "all networks of a batch need the same fracture_mode"; return DFN_ERR_ARG; }
+        if (probs[i].permeability_coupling != probs[0].permeability_coupling) {
+            g_err = "all networks of a batch need the same permeability_coupling";
+            return DFN_ERR_ARG;
+        }
+    }
+    if (probs[0].permeability_coupling == 1 && opt.formulation == DFN_FORM_NEWTON) {
+        g_err = "permeability coupling follows the state's sigmaN: the V formulation only";
+        return DFN_ERR_UNSUPPORTED;
     }
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
@@ -1599,6 +1654,21 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         CKC(cudaGetLastError());
     }
     HCOPY(h->inst_of, inst_of.data(), Nt);
+    h->pcoup = probs[0].permeability_coupling == 1;
+    if (h->pcoup) {
+        DALLOC(h->kstar, Nt); DALLOC(h->kmin, Nt); DALLOC(h->Snk, Nt);
+        for (int i = 0; i < count; i++) {
+            const Inst &I = h->hinst[i];
+            HCOPY(h->kmin + I.eoff, probs[i].kmin, I.N);
+            HCOPY(h->Snk + I.eoff, probs[i].Snk, I.N);
+        }
+        // k* from the state after the geometry's loading projection
+        // (src/initialisation.f90:256-261)
+        perm_init_kernel<<<blocks_of(Nt, 256), 256, 0, h->stream>>>(elem_params(h), h->Y, h->P, h->perm, h->kmin,
+                                                                   h->Snk, h->kstar);
+        h->launches++;
+        CKC(cudaGetLastError());
+    }
     CKC(cudaMalloc((void **)&h->mlp, kMlpImgBytes));
     CKC(cudaMemset(h->mlp, 0, kMlpImgBytes));
     DALLOC(h->rec_n, 1);
@@ -1807,6 +1877,12 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         std::vector<int64_t> xp;
         std::vector<XCon> xc;
         h->ncross = build_crossings(probs, count, h->hinst, xp, xc);
+        if (h->ncross > 0 && h->pcoup) {
+            g_err = "permeability coupling of networks with fault crossings is not supported (the crossing "
+                    "coefficients hold the permeabilities of set-up)";
+            dfn_destroy(h);
+            return DFN_ERR_UNSUPPORTED;
+        }
         if (h->ncross > 0) {
             if (h->pressure == DFN_PRESSURE_TRIDIAG) {
                 g_err = "the network has fault crossings, which couple pressure rows outside the three diagonals: "
@@ -2230,6 +2306,7 @@ int32_t dfn_compute_P(dfn_handle *h, double dt, double *P_temp, double *P_dot, i
     const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
     TRY(reset_status0(h));
+    if (h->pcoup) TRY(perm_refresh(h, M_ALL, 0));
     TRY(launch_pressure(h, M_ALL, 2, 0, 1, dt, 1));
     TRY(sync_ctl(h));
     int st = h->h_ctl[0].status;
@@ -2250,6 +2327,7 @@ int32_t dfn_friction_law(dfn_handle *h, double x, int64_t nv, const double *Y, d
     CK(cudaSetDevice(h->dev));
     TRY(reset_status0(h));
     CK(cudaMemcpyAsync(h->ytmp, Y, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, h->stream));
+    if (h->pcoup) TRY(perm_refresh(h, M_ALL, 0));
     TRY(launch_pressure(h, M_ALL, 2, 0, 1, x, 1));
     TRY(launch_gemv(h, M_ALL, h->ytmp, 3, true));
     TRY(launch_friction(h, 0, 0, M_ALL, N, x));
@@ -2277,6 +2355,7 @@ int32_t dfn_rkqs(dfn_handle *h, double *y, const double *dydx, int64_t nv, doubl
     c.x = *x; c.h = htry; c.eps = eps; c.accepted = 0; c.status = 0; c.phase = PH_RETRY; c.step_attempts = 0;
     c.max_attempts = h->max_attempts;
     TRY(put_ctl(h));
+    if (h->pcoup) TRY(perm_refresh(h, M_ALL, 0));
     for (;;) {
         TRY(run_attempt(h, M_ACTIVE));
         TRY(sync_ctl(h));

@@ -337,6 +337,13 @@ __device__ __forceinline__ bool takes_part(const StepCtl *ctl, int i, int mask)
     return (mask >> ctl[i].phase) & 1;
 }
 
+// Pressure solves: kind 3 (the commit solve of the permeability coupling,
+// dt = the step just accepted) only for networks whose attempt was accepted.
+__device__ __forceinline__ bool press_takes_part(const StepCtl *ctl, int i, int mask, int kind)
+{
+    return takes_part(ctl, i, mask) && !(kind == 3 && (!ctl[i].accepted || ctl[i].status != 0));
+}
+
 // K.V streaming kernel (direct 128-bit loads).
 //
 // Work unit (tile): one 4 KiB column chunk of one instance for a block of
@@ -748,10 +755,13 @@ struct PressSys {
     double dt_explicit;
 };
 
+// dt of a pressure system: 0 the probe (t_try), 1 a stage (x + c h),
+// 2 explicit, 3 the commit solve of the step just accepted (its hdid).
 __device__ __forceinline__ double sys_dt(const StepCtl *ctl, int kind, int sys, double dt_explicit)
 {
     if (kind == 0) return ctl->t_try;
     if (kind == 1) return add_(ctl->x, mul_(ck_a(sys + 1), ctl->h));
+    if (kind == 3) return ctl->hdid;
     return dt_explicit;
 }
 
@@ -1005,6 +1015,10 @@ __device__ void cg_system(const PressParams &p, StepCtl *ctl, int kind, int sys,
             if (kind == 1) {
                 atomicOr(&ctl->pfail_mask, 1 << sys);
                 atomicAdd((unsigned long long *)&ctl->stage_noconv, 1ull);
+            } else if (kind == 3) {
+                // the commit solve: P stays as it was (the reference's
+                // compute_P(t_did) returns early; its ier is not checked)
+                atomicOr(&ctl->pfail_mask, 1 << 6);
             } else {
                 if (kind == 0) ctl->probe_ier = 1;
                 atomicCAS(&ctl->status, 0, 1);
@@ -1068,7 +1082,7 @@ __global__ void __launch_bounds__(1024) pressure_cg_batch_kernel(PressGlobal g, 
     __shared__ double red[66];
     __shared__ long long iters;
     const int i = blockIdx.y;
-    if (!takes_part(ctl, i, mask)) return;
+    if (!press_takes_part(ctl, i, mask, kind)) return;
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + blockIdx.x;
@@ -1276,7 +1290,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 1)
     cgrp::cluster_group cl = cgrp::this_cluster();
     const int ncl = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const int i = blockIdx.y;
-    if (!takes_part(ctl, i, mask)) return;   // uniform over the cluster
+    if (!press_takes_part(ctl, i, mask, kind)) return;   // uniform over the cluster
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + (int)(blockIdx.x / ncl);
@@ -1336,6 +1350,8 @@ __global__ void __launch_bounds__(PCL_THREADS, 1)
             if (kind == 1) {
                 atomicOr(&c->pfail_mask, 1 << sys);
                 atomicAdd((unsigned long long *)&c->stage_noconv, 1ull);
+            } else if (kind == 3) {
+                atomicOr(&c->pfail_mask, 1 << 6);   // the commit solve: P stays (as cg_system)
             } else {
                 if (kind == 0) c->probe_ier = 1;
                 atomicCAS(&c->status, 0, 1);
@@ -1557,7 +1573,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_thread_kernel(PressGloba
     if (q >= nlist) return;
     const int sg = seg_list[q];
     const int i = seg_inst[sg];
-    if (!takes_part(ctl, i, mask)) return;
+    if (!press_takes_part(ctl, i, mask, kind)) return;
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + blockIdx.y;
@@ -1647,7 +1663,7 @@ __global__ void __launch_bounds__(128) pressure_tridiag_tile_kernel(PressGlobal 
     const int2 t = tiles[blockIdx.x];
     const int sg0 = seg_list[t.x];
     const int i = seg_inst[sg0];
-    if (!takes_part(ctl, i, mask)) return;   // one instance per tile
+    if (!press_takes_part(ctl, i, mask, kind)) return;   // one instance per tile
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + blockIdx.y;
@@ -1711,7 +1727,7 @@ __global__ void __launch_bounds__(256) pressure_tridiag_kernel(PressGlobal g, co
     if (q >= nlist) return;                      // whole warp
     const int sg = seg_list[q];
     const int i = seg_inst[sg];
-    if (!takes_part(ctl, i, mask)) return;       // whole warp
+    if (!press_takes_part(ctl, i, mask, kind)) return;       // whole warp
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + blockIdx.y;
@@ -1737,7 +1753,7 @@ __global__ void __launch_bounds__(TRI_NT, 1) pressure_tridiag_long_kernel(PressG
     __shared__ int sbad;
     const int sg = long_seg[blockIdx.x];
     const int i = seg_inst[sg];
-    if (!takes_part(ctl, i, mask)) return;       // uniform over the CTA
+    if (!press_takes_part(ctl, i, mask, kind)) return;       // uniform over the CTA
     const Inst I = inst[i];
     const PressParams p = press_params(g, I, i, ctl);
     const int sys = sys0 + blockIdx.y;
@@ -2211,6 +2227,66 @@ __global__ void set_h_kernel(StepCtl *ctl, int B)
     ctl[i].h = ctl[i].t_try;
 }
 
+// ---------------------------------------------------------------------------
+// Permeability evolution (permeability_coupling = 1). k* is fixed from the
+// initial state (src/initialisation.f90:256-261),
+//   k* = kmin + (k - kmin) exp(|sigmaN + P| / |Snk|),
+// and before every pressure solve the permeability and the face values
+// follow the committed sigmaN and P (src/fluid_diffusion.f90:68-70, 74-75):
+//   k = (k* - kmin) exp(-|sigmaN + P| / |Snk|) + kmin,
+//   k_x(face j) = 2 k(j-1) k(j) / (k(j-1) + k(j)),  j = 1 .. N-1.
+__device__ __forceinline__ double perm_coupled(double kstar, double kmin, double Snk, double sig, double P)
+{
+    return add_(mul_(kstar - kmin, exp(-(fabs(sig + P) / fabs(Snk)))), kmin);
+}
+
+__global__ void perm_init_kernel(ElemParams ep, const double *Y, const double *P, const double *perm,
+                                 const double *kmin, const double *Snk, double *kstar)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ep.Ntot) return;
+    const Inst &I = ep.inst[ep.inst_of[e]];
+    const double sig = Y[3 * I.eoff + 2 * I.N + (e - I.eoff)];
+    kstar[e] = add_(kmin[e], mul_(perm[e] - kmin[e], exp(fabs(sig + P[e]) / fabs(Snk[e]))));
+}
+
+// Networks in `mask` (with accepted_only, those whose attempt of this round
+// was accepted: the state is the new one, P still the old).
+__global__ void perm_update_kernel(ElemParams ep, int mask, int accepted_only, const double *Y, const double *P,
+                                   const double *kstar, const double *kmin, const double *Snk, double *perm,
+                                   double *permx)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ep.Ntot) return;
+    const int i = ep.inst_of[e];
+    if (!takes_part(ep.ctl, i, mask)) return;
+    if (accepted_only && (!ep.ctl[i].accepted || ep.ctl[i].status != 0)) return;
+    const Inst &I = ep.inst[i];
+    const int64_t N = I.N, k = e - I.eoff;
+    const double *sg = Y + 3 * I.eoff + 2 * N;
+    const double pk = perm_coupled(kstar[e], kmin[e], Snk[e], sg[k], P[e]);
+    perm[e] = pk;
+    if (k >= 1) {
+        const double pl = perm_coupled(kstar[e - 1], kmin[e - 1], Snk[e - 1], sg[k - 1], P[e - 1]);
+        permx[I.eoff + i + k] = __ddiv_rn(mul_(mul_(2.0, pl), pk), add_(pl, pk));
+    }
+}
+
+// The commit of the coupled pressure: P of the commit solve (system slot 5,
+// dt = hdid) where it converged.
+__global__ void commit_p_kernel(ElemParams ep, double *P, double *Pdot, const double *Ptemp, const double *Pdot_s)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ep.Ntot) return;
+    const int i = ep.inst_of[e];
+    const StepCtl &c = ep.ctl[i];
+    if (!takes_part(ep.ctl, i, M_ACTIVE) || !c.accepted || c.status != 0 || (c.pfail_mask & (1 << 6))) return;
+    const Inst &I = ep.inst[i];
+    const int64_t N = I.N, k = e - I.eoff;
+    P[e] = Ptemp[6 * I.eoff + 5 * N + k];
+    Pdot[e] = Pdot_s[6 * I.eoff + 5 * N + k];
+}
+
 // Accepted attempts: Y = yout, and the pressure commit compute_P(t_did),
 // which equals the stage-5 solve of the accepted attempt (dt = 0 + 1.0*h).
 // The whole state is committed before the stop rules look at it, as the
@@ -2218,7 +2294,8 @@ __global__ void set_h_kernel(StepCtl *ctl, int B)
 // 170-197): an extensional or non-finite component only raises a flag here,
 // which finish_kernel turns into the status after the time update.
 __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, double *P, double *Pdot,
-                              const double *Ptemp, const double *Pdot_s, double *slip, const double *slip_out)
+                              const double *Ptemp, const double *Pdot_s, double *slip, const double *slip_out,
+                              int commit_p)
 {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= ep.Ntot) return;
@@ -2239,7 +2316,7 @@ __global__ void commit_kernel(ElemParams ep, double *y, const double *yout, doub
     }
     if (bad) atomicOr(&ep.ctl[i].commit_bad, bad);
     if (slip) slip[e] = slip_out[e];
-    if (!(c.pfail_mask & (1 << 4))) {
+    if (commit_p && !(c.pfail_mask & (1 << 4))) {
         P[e] = Ptemp[6 * I.eoff + 4 * N + k];
         Pdot[e] = Pdot_s[6 * I.eoff + 4 * N + k];
     }

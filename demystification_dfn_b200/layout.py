@@ -64,6 +64,9 @@ class ProblemArrays:
     stride_time: int = 1
     freq_writing_file: int = 10
     simulation_name: str = "test"
+    permeability_coupling: int = 0
+    kmin: np.ndarray = None     # [N] (fake elements 0)
+    Snk: np.ndarray = None      # [N] (fake elements 1, the reader's preset)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -108,6 +111,8 @@ def build_arrays(problem) -> ProblemArrays:
                                      "normal_loading_dot", "shear_loading_dot", "permeability")}
     for k in ("a", "b", "Dc", "f0", "V0"):
         per[k][:] = 1.0
+    coupling = int(getattr(hp, "permeability_coupling", 0))
+    kmin, Snk = np.zeros(N), np.ones(N)   # src/configuration.f90:224-225 (Snk = 1 between faults)
     src = {"fault": [], "index": [], "Q": [], "tb": [], "te": []}
     for fi, f in enumerate(faults):
         n, s = int(f.nb_element), int(first[fi])
@@ -117,6 +122,9 @@ def build_arrays(problem) -> ProblemArrays:
         node[s:s + n + 1, :] = nd.T
         for k in per:
             per[k][s:s + n] = _arr(getattr(f, k), n, f"fault {fi + 1} {k}")
+        if coupling:
+            kmin[s:s + n] = _arr(getattr(f, "kmin"), n, f"fault {fi + 1} kmin")
+            Snk[s:s + n] = _arr(getattr(f, "Snk"), n, f"fault {fi + 1} Snk")
         ns = int(f.nb_source)
         if ns >= 1:
             Q = _arr(f.Q, ns, "Q")
@@ -139,8 +147,8 @@ def build_arrays(problem) -> ProblemArrays:
     kern = KERNEL.get(hp.static_kernel)
     if kern is None:
         raise ValueError(f"unsupported static_kernel {hp.static_kernel!r}")
-    if int(getattr(hp, "permeability_coupling", 0)) != 0:
-        raise ValueError("permeability_coupling=1 is disabled in the reference and not supported")
+    if coupling not in (0, 1):
+        raise ValueError("permeability_coupling must be 0 or 1")
     return ProblemArrays(
         N=N, fault_nb_element=nfe, fracture_mode=mode, static_kernel=kern, node=node,
         mu=float(ml.mu), cp=float(ml.cp), cs=float(ml.cs),
@@ -154,7 +162,7 @@ def build_arrays(problem) -> ProblemArrays:
         src_t_end=np.array(src["te"], dtype=np.float64), tol_solver=float(hp.tol_solver),
         max_it=int(hp.max_it), stride_time=int(hp.stride_time),
         freq_writing_file=int(hp.freq_writing_file), simulation_name=str(hp.simulation_name),
-        **per)
+        permeability_coupling=coupling, kmin=kmin, Snk=Snk, **per)
 
 
 # ---------------------------------------------------------------------------
@@ -180,6 +188,7 @@ class DfnProblem(ctypes.Structure):
         ("src_Q", _dp), ("src_t_beg", _dp), ("src_t_end", _dp),
         ("tol_solver", ctypes.c_double), ("time0", ctypes.c_double),
         ("max_it", ctypes.c_int64), ("stride_time", ctypes.c_int64), ("freq_writing_file", ctypes.c_int64),
+        ("permeability_coupling", ctypes.c_int64), ("kmin", _dp), ("Snk", _dp),
     ]
 
 
@@ -244,6 +253,8 @@ def to_c(pa: ProblemArrays) -> DfnProblem:
         src_fault=i(pa.src_fault), src_index=i(pa.src_index), src_Q=dd(pa.src_Q),
         src_t_beg=dd(pa.src_t_beg), src_t_end=dd(pa.src_t_end), tol_solver=pa.tol_solver,
         time0=pa.time0, max_it=pa.max_it, stride_time=pa.stride_time,
-        freq_writing_file=pa.freq_writing_file)
+        freq_writing_file=pa.freq_writing_file, permeability_coupling=int(pa.permeability_coupling),
+        kmin=d(pa.kmin if pa.kmin is not None else np.zeros(pa.N)),
+        Snk=d(pa.Snk if pa.Snk is not None else np.ones(pa.N)))
     c._keep = keep
     return c

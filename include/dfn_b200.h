@@ -107,6 +107,16 @@ typedef struct dfn_problem {
     double tol_solver;
     double time0;
     int64_t max_it, stride_time, freq_writing_file;
+    /* Permeability evolution (hyperparameter/permeability_coupling = 1,
+     * src/fluid_diffusion.f90:68-70): before every pressure solve,
+     *   permeability = (k* - kmin) exp(-|sigmaN + P| / |Snk|) + kmin
+     * from the committed sigmaN and P, with k* = kmin + (k - kmin)
+     * exp(|sigmaN + P| / |Snk|) fixed from the initial state
+     * (src/initialisation.f90:256-261), and the face permeabilities follow.
+     * V formulation, networks without fault crossings. kmin and Snk may be
+     * NULL when the coupling is 0. */
+    int64_t permeability_coupling;
+    const double *kmin, *Snk;                  /* [N] */
 } dfn_problem;
 
 /* Options of this implementation (no counterpart in the reference). */

@@ -68,6 +68,9 @@ typedef struct orc {
     int form, nguess, nmaxit;
     double ntol, time0;
     double max_step; /* cap on t_try after a step (the reference's one day) */
+    /* permeability evolution (permeability_coupling = 1) */
+    int pcoup;
+    double *kstar, *kmin, *Snk;
     double *tau0;
     int64_t newton_solves, newton_iters, newton_fail;
 } orc;
@@ -271,7 +274,14 @@ orc *orc_create(const dfn_problem *p)
     o->time0 = p->time0;
     o->nmaxit = 50; o->ntol = 1e-13;
     o->max_step = 24 * 60 * 60;
+    o->pcoup = p->permeability_coupling == 1;
+    o->kstar = (double *)xcalloc(N, 8); o->kmin = (double *)xcalloc(N, 8); o->Snk = (double *)xcalloc(N, 8);
+    if (o->pcoup) { memcpy(o->kmin, p->kmin, 8 * N); memcpy(o->Snk, p->Snk, 8 * N); }
     orc_ini_value(o);
+    /* src/initialisation.f90:256-261, from the state after ini_value */
+    if (o->pcoup)
+        for (int64_t k = 0; k < N; k++)
+            o->kstar[k] = o->kmin[k] + (o->perm[k] - o->kmin[k]) * exp(fabs(o->Y[2 * N + k] + o->P[k]) / fabs(o->Snk[k]));
     orc_find_crossings(o);
     /* solve() entry: src/solver.f90:50-56 */
     o->time = p->time0; o->t_try = 100.0; o->it_count = 0;
@@ -286,7 +296,8 @@ void orc_destroy(orc *o)
     void *ptrs[] = {o->fault_n, o->fault_first, o->node, o->elem, o->ds, o->tan, o->nrm, o->a, o->b,
                     o->Dc, o->f0, o->V0, o->nload, o->sload, o->perm, o->permx, o->fake, o->src_fault,
                     o->src_index, o->src_Q, o->src_tb, o->src_te, o->Y, o->P, o->Pdot, o->SigmaT_dot,
-                    o->SigmaN_dot, o->KT, o->KN, o->xptr, o->xa, o->xb, o->xkl, o->xkr, o->slip, o->tau0};
+                    o->SigmaN_dot, o->KT, o->KN, o->xptr, o->xa, o->xb, o->xkl, o->xkr, o->slip, o->tau0,
+                    o->kstar, o->kmin, o->Snk};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     orc_hmat_free((struct orc_hmat *)o->hmat);
     free(o);
@@ -566,6 +577,19 @@ int orc_compute_P(orc *o, double dt, double *P_temp, double *P_dot)
     return orc_compute_P_mode(o, dt, P_temp, P_dot, 0);
 }
 
+/* permeability_coupling = 1: permeability from the committed sigmaN and P,
+ * and the face values (src/fluid_diffusion.f90:68-70, 74-75). The
+ * reference updates them after compute_diag, so its Jacobi scaling uses the
+ * previous call's faces; the scaling cancels from the solved system
+ * (M x / d = b / d), and here the diagonal follows the updated faces. */
+static void orc_perm_update(orc *o)
+{
+    int64_t N = o->N;
+    for (int64_t k = 0; k < N; k++)
+        o->perm[k] = (o->kstar[k] - o->kmin[k]) * exp(-(fabs(o->Y[2 * N + k] + o->P[k]) / fabs(o->Snk[k]))) + o->kmin[k];
+    for (int64_t k = 1; k < N; k++) o->permx[k] = 2.0 * o->perm[k - 1] * o->perm[k] / (o->perm[k - 1] + o->perm[k]);
+}
+
 static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, int stage)
 {
     int64_t N = o->N;
@@ -573,6 +597,7 @@ static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, 
     double *pk = w, *rk = w + N, *rk1 = w + 2 * N, *xk = w + 3 * N, *b1 = w + 4 * N, *diag = w + 5 * N,
            *Mp = w + 6 * N;
     int ier = 0;
+    if (o->pcoup) orc_perm_update(o);
     orc_diag(o, dt, diag);
     orc_rhs_b1(o, dt, diag, b1);
     /* permeability_coupling == 0: permeability_x is recomputed from the
@@ -630,9 +655,10 @@ static int orc_compute_P_mode(orc *o, double dt, double *P_temp, double *P_dot, 
  * tridiagonal solver. Not a reference routine. */
 /* Exact tridiagonal solve of the same implicit step (networks without
  * fault crossings: a crossing couples rows outside the three diagonals). */
-void orc_pressure_exact(const orc *o, double dt, double *P_temp)
+void orc_pressure_exact(orc *o, double dt, double *P_temp)
 {
     int64_t N = o->N;
+    if (o->pcoup) orc_perm_update(o);
     double *diag = (double *)malloc(8 * N), *b1 = (double *)malloc(8 * N);
     double *lo = (double *)malloc(8 * N), *di = (double *)malloc(8 * N), *up = (double *)malloc(8 * N);
     orc_diag(o, dt, diag);
@@ -1370,6 +1396,8 @@ void orc_get_geometry(const orc *o, double *elem, double *ds, double *tan, doubl
     if (nrm) memcpy(nrm, o->nrm, 16 * N);
     if (permx) memcpy(permx, o->permx, 8 * (N + 1));
 }
+/* Current permeability (the last solve's, with the coupling). */
+void orc_get_permeability(const orc *o, double *perm) { memcpy(perm, o->perm, 8 * o->N); }
 void orc_get_loads(const orc *o, double *nload, double *sload, unsigned char *fake)
 {
     if (nload) memcpy(nload, o->nload, 8 * o->N);

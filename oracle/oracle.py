@@ -62,6 +62,7 @@ def load():
         "orc_hmat_stats": (None, [V, ctypes.POINTER(i64)]),
         "orc_set_formulation": (cint, [V, cint, cint, cint, dbl]),
         "orc_set_max_step": (None, [V, dbl]),
+        "orc_get_permeability": (None, [V, dp]),
         "orc_velocity": (None, [V, dp]),
         "orc_get_slip": (None, [V, dp]),
         "orc_set_slip": (None, [V, dp]),
@@ -113,6 +114,12 @@ class Oracle:
     def set_max_step(self, seconds):
         """Cap on the trial step after each step (0: the reference's one day)."""
         self.lib.orc_set_max_step(self.o, float(seconds))
+
+    def permeability(self):
+        """Permeability of the last pressure solve (evolving with the coupling)."""
+        k = np.empty(self.N)
+        self.lib.orc_get_permeability(self.o, ptr(k))
+        return k
 
     def velocity(self):
         V = np.empty(self.N)

@@ -255,3 +255,46 @@ def test_formulation_gap_under_pressure_is_first_order_in_the_step():
     assert gaps[0] > 0.02
     for g1, g2 in zip(gaps, gaps[1:]):
         assert 1.8 <= g1 / g2 <= 2.2, gaps
+
+
+def coupled_fault(kmin=1e-16, Snk=20e6, n_el=500):
+    """One 5 km fault with 50 kg/s injection and permeability coupling
+    (permeability_coupling = 1): permeability grows as the pore pressure
+    lowers the effective normal stress."""
+    p = networks.single_fault(n_el=n_el, length=10.0 * n_el, mode="modeII", tol=1e-6, q_kgs=50.0)
+    p.hyperparameter.permeability_coupling = 1
+    for f in p.faults:
+        f.kmin[:] = kmin
+        f.Snk[:] = Snk
+    return p
+
+
+def test_permeability_coupling_follows_the_committed_state():
+    """k* = kmin + (k - kmin) exp(|sigmaN + P| / |Snk|) at the start
+    (src/initialisation.f90:256-261), then before every pressure solve
+    k = (k* - kmin) exp(-|sigmaN + P| / |Snk|) + kmin from the committed state
+    (src/fluid_diffusion.f90:68-70): the initial permeability is recovered,
+    and after some steps the permeability at the injection has grown."""
+    p = coupled_fault()
+    a = build_arrays(p)
+    o = Oracle(p)
+    o.use_dense()
+    o.compute_P(10.0)
+    assert np.allclose(o.permeability(), a.permeability, rtol=1e-14, atol=0.0)
+    st, _ = o.solve_steps(20)
+    assert st == 0
+    s = o.state()
+    N = o.N
+    o.compute_P(10.0)
+    kstar = a.kmin + (a.permeability - a.kmin) * np.exp(np.abs(a.sigmaN + a.P) / np.abs(a.Snk))
+    expect = (kstar - a.kmin) * np.exp(-np.abs(s["Y"][2 * N:] + s["P"]) / np.abs(a.Snk)) + a.kmin
+    k = o.permeability()
+    assert np.allclose(k, expect, rtol=1e-13, atol=0.0)
+    src = int(np.argmax(s["P"]))
+    assert k[src] > 1.05 * a.permeability[src]
+    # the coupled run differs from the uncoupled one
+    q = networks.single_fault(n_el=500, length=5000.0, mode="modeII", tol=1e-6, q_kgs=50.0)
+    o2 = Oracle(q)
+    o2.use_dense()
+    o2.solve_steps(20)
+    assert np.abs(o2.state()["P"] - s["P"]).max() > 1e-3 * np.abs(s["P"]).max()
