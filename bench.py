@@ -54,12 +54,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) per K.V launch of the headline workload from ncu:
+# FP64 storage, the 800-fault network, scaled by matrix bytes from the
+# capture of the N = 4 395 case (profiles/kv_gemv_tma_fp64_network800.md)
+TRAFFIC = {"fp64": 4194000000}
+
+
 def traffic_per_launch(storage):
-    p = os.path.join(ROOT, "profiles", "kv_traffic.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get(storage)
-    return None
+    return TRAFFIC.get(storage)
 
 
 class Clocks:

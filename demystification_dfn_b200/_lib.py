@@ -96,7 +96,6 @@ def load():
         "dfn_crossing_count": (i64, [P]),
         "dfn_set_tri_shape": (i32, [P, i32]),
         "dfn_set_hmat_grids": (i32, [P, i64, i64]),
-        "dfn_set_hmat_form": (i32, [P, i32]),
         "dfn_autotune": (i32, [P, ctypes.c_void_p]),
         "dfn_kernel_batch": (i32, [P, dp, dp, dp]),
         "dfn_velocity": (i32, [P, dp]),
@@ -146,8 +145,8 @@ def autotune(lib, h, storage, pressure, hmat=False):
         names = ("tc_persistent", "tc_ring_deep", "tc_ring_2stage")
         ms = {"kv_tc_persistent": t.ms[0], "kv_tc_ring_deep": t.ms[1], "kv_tc_ring_2stage": t.ms[4]}
     elif hmat:
-        names = ("hmat_slots", "hmat_row_tiles")
-        ms = {"kv_hmat_best": t.ms[0], "kv_hmat_slots_one_cta_per_task": t.ms[1], "kv_hmat_row_tiles": t.ms[4]}
+        names = ("tma", "ldg")
+        ms = {"kv_hmat_best": t.ms[0], "kv_hmat_one_cta_per_task": t.ms[1]}
         extra = {"hm_dense_grid": int(t.hm_dense_grid), "hm_warp_grid": int(t.hm_warp_grid)}
     else:
         names = ("tma", "ldg")

@@ -174,12 +174,6 @@ struct dfn_handle {
     int *hl5 = nullptr;                                // their blocks (one CTA each when small_form = 1)
     HLeafW *hlw = nullptr;                             // their descriptors (one warp each)
     int small_form = 0;                                // small leaves: 0 one warp each, 1 one CTA each
-    int hm_form = 0;                                   // K.V form: 0 leaf slots + gather, 1 row tiles
-    HTile *htile = nullptr;                            // row tiles (row-tile form)
-    int *htb = nullptr;                                // their block lists
-    int64_t nht = 0, nht0 = 0;
-    HTask *ht1z = nullptr;                             // column chunks of the low-rank leaves not done by a warp
-    int64_t n1z = 0, n1z0 = 0;
     int64_t hm_dense_grid = 0, hm_warp_grid = 0;       // CTAs of the dense-row and small-leaf kernels (0: one
                                                        // per task / per four leaves; else a persistent grid)
     void *hvals = nullptr;
@@ -250,45 +244,7 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
                                                                  Vbase, vmul, h->hxp);
     h->launches++;
     CKL();
-    if (h->hm_form == 1) {
-        // row-tile form: z of every low-rank leaf, then the tiles' rows
-        const int64_t nz = only0 ? h->n1z0 : h->n1z, nt = only0 ? h->nht0 : h->nht;
-        if (n5 > 0) {
-            const int64_t gfull = (n5 + 3) / 4;
-            const unsigned g = (unsigned)((h->hm_warp_grid > 0 && h->hm_warp_grid < gfull) ? h->hm_warp_grid : gfull);
-            if (h->store == 0)
-                hm_z_warp_kernel<double><<<g, 128, 0, h->stream>>>(h->hlw, n5, h->ctl, mask, (const double *)h->hvals,
-                                                                   h->hxp, h->hz);
-            else
-                hm_z_warp_kernel<float><<<g, 128, 0, h->stream>>>(h->hlw, n5, h->ctl, mask, (const float *)h->hvals,
-                                                                  h->hxp, h->hz);
-            h->launches++;
-            CKL();
-        }
-        if (nz > 0) {
-            if (h->store == 0)
-                hm_lowrank_kernel<double><<<(unsigned)nz, 256, 0, h->stream>>>(
-                    h->ht1z, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hz);
-            else
-                hm_lowrank_kernel<float><<<(unsigned)nz, 256, 0, h->stream>>>(
-                    h->ht1z, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hz);
-            h->launches++;
-            CKL();
-        }
-        if (nt > 0) {
-            if (h->store == 0)
-                hm_tile_rows_kernel<double><<<(unsigned)nt, 256, 0, h->stream>>>(
-                    h->htile, h->htb, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hz,
-                    h->hperm, h->partT, h->partN);
-            else
-                hm_tile_rows_kernel<float><<<(unsigned)nt, 256, 0, h->stream>>>(
-                    h->htile, h->htb, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hz,
-                    h->hperm, h->partT, h->partN);
-            h->launches++;
-            CKL();
-        }
-        return DFN_OK;
-    }
+
     // the low-rank leaves (latency-bound; the rows of the wide ones after
     // their z partials) on the side stream, issued first, beside the dense
     // rows (bandwidth-bound) on the handle's stream
@@ -309,13 +265,22 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         CKL();
     } else if (n5 > 0) {
         const int64_t gfull = (n5 + 3) / 4;
-        const unsigned g = (unsigned)((h->hm_warp_grid > 0 && h->hm_warp_grid < gfull) ? h->hm_warp_grid : gfull);
-        if (h->store == 0)
-            hm_lowrank_warp_kernel<double><<<g, 128, 0, ls>>>(h->hlw, n5, h->ctl, mask, (const double *)h->hvals,
-                                                              h->hxp, h->hout);
-        else
-            hm_lowrank_warp_kernel<float><<<g, 128, 0, ls>>>(h->hlw, n5, h->ctl, mask, (const float *)h->hvals,
-                                                             h->hxp, h->hout);
+        if (h->hm_warp_grid > 0 && h->hm_warp_grid < gfull) {
+            const unsigned g = (unsigned)h->hm_warp_grid;
+            if (h->store == 0)
+                hm_lowrank_warp_persistent_kernel<double><<<g, 128, 0, ls>>>(
+                    h->hlw, n5, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+            else
+                hm_lowrank_warp_persistent_kernel<float><<<g, 128, 0, ls>>>(
+                    h->hlw, n5, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        } else {
+            if (h->store == 0)
+                hm_lowrank_warp_kernel<double><<<(unsigned)gfull, 128, 0, ls>>>(
+                    h->hlw, n5, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+            else
+                hm_lowrank_warp_kernel<float><<<(unsigned)gfull, 128, 0, ls>>>(
+                    h->hlw, n5, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        }
         h->launches++;
         CKL();
     }
@@ -350,13 +315,22 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         CKL();
     }
     if (n3 > 0) {
-        const unsigned g3 = (unsigned)((h->hm_dense_grid > 0 && h->hm_dense_grid < n3) ? h->hm_dense_grid : n3);
-        if (h->store == 0)
-            hm_dense_kernel<double><<<g3, 256, 0, h->stream>>>(h->ht3, n3, h->hblk, h->inst, h->ctl, mask,
-                                                               (const double *)h->hvals, h->hxp, h->hout);
-        else
-            hm_dense_kernel<float><<<g3, 256, 0, h->stream>>>(h->ht3, n3, h->hblk, h->inst, h->ctl, mask,
-                                                              (const float *)h->hvals, h->hxp, h->hout);
+        if (h->hm_dense_grid > 0 && h->hm_dense_grid < n3) {
+            const unsigned g3 = (unsigned)h->hm_dense_grid;
+            if (h->store == 0)
+                hm_dense_persistent_kernel<double><<<g3, 256, 0, h->stream>>>(
+                    h->ht3, n3, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+            else
+                hm_dense_persistent_kernel<float><<<g3, 256, 0, h->stream>>>(
+                    h->ht3, n3, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        } else {
+            if (h->store == 0)
+                hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(
+                    h->ht3, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+            else
+                hm_dense_kernel<float><<<(unsigned)n3, 256, 0, h->stream>>>(
+                    h->ht3, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+        }
         h->launches++;
         CKL();
     }
@@ -1002,9 +976,6 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     std::vector<int> l4;
     std::vector<int> l5;     // small whole low-rank leaves (one warp each), and their descriptors
     std::vector<HLeafW> lw;
-    std::vector<HTask> t1z;  // row-tile form: column chunks of the low-rank leaves not done by a warp
-    std::vector<HTile> tiles;
-    std::vector<std::vector<int>> tile_blocks;
     int64_t dense_off = 0;   // values of the dense region (first in the device array)
     int64_t lr_off = 0;      // values of the low-rank region (after it)
     const size_t vsz = h->store == DFN_STORE_FP64 ? 8 : 4;
@@ -1025,19 +996,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
         CK(cudaMemcpy(dperm.p, tree.perm.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
         std::vector<hmat::Block> leaves;
         hmat::build_blocks(tree, hmat::boxes(tree, E), eta, 0, 0, leaves);
-        // row tiles: the leaf clusters in position order, per component
-        std::vector<std::pair<int, int>> lcl;
-        for (const hmat::Cluster &cl : tree.clus)
-            if (cl.son1 < 0) lcl.emplace_back(cl.first, cl.last - cl.first + 1);
-        std::sort(lcl.begin(), lcl.end());
-        std::vector<int> tile_at((size_t)N, -1);   // first position of a tile -> its index within the component
-        for (size_t t = 0; t < lcl.size(); t++) tile_at[(size_t)lcl[t].first] = (int)t;
         for (int c = 0; c < nc; c++) {
-            const size_t tbase = tiles.size();
-            for (const auto &pr : lcl) {
-                tiles.push_back(HTile{i, c, pr.first, pr.second, 0, 0});
-                tile_blocks.emplace_back();
-            }
             // admissible leaves: partial-pivot ACA and recompression on the
             // device (hm_aca_kernel), in batches whose scratch stays within
             // kAcaScratch; factors placed in leaf order into segments of the
@@ -1158,12 +1117,6 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 }
                 const int bi = (int)blks.size();
                 blks.push_back(hb);
-                // the tiles of the block's rows
-                for (int pos = L.r0; pos < L.r0 + L.nr;) {
-                    const int t = tile_at[(size_t)pos];
-                    tile_blocks[tbase + (size_t)t].push_back(bi);
-                    pos += lcl[(size_t)t].second;
-                }
                 if (H.dense) {
                     for (int r = 0; r < L.nr; r += HM_ROWS) t3.push_back(HTask{bi, r, std::min(HM_ROWS, L.nr - r), 0});
                 } else if (L.nc <= HM_COLS) {
@@ -1171,16 +1124,13 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                     if ((int64_t)H.rank * (hb.lda + hb.ld) * (int64_t)vsz <= HM_WARP_LEAF_BYTES &&
                         hb.ld / VW <= 32 * HM_WARP_XV) {
                         l5.push_back(bi);
-                        lw.push_back(HLeafW{hb.foff, e0 + L.c0, slot, hb.zoff, i, H.rank, hb.lda, hb.ld, L.nr, bi});
+                        lw.push_back(HLeafW{hb.foff, e0 + L.c0, slot, i, H.rank, hb.lda, hb.ld, L.nr, bi});
                     } else {
                         l4.push_back(bi);
-                        t1z.push_back(HTask{bi, 0, L.nc, 0});
                     }
                 } else {
-                    for (int j = 0; j < hb.ntask1; j++) {
+                    for (int j = 0; j < hb.ntask1; j++)
                         t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
-                        t1z.push_back(t1.back());
-                    }
                     for (int r = 0; r < L.nr; r += HM_LROWS) t2.push_back(HTask{bi, r, std::min(HM_LROWS, L.nr - r), 0});
                 }
                 for (int r = 0; r < L.nr; r++) rows[(size_t)c * Nt + e0 + L.r0 + r].push_back(slot + r);
@@ -1188,8 +1138,6 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
             }
         }
         if (i == 0) {
-            h->nht0 = (int64_t)tiles.size();
-            h->n1z0 = (int64_t)t1z.size();
             h->hn1_0 = (int64_t)t1.size();
             h->hn2_0 = (int64_t)t2.size();
             h->hn3_0 = (int64_t)t3.size();
@@ -1239,24 +1187,6 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     if (!t3.empty()) CK(cudaMemcpy(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
     CK(cudaMemcpy(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice));
-    // row tiles and their block lists (CSR), and the chunk tasks of the
-    // row-tile form
-    {
-        std::vector<int> tb;
-        for (size_t t = 0; t < tiles.size(); t++) {
-            tiles[t].b0 = (int64_t)tb.size();
-            tb.insert(tb.end(), tile_blocks[t].begin(), tile_blocks[t].end());
-            tiles[t].b1 = (int64_t)tb.size();
-        }
-        h->nht = (int64_t)tiles.size();
-        h->n1z = (int64_t)t1z.size();
-        CK(cudaMalloc((void **)&h->htile, std::max<size_t>(tiles.size(), 1) * sizeof(HTile)));
-        if (!tiles.empty()) CK(cudaMemcpy(h->htile, tiles.data(), tiles.size() * sizeof(HTile), cudaMemcpyHostToDevice));
-        CK(cudaMalloc((void **)&h->htb, std::max<size_t>(tb.size(), 1) * sizeof(int)));
-        if (!tb.empty()) CK(cudaMemcpy(h->htb, tb.data(), tb.size() * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMalloc((void **)&h->ht1z, std::max<size_t>(t1z.size(), 1) * sizeof(HTask)));
-        if (!t1z.empty()) CK(cudaMemcpy(h->ht1z, t1z.data(), t1z.size() * sizeof(HTask), cudaMemcpyHostToDevice));
-    }
     CK(cudaMalloc((void **)&h->hrowptr, sizeof(int64_t) * rowptr.size()));
     CK(cudaMemcpy(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
@@ -1332,7 +1262,7 @@ int32_t dfn_destroy(dfn_handle *h)
     if (!h) return DFN_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void *ptrs[] = {h->kstar, h->kmin, h->Snk, h->htile, h->htb, h->ht1z, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
+    void *ptrs[] = {h->kstar, h->kmin, h->Snk, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
                     h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
@@ -2031,35 +1961,25 @@ int32_t dfn_autotune(dfn_handle *h, dfn_tuning *t)
         (void)keep;
     }
     if (h->hmat) {
-        // the K.V form (leaf slots + gather, or row tiles), and the grids of
-        // the dense-row and small-leaf kernels: one CTA per task (0) or
-        // persistent grids of 4 or 8 CTAs per SM (identical results within
-        // a form; the forms sum each row in another order)
+        // grids of the dense-row and small-leaf kernels: one CTA per task
+        // (0) or persistent grids of 4 or 8 CTAs per SM; identical results
         const int64_t opts[3] = {0, 4 * (int64_t)h->sms, 8 * (int64_t)h->sms};
         double best = 1e300;
         int64_t bd = 0, bw = 0;
-        int bf = 0;
-        for (int form = 0; form < 2; form++) {
-            h->hm_form = form;
-            for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) {
-                    if (form == 1 && a > 0) continue;   // the row-tile form has no dense-row kernel
-                    h->hm_dense_grid = opts[a];
-                    h->hm_warp_grid = 2 * opts[b];
-                    double ms = 0.0;
-                    TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, ms));
-                    if (ms < best) { best = ms; bd = opts[a]; bw = 2 * opts[b]; bf = form; }
-                    if (form == 0 && a == 0 && b == 0) r.ms[1] = ms;
-                    if (form == 1 && b == 0) r.ms[4] = ms;
-                }
-        }
-        h->hm_form = bf;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                h->hm_dense_grid = opts[a];
+                h->hm_warp_grid = 2 * opts[b];
+                double ms = 0.0;
+                TRY(time_it([&]() { return launch_gemv(h, M_ALL, h->Y, 3, false); }, 5, ms));
+                if (ms < best) { best = ms; bd = opts[a]; bw = 2 * opts[b]; }
+                if (a == 0 && b == 0) r.ms[1] = ms;
+            }
         h->hm_dense_grid = bd;
         h->hm_warp_grid = bw;
         r.ms[0] = best;
         r.hm_dense_grid = bd;
         r.hm_warp_grid = bw;
-        r.gemv_impl = bf;
     }
     if (h->tc) {
         // persistent -> ms[0], unit per CTA with the deepest ring -> ms[1],
@@ -2145,17 +2065,6 @@ int32_t dfn_set_wait_limit(dfn_handle *h, int32_t polls)
 }
 
 int64_t dfn_crossing_count(const dfn_handle *h) { return h ? h->ncross : -1; }
-
-int32_t dfn_set_hmat_form(dfn_handle *h, int32_t form)
-{
-    if (!h || form < 0 || form > 1) return DFN_ERR_ARG;
-    if (!h->hmat) return DFN_ERR_UNSUPPORTED;
-    CK(cudaSetDevice(h->dev));
-    CK(cudaStreamSynchronize(h->stream));
-    h->hm_form = form;
-    drop_graph(h);
-    return DFN_OK;
-}
 
 int32_t dfn_set_hmat_grids(dfn_handle *h, int64_t dense_ctas, int64_t warp_ctas)
 {

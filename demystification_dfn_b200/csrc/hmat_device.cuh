@@ -116,6 +116,59 @@ __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict
     }
 }
 
+// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
+// xp; four rows per half-warp in flight (their loads issued together).
+template <typename T>
+__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
+                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
+                                                       int mask, const T *__restrict__ vals,
+                                                       const double *__restrict__ xp, double *__restrict__ out)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    constexpr int U = 4;
+    const HTask t = tasks[blockIdx.x];
+    const HBlk b = blks[t.blk];
+    if (!takes_part(ctl, b.inst, mask)) return;
+    const Inst &I = inst[b.inst];
+    const double *x = xp + I.eoff + b.c0;
+    const int hl = threadIdx.x & 15, w = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
+    const int nv = (b.nc + W - 1) / W;
+    const VT zero{};
+    // the loop runs the same trips in both half-warps (shuffles below)
+    for (int wb = w * 2 * U; wb < t.count; wb += 8 * 2 * U) {
+        const int i0 = wb + half * U;
+        double s[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) s[u] = 0.0;
+        for (int v = hl; v < nv; v += 16) {
+            double xv[W];
+#pragma unroll
+            for (int j = 0; j < W; j++) xv[j] = x[v * W + j];
+            VT fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int row = t.start + i0 + u;
+                fv[u] = (i0 + u < t.count) ? reinterpret_cast<const VT *>(vals + b.foff + (int64_t)row * b.ld)[v]
+                                           : zero;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                double a[W];
+                HVec<T>::unpack(fv[u], a);
+#pragma unroll
+                for (int j = 0; j < W; j++) s[u] = fma(a[j], xv[j], s[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+            if (hl == 0 && i0 + u < t.count) out[b.outoff + t.start + i0 + u] = s[u];
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restrict__ blks,
                                               const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl, int mask,
@@ -166,13 +219,11 @@ __device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restr
     }
 }
 
-// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
-// xp; four rows per half-warp in flight (their loads issued together). CTA
-// c takes tasks c, c + gridDim.x, ... (a grid of one CTA per task, or a
-// persistent grid: the leaves are a few KB each, so a CTA per task spends
-// much of its life starting up; the rows' arithmetic is the same either way).
+// The same rows on a persistent grid: CTA c takes tasks c, c + gridDim.x,
+// ... (the leaves are a few KB each, so a CTA per task spends much of its
+// life starting up; each row's arithmetic is that of hm_dense_kernel).
 template <typename T>
-__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
+__global__ void __launch_bounds__(256) hm_dense_persistent_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
                                                        const HBlk *__restrict__ blks,
                                                        const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                        int mask, const T *__restrict__ vals,
@@ -271,9 +322,78 @@ struct HLeafW {
     int64_t aoff;     // A^T offset (values); B^T follows at aoff + rank * lda
     int64_t xoff;     // first column of the leaf in xp
     int64_t outoff;   // first output slot of the leaf's rows
-    int64_t zoff;     // its z in the partial-sum array (row-tile form)
     int inst, rank, lda, ld, nr, blk;
 };
+
+template <typename T>
+__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+                                                                  const StepCtl *__restrict__ ctl, int mask,
+                                                                  const T *__restrict__ vals,
+                                                                  const double *__restrict__ xp,
+                                                                  double *__restrict__ out)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    __shared__ double zs[4][hmat::kMaxRank];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t k = (int64_t)blockIdx.x * 4 + warp;
+    if (k >= n) return;   // warp-uniform; the kernel has no block barrier
+    const HLeafW d = leaves[k];
+    if (!takes_part(ctl, d.inst, mask)) return;
+    const int rank = d.rank, nv = d.ld / W;
+    int g = 1;
+    while (g < nv && g < 32) g <<= 1;
+    const int sub = lane / g, v0 = lane % g, rp = 32 / g;
+    double xv[HM_WARP_XV][W];
+#pragma unroll
+    for (int m = 0; m < HM_WARP_XV; m++) {
+        const int v = v0 + m * g;
+#pragma unroll
+        for (int c = 0; c < W; c++) xv[m][c] = (v < nv) ? __ldg(xp + d.xoff + v * W + c) : 0.0;
+    }
+    const T *A = vals + d.aoff;
+    const VT *Bt = reinterpret_cast<const VT *>(A + (int64_t)rank * d.lda);
+    double *z = zs[warp];
+#pragma unroll 4
+    for (int q0 = 0; q0 < rank; q0 += rp) {
+        const int q = q0 + sub;
+        double acc = 0.0;
+        if (q < rank) {
+#pragma unroll
+            for (int m = 0; m < HM_WARP_XV; m++) {
+                const int v = v0 + m * g;
+                if (v < nv) {
+                    double f[W];
+                    HVec<T>::unpack(Bt[(int64_t)q * nv + v], f);
+#pragma unroll
+                    for (int c = 0; c < W; c++) acc = fma(f[c], xv[m][c], acc);
+                }
+            }
+        }
+        for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (v0 == 0 && q < rank) z[q] = acc;
+    }
+    __syncwarp();
+    const int nav = (d.nr + W - 1) / W;   // vectors of an A row (padding rows are zero)
+    const int avl = d.lda / W;
+    const VT *Av = reinterpret_cast<const VT *>(A);
+    for (int rv = lane; rv < nav; rv += 32) {
+        double acc[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) acc[c] = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < rank; q++) {
+            double a[W];
+            HVec<T>::unpack(Av[(int64_t)q * avl + rv], a);
+            const double zq = z[q];
+#pragma unroll
+            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < W; c++)
+            if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
+    }
+}
 
 template <typename T>
 __device__ __forceinline__ void hm_lowrank_warp_leaf(const HLeafW &d, const T *__restrict__ vals,
@@ -338,10 +458,11 @@ __device__ __forceinline__ void hm_lowrank_warp_leaf(const HLeafW &d, const T *_
     __syncwarp();   // z is rewritten by the warp's next leaf
 }
 
-// Warp w of CTA c takes leaves 4c + w, 4c + w + 4 gridDim.x, ... (one leaf
-// per warp with a grid covering the list, or a persistent grid).
+// The same leaves on a persistent grid: warp w of CTA c takes leaves
+// 4c + w, 4c + w + 4 gridDim.x, ... (each leaf's arithmetic is that of
+// hm_lowrank_warp_kernel).
 template <typename T>
-__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_persistent_kernel(const HLeafW *__restrict__ leaves, int64_t n,
                                                                   const StepCtl *__restrict__ ctl, int mask,
                                                                   const T *__restrict__ vals,
                                                                   const double *__restrict__ xp,
@@ -354,133 +475,6 @@ __global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *_
         if (!takes_part(ctl, d.inst, mask)) continue;   // warp-uniform; the kernel has no block barrier
         hm_lowrank_warp_leaf<T>(d, vals, xp, out, zs[warp]);
     }
-}
-
-// ---------------------------------------------------------------------------
-// Row-tile form of the K.V (no per-leaf output slots, no gather):
-//   Z. z_b = B_b^T xp of every low-rank leaf: the small ones one warp each
-//      (hm_z_warp_kernel), the others in column chunks (hm_lowrank_kernel),
-//      partial sums per chunk;
-//   R. one CTA per row tile, a leaf cluster of the cluster tree (at most
-//      nleaf rows) of one network and component: every block whose row
-//      cluster contains the tile adds its rows' part, F xp for a dense leaf
-//      and A z for a low-rank one, in block order, and the tile's rows go
-//      straight to the K.V partial sums in element order.
-// The block partition is built from pairs of clusters, so a leaf cluster
-// lies inside the row cluster of every block it meets: the tiles split each
-// block's rows, and every stored value is read once per K.V.
-struct HTile {
-    int inst, comp, p0, nr;   // network, component, first position (cluster order), rows
-    int64_t b0, b1;           // its blocks: tile_blk[b0 .. b1), in block order
-};
-
-// z of the small low-rank leaves, one warp each (CTA c: leaves 4c + w,
-// 4c + w + 4 gridDim.x, ...): lanes in groups of the B^T row's vector
-// count, several rank rows per pass, as hm_lowrank_warp_kernel's first half.
-template <typename T>
-__global__ void __launch_bounds__(128, 8) hm_z_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
-                                                            const StepCtl *__restrict__ ctl, int mask,
-                                                            const T *__restrict__ vals, const double *__restrict__ xp,
-                                                            double *__restrict__ zpart)
-{
-    using VT = typename HVec<T>::V;
-    constexpr int W = HVec<T>::W;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int64_t k = (int64_t)blockIdx.x * 4 + warp; k < n; k += (int64_t)gridDim.x * 4) {
-        const HLeafW d = leaves[k];
-        if (!takes_part(ctl, d.inst, mask)) continue;   // warp-uniform; no block barrier
-        const int rank = d.rank, nv = d.ld / W;
-        int g = 1;
-        while (g < nv && g < 32) g <<= 1;
-        const int sub = lane / g, v0 = lane % g, rp = 32 / g;
-        double xv[HM_WARP_XV][W];
-#pragma unroll
-        for (int m = 0; m < HM_WARP_XV; m++) {
-            const int v = v0 + m * g;
-#pragma unroll
-            for (int c = 0; c < W; c++) xv[m][c] = (v < nv) ? __ldg(xp + d.xoff + v * W + c) : 0.0;
-        }
-        const VT *Bt = reinterpret_cast<const VT *>(vals + d.aoff + (int64_t)rank * d.lda);
-#pragma unroll 4
-        for (int q0 = 0; q0 < rank; q0 += rp) {
-            const int q = q0 + sub;
-            double acc = 0.0;
-            if (q < rank) {
-#pragma unroll
-                for (int m = 0; m < HM_WARP_XV; m++) {
-                    const int v = v0 + m * g;
-                    if (v < nv) {
-                        double f[W];
-                        HVec<T>::unpack(Bt[(int64_t)q * nv + v], f);
-#pragma unroll
-                        for (int c = 0; c < W; c++) acc = fma(f[c], xv[m][c], acc);
-                    }
-                }
-            }
-            for (int o = g >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (v0 == 0 && q < rank) zpart[d.zoff + q] = acc;
-        }
-    }
-}
-
-// Rows of one tile: warp w takes tile rows 8w .. 8w+7, four lanes per row
-// (lane group g takes F vectors v = g, g+4, ... of a dense row, rank terms
-// q = g, g+4, ... of a low-rank one); the four partials are summed by two
-// shuffles in fixed order and added to the row's sum block after block.
-template <typename T>
-__global__ void __launch_bounds__(256) hm_tile_rows_kernel(const HTile *__restrict__ tiles,
-                                                           const int *__restrict__ tile_blk,
-                                                           const HBlk *__restrict__ blks,
-                                                           const Inst *__restrict__ inst,
-                                                           const StepCtl *__restrict__ ctl, int mask,
-                                                           const T *__restrict__ vals,
-                                                           const double *__restrict__ xp,
-                                                           const double *__restrict__ zpart,
-                                                           const int *__restrict__ perm, double *__restrict__ partT,
-                                                           double *__restrict__ partN)
-{
-    using VT = typename HVec<T>::V;
-    constexpr int W = HVec<T>::W;
-    const HTile tl = tiles[blockIdx.x];
-    if (!takes_part(ctl, tl.inst, mask)) return;
-    const Inst &I = inst[tl.inst];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row = warp * 8 + (lane >> 2), g = lane & 3;
-    if (warp * 8 >= tl.nr) return;   // warp-uniform: whole warps past the tile's rows
-    const bool active = row < tl.nr;
-    const double *x0 = xp + I.eoff;
-    double acc = 0.0;
-    for (int64_t k = tl.b0; k < tl.b1; k++) {
-        const HBlk b = blks[tile_blk[k]];
-        const int lr = tl.p0 - b.r0 + row;   // row within the block
-        double s = 0.0;
-        if (active) {
-            if (b.dense) {
-                const VT *F = reinterpret_cast<const VT *>(vals + b.foff + (int64_t)lr * b.ld);
-                const double *x = x0 + b.c0;
-                const int nv = (b.nc + W - 1) / W;
-                for (int v = g; v < nv; v += 4) {
-                    double f[W];
-                    HVec<T>::unpack(F[v], f);
-#pragma unroll
-                    for (int c = 0; c < W; c++) s = fma(f[c], x[v * W + c], s);
-                }
-            } else {
-                const T *At = vals + b.foff + lr;
-                const double *zp = zpart + b.zoff;
-                const int r = b.rank;
-                for (int q = g; q < r; q += 4) {
-                    double z = zp[q];
-                    for (int j = 1; j < b.ntask1; j++) z += zp[(int64_t)j * r + q];
-                    s = fma((double)At[(int64_t)q * b.lda], z, s);
-                }
-            }
-        }
-        s += __shfl_xor_sync(0xffffffffu, s, 1);
-        s += __shfl_xor_sync(0xffffffffu, s, 2);
-        acc += s;
-    }
-    if (active && g == 0) (tl.comp == 0 ? partT : partN)[I.poff + perm[I.eoff + tl.p0 + row]] = acc;
 }
 
 // Rows of low-rank leaves: a 16-byte vector of A rows per thread (rows of a

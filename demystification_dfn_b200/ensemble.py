@@ -75,10 +75,6 @@ class Ensemble:
         "warp" each (the default) or one "cta" each."""
         _lib.check(self.lib.dfn_set_hmat_small_leaves(self.h, {"warp": 0, "cta": 1}[form]), self.lib)
 
-    def set_hmat_form(self, form):
-        """H-matrix K.V by "slots" (default) or "row_tiles"."""
-        _lib.check(self.lib.dfn_set_hmat_form(self.h, {"slots": 0, "row_tiles": 1}[form]), self.lib)
-
     def set_cg_form(self, form):
         """CG pressure solves by "cta" (one CTA per system, global memory),
         "cluster" (a thread-block cluster per system, shared memory),

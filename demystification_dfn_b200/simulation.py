@@ -114,11 +114,6 @@ class Simulation:
         "warp" each (the default) or one "cta" each."""
         _lib.check(self.lib.dfn_set_hmat_small_leaves(self.h, {"warp": 0, "cta": 1}[form]), self.lib)
 
-    def set_hmat_form(self, form):
-        """H-matrix K.V by "slots" (default: per-leaf slots and a gather) or
-        "row_tiles"; agreement to rounding."""
-        _lib.check(self.lib.dfn_set_hmat_form(self.h, {"slots": 0, "row_tiles": 1}[form]), self.lib)
-
     def set_hmat_grids(self, dense_ctas=0, warp_ctas=0):
         """H-matrix handles: CTAs of the dense-row and small-leaf kernels
         (0: one per task; n: a persistent grid of n CTAs). Identical results."""

@@ -246,12 +246,9 @@ int32_t dfn_create(const dfn_problem *prob, const dfn_options *opt, dfn_handle *
  * form kept, cg_cluster_ctas = CTAs per cluster of this handle's cluster
  * form (2 to 16; 0 when it has none). The forms differ in the order of the
  * dot-product sums (equal to rounding).
- * H-matrix handles: the K.V form (gemv_impl 0: leaf slots and a row
- * gather; 1: row tiles) and the dense-row and small-leaf kernels on one CTA
- * per task or on persistent grids of 4 or 8 CTAs per SM (identical results
- * within a form; the forms sum each row in another order); ms[0] the
- * fastest combination, ms[1] the slot form with one CTA per task, ms[4] the
- * row-tile form with one warp per small leaf.
+ * H-matrix handles: the dense-row and small-leaf kernels on one CTA per
+ * task or on persistent grids of 4 or 8 CTAs per SM (identical results);
+ * ms[0] the fastest combination, ms[1] one CTA per task.
  * Without a call, K.V uses options.gemv_impl (0..2 for tensor-core handles),
  * the short segments use tiles once a launch has at least 16384 of them,
  * and the CG uses clusters when all of a launch's clusters fit on the GPU at
@@ -311,19 +308,6 @@ int32_t dfn_set_tri_shape(dfn_handle *h, int32_t shape);
  * row, identical results. dfn_autotune sets the fastest. No counterpart in
  * the reference. */
 int32_t dfn_set_hmat_grids(dfn_handle *h, int64_t dense_ctas, int64_t warp_ctas);
-/* H-matrix handles: the form of the K.V. 0 (the default) leaf slots: each
- * leaf writes its rows' part to its own slots (dense rows, low-rank leaves
- * by a warp, a CTA or in column chunks, beside each other on two streams),
- * then a gather sums each row's slots in fixed order. 1 row tiles: z = B^T x
- * of every low-rank leaf first, then one CTA per leaf cluster of the
- * cluster tree (at most nleaf rows) that adds every block's part of its
- * rows (F x or A z) in block order and writes them to the partial sums, no
- * slots (each warp walks all blocks of its tile, about 170 at N = 81 750,
- * which makes this form latency-bound there). The forms sum in another
- * order (agreement to rounding); dfn_autotune keeps the faster. No
- * counterpart in the reference (ZGEMV per leaf,
- * src/hmatrix/calculation_hmat.f90:3-165). */
-int32_t dfn_set_hmat_form(dfn_handle *h, int32_t form);
 /* A batch of independent networks in one handle (no counterpart in the
  * reference, which runs one network per process). All networks share the
  * fracture mode and the options; each keeps its own state, step size,

@@ -27,13 +27,11 @@ def hnet(mode="modeII", seed=3, n=40, box=1500.0, **kw):
 
 @pytest.mark.parametrize("mode", ["modeII", "modeIII"])
 @pytest.mark.parametrize("storage", ["fp64", "fp32"])
-@pytest.mark.parametrize("form", ["row_tiles", "slots"])
-def test_hmat_kv_against_dense_oracle(mode, storage, form):
+def test_hmat_kv_against_dense_oracle(mode, storage):
     p = hnet(mode)
     eps = 1e-6
     o = Oracle(p)
     with Simulation(p, storage=storage, hmat_leaf=32, hmat_eta=2.0, hmat_eps=eps) as s:
-        s.set_hmat_form(form)
         st = s.hmat_stats()
         assert st["lowrank_leaves"] > 0 and st["values"] < s.N * s.N * (2 if mode == "modeII" else 1)
         o.use_hmatrix(leaf=32, eta=2.0, eps=eps)
@@ -59,7 +57,6 @@ def test_hmat_small_leaves_by_warp_or_cta(storage):
     kw = dict(storage=storage, pressure="tridiag", hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6)
     with Simulation(p, **kw) as s:
         assert s.hmat_stats()["lowrank_leaves"] > 400
-        s.set_hmat_form("slots")
         v = np.random.default_rng(3).normal(size=s.N) * 1e-9
         warp = s.kernel(v)
         assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), warp))
@@ -73,35 +70,28 @@ def test_hmat_small_leaves_by_warp_or_cta(storage):
 
 @pytest.mark.parametrize("storage", ["fp64", "fp32"])
 def test_hmat_persistent_grids_are_bitwise(storage):
-    """In each K.V form (leaf slots + gather, row tiles), the dense-row and
-    small-leaf kernels on persistent grids (a few CTAs looping over the
-    tasks) do each row's arithmetic as with one CTA per task: K.V and a few
-    solve steps are bitwise identical, and the autotuner's pick keeps them
-    so. The two forms agree to rounding."""
+    """The dense-row and small-leaf kernels on persistent grids (a few CTAs
+    looping over the tasks) do each row's arithmetic as with one CTA per
+    task: K.V and a few solve steps are bitwise identical, and the
+    autotuner's pick keeps them so."""
     p = hnet("modeII", seed=4, n=60, box=2000.0)
     kw = dict(storage=storage, pressure="tridiag", hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6)
-    base, ref = {}, {}
-    for form in ("slots", "row_tiles"):
-        with Simulation(p, **kw) as s:
-            s.set_hmat_form(form)
-            v = np.random.default_rng(5).normal(size=s.N) * 1e-9
-            base[form] = s.kernel(v)
-            for dense, warp in ((148, 296), (1, 1), (37, 5)):
-                s.set_hmat_grids(dense, warp)
-                assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base[form])), (form, dense, warp)
-            s.set_hmat_grids(0, 0)
-            s.solve_steps(6)
-            ref[form] = s.state()
-    # the two forms sum each row in another order
-    for a, b in zip(base["slots"], base["row_tiles"]):
-        assert rel(a, b) < 1e-12
+    with Simulation(p, **kw) as s:
+        v = np.random.default_rng(5).normal(size=s.N) * 1e-9
+        base = s.kernel(v)
+        for dense, warp in ((148, 296), (1, 1), (37, 5)):
+            s.set_hmat_grids(dense, warp)
+            assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base)), (dense, warp)
+        s.set_hmat_grids(0, 0)
+        s.solve_steps(6)
+        ref = s.state()
     with Simulation(p, **kw) as s:
         tune = s.autotune()
-        form = {"hmat_slots": "slots", "hmat_row_tiles": "row_tiles"}[tune["gemv_impl"]]
-        assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base[form]))
+        assert "hm_dense_grid" in tune
+        assert all(np.array_equal(a, b) for a, b in zip(s.kernel(v), base))
         s.solve_steps(6)
         g = s.state()
-    assert np.array_equal(g["Y"], ref[form]["Y"]) and g["time"] == ref[form]["time"]
+    assert np.array_equal(g["Y"], ref["Y"]) and g["time"] == ref["time"]
 
 
 def test_hmat_reference_defaults_on_shipped_bp6():
@@ -135,18 +125,15 @@ def test_hmat_run_close_to_dense_oracle():
         assert rel(g["Y"][:N], r["Y"][:N]) < 1e-6
 
 
-@pytest.mark.parametrize("form", ["row_tiles", "slots"])
-def test_hmat_batch_equals_single(form):
+def test_hmat_batch_equals_single():
     from demystification_dfn_b200.ensemble import Ensemble
 
     ps = [hnet("modeII", seed=s, n=12, box=700.0) for s in (7, 8)]
     kw = dict(hmat_leaf=32, hmat_eta=2.0, hmat_eps=1e-6, pressure="tridiag")
     with Ensemble(ps, **kw) as ens:
-        ens.set_hmat_form(form)
         ens.solve(n_steps=8)
         for i, p in enumerate(ps):
             with Simulation(p, **kw) as s:
-                s.set_hmat_form(form)
                 s.solve_steps(8)
                 assert np.array_equal(ens.state(i)["Y"], s.state()["Y"])
 
