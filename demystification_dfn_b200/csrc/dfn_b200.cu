@@ -695,7 +695,7 @@ static int sync_ctl(dfn_handle *h)
     if (flag) {
         // reported once: the flag is cleared so that the handle can be
         // reused after the caller has restored its state
-        CK(cudaMemset(h->err_flag, 0, sizeof(int)));
+        CK(cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->stream));
         g_err = "a bounded wait of a K.V pipeline expired (its partial sums are incomplete)";
         return DFN_ERR_TIMEOUT;
     }
@@ -965,6 +965,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     const int B = h->B, nc = h->ncomp;
     const int64_t Nt = h->Ntot;
     std::vector<double> el(2 * Nt);   // midpoints: cluster tree and admissibility on the host
+    CK(cudaStreamSynchronize(h->stream));
     CK(cudaMemcpy(el.data(), h->elem, sizeof(double) * 2 * Nt, cudaMemcpyDeviceToHost));
 
     // values per 16-byte vector of the stored type; factor rows padded to it
@@ -993,7 +994,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
         hmat::Tree tree = hmat::build_tree(E, (int)N, leaf);
         for (int64_t p = 0; p < N; p++) perm[e0 + p] = tree.perm[p];
         TRY(dperm.reserve(sizeof(int) * (size_t)N));
-        CK(cudaMemcpy(dperm.p, tree.perm.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(dperm.p, tree.perm.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice, h->stream));
         std::vector<hmat::Block> leaves;
         hmat::build_blocks(tree, hmat::boxes(tree, E), eta, 0, 0, leaves);
         for (int c = 0; c < nc; c++) {
@@ -1171,26 +1172,26 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     CK(cudaStreamSynchronize(h->stream));
     segs.clear();
     CK(cudaMalloc((void **)&h->hblk, std::max<size_t>(blks.size(), 1) * sizeof(HBlk)));
-    CK(cudaMemcpy(h->hblk, blks.data(), blks.size() * sizeof(HBlk), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->hblk, blks.data(), blks.size() * sizeof(HBlk), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->ht1, std::max<size_t>(t1.size(), 1) * sizeof(HTask)));
-    if (!t1.empty()) CK(cudaMemcpy(h->ht1, t1.data(), t1.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    if (!t1.empty()) CK(cudaMemcpyAsync(h->ht1, t1.data(), t1.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->ht2, std::max<size_t>(t2.size(), 1) * sizeof(HTask)));
-    if (!t2.empty()) CK(cudaMemcpy(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    if (!t2.empty()) CK(cudaMemcpyAsync(h->ht2, t2.data(), t2.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hl4, std::max<size_t>(l4.size(), 1) * sizeof(int)));
-    if (!l4.empty()) CK(cudaMemcpy(h->hl4, l4.data(), l4.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!l4.empty()) CK(cudaMemcpyAsync(h->hl4, l4.data(), l4.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hl5, std::max<size_t>(l5.size(), 1) * sizeof(int)));
-    if (!l5.empty()) CK(cudaMemcpy(h->hl5, l5.data(), l5.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!l5.empty()) CK(cudaMemcpyAsync(h->hl5, l5.data(), l5.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     for (HLeafW &w : lw) w.aoff += dense_off;   // low-rank values follow the dense region
     CK(cudaMalloc((void **)&h->hlw, std::max<size_t>(lw.size(), 1) * sizeof(HLeafW)));
-    if (!lw.empty()) CK(cudaMemcpy(h->hlw, lw.data(), lw.size() * sizeof(HLeafW), cudaMemcpyHostToDevice));
+    if (!lw.empty()) CK(cudaMemcpyAsync(h->hlw, lw.data(), lw.size() * sizeof(HLeafW), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->ht3, std::max<size_t>(t3.size(), 1) * sizeof(HTask)));
-    if (!t3.empty()) CK(cudaMemcpy(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice));
+    if (!t3.empty()) CK(cudaMemcpyAsync(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
-    CK(cudaMemcpy(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hrowptr, sizeof(int64_t) * rowptr.size()));
-    CK(cudaMemcpy(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
-    CK(cudaMemcpy(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice, h->stream));
     if (!t3.empty()) {
         if (h->store == DFN_STORE_FP64)
             hm_fill_dense_kernel<double><<<(unsigned)t3.size(), 256, 0, h->stream>>>(
@@ -1206,7 +1207,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     }
     CK(cudaMalloc((void **)&h->hz, sizeof(double) * std::max<int64_t>(zoff, 1)));
     CK(cudaMalloc((void **)&h->hxp, sizeof(double) * (Nt + HM_XPAD)));
-    CK(cudaMemset(h->hxp, 0, sizeof(double) * (Nt + HM_XPAD)));
+    CK(cudaMemsetAsync(h->hxp, 0, sizeof(double) * (Nt + HM_XPAD), h->stream));
     CK(cudaMalloc((void **)&h->hout, sizeof(double) * std::max<int64_t>(slot, 1)));
     return DFN_OK;
 }
@@ -1352,7 +1353,7 @@ static int check_problem(const dfn_problem *p)
 #define HCOPY(dst, src, count)                                                                          \
     do {                                                                                                \
         if ((count) > 0) {                                                                              \
-            cudaError_t e_ = cudaMemcpy((dst), (src), sizeof(*(dst)) * (size_t)(count), cudaMemcpyHostToDevice); \
+            cudaError_t e_ = cudaMemcpyAsync((dst), (src), sizeof(*(dst)) * (size_t)(count), cudaMemcpyHostToDevice, h->stream); \
             if (e_ != cudaSuccess) {                                                                    \
                 set_err("cudaMemcpy " #dst, e_, __FILE__, __LINE__);                                    \
                 dfn_destroy(h);                                                                         \
@@ -1534,14 +1535,14 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
     DALLOC(h->vin, 3 * h->hinst[0].N); DALLOC(h->vout, 3 * h->hinst[0].N); DALLOC(h->snap, 5 * Nt);
     DALLOC(h->err_flag, 1); DALLOC(h->ctl, count);
     DALLOC(h->slip, Nt); DALLOC(h->slip_out, Nt); DALLOC(h->slip_acc, Nt);
-    CKC(cudaMemset(h->slip, 0, sizeof(double) * Nt));
+    CKC(cudaMemsetAsync(h->slip, 0, sizeof(double) * Nt, h->stream));
     DALLOC(h->src_fault, soff); DALLOC(h->src_elem, soff); DALLOC(h->src_Q, soff); DALLOC(h->src_tb, soff);
     DALLOC(h->src_te, soff);
-    CKC(cudaMemset(h->err_flag, 0, sizeof(int)));
-    CKC(cudaMemset(h->partN, 0, sizeof(double) * std::max<int64_t>(poff, 1)));
-    CKC(cudaMemset(h->Pdot, 0, sizeof(double) * Nt));
-    CKC(cudaMemset(h->SigT, 0, sizeof(double) * Nt));
-    CKC(cudaMemset(h->SigN, 0, sizeof(double) * Nt));
+    CKC(cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->stream));
+    CKC(cudaMemsetAsync(h->partN, 0, sizeof(double) * std::max<int64_t>(poff, 1), h->stream));
+    CKC(cudaMemsetAsync(h->Pdot, 0, sizeof(double) * Nt, h->stream));
+    CKC(cudaMemsetAsync(h->SigT, 0, sizeof(double) * Nt, h->stream));
+    CKC(cudaMemsetAsync(h->SigN, 0, sizeof(double) * Nt, h->stream));
     CKC(cudaMallocHost((void **)&h->h_ctl, sizeof(StepCtl) * count));
     HCOPY(h->inst, h->hinst.data(), count);
 
@@ -1600,12 +1601,12 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         CKC(cudaGetLastError());
     }
     CKC(cudaMalloc((void **)&h->mlp, kMlpImgBytes));
-    CKC(cudaMemset(h->mlp, 0, kMlpImgBytes));
+    CKC(cudaMemsetAsync(h->mlp, 0, kMlpImgBytes, h->stream));
     DALLOC(h->rec_n, 1);
-    CKC(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
+    CKC(cudaMemsetAsync(h->rec_n, 0, sizeof(unsigned long long), h->stream));
     if (h->form == DFN_FORM_NEWTON) {
         DALLOC(h->tau0, Nt); DALLOC(h->wlast, Nt); DALLOC(h->vnow, Nt);
-        CKC(cudaMemset(h->vnow, 0, sizeof(double) * Nt));
+        CKC(cudaMemsetAsync(h->vnow, 0, sizeof(double) * Nt, h->stream));
         HCOPY(h->fake, fake.data(), Nt);
         newton_init_kernel<<<blocks_of(Nt, 256), 256, 0, h->stream>>>(Nt, h->inst_of, h->inst, h->a, h->b, h->f0,
                                                                        h->V0, h->fake, h->P, h->Y, h->tau0,
@@ -1821,9 +1822,9 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
                 return DFN_ERR_ARG;
             }
             CKC(cudaMalloc((void **)&h->xptr, sizeof(int64_t) * xp.size()));
-            CKC(cudaMemcpy(h->xptr, xp.data(), sizeof(int64_t) * xp.size(), cudaMemcpyHostToDevice));
+            CKC(cudaMemcpyAsync(h->xptr, xp.data(), sizeof(int64_t) * xp.size(), cudaMemcpyHostToDevice, h->stream));
             CKC(cudaMalloc((void **)&h->xcon, sizeof(XCon) * std::max<size_t>(xc.size(), 1)));
-            if (!xc.empty()) CKC(cudaMemcpy(h->xcon, xc.data(), sizeof(XCon) * xc.size(), cudaMemcpyHostToDevice));
+            if (!xc.empty()) CKC(cudaMemcpyAsync(h->xcon, xc.data(), sizeof(XCon) * xc.size(), cudaMemcpyHostToDevice, h->stream));
             // per network, its rows that have crossings (network-local indices)
             std::vector<int64_t> rows, rptr(1, 0);
             for (int i = 0; i < count; i++) {
@@ -1833,9 +1834,9 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
                 rptr.push_back((int64_t)rows.size());
             }
             CKC(cudaMalloc((void **)&h->xrows, sizeof(int64_t) * std::max<size_t>(rows.size(), 1)));
-            if (!rows.empty()) CKC(cudaMemcpy(h->xrows, rows.data(), sizeof(int64_t) * rows.size(), cudaMemcpyHostToDevice));
+            if (!rows.empty()) CKC(cudaMemcpyAsync(h->xrows, rows.data(), sizeof(int64_t) * rows.size(), cudaMemcpyHostToDevice, h->stream));
             CKC(cudaMalloc((void **)&h->xrows_ptr, sizeof(int64_t) * rptr.size()));
-            CKC(cudaMemcpy(h->xrows_ptr, rptr.data(), sizeof(int64_t) * rptr.size(), cudaMemcpyHostToDevice));
+            CKC(cudaMemcpyAsync(h->xrows_ptr, rptr.data(), sizeof(int64_t) * rptr.size(), cudaMemcpyHostToDevice, h->stream));
             pg.xptr = h->xptr;
             pg.xcon = h->xcon;
             pg.xrows = h->xrows;
@@ -1911,7 +1912,7 @@ int32_t dfn_create_batch(const dfn_problem *probs, int32_t count, const dfn_opti
         c.time = probs[i].time0; c.t_try = 100.0; c.eps = probs[i].tol_solver; c.h = 100.0;
         c.phase = PH_DONE; c.max_attempts = h->max_attempts;
     }
-    CKC(cudaMemcpy(h->ctl, h->h_ctl, sizeof(StepCtl) * count, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(StepCtl) * count, cudaMemcpyHostToDevice, h->stream));
     CKC(cudaEventCreate(&h->ev0));
     CKC(cudaEventCreate(&h->ev1));
     CKC(cudaStreamSynchronize(h->stream));
@@ -2181,7 +2182,7 @@ int32_t dfn_kernel_batch(dfn_handle *h, const double *slip, double *sT, double *
     int flag = 0;
     CK(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
-        CK(cudaMemset(h->err_flag, 0, sizeof(int)));
+        CK(cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->stream));
         g_err = "a bounded wait of a K.V pipeline expired (its partial sums are incomplete)";
         return DFN_ERR_TIMEOUT;
     }
@@ -2556,7 +2557,7 @@ int32_t dfn_record(dfn_handle *h, int64_t capacity)
     if (h->rec_t) { cudaFree(h->rec_t); h->rec_t = nullptr; }
     h->rec_cap = 0;
     drop_graph(h);        // the friction launches carry the recording buffers
-    CK(cudaMemset(h->rec_n, 0, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(h->rec_n, 0, sizeof(unsigned long long), h->stream));
     if (capacity > 0) {
         CK(cudaMalloc((void **)&h->rec_x, sizeof(float) * MLP_IN * capacity));
         CK(cudaMalloc((void **)&h->rec_t, sizeof(float) * capacity));
@@ -2707,6 +2708,7 @@ int32_t dfn_velocity(dfn_handle *h, double *V)
     const int64_t N = h->hinst[0].N;
     CK(cudaSetDevice(h->dev));
     if (h->form != DFN_FORM_NEWTON) {
+        CK(cudaStreamSynchronize(h->stream));
         CK(cudaMemcpy(V, h->Y, sizeof(double) * N, cudaMemcpyDeviceToHost));
         return DFN_OK;
     }
