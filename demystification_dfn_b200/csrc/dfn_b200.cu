@@ -178,7 +178,8 @@ struct dfn_handle {
                                                        // per task / per four leaves; else a persistent grid)
     void *hvals = nullptr;
     int *hperm = nullptr;
-    int64_t *hrowptr = nullptr, *hslots = nullptr;
+    int32_t *hsegof = nullptr;            // row sums: segment of every (component, row)
+    int64_t *hsegptr = nullptr, *hsegbase = nullptr;   // a segment's slot bases
     double *hz = nullptr, *hout = nullptr, *hxp = nullptr;
     std::vector<int> hranks;              // rank of every low-rank leaf (report)
     int64_t hdense_vals = 0, hlr_vals = 0, hblocks = 0;
@@ -339,7 +340,8 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
         CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
     hm_gather_kernel<<<blocks_of(ne, 256), 256, 0, h->stream>>>(ne, h->ncomp, h->inst_of, h->inst, h->ctl, mask,
-                                                                h->hperm, h->hrowptr, h->hslots, h->hout, h->partT,
+                                                                h->hperm, h->hsegof, h->hsegptr, h->hsegbase, h->hout,
+                                                                h->partT,
                                                                 h->partN);
     h->launches++;
     CKL();
@@ -1147,12 +1149,24 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
         }
     }
     // tasks must list network 0 first for the operator entry points; they
-    // do, since networks are built in order. Row slot lists (CSR).
-    std::vector<int64_t> rowptr((size_t)nc * Nt + 1, 0), slots;
+    // do, since networks are built in order. Row sums: leaf b's result for
+    // the row at position e sits in slot base_b + e (base_b = its first slot
+    // minus its first row), so consecutive rows with the same blocks share
+    // one list of bases (a segment), in block order.
+    std::vector<int32_t> segof((size_t)nc * Nt);
+    std::vector<int64_t> segptr(1, 0), segbase;
     for (size_t q = 0; q < rows.size(); q++) {
-        rowptr[q + 1] = rowptr[q] + (int64_t)rows[q].size();
-        slots.insert(slots.end(), rows[q].begin(), rows[q].end());
+        const int64_t e = (int64_t)(q % (size_t)Nt);
+        bool same = e > 0 && rows[q].size() == rows[q - 1].size();
+        for (size_t k = 0; same && k < rows[q].size(); k++)
+            if (rows[q][k] - e != rows[q - 1][k] - (e - 1)) same = false;
+        if (!same) {
+            for (int64_t v : rows[q]) segbase.push_back(v - e);
+            segptr.push_back((int64_t)segbase.size());
+        }
+        segof[q] = (int32_t)(segptr.size() - 2);
     }
+    rows.clear();
     h->hn1 = (int64_t)t1.size();
     h->hn2 = (int64_t)t2.size();
     h->hn3 = (int64_t)t3.size();
@@ -1188,10 +1202,14 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     if (!t3.empty()) CK(cudaMemcpyAsync(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
     CK(cudaMemcpyAsync(h->hperm, perm.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMalloc((void **)&h->hrowptr, sizeof(int64_t) * rowptr.size()));
-    CK(cudaMemcpyAsync(h->hrowptr, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMalloc((void **)&h->hslots, sizeof(int64_t) * std::max<size_t>(slots.size(), 1)));
-    CK(cudaMemcpyAsync(h->hslots, slots.data(), sizeof(int64_t) * slots.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->hsegof, sizeof(int32_t) * segof.size()));
+    CK(cudaMemcpyAsync(h->hsegof, segof.data(), sizeof(int32_t) * segof.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->hsegptr, sizeof(int64_t) * segptr.size()));
+    CK(cudaMemcpyAsync(h->hsegptr, segptr.data(), sizeof(int64_t) * segptr.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->hsegbase, sizeof(int64_t) * std::max<size_t>(segbase.size(), 1)));
+    CK(cudaMemcpyAsync(h->hsegbase, segbase.data(), sizeof(int64_t) * segbase.size(), cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));   // the host vectors go out of scope
     if (!t3.empty()) {
         if (h->store == DFN_STORE_FP64)
             hm_fill_dense_kernel<double><<<(unsigned)t3.size(), 256, 0, h->stream>>>(
@@ -1264,7 +1282,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->kstar, h->kmin, h->Snk, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hrowptr, h->hslots, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hsegof, h->hsegptr, h->hsegbase, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,

@@ -949,13 +949,15 @@ __global__ void __launch_bounds__(256) hm_aca_place_kernel(const AcaLeaf *__rest
     }
 }
 
-// y(pos) = sum of the slots of row pos (fixed order), stored at the
+// y(pos) = sum of the slots of row pos (fixed order: the leaves of its
+// segment of rows in block order; a warp's rows mostly share a segment, so
+// the bases are broadcast and the slot reads coalesced), stored at the
 // original element index in the K.V result arrays (partials with one chunk).
 __global__ void hm_gather_kernel(int64_t Ntot, int ncomp, const int *__restrict__ inst_of,
                                  const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl, int mask,
-                                 const int *__restrict__ perm, const int64_t *__restrict__ rowptr,
-                                 const int64_t *__restrict__ slots, const double *__restrict__ out, double *partT,
-                                 double *partN)
+                                 const int *__restrict__ perm, const int32_t *__restrict__ segof,
+                                 const int64_t *__restrict__ segptr, const int64_t *__restrict__ segbase,
+                                 const double *__restrict__ out, double *partT, double *partN)
 {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= Ntot) return;
@@ -964,9 +966,9 @@ __global__ void hm_gather_kernel(int64_t Ntot, int ncomp, const int *__restrict_
     const Inst &I = inst[i];
     const int64_t orig = perm[e];   // perm[eoff + pos], a network-local index
     for (int c = 0; c < ncomp; c++) {
-        const int64_t q = (int64_t)c * Ntot + e;
+        const int sg = segof[(int64_t)c * Ntot + e];
         double s = 0.0;
-        for (int64_t j = rowptr[q]; j < rowptr[q + 1]; j++) s += out[slots[j]];
+        for (int64_t j = segptr[sg]; j < segptr[sg + 1]; j++) s += out[segbase[j] + e];
         (c == 0 ? partT : partN)[I.poff + orig] = s;
     }
 }
