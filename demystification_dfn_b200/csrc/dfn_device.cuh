@@ -1946,8 +1946,12 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double 
 // LEARNED: Newton formulation with the learned guess (a separate
 // instantiation keeps the tensor-core inference's registers out of the
 // other variants).
+// Without the learned guess the kernel is held to 64 registers (8 blocks of
+// 128 threads per SM, 136 bytes of spills to L1): it waits on memory, and
+// the extra warps raise the tensor-core round by 5-6 % over 5 blocks at 84
+// registers.
 template <bool LEARNED>
-__global__ void __launch_bounds__(128, 5) friction_kernel(FricParams f, int stage, int sys, int mask)
+__global__ void __launch_bounds__(128, LEARNED ? 5 : 8) friction_kernel(FricParams f, int stage, int sys, int mask)
 {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int myi = -1;
