@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict
 // Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
 // xp; four rows per half-warp in flight (their loads issued together).
 template <typename T>
-__global__ void __launch_bounds__(256) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
+__global__ void __launch_bounds__(256, 5) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
                                                        const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                        int mask, const T *__restrict__ vals,
                                                        const double *__restrict__ xp, double *__restrict__ out)
@@ -223,7 +223,7 @@ __device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restr
 // ... (the leaves are a few KB each, so a CTA per task spends much of its
 // life starting up; each row's arithmetic is that of hm_dense_kernel).
 template <typename T>
-__global__ void __launch_bounds__(256) hm_dense_persistent_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
+__global__ void __launch_bounds__(256, 5) hm_dense_persistent_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
                                                        const HBlk *__restrict__ blks,
                                                        const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
                                                        int mask, const T *__restrict__ vals,
@@ -314,7 +314,10 @@ __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__rest
 // output slots. Leaves qualify when their factors take at most
 // HM_WARP_LEAF_BYTES and their B^T rows at most 32 * HM_WARP_XV vectors.
 // These leaves are a few KB each and latency-bound: a SM holds the loads of
-// dozens of them in flight, against 8 with one CTA per leaf.
+// dozens of them in flight, against 8 with one CTA per leaf. The kernel is
+// held to 40 registers (12 CTAs of four warps per SM, a few spills to L1)
+// and the dense-row kernel to 48 (five CTAs of 256): K.V 0.840 -> 0.823 ms
+// at N = 81 750 (8 CTAs and 64 registers each before).
 constexpr int HM_WARP_LEAF_BYTES = 32 * 1024;
 constexpr int HM_WARP_XV = 2;
 
@@ -326,7 +329,7 @@ struct HLeafW {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+__global__ void __launch_bounds__(128, 12) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
                                                                   const StepCtl *__restrict__ ctl, int mask,
                                                                   const T *__restrict__ vals,
                                                                   const double *__restrict__ xp,
@@ -462,7 +465,7 @@ __device__ __forceinline__ void hm_lowrank_warp_leaf(const HLeafW &d, const T *_
 // 4c + w, 4c + w + 4 gridDim.x, ... (each leaf's arithmetic is that of
 // hm_lowrank_warp_kernel).
 template <typename T>
-__global__ void __launch_bounds__(128, 8) hm_lowrank_warp_persistent_kernel(const HLeafW *__restrict__ leaves, int64_t n,
+__global__ void __launch_bounds__(128, 12) hm_lowrank_warp_persistent_kernel(const HLeafW *__restrict__ leaves, int64_t n,
                                                                   const StepCtl *__restrict__ ctl, int mask,
                                                                   const T *__restrict__ vals,
                                                                   const double *__restrict__ xp,
