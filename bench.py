@@ -697,6 +697,10 @@ def run_case(argv):
         factors): three K.V launches (several kernels each); "tuned" runs the
         autotuner first, "grids D W" sets the CTAs of the dense-row and
         small-leaf kernels (dfn_set_hmat_grids).
+    python bench.py --case hmatrix_ensemble_kv [tuned]
+        the 64 networks of the north-star leg as H-matrices (leaf 64, eta 2,
+        ACA 1e-7, FP32 factors) in one batch: three K.V launches of the
+        batch; "tuned" runs the autotuner first (one JSON line).
     python bench.py --case s64_kv [R]
         R realisations (default 64) of the 800-fault network sharing one FP64
         kernel matrix: three K.V launches of the FP64 GEMM (4.1 GB per launch).
@@ -770,6 +774,16 @@ def run_case(argv):
         rng = np.random.default_rng(0)
         for _ in range(3):
             e.kernel(rng.normal(size=e.N))
+    elif case == "hmatrix_ensemble_kv":
+        import json
+
+        members = networks.ensemble(64, kernel="hmatrix")
+        e = Ensemble(members, storage="fp32", pressure="tridiag", hmat_leaf=64, hmat_eta=2.0, hmat_eps=1e-7)
+        if len(argv) > 1 and argv[1] == "tuned":
+            print(json.dumps({"kv_bytes": e.kernel_bytes, "tune": e.autotune()}))
+        rng = np.random.default_rng(0)
+        for _ in range(3):
+            e.kernel([rng.normal(size=n) for n in e.n_elements])
     elif case == "s64_kv":
         # R realisations of the 800-fault network, FP64 shared kernel matrix:
         # three K.V launches of the FP64 GEMM (4.1 GB of K per launch)

@@ -22,6 +22,7 @@
 #include <unordered_map>
 #include <array>
 #include <deque>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -167,7 +168,10 @@ struct dfn_handle {
     HTask *ht1 = nullptr, *ht2 = nullptr;
     int64_t hn1 = 0, hn2 = 0, hn1_0 = 0, hn2_0 = 0;   // low-rank column tasks, low-rank row tasks
     int64_t hn3 = 0, hn3_0 = 0;                        // dense row tasks
-    HTask *ht3 = nullptr;
+    HTask *ht3 = nullptr;                              // dense leaf rows (setup: filling the values)
+    HTask *htg = nullptr;                              // dense row tasks: (group, rows)
+    HDGroup *hdg = nullptr;                            // dense leaves sharing a row cluster
+    HDLeaf *hdl = nullptr;                             // their leaves
     int64_t hn4 = 0, hn4_0 = 0;                        // low-rank leaves done whole
     int *hl4 = nullptr;
     int64_t hn5 = 0, hn5_0 = 0;                        // small low-rank leaves done whole, one warp each
@@ -320,17 +324,17 @@ static int launch_hmat(dfn_handle *h, int mask, const double *Vbase, int vmul, b
             const unsigned g3 = (unsigned)h->hm_dense_grid;
             if (h->store == 0)
                 hm_dense_persistent_kernel<double><<<g3, 256, 0, h->stream>>>(
-                    h->ht3, n3, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+                    h->htg, n3, h->hdg, h->hdl, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
             else
                 hm_dense_persistent_kernel<float><<<g3, 256, 0, h->stream>>>(
-                    h->ht3, n3, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+                    h->htg, n3, h->hdg, h->hdl, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
         } else {
             if (h->store == 0)
                 hm_dense_kernel<double><<<(unsigned)n3, 256, 0, h->stream>>>(
-                    h->ht3, h->hblk, h->inst, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
+                    h->htg, h->hdg, h->hdl, h->ctl, mask, (const double *)h->hvals, h->hxp, h->hout);
             else
                 hm_dense_kernel<float><<<(unsigned)n3, 256, 0, h->stream>>>(
-                    h->ht3, h->hblk, h->inst, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
+                    h->htg, h->hdg, h->hdl, h->ctl, mask, (const float *)h->hvals, h->hxp, h->hout);
         }
         h->launches++;
         CKL();
@@ -975,7 +979,9 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     auto rup = [VW](int64_t n) { return (n + VW - 1) / VW * VW; };
     std::vector<int> perm(Nt);
     std::vector<HBlk> blks;
-    std::vector<HTask> t1, t2, t3;
+    std::vector<HTask> t1, t2, t3, tg;
+    std::vector<HDGroup> dgroups;   // dense leaves by row cluster, and their row tasks
+    std::vector<HDLeaf> dleaves;
     std::vector<int> l4;
     std::vector<int> l5;     // small whole low-rank leaves (one warp each), and their descriptors
     std::vector<HLeafW> lw;
@@ -989,6 +995,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     int64_t zoff = 0, slot = 0;
     // row contributions: per component, per global position, slot indices
     std::vector<std::vector<int64_t>> rows((size_t)nc * Nt);
+    std::map<std::pair<int, int>, std::vector<int>> dgrp;   // dense leaves by row cluster (r0, nr)
     for (int i = 0; i < B; i++) {
         const Inst &I = h->hinst[i];
         const int64_t e0 = I.eoff, N = I.N;
@@ -1097,7 +1104,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                 HBlk hb{};
                 hb.inst = i; hb.comp = c; hb.dense = H.dense; hb.rank = H.rank;
                 hb.r0 = L.r0; hb.nr = L.nr; hb.c0 = L.c0; hb.nc = L.nc;
-                hb.outoff = slot;
+                hb.outoff = H.dense ? -1 : slot;
                 if (H.dense) {
                     // F row-major, rows padded with zeros, in the dense region
                     // (filled on the device)
@@ -1136,14 +1143,32 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
                         t1.push_back(HTask{bi, j * HM_COLS, std::min(HM_COLS, L.nc - j * HM_COLS), j});
                     for (int r = 0; r < L.nr; r += HM_LROWS) t2.push_back(HTask{bi, r, std::min(HM_LROWS, L.nr - r), 0});
                 }
+                if (H.dense) {
+                    dgrp[std::make_pair(L.r0, L.nr)].push_back(bi);
+                    continue;
+                }
                 for (int r = 0; r < L.nr; r++) rows[(size_t)c * Nt + e0 + L.r0 + r].push_back(slot + r);
                 slot += L.nr;
             }
+            // the dense leaves of each row cluster: one group, one slot per row
+            for (const auto &kv : dgrp) {
+                const int r0 = kv.first.first, nr = kv.first.second;
+                const int gi = (int)dgroups.size();
+                dgroups.push_back(HDGroup{slot, (int)dleaves.size(), (int)kv.second.size(), i, 0});
+                for (int bi : kv.second) {
+                    const HBlk &b = blks[bi];
+                    dleaves.push_back(HDLeaf{b.foff, e0 + b.c0, b.ld, (b.nc + VW - 1) / VW});
+                }
+                for (int r = 0; r < nr; r += HM_ROWS) tg.push_back(HTask{gi, r, std::min(HM_ROWS, nr - r), 0});
+                for (int r = 0; r < nr; r++) rows[(size_t)c * Nt + e0 + r0 + r].push_back(slot + r);
+                slot += nr;
+            }
+            dgrp.clear();
         }
         if (i == 0) {
             h->hn1_0 = (int64_t)t1.size();
             h->hn2_0 = (int64_t)t2.size();
-            h->hn3_0 = (int64_t)t3.size();
+            h->hn3_0 = (int64_t)tg.size();
             h->hn4_0 = (int64_t)l4.size();
             h->hn5_0 = (int64_t)l5.size();
         }
@@ -1169,7 +1194,7 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     rows.clear();
     h->hn1 = (int64_t)t1.size();
     h->hn2 = (int64_t)t2.size();
-    h->hn3 = (int64_t)t3.size();
+    h->hn3 = (int64_t)tg.size();
     h->hn4 = (int64_t)l4.size();
     h->hn5 = (int64_t)l5.size();
     h->hblocks = (int64_t)blks.size();
@@ -1198,6 +1223,14 @@ static int build_hmatrix(dfn_handle *h, const dfn_problem *probs, const dfn_opti
     for (HLeafW &w : lw) w.aoff += dense_off;   // low-rank values follow the dense region
     CK(cudaMalloc((void **)&h->hlw, std::max<size_t>(lw.size(), 1) * sizeof(HLeafW)));
     if (!lw.empty()) CK(cudaMemcpyAsync(h->hlw, lw.data(), lw.size() * sizeof(HLeafW), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->htg, std::max<size_t>(tg.size(), 1) * sizeof(HTask)));
+    if (!tg.empty()) CK(cudaMemcpyAsync(h->htg, tg.data(), tg.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->hdg, std::max<size_t>(dgroups.size(), 1) * sizeof(HDGroup)));
+    if (!dgroups.empty())
+        CK(cudaMemcpyAsync(h->hdg, dgroups.data(), dgroups.size() * sizeof(HDGroup), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMalloc((void **)&h->hdl, std::max<size_t>(dleaves.size(), 1) * sizeof(HDLeaf)));
+    if (!dleaves.empty())
+        CK(cudaMemcpyAsync(h->hdl, dleaves.data(), dleaves.size() * sizeof(HDLeaf), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->ht3, std::max<size_t>(t3.size(), 1) * sizeof(HTask)));
     if (!t3.empty()) CK(cudaMemcpyAsync(h->ht3, t3.data(), t3.size() * sizeof(HTask), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMalloc((void **)&h->hperm, sizeof(int) * Nt));
@@ -1282,7 +1315,7 @@ int32_t dfn_destroy(dfn_handle *h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->kstar, h->kmin, h->Snk, h->s64_vt, h->slip, h->slip_out, h->slip_acc, h->tau0, h->wlast, h->vnow, h->mlp, h->rec_x, h->rec_t, h->rec_n,
-                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hsegof, h->hsegptr, h->hsegbase, h->hz, h->hout, h->hxp, h->ht3, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
+                    h->hblk, h->ht1, h->ht2, h->hvals, h->hperm, h->hsegof, h->hsegptr, h->hsegbase, h->hz, h->hout, h->hxp, h->ht3, h->htg, h->hdg, h->hdl, h->hl4, h->hl5, h->hlw, h->xptr, h->xcon, h->xrows, h->xrows_ptr, h->tri_tiles, h->tcoef,
                     h->inst, h->inst_of, h->tiles, h->seg_start, h->seg_inst, h->long_seg, h->short_seg, h->tc_A, h->tc_B, h->node, h->elem, h->ds, h->tan,
                     h->nrm, h->permx, h->a, h->b, h->Dc, h->f0, h->V0, h->nload, h->sload, h->perm, h->fake,
                     h->src_fault, h->src_elem, h->src_Q, h->src_tb, h->src_te, h->Y, h->P, h->Pdot, h->yout,

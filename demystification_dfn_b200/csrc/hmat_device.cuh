@@ -116,74 +116,37 @@ __global__ void __launch_bounds__(256) hm_lowrank_kernel(const HTask *__restrict
     }
 }
 
-// Rows of dense leaves: a half-warp per row, 16-byte vectors of F against
-// xp; four rows per half-warp in flight (their loads issued together).
-template <typename T>
-__global__ void __launch_bounds__(256, 5) hm_dense_kernel(const HTask *__restrict__ tasks, const HBlk *__restrict__ blks,
-                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
-                                                       int mask, const T *__restrict__ vals,
-                                                       const double *__restrict__ xp, double *__restrict__ out)
-{
-    using VT = typename HVec<T>::V;
-    constexpr int W = HVec<T>::W;
-    constexpr int U = 4;
-    const HTask t = tasks[blockIdx.x];
-    const HBlk b = blks[t.blk];
-    if (!takes_part(ctl, b.inst, mask)) return;
-    const Inst &I = inst[b.inst];
-    const double *x = xp + I.eoff + b.c0;
-    const int hl = threadIdx.x & 15, w = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
-    const int nv = (b.nc + W - 1) / W;
-    const VT zero{};
-    // the loop runs the same trips in both half-warps (shuffles below)
-    for (int wb = w * 2 * U; wb < t.count; wb += 8 * 2 * U) {
-        const int i0 = wb + half * U;
-        double s[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) s[u] = 0.0;
-        for (int v = hl; v < nv; v += 16) {
-            double xv[W];
-#pragma unroll
-            for (int j = 0; j < W; j++) xv[j] = x[v * W + j];
-            VT fv[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int row = t.start + i0 + u;
-                fv[u] = (i0 + u < t.count) ? reinterpret_cast<const VT *>(vals + b.foff + (int64_t)row * b.ld)[v]
-                                           : zero;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                double a[W];
-                HVec<T>::unpack(fv[u], a);
-#pragma unroll
-                for (int j = 0; j < W; j++) s[u] = fma(a[j], xv[j], s[u]);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
-            if (hl == 0 && i0 + u < t.count) out[b.outoff + t.start + i0 + u] = s[u];
-        }
-    }
-}
+// Rows of dense leaves. The dense leaves that share a row cluster form a
+// group; one CTA takes up to HM_ROWS rows of a group and walks all of its
+// leaves, so one accumulator per row sums the row over every dense leaf of
+// the group (one output slot per row of the group, not per leaf) and each
+// task streams the group's bytes behind one chain of dependent loads
+// (task, group, network phase). A half-warp per row, 16-byte vectors of F
+// against xp, four rows per half-warp in flight; each row summed over the
+// group's leaves in order, each leaf's vectors by lane, then a fixed
+// half-warp tree.
+struct HDLeaf {
+    int64_t foff;   // values of F (row-major, rows of ld values)
+    int64_t xoff;   // xp index of the leaf's first column
+    int ld, nv;     // padded row length, 16-byte vectors covering the columns
+};
+struct HDGroup {
+    int64_t outoff;            // output slot of the group's first row
+    int first, count, inst, pad;   // its leaves dl[first .. first + count), network
+};
 
 template <typename T>
-__device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restrict__ blks,
-                                              const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl, int mask,
-                                              const T *__restrict__ vals, const double *__restrict__ xp,
+__device__ __forceinline__ void hm_dense_task(const HTask t, const HDGroup *__restrict__ groups,
+                                              const HDLeaf *__restrict__ dl, const StepCtl *__restrict__ ctl,
+                                              int mask, const T *__restrict__ vals, const double *__restrict__ xp,
                                               double *__restrict__ out)
 {
     using VT = typename HVec<T>::V;
     constexpr int W = HVec<T>::W;
     constexpr int U = 4;
-    const HBlk b = blks[t.blk];
-    if (!takes_part(ctl, b.inst, mask)) return;
-    const Inst &I = inst[b.inst];
-    const double *x = xp + I.eoff + b.c0;
+    const HDGroup g = groups[t.blk];
+    if (!takes_part(ctl, g.inst, mask)) return;
     const int hl = threadIdx.x & 15, w = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
-    const int nv = (b.nc + W - 1) / W;
     const VT zero{};
     // the loop runs the same trips in both half-warps (shuffles below)
     for (int wb = w * 2 * U; wb < t.count; wb += 8 * 2 * U) {
@@ -191,46 +154,63 @@ __device__ __forceinline__ void hm_dense_task(const HTask t, const HBlk *__restr
         double s[U];
 #pragma unroll
         for (int u = 0; u < U; u++) s[u] = 0.0;
-        for (int v = hl; v < nv; v += 16) {
-            double xv[W];
+        for (int j = 0; j < g.count; j++) {
+            const HDLeaf L = dl[g.first + j];
+            const double *x = xp + L.xoff;
+            for (int v = hl; v < L.nv; v += 16) {
+                double xv[W];
 #pragma unroll
-            for (int j = 0; j < W; j++) xv[j] = x[v * W + j];
-            VT fv[U];
+                for (int q = 0; q < W; q++) xv[q] = x[v * W + q];
+                VT fv[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int row = t.start + i0 + u;
-                fv[u] = (i0 + u < t.count) ? reinterpret_cast<const VT *>(vals + b.foff + (int64_t)row * b.ld)[v]
-                                           : zero;
-            }
+                for (int u = 0; u < U; u++) {
+                    const int row = t.start + i0 + u;
+                    fv[u] = (i0 + u < t.count) ? reinterpret_cast<const VT *>(vals + L.foff + (int64_t)row * L.ld)[v]
+                                               : zero;
+                }
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                double a[W];
-                HVec<T>::unpack(fv[u], a);
+                for (int u = 0; u < U; u++) {
+                    double a[W];
+                    HVec<T>::unpack(fv[u], a);
 #pragma unroll
-                for (int j = 0; j < W; j++) s[u] = fma(a[j], xv[j], s[u]);
+                    for (int q = 0; q < W; q++) s[u] = fma(a[q], xv[q], s[u]);
+                }
             }
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
 #pragma unroll
             for (int o = 8; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
-            if (hl == 0 && i0 + u < t.count) out[b.outoff + t.start + i0 + u] = s[u];
+            if (hl == 0 && i0 + u < t.count) out[g.outoff + t.start + i0 + u] = s[u];
         }
     }
 }
 
+// one CTA per task
+template <typename T>
+__global__ void __launch_bounds__(256, 5) hm_dense_kernel(const HTask *__restrict__ tasks,
+                                                          const HDGroup *__restrict__ groups,
+                                                          const HDLeaf *__restrict__ dl,
+                                                          const StepCtl *__restrict__ ctl, int mask,
+                                                          const T *__restrict__ vals, const double *__restrict__ xp,
+                                                          double *__restrict__ out)
+{
+    hm_dense_task<T>(tasks[blockIdx.x], groups, dl, ctl, mask, vals, xp, out);
+}
+
 // The same rows on a persistent grid: CTA c takes tasks c, c + gridDim.x,
-// ... (the leaves are a few KB each, so a CTA per task spends much of its
-// life starting up; each row's arithmetic is that of hm_dense_kernel).
+// ... (each row's arithmetic is that of hm_dense_kernel).
 template <typename T>
 __global__ void __launch_bounds__(256, 5) hm_dense_persistent_kernel(const HTask *__restrict__ tasks, int64_t ntasks,
-                                                       const HBlk *__restrict__ blks,
-                                                       const Inst *__restrict__ inst, const StepCtl *__restrict__ ctl,
-                                                       int mask, const T *__restrict__ vals,
-                                                       const double *__restrict__ xp, double *__restrict__ out)
+                                                                     const HDGroup *__restrict__ groups,
+                                                                     const HDLeaf *__restrict__ dl,
+                                                                     const StepCtl *__restrict__ ctl, int mask,
+                                                                     const T *__restrict__ vals,
+                                                                     const double *__restrict__ xp,
+                                                                     double *__restrict__ out)
 {
     for (int64_t tk = blockIdx.x; tk < ntasks; tk += gridDim.x)
-        hm_dense_task<T>(tasks[tk], blks, inst, ctl, mask, vals, xp, out);
+        hm_dense_task<T>(tasks[tk], groups, dl, ctl, mask, vals, xp, out);
 }
 
 // Low-rank leaves of at most HM_COLS columns, whole: x staged in shared
