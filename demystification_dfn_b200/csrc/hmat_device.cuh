@@ -308,6 +308,49 @@ struct HLeafW {
     int inst, rank, lda, ld, nr, blk;
 };
 
+// y = A z of a small leaf by one warp: nav2 lanes (a power of two, at most
+// 32) over the vectors of leaf rows, 32 / nav2 groups of them over the rank
+// rows (group g takes rows g, g + 32 / nav2, ... in order), the groups
+// added by a fixed butterfly. Leaves of 128 rows or more keep one group
+// (each lane sums all rank rows of its vectors in order).
+template <typename T>
+__device__ __forceinline__ void hm_warp_az(const HLeafW &d, const T *__restrict__ A, const double *z,
+                                           double *__restrict__ out, int lane)
+{
+    using VT = typename HVec<T>::V;
+    constexpr int W = HVec<T>::W;
+    const int nav = (d.nr + W - 1) / W;   // vectors of an A row (padding rows are zero)
+    const int avl = d.lda / W;
+    const VT *Av = reinterpret_cast<const VT *>(A);
+    const int lgv = nav >= 32 ? 5 : 32 - __clz(nav - 1);
+    const int nav2 = 1 << lgv, hq = 32 >> lgv;
+    const int v0 = lane & (nav2 - 1), qg = lane >> lgv;
+    for (int rb = 0; rb < nav; rb += nav2) {   // the same trips in every lane (shuffles)
+        const int rv = rb + v0;
+        double acc[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) acc[c] = 0.0;
+        if (rv < nav) {
+#pragma unroll 4
+            for (int q = qg; q < d.rank; q += hq) {
+                double a[W];
+                HVec<T>::unpack(Av[(int64_t)q * avl + rv], a);
+                const double zq = z[q];
+#pragma unroll
+                for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+            }
+        }
+        for (int o = nav2; o < 32; o <<= 1)
+#pragma unroll
+            for (int c = 0; c < W; c++) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+        if (qg == 0 && rv < nav) {
+#pragma unroll
+            for (int c = 0; c < W; c++)
+                if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
+        }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128, 12) hm_lowrank_warp_kernel(const HLeafW *__restrict__ leaves, int64_t n,
                                                                   const StepCtl *__restrict__ ctl, int mask,
@@ -357,25 +400,7 @@ __global__ void __launch_bounds__(128, 12) hm_lowrank_warp_kernel(const HLeafW *
         if (v0 == 0 && q < rank) z[q] = acc;
     }
     __syncwarp();
-    const int nav = (d.nr + W - 1) / W;   // vectors of an A row (padding rows are zero)
-    const int avl = d.lda / W;
-    const VT *Av = reinterpret_cast<const VT *>(A);
-    for (int rv = lane; rv < nav; rv += 32) {
-        double acc[W];
-#pragma unroll
-        for (int c = 0; c < W; c++) acc[c] = 0.0;
-#pragma unroll 4
-        for (int q = 0; q < rank; q++) {
-            double a[W];
-            HVec<T>::unpack(Av[(int64_t)q * avl + rv], a);
-            const double zq = z[q];
-#pragma unroll
-            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
-        }
-#pragma unroll
-        for (int c = 0; c < W; c++)
-            if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
-    }
+    hm_warp_az<T>(d, A, z, out, lane);
 }
 
 template <typename T>
@@ -419,25 +444,7 @@ __device__ __forceinline__ void hm_lowrank_warp_leaf(const HLeafW &d, const T *_
         if (v0 == 0 && q < rank) z[q] = acc;
     }
     __syncwarp();
-    const int nav = (d.nr + W - 1) / W;   // vectors of an A row (padding rows are zero)
-    const int avl = d.lda / W;
-    const VT *Av = reinterpret_cast<const VT *>(A);
-    for (int rv = lane; rv < nav; rv += 32) {
-        double acc[W];
-#pragma unroll
-        for (int c = 0; c < W; c++) acc[c] = 0.0;
-#pragma unroll 4
-        for (int q = 0; q < rank; q++) {
-            double a[W];
-            HVec<T>::unpack(Av[(int64_t)q * avl + rv], a);
-            const double zq = z[q];
-#pragma unroll
-            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
-        }
-#pragma unroll
-        for (int c = 0; c < W; c++)
-            if (rv * W + c < d.nr) out[d.outoff + rv * W + c] = acc[c];
-    }
+    hm_warp_az<T>(d, A, z, out, lane);
     __syncwarp();   // z is rewritten by the warp's next leaf
 }
 
