@@ -215,9 +215,9 @@ __global__ void __launch_bounds__(256, 5) hm_dense_persistent_kernel(const HTask
 
 // Low-rank leaves of at most HM_COLS columns, whole: x staged in shared
 // memory, z = B^T xp into shared memory (warp per rank row, two rows at a
-// time), then the rows y = A z (a 16-byte vector of A rows per thread, each
-// row summed over the rank in order); one CTA per leaf, no partial sums in
-// global memory.
+// time), then the rows y = A z (a 16-byte vector of A rows per thread, the
+// rank rows split over groups of threads when the leaf has fewer than 1024
+// rows); one CTA per leaf, no partial sums in global memory.
 template <typename T>
 __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__restrict__ leaves,
                                                                const HBlk *__restrict__ blks,
@@ -265,23 +265,47 @@ __global__ void __launch_bounds__(256) hm_lowrank_fused_kernel(const int *__rest
         }
     }
     __syncthreads();
+    // y = A z: nav2 threads (a power of two, at most 256) over the vectors
+    // of leaf rows, 256 / nav2 groups of them over the rank rows (group g
+    // takes rows g, g + 256 / nav2, ... in order); the groups' sums added in
+    // group order through shared memory (xs, no longer needed). Leaves of
+    // 1024 rows or more keep one group.
     const int nav = (b.nr + W - 1) / W, avl = b.lda / W;
     const VT *Av = reinterpret_cast<const VT *>(vals + b.foff);
-    for (int iv = threadIdx.x; iv < nav; iv += blockDim.x) {
+    const int lgv = nav >= 256 ? 8 : 32 - __clz(nav - 1);
+    const int nav2 = 1 << lgv, hq = 256 >> lgv;   // 256 threads
+    const int v0 = threadIdx.x & (nav2 - 1), qg = threadIdx.x >> lgv;
+    double *red = xs;   // 256 x W doubles at most
+    for (int rb = 0; rb < nav; rb += nav2) {   // the same trips in every thread (barriers)
+        const int iv = rb + v0;
         double acc[W];
 #pragma unroll
         for (int c = 0; c < W; c++) acc[c] = 0.0;
+        if (iv < nav) {
 #pragma unroll 4
-        for (int q = 0; q < b.rank; q++) {
-            double a[W];
-            HVec<T>::unpack(Av[(int64_t)q * avl + iv], a);
-            const double zq = z[q];
+            for (int q = qg; q < b.rank; q += hq) {
+                double a[W];
+                HVec<T>::unpack(Av[(int64_t)q * avl + iv], a);
+                const double zq = z[q];
 #pragma unroll
-            for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+                for (int c = 0; c < W; c++) acc[c] = fma(a[c], zq, acc[c]);
+            }
         }
+        if (hq > 1) {   // CTA-uniform
 #pragma unroll
-        for (int c = 0; c < W; c++)
-            if (iv * W + c < b.nr) out[b.outoff + iv * W + c] = acc[c];
+            for (int c = 0; c < W; c++) red[(qg * nav2 + v0) * W + c] = acc[c];
+            __syncthreads();
+            if (qg == 0)
+                for (int g = 1; g < hq; g++)
+#pragma unroll
+                    for (int c = 0; c < W; c++) acc[c] += red[(g * nav2 + v0) * W + c];
+            __syncthreads();
+        }
+        if (qg == 0 && iv < nav) {
+#pragma unroll
+            for (int c = 0; c < W; c++)
+                if (iv * W + c < b.nr) out[b.outoff + iv * W + c] = acc[c];
+        }
     }
 }
 
