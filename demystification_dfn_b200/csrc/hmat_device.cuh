@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(256) hm_rows_kernel(const HTask *__restrict__ 
         double acc[W];
 #pragma unroll
         for (int c = 0; c < W; c++) acc[c] = 0.0;
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < r; q++) {
             double a[W];
             HVec<T>::unpack(Av[(int64_t)q * avl + v0 + iv], a);
