@@ -9,10 +9,13 @@
 //      their columns contiguously);
 //   1. z_b = B_b^T xp for every low-rank block b, split in column chunks
 //      (partial sums per chunk, added in fixed order in step 2);
-//   2. the rows of every leaf: F_b xp (dense leaves) and A_b z_b (low-rank
-//      leaves), two launches, one output slot per (leaf, row);
+//   2. the rows: F xp over the dense leaves of a row cluster (one output
+//      slot per (group, row)) and A_b z_b of the low-rank leaves (one output
+//      slot per (leaf, row));
 //   3. y(row) = sum of the row's slots in a fixed order, written in the
 //      original element order (y[perm[pos]]).
+// Small whole low-rank leaves go one warp each, larger ones one CTA each,
+// those wider than HM_COLS columns through split z partials and row tasks.
 // Factors are stored in FP64 or FP32 with rows padded to whole 16-byte
 // vectors and 16-byte aligned: dense F row-major (nr x ldf), low-rank A and
 // B transposed, rank-major (r x lda, r x ldb), so that every factor streams
