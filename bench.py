@@ -400,6 +400,15 @@ def hmat_eps(name):
     return 1e-7
 
 
+def hmat_leaf(name):
+    """Leaf size of a north-star H-matrix variant (64 unless its name says
+    otherwise)."""
+    for n in ("96", "128"):
+        if "leaf" + n in name:
+            return int(n)
+    return 64
+
+
 def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
     """The ensemble comparison the metric is quoted on: 64 seeded networks
     (seeds 0-63, 100-400 faults each, 2k-10k elements, distinct geometries,
@@ -411,9 +420,9 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
     integrated as a passive component; Newton: slip is the state). The FP64
     GPU paths follow the oracle to 1e-8 in the parity tests. The learned
     guess is trained on solves recorded from eight held-out networks (seeds
-    64-71). The H-matrix variants use leaf 64, eta 2 and an ACA tolerance of
-    1e-7, 1e-6 or 1e-5 (fewer stored factors; their slip error is reported
-    like the others')."""
+    64-71). The H-matrix variants use eta 2, leaves of 64 (or 96, 128)
+    elements and an ACA tolerance of 1e-7 (or 1e-6, 1e-5: fewer stored
+    factors; their slip error is reported like the others')."""
     from demystification_dfn_b200 import learned, networks
     from demystification_dfn_b200.ensemble import Ensemble
 
@@ -424,7 +433,9 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
                 ("newton_fp32", "newton", "fp32", "analytic"), ("newton_fp32_mlp", "newton", "fp32", "mlp"),
                 ("newton_bf16x2_mlp", "newton", "bf16x2", "mlp"), ("newton_hmat_fp32", "newton", "fp32", "analytic"),
                 ("newton_hmat_eps1e-6_fp32", "newton", "fp32", "analytic"),
-                ("newton_hmat_eps1e-5_fp32", "newton", "fp32", "analytic"))
+                ("newton_hmat_eps1e-5_fp32", "newton", "fp32", "analytic"),
+                ("newton_hmat_leaf96_eps1e-5_fp32", "newton", "fp32", "analytic"),
+                ("newton_hmat_leaf128_eps1e-5_fp32", "newton", "fp32", "analytic"))
     hmembers = networks.ensemble(64, kernel="hmatrix")
     # the learned guess: solves recorded on held-out networks, trained on the GPU
     held = [networks.ensemble_member(s) for s in range(64, 72)]
@@ -446,7 +457,7 @@ def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
         t0 = time.perf_counter()
         e = Ensemble(hmembers if hm else members, storage=store, pressure="tridiag", device=local,
                      formulation=form, guess=guess,
-                     **(dict(hmat_leaf=64, hmat_eta=2.0, hmat_eps=hmat_eps(name)) if hm else {}))
+                     **(dict(hmat_leaf=hmat_leaf(name), hmat_eta=2.0, hmat_eps=hmat_eps(name)) if hm else {}))
         create_s = time.perf_counter() - t0
         e.set_stream(stream.cuda_stream)
         if guess == "mlp":
