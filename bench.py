@@ -392,8 +392,8 @@ def leg_learned(args, local, stream):
 
 
 def hmat_eps(name):
-    """ACA tolerance of a north-star H-matrix variant (1e-7 unless its name
-    says otherwise)."""
+    """ACA tolerance of an H-matrix variant of the 64-network comparison
+    (1e-7 unless its name says otherwise)."""
     for e in ("1e-5", "1e-6"):
         if "eps" + e in name:
             return float(e)
@@ -401,15 +401,15 @@ def hmat_eps(name):
 
 
 def hmat_leaf(name):
-    """Leaf size of a north-star H-matrix variant (64 unless its name says
-    otherwise)."""
+    """Leaf size of an H-matrix variant of the 64-network comparison (64
+    unless its name says otherwise)."""
     for n in ("96", "128"):
         if "leaf" + n in name:
             return int(n)
     return 64
 
 
-def leg_north_star(args, local, stream, t_end=3.0e5, n_steps=10):
+def leg_ensemble64(args, local, stream, t_end=3.0e5, n_steps=10):
     """The ensemble comparison the metric is quoted on: 64 seeded networks
     (seeds 0-63, 100-400 faults each, 2k-10k elements, distinct geometries,
     so one kernel matrix per network, 25 GB in FP64), injection and
@@ -723,7 +723,7 @@ def run_case(argv):
         autotuner first, "grids D W" sets the CTAs of the dense-row and
         small-leaf kernels (dfn_set_hmat_grids).
     python bench.py --case hmatrix_ensemble_kv [tuned]
-        the 64 networks of the north-star leg as H-matrices (leaf 64, eta 2,
+        the 64 networks of the ensemble64 leg as H-matrices (leaf 64, eta 2,
         ACA 1e-7, FP32 factors) in one batch: three K.V launches of the
         batch; "tuned" runs the autotuner first (one JSON line).
     python bench.py --case s64_kv [R]
@@ -875,13 +875,13 @@ def _sig(x, n=4):
     return float(f"{x:.{n}g}") if isinstance(x, float) else x
 
 
-def north_star_summary(extras):
+def metric_summary(extras):
     """Small keys for the end of the line: the metric's comparison (batched
     mixed precision vs plain FP64 on the 64-network ensemble, steps/s and
     slip error), the shared-geometry tensor-core batch against its FP64
     shared-K counterpart, and the H-matrix K.V fraction of HBM."""
     out = {}
-    ns = extras.get("north_star")
+    ns = extras.get("ensemble64")
     if ns:
         keys = ("network_steps_per_s", "steps_per_s_vs_v_fp64", "time_to_t_end_vs_v_fp64", "slip_rel_err_vs_fp64",
                 "kv_frac_of_measured_hbm")
@@ -916,7 +916,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and CPU legs")
     ap.add_argument("--ensemble", type=int, default=64, help="networks in the ensemble leg (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
-    ap.add_argument("--legs", default="precision,north_star,single_fault,hmatrix,tensor_core,span,learned,cpu",
+    ap.add_argument("--legs", default="precision,ensemble64,single_fault,hmatrix,tensor_core,span,learned,cpu",
                     help="comma list of the extra legs to run (ensemble, the 64 networks in three storages "
                          "sharded over the ranks; ensemble_span, the 64 networks over 1 simulated year; and "
                          "hmatrix_span, the H-matrix network toward 100 years, are available but not in the "
@@ -1113,8 +1113,8 @@ def main():
         extras["hmatrix_span"] = leg_hmatrix_span(args, local, stream)
     if rank == 0 and "learned" in legs:
         extras["learned_newton"] = leg_learned(args, local, stream)
-    if rank == 0 and "north_star" in legs:
-        extras["north_star"] = leg_north_star(args, local, stream)
+    if rank == 0 and "ensemble64" in legs:
+        extras["ensemble64"] = leg_ensemble64(args, local, stream)
 
     if rank == 0:
         hbm, src = peaks()
@@ -1159,9 +1159,9 @@ def main():
             line["extras"] = extras
         # the compact summary goes last: the tail of a long line is what a
         # truncated log keeps
-        summary = north_star_summary(extras)
+        summary = metric_summary(extras)
         if summary:
-            line["north_star"] = summary
+            line["summary"] = summary
         print(json.dumps(line))
     sim.close()
     if world > 1:

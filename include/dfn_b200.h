@@ -40,7 +40,7 @@ typedef enum dfn_status {
     DFN_ERR_NONFINITE = 4,   /* NaN/Inf in the state or in a pressure solve */
     DFN_ERR_ARG = 5,         /* invalid argument or size */
     DFN_ERR_CUDA = 6,        /* a CUDA runtime call failed */
-    DFN_ERR_UNSUPPORTED = 7, /* feature not available in this build */
+    DFN_ERR_UNSUPPORTED = 7, /* feature not available in this library */
     DFN_ERR_ATTEMPTS = 8,    /* more rejected RK attempts in one step than the device budget */
     DFN_ERR_NOMEM = 9,       /* device allocation failed */
     DFN_ERR_TIMEOUT = 10     /* a bounded wait inside a kernel expired (the kernel stopped early) */
