@@ -136,3 +136,38 @@ def test_tectonic_loading_and_crossing_pair_builders():
         a, b = c.faults[0].node.T, c.faults[1].node.T
         d = np.sqrt(((a[:, None, :] - b[None, :, :]) ** 2).sum(-1))
         assert int((d < 1e-9).sum()) == shared
+
+
+def test_bench_summary_and_hmatrix_variants():
+    """The bench line ends with a compact summary of the 64-network
+    comparison, the shared-geometry batch and the H-matrix K.V fraction; the
+    H-matrix variants of the comparison take their ACA tolerance and leaf
+    size from their names."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), ".."))
+    import bench
+
+    assert bench.hmat_eps("newton_hmat_fp32") == 1e-7
+    assert bench.hmat_eps("newton_hmat_eps1e-6_fp32") == 1e-6
+    assert bench.hmat_eps("newton_hmat_leaf96_eps1e-5_fp32") == 1e-5
+    assert bench.hmat_leaf("newton_hmat_eps1e-5_fp32") == 64
+    assert bench.hmat_leaf("newton_hmat_leaf128_eps1e-5_fp32") == 128
+    extras = {
+        "ensemble64": {"networks": 64,
+                       "v_fp64": {"network_steps_per_s": 2790.123, "steps_per_s_vs_v_fp64": 1.0,
+                                  "time_to_t_end_vs_v_fp64": 1.0, "kv_frac_of_measured_hbm": 1.0712},
+                       "newton_hmat_fp32": {"network_steps_per_s": 9410.5, "steps_per_s_vs_v_fp64": 3.3812,
+                                            "time_to_t_end_vs_v_fp64": 11.04, "slip_rel_err_vs_fp64": 3.7745e-07,
+                                            "kv_frac_of_measured_hbm": 0.5192}},
+        "tensor_core": {"tc_v": {"network_steps_per_s": 21800.4, "kv_avg_ms": 0.3797},
+                        "tc_over_fp64_shared_v": {"network_steps_per_s": 6.7812, "time_to_t_end": 7.41}},
+        "hmatrix": {"kv_frac_of_measured_hbm": 0.65812},
+    }
+    s = bench.metric_summary(extras)
+    assert set(s) == {"ensemble64", "shared_geometry64", "hmatrix_kv_frac_of_measured_hbm"}
+    assert set(s["ensemble64"]) == {"v_fp64", "newton_hmat_fp32"}
+    assert s["ensemble64"]["newton_hmat_fp32"]["steps_per_s_vs_v_fp64"] == 3.38
+    assert s["ensemble64"]["newton_hmat_fp32"]["slip_rel_err_vs_fp64"] == 3.77e-07
+    assert s["shared_geometry64"]["tc_over_fp64_shared_v"]["network_steps_per_s"] == 6.78
+    assert s["hmatrix_kv_frac_of_measured_hbm"] == 0.658
